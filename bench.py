@@ -1,0 +1,451 @@
+"""Benchmark: MLUPS of the fused LBM step on the D3Q19 MRT channel flow past a sphere.
+
+Workload (one "step" = one fused time step of the whole grid): 512 x 256 x 256
+cells, sphere of diameter 32 at (128, 128, 128), Zou/He velocity inlet
+u = 0.04, pressure outlet rho = 1, periodic y/z, Re = 300
+(tau = 3 u D / Re + 0.5), float32 populations, momentum-exchange drag
+accumulated in float64 every step.  Synthetic initial state: the equilibrium
+of the inlet velocity (zero inside the sphere), as TensorLBM's sphere runner
+starts.  The same grid is also timed with the D3Q27 cumulant collision and
+with D3Q19 MRT on float16 shifted storage ("variants").
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: each rank advances its own replica (the step does
+not shard; nothing is exchanged), the time is the max over ranks and the value
+is the total cell updates of all ranks per second.  Rank 0 prints one JSON line.
+
+--impl reference times the CPU implementation of the same step (the numpy
+restatement of TensorLBM's torch operators in oracle/) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+NZ, NY, NX = 256, 256, 512
+D, CX, CY, CZ = 32, 128, 128, 128
+U_IN, RE = 0.04, 300.0
+TAU = 3.0 * U_IN * D / RE + 0.5
+METRIC = "MLUPS (D3Q19 MRT sphere channel 512x256x256, fused step)"
+WORKLOAD = "d3q19_mrt_sphere_channel_512x256x256"
+HBM_FALLBACK_GBS = 6650.0
+SPEC_HBM_GBS = 8000.0
+
+
+def _peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def _traffic(workload: str):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        return json.loads(p.read_text()).get(workload)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+
+def _make_solver(torch, dev, lattice, collision, storage, track_force):
+    from tensorlbm_b200 import LBMSolver, boundaries3d
+
+    obst = boundaries3d.sphere_mask(NX, NY, NZ, CX, CY, CZ, D / 2, dev)
+    s = LBMSolver(lattice, (NZ, NY, NX), TAU, collision, device=dev, storage=storage, obstacle_mask=obst,
+                  u_in=U_IN, rho_out=1.0, track_force=track_force)
+    return s, obst
+
+
+def _initial_state(torch, dev, lattice, obst):
+    from tensorlbm_b200.d3q19 import equilibrium3d
+    from tensorlbm_b200.d3q27 import equilibrium27
+
+    ux = torch.full((NZ, NY, NX), U_IN, device=dev)
+    ux[obst] = 0.0
+    z = torch.zeros_like(ux)
+    eq = equilibrium3d if lattice == "D3Q19" else equilibrium27
+    return eq(torch.ones_like(ux), ux, z, z)
+
+
+def _time_steps(torch, s, steps, warmup, force_buf):
+    """Device time of `steps` fused launches on the launching stream (CUDA events)."""
+    from tensorlbm_b200 import _lib
+
+    cur = torch.cuda.current_stream(s.device)
+    for _ in range(warmup):
+        s._launch(s._buf[s._cur], s._buf[1 - s._cur], force_buf)
+        s._cur ^= 1
+    torch.cuda.synchronize(s.device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(cur)
+    for _ in range(steps):
+        s._launch(s._buf[s._cur], s._buf[1 - s._cur], force_buf)
+        s._cur ^= 1
+    e1.record(cur)
+    torch.cuda.synchronize(s.device)
+    s.steps_done += steps + warmup
+    del _lib
+    return e0.elapsed_time(e1) / 1e3
+
+
+def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_cell, peak):
+    s, obst = _make_solver(torch, dev, lattice, collision, storage, False)
+    s.load(_initial_state(torch, dev, lattice, obst))
+    force = torch.zeros(3, dtype=torch.float64, device=dev)
+    t = _time_steps(torch, s, steps, warmup, force)
+    cells = NX * NY * NZ
+    mlups = cells * steps / t / 1e6
+    gbs = bytes_per_cell * cells / (t / steps) / 1e9
+    finite = not s.nonfinite_seen()
+    del s
+    torch.cuda.empty_cache()
+    return {"mlups": round(mlups, 1), "ms_per_step": round(1e3 * t / steps, 4), "achieved_gbs": round(gbs, 1),
+            "roofline_frac": round(gbs / peak, 4), "bytes_per_cell": bytes_per_cell, "finite": finite}
+
+
+def run_ours(args) -> None:
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    peak, peak_kind = _peaks()
+    cells = NX * NY * NZ
+    bpc = 2 * 19 * 4
+
+    # ---- headline: D3Q19 MRT float32, one fused kernel per step, FP64 drag ----
+    s, obst = _make_solver(torch, dev, "D3Q19", "mrt", "f32", False)
+    f0 = _initial_state(torch, dev, "D3Q19", obst)
+    s.load(f0)
+    force = torch.zeros(3, dtype=torch.float64, device=dev)
+    for _ in range(args.warmup):
+        s._launch(s._buf[s._cur], s._buf[1 - s._cur], force)
+        s._cur ^= 1
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    cur = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        e0.record(cur)
+        for _ in range(args.steps):
+            s._launch(s._buf[s._cur], s._buf[1 - s._cur], force)
+            s._cur ^= 1
+        e1.record(cur)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    t = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        tt = torch.tensor([t], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t = float(tt)
+    s.steps_done += args.steps + args.warmup
+    drag = float(force[0])
+    finite = not s.nonfinite_seen()
+    value = world * cells * args.steps / t / 1e6
+    per_launch = t / args.steps
+    achieved = bpc * cells / per_launch / 1e9
+    del s
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the public API with host buffers ----
+    from tensorlbm_b200 import LBMSolver
+
+    host_f0 = f0.cpu().pin_memory()
+    del f0
+    host_out = torch.empty(host_f0.shape, dtype=torch.float32).pin_memory()
+    host_drag = torch.empty((args.steps, 3), dtype=torch.float64).pin_memory()
+    s2 = LBMSolver("D3Q19", (NZ, NY, NX), TAU, "mrt", device=dev, obstacle_mask=obst, u_in=U_IN, rho_out=1.0)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    drag_buf = torch.zeros((args.steps, 3), dtype=torch.float64, device=dev)
+    e2.record(cur)
+    f_dev = host_f0.to(dev, non_blocking=True)
+    s2.load(f_dev)
+    for k in range(args.steps):
+        s2._launch(s2._buf[s2._cur], s2._buf[1 - s2._cur], drag_buf[k])
+        s2._cur ^= 1
+        s2.steps_done += 1
+        host_drag[k].copy_(drag_buf[k], non_blocking=True)  # the step's result, read back every step
+    host_out.copy_(s2.f, non_blocking=True)
+    e3.record(cur)
+    torch.cuda.synchronize(dev)
+    t_e2e = e2.elapsed_time(e3) / 1e3
+    if world > 1:
+        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_e2e = float(tt)
+    e2e_value = world * cells * args.steps / t_e2e / 1e6
+    state_bytes = host_f0.numel() * 4
+    del s2, f_dev
+    torch.cuda.empty_cache()
+
+    # ---- variants on the same grid (rank 0 device only, N=1 semantics) ----
+    variants = {}
+    if not args.no_variants:
+        variants["d3q27_cumulant_f32"] = _variant(torch, dev, "D3Q27", "cumulant", "f32", max(args.steps // 2, 5),
+                                                  args.warmup, 2 * 27 * 4, peak)
+        variants["d3q19_mrt_f16_shifted"] = _variant(torch, dev, "D3Q19", "mrt", "f16", args.steps, args.warmup,
+                                                     2 * 19 * 2, peak)
+        variants["d3q19_bgk_f32"] = _variant(torch, dev, "D3Q19", "bgk", "f32", args.steps, args.warmup, bpc, peak)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(args, processes=1)
+
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC,
+        "value": round(value, 1),
+        "unit": "MLUPS",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1e3 * t / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: equilibrium initial state of the inlet velocity (zero in the sphere)",
+        "config": {
+            "workload": WORKLOAD,
+            "grid": [NX, NY, NZ],
+            "lattice": "D3Q19",
+            "collision": "mrt",
+            "sphere": {"diameter": D, "center": [CX, CY, CZ]},
+            "u_in": U_IN, "re": RE, "tau": TAU,
+            "boundaries": "zou_he velocity inlet x=0, zou_he pressure outlet x=nx-1, periodic y/z, "
+                          "full-way bounce-back + FP64 momentum-exchange drag on the sphere",
+            "l2": "no flush: the two population buffers are 5.1 GB, 40x the 126 MB L2",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "drag_fx_last_step": drag,
+            "finite": finite,
+        },
+        "roofline": {
+            "bound": "hbm",
+            "achieved": round(achieved, 1),
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "peak_kind": peak_kind,
+            "frac_of_spec_8tbs": round(achieved / SPEC_HBM_GBS, 4),
+            "bytes_per_cell": bpc,
+            "traffic": _traffic(WORKLOAD),
+        },
+        "e2e": {
+            "value": round(e2e_value, 1),
+            "unit": "MLUPS",
+            "h2d_bytes_per_step": int(round(state_bytes / args.steps)),
+            "d2h_bytes_per_step": int(round((state_bytes + args.steps * 24) / args.steps)),
+            "what": "pinned host f0 -> device, load (collision pass), K fused steps through LBMSolver with the "
+                    "float64 drag copied to pinned host memory every step, final TensorLBM-phase f -> host",
+        },
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary(),
+        "variants": variants,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline / reference arm: the numpy restatement of TensorLBM's chain
+# ---------------------------------------------------------------------------
+
+
+def _cpu_slab_worker(args_tuple):
+    nzs, steps = args_tuple
+    import numpy as np
+
+    from oracle import lbm as O
+
+    obst = O.sphere_mask(NX, NY, nzs, CX, CY, nzs / 2, D / 2)
+    ux = np.full((nzs, NY, NX), U_IN, np.float32)
+    ux[obst] = 0.0
+    z = np.zeros_like(ux)
+    f = O.equilibrium(19, np.ones_like(ux), ux, z, z)
+    O.channel_step(f, TAU, U_IN, 1.0, None, obst, "mrt")  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        f, _ = O.channel_step(f, TAU, U_IN, 1.0, None, obst, "mrt")
+    return time.perf_counter() - t0
+
+
+def cpu_sample(args, processes: int) -> dict:
+    """Time the oracle's D3Q19 MRT channel step on z-slabs of the bench grid."""
+    import multiprocessing as mp
+
+    nzs = args.cpu_slab
+    steps = max(1, args.cpu_steps)
+    if processes == 1:
+        from threadpoolctl import threadpool_limits
+
+        with threadpool_limits(1):
+            t = _cpu_slab_worker((nzs, steps))
+        cells = NX * NY * nzs
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(processes, initializer=_limit_blas) as pool:
+            t0 = time.perf_counter()
+            times = pool.map(_cpu_slab_worker, [(nzs, steps)] * processes)
+            t = max(times)
+            del t0
+        cells = NX * NY * nzs * processes
+    mlups = cells * steps / t / 1e6
+    return {"value": round(mlups, 3), "unit": "MLUPS", "cores": processes, "kind": "port",
+            "sample": f"{processes} x {NX}x{NY}x{nzs} z-slab(s) of the channel with the sphere, {steps} step(s) "
+                      f"each (numpy restatement of collide_mrt3d -> stream3d -> forces -> zou_he -> bounce_back)"}
+
+
+def _limit_blas():
+    from threadpoolctl import threadpool_limits
+
+    threadpool_limits(1)
+
+
+def run_reference(args) -> None:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    # bounded: each step is `procs` slabs in parallel; steps/warmup follow the CLI
+    cpu_steps = max(1, min(args.steps, 3))
+    args.cpu_steps = cpu_steps
+    sample = cpu_sample(args, processes=procs)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": sample["value"],
+        "unit": "MLUPS",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "higher_is_better": True,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "lattice": "D3Q19", "collision": "mrt"},
+        "cpu_baseline": sample,
+        "e2e": {"value": sample["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "TensorLBM is a Python package whose CPU path is torch; its restatement in oracle/ is timed here "
+                "because the reference source is not present on the GPU machine",
+    }
+    print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-slab", type=int, default=8, help="z-planes per CPU sample slab")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

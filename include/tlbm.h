@@ -1,0 +1,235 @@
+/*
+ * tlbm.h - C ABI of the B200 lattice-Boltzmann step library (libtlbm.so).
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * (passed as void*), enqueues its kernels on that stream and returns a
+ * tlbm_status without synchronising.  The caller owns every buffer.
+ *
+ * Population layout (all lattices): structure of arrays, shape (Q, nz, ny, nx)
+ * with x fastest; 2-D lattices use nz = 1, i.e. (Q, ny, nx).  Element q of
+ * cell (z, y, x) sits at  q*N + (z*ny + y)*nx + x,  N = nx*ny*nz.  Direction
+ * numbering is TensorLBM's (tensorlbm/d2q9.py:8-26, tensorlbm/d3q19.py:6-67,
+ * tensorlbm/d3q27.py:32-84).
+ *
+ * Each declaration names the TensorLBM function (file:line, paths inside the
+ * TensorLBM source tree) whose behaviour it reproduces.
+ */
+#ifndef TLBM_H
+#define TLBM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TLBM_API __attribute__((visibility("default")))
+#define TLBM_ABI_VERSION 1
+
+typedef enum tlbm_status {
+  TLBM_OK = 0,
+  TLBM_ERR_SHAPE = 1,       /* bad sizes / plane too small */
+  TLBM_ERR_DTYPE = 2,       /* unsupported dtype or dtype combination */
+  TLBM_ERR_ALIAS = 3,       /* f_in == f_out where the kernel pulls from neighbours */
+  TLBM_ERR_LAUNCH = 4,      /* a CUDA launch or runtime call failed */
+  TLBM_ERR_TIMEOUT = 5,     /* a bounded device-side wait expired */
+  TLBM_ERR_NONFINITE = 6,   /* reported by callers that read the status word */
+  TLBM_ERR_ARG = 7,         /* null pointer or invalid parameter */
+  TLBM_ERR_UNSUPPORTED = 8  /* lattice / collision / boundary combination not built */
+} tlbm_status;
+
+typedef enum tlbm_lattice { TLBM_D2Q9 = 9, TLBM_D3Q19 = 19, TLBM_D3Q27 = 27 } tlbm_lattice;
+
+/* Storage / arithmetic formats.  The shifted half formats store f_q - w_q and
+ * compute in float32. */
+typedef enum tlbm_dtype {
+  TLBM_F32 = 0,
+  TLBM_F64 = 1,
+  TLBM_F16_SHIFTED = 2,
+  TLBM_BF16_SHIFTED = 3
+} tlbm_dtype;
+
+typedef enum tlbm_collision {
+  TLBM_COLL_NONE = 0,             /* no collision (stream / boundary only, or a format conversion) */
+  TLBM_COLL_BGK = 1,              /* solver.py:67, solver3d.py:100, d3q27.py:423 */
+  TLBM_COLL_MRT = 2,              /* solver.py:249, solver3d.py:107, d3q27.py:643 */
+  TLBM_COLL_CUMULANT = 3,         /* D3Q27 legacy, cumulant.py:935 */
+  TLBM_COLL_CUMULANT_GEIER = 4,   /* D3Q27 Geier 2015, cumulant.py:1050 */
+  TLBM_COLL_CUMULANT_D3Q19 = 5,   /* cumulant.py:1159 (Smagorinsky via c_smag) */
+  TLBM_COLL_SMAGORINSKY = 6       /* turbulence.py:245 (D3Q19), :216 (D2Q9), :472 (D3Q27) */
+} tlbm_collision;
+
+/* Boundary conditions applied by tlbm_step after the pull, in this order:
+ *   obstacle force sample -> Zou/He inlet (x=0) -> Zou/He outlet (x=nx-1)
+ *   -> full-way bounce-back on TLBM_FLAG_SOLID cells -> moving lid (y=ny-1).
+ * This is the order of tensorlbm/d3q27_sphere_flow.py:246-256 and
+ * benchmarks/verified/cavity_3d_full (collide, stream, walls, lid). */
+typedef enum tlbm_bc_bits {
+  TLBM_BC_LID = 1u,        /* boundaries3d.py:324 / lid_driven_cavity.py:431 */
+  TLBM_BC_ZH_INLET = 2u,   /* boundaries.py:50, boundaries3d.py:205, boundaries_d3q27.py:107 */
+  TLBM_BC_ZH_OUTLET = 4u   /* boundaries.py:102, boundaries3d.py:269, boundaries_d3q27.py:179 */
+} tlbm_bc_bits;
+
+/* Per-cell flag byte. */
+typedef enum tlbm_flag_bits {
+  TLBM_FLAG_SOLID = 1u,     /* post-stream full-way bounce-back (wall XOR obstacle, as two
+                               successive swaps cancel): bounce_back_cells* after stream */
+  TLBM_FLAG_OBSTACLE = 2u,  /* summed into the momentum-exchange force */
+  TLBM_FLAG_HALFWAY = 4u    /* pre-stream half-way wall: the cell is not collided, its
+                               populations are stored reversed (where(wall, f_pre[opp], f)
+                               before stream: cases/base.py:270-289 pre-boundaries,
+                               lbm_step_correct.py:62 "bb" mode) */
+} tlbm_flag_bits;
+
+typedef struct tlbm_desc {
+  int32_t lattice;     /* tlbm_lattice */
+  int32_t dtype;       /* tlbm_dtype of the population buffers */
+  int32_t collision;   /* tlbm_collision */
+  int32_t nx, ny, nz;  /* nz = 1 for D2Q9 */
+  uint32_t bc;         /* tlbm_bc_bits */
+  double tau;          /* shear relaxation time */
+  double s_e, s_eps, s_q, s_pi;          /* MRT rates; s_pi < 0 means s_pi = s_e */
+  double omega_b, omega_odd, omega_even; /* cumulant rates */
+  double c_smag;       /* Smagorinsky constant (TLBM_COLL_SMAGORINSKY, CUMULANT_D3Q19) */
+  double u_lid;        /* lid x-velocity */
+  double u_in[3];      /* Zou/He inlet velocity */
+  double rho_out;      /* Zou/He outlet density */
+} tlbm_desc;
+
+/* ---- fused time step ------------------------------------------------------
+ * One kernel pass: periodic pull f_in[q, x - c_q] -> boundary conditions ->
+ * collision -> store at x in f_out.  The stored state is post-collision, so
+ * repeated calls advance the TensorLBM chain collide -> stream -> boundaries
+ * by one step each with the phase shifted by half a step (a collision-only
+ * call with tlbm_collide turns a TensorLBM state into this phase, and a call
+ * with collision = TLBM_COLL_NONE turns it back).
+ * f_in must not alias f_out.  force (3 doubles, may be NULL) accumulates
+ * 2*sum_{obstacle} sum_q c_q f_q (post-stream, pre-bounce-back; obstacles.py:91,
+ * :197, boundaries.py:162) - zero it before the first step you want summed.
+ * status (may be NULL) gets bit 0 set if a non-finite density was seen.
+ * tau_field (may be NULL) gives a per-cell tau for BGK / MRT shear rates.
+ * Replaces: cases/base.py:270-289 make_step() closures, triton_fused.py:804
+ * TritonFusedSolver3D.step, triton_fused_obstacle.py:1695. */
+TLBM_API int tlbm_step(const tlbm_desc* d, const void* f_in, void* f_out, const uint8_t* flags,
+                       const float* tau_field, double* force, unsigned int* status, void* stream);
+
+/* Local collision only (no streaming, no boundaries); f_in may equal f_out.
+ * dtype_out may differ from d->dtype only for TLBM_COLL_NONE (format
+ * conversion).  flags (may be NULL): TLBM_FLAG_HALFWAY cells are stored
+ * reversed instead of collided.
+ * Replaces: collide_bgk (solver.py:67), collide_mrt (solver.py:249),
+ * collide_bgk3d (solver3d.py:100), collide_mrt3d (solver3d.py:107),
+ * collide_bgk27 (d3q27.py:423), collide_mrt27 (d3q27.py:643),
+ * collide_cumulant_d3q27 (cumulant.py:935), collide_cumulant_geier_d3q27
+ * (cumulant.py:1050), collide_cumulant_d3q19 (cumulant.py:1159),
+ * collide_smagorinsky_bgk3d (turbulence.py:245). */
+TLBM_API int tlbm_collide(const tlbm_desc* d, int32_t dtype_out, const void* f_in, void* f_out,
+                          const uint8_t* flags, const float* tau_field, void* stream);
+
+/* Periodic pull streaming.  Replaces stream (solver.py:396), stream3d
+ * (solver3d.py:210), stream3d_roll (solver3d.py:266), stream27 (d3q27.py:766). */
+TLBM_API int tlbm_stream(int32_t lattice, int32_t dtype, int32_t nx, int32_t ny, int32_t nz,
+                         const void* f_in, void* f_out, void* stream);
+
+/* f_eq from (rho, ux, uy[, uz]); uz ignored for D2Q9.  F32/F64 only.
+ * Replaces equilibrium (d2q9.py:39), equilibrium3d (d3q19.py:83),
+ * equilibrium27 (d3q27.py:353). */
+TLBM_API int tlbm_equilibrium(int32_t lattice, int32_t dtype, int64_t ncells, const void* rho,
+                              const void* ux, const void* uy, const void* uz, void* f_out,
+                              void* stream);
+
+/* (rho, ux, uy[, uz]) from f; uz may be NULL for D2Q9.  F32/F64 only.
+ * Replaces macroscopic (d2q9.py:61), macroscopic3d (d3q19.py:165),
+ * macroscopic27 (d3q27.py:395). */
+TLBM_API int tlbm_macroscopic(int32_t lattice, int32_t dtype, int64_t ncells, const void* f,
+                              void* rho, void* ux, void* uy, void* uz, void* stream);
+
+/* f_out = where(mask, f_in[opp], f_in); mask is one byte per cell.
+ * Replaces bounce_back_cells (boundaries.py:39), bounce_back_cells_3d
+ * (boundaries3d.py:112), bounce_back_cells_27 (boundaries_d3q27.py:45). */
+TLBM_API int tlbm_bounce_back(int32_t lattice, int32_t dtype, int64_t ncells, const void* f_in,
+                              const uint8_t* mask, void* f_out, void* stream);
+
+/* Zou/He velocity inlet on the x = 0 plane, in place.  ux_profile / uy_profile
+ * (D2Q9 only, length ny, may be NULL) override u_in / uy_in per row.
+ * Replaces zou_he_inlet_velocity (boundaries.py:50), zou_he_inlet_velocity_3d
+ * (boundaries3d.py:205), zou_he_inlet_velocity_27 (boundaries_d3q27.py:107). */
+TLBM_API int tlbm_zou_he_inlet(int32_t lattice, int32_t dtype, int32_t nx, int32_t ny, int32_t nz,
+                               void* f, double u_in, double uy_in, double uz_in,
+                               const void* ux_profile, const void* uy_profile, void* stream);
+
+/* Zou/He pressure outlet on the x = nx-1 plane, in place.
+ * Replaces zou_he_outlet_pressure (boundaries.py:102), zou_he_outlet_pressure_3d
+ * (boundaries3d.py:269), zou_he_outlet_pressure_27 (boundaries_d3q27.py:179). */
+TLBM_API int tlbm_zou_he_outlet(int32_t lattice, int32_t dtype, int32_t nx, int32_t ny, int32_t nz,
+                                void* f, double rho_out, void* stream);
+
+/* Zou/He moving lid on the y = ny-1 plane (all cells, corners included), in place.
+ * Replaces zou_he_moving_lid (lid_driven_cavity.py:431) and zou_he_moving_lid_3d
+ * (boundaries3d.py:324).  D2Q9 / D3Q19 only. */
+TLBM_API int tlbm_moving_lid(int32_t lattice, int32_t dtype, int32_t nx, int32_t ny, int32_t nz,
+                             void* f, double u_lid, void* stream);
+
+/* Momentum-exchange force 2*sum_{mask} sum_q c_q f_q into out[0..2] (float64,
+ * overwritten).  Replaces compute_obstacle_forces (boundaries.py:162),
+ * compute_obstacle_forces_3d (obstacles.py:91), compute_obstacle_forces_27
+ * (obstacles.py:197). */
+TLBM_API int tlbm_obstacle_force(int32_t lattice, int32_t dtype, int64_t ncells, const void* f,
+                                 const uint8_t* mask, double* out, void* stream);
+
+/* f_out = f_in * (target_mass / sum(f_in)), unless |sum| < 1e-30 (then a copy).
+ * The sum is accumulated in float64 in scratch[0] (one double the caller
+ * provides).  Replaces correct_mass (solver.py:420), correct_mass3d
+ * (solver3d.py:287), correct_mass27 (d3q27.py:729). */
+TLBM_API int tlbm_correct_mass(int32_t dtype, int64_t count, const void* f_in, void* f_out,
+                               double target_mass, double* scratch, void* stream);
+
+/* float64 sums over cells: out[0] = sum rho, out[1..3] = sum j (momentum).
+ * out overwritten.  Diagnostic counterpart of the mass / momentum checks in
+ * tensorlbm/reporters.py and utils.DiagnosticPoint. */
+TLBM_API int tlbm_moment_sums(int32_t lattice, int32_t dtype, int64_t ncells, const void* f,
+                              double* out, void* stream);
+
+/* Obstacle masks, one byte per cell, evaluated in float32 exactly as
+ * sphere_mask (boundaries3d.py:29) and cylinder_mask (boundaries.py:8). */
+TLBM_API int tlbm_sphere_mask(int32_t nx, int32_t ny, int32_t nz, double cx, double cy, double cz,
+                              double radius, uint8_t* out, void* stream);
+TLBM_API int tlbm_cylinder_mask(int32_t nx, int32_t ny, double cx, double cy, double radius,
+                                uint8_t* out, void* stream);
+
+/* With wall_flag = TLBM_FLAG_SOLID:
+ *   flags = (wall XOR obstacle ? SOLID : 0) | (obstacle ? OBSTACLE : 0),
+ * which encodes the successive bounce_back_cells(wall),
+ * bounce_back_cells(obstacle) calls of apply_zou_he_channel_boundaries_3d
+ * (boundaries3d.py:707).  With wall_flag = TLBM_FLAG_HALFWAY, wall cells get
+ * HALFWAY (pre-stream walls) and obstacle cells SOLID | OBSTACLE.
+ * wall or obstacle may be NULL. */
+TLBM_API int tlbm_build_flags(int64_t ncells, const uint8_t* wall, const uint8_t* obstacle,
+                              uint32_t wall_flag, uint8_t* flags, void* stream);
+
+/* missing[q, cell] = 1 where the pull source cell - c_q is solid or outside a
+ * non-periodic face.  periodic_bits: 1 = x, 2 = y, 4 = z periodic.
+ * Replaces derive_missing_mask (boundary_registry.py:488). */
+TLBM_API int tlbm_missing_mask(int32_t lattice, int32_t nx, int32_t ny, int32_t nz,
+                               const uint8_t* solid, int32_t periodic_bits, uint8_t* missing,
+                               void* stream);
+
+/* Link list of a byte mask: the flat indices of its non-zero entries in
+ * increasing order (torch.nonzero order of the (q, z, y, x) mask).
+ * tlbm_link_count writes the count to *count_out (device int64);
+ * block_counts must hold tlbm_link_blocks(count) int64 values.
+ * tlbm_link_list writes the indices (int64) using the same block_counts. */
+TLBM_API int64_t tlbm_link_blocks(int64_t count);
+TLBM_API int tlbm_link_count(const uint8_t* mask, int64_t count, int64_t* block_counts,
+                             int64_t* count_out, void* stream);
+TLBM_API int tlbm_link_list(const uint8_t* mask, int64_t count, const int64_t* block_counts,
+                            int64_t* out, void* stream);
+
+TLBM_API const char* tlbm_status_string(int status);
+TLBM_API int tlbm_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TLBM_H */

@@ -1,0 +1,668 @@
+"""CPU oracle: a numpy restatement of TensorLBM's lattice-Boltzmann time step.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker for the CUDA kernels of
+tensorlbm_b200: only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline / reference leg import it.  The product never calls it.
+
+Every function restates the TensorLBM function cited beside it (paths inside
+the TensorLBM source tree) in plain numpy, keeping the reference's arithmetic
+order and dtype behaviour (float32 fields stay float32; the MRT matrices of
+D3Q19/D3Q27 are rounded to float32 like the reference's cached tensors).
+Parity of this oracle with TensorLBM itself is pinned by the golden vectors in
+tests/golden/ (generated by tests/golden/make_golden.py from the unmodified
+reference) and checked by tests/test_oracle_golden.py.
+
+Layout: f has shape (Q, nz, ny, nx) for 3-D lattices and (9, ny, nx) for D2Q9.
+"""
+
+from __future__ import annotations
+
+from fractions import Fraction
+
+import numpy as np
+
+# ---------------------------------------------------------------------------
+# lattice tables (tensorlbm/d2q9.py:8-26, d3q19.py:6-67, d3q27.py:32-84)
+# ---------------------------------------------------------------------------
+
+_C9 = [(0, 0), (1, 0), (0, 1), (-1, 0), (0, -1), (1, 1), (-1, 1), (-1, -1), (1, -1)]
+_C19 = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1),
+        (1, 1, 0), (-1, -1, 0), (1, -1, 0), (-1, 1, 0), (1, 0, 1), (-1, 0, -1), (1, 0, -1), (-1, 0, 1),
+        (0, 1, 1), (0, -1, -1), (0, 1, -1), (0, -1, 1)]
+_C27 = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1),
+        (1, 1, 0), (-1, 1, 0), (1, -1, 0), (-1, -1, 0), (1, 0, 1), (-1, 0, 1), (1, 0, -1), (-1, 0, -1),
+        (0, 1, 1), (0, -1, 1), (0, 1, -1), (0, -1, -1),
+        (1, 1, 1), (-1, 1, 1), (1, -1, 1), (-1, -1, 1), (1, 1, -1), (-1, 1, -1), (1, -1, -1), (-1, -1, -1)]
+C = {9: np.array(_C9, dtype=np.int64), 19: np.array(_C19, dtype=np.int64), 27: np.array(_C27, dtype=np.int64)}
+_WFRAC = {
+    9: [Fraction(4, 9)] + [Fraction(1, 9)] * 4 + [Fraction(1, 36)] * 4,
+    19: [Fraction(1, 3)] + [Fraction(1, 18)] * 6 + [Fraction(1, 36)] * 12,
+    27: [Fraction(8, 27)] + [Fraction(2, 27)] * 6 + [Fraction(1, 54)] * 12 + [Fraction(1, 216)] * 8,
+}
+W64 = {q: np.array([float(v) for v in w]) for q, w in _WFRAC.items()}
+
+
+def opposite(q: int) -> np.ndarray:
+    c = C[q]
+    idx = {tuple(r): i for i, r in enumerate(c.tolist())}
+    return np.array([idx[tuple((-c[i]).tolist())] for i in range(q)], dtype=np.int64)
+
+
+def zou_he_partner(q: int) -> np.ndarray:
+    """Known population paired with each unknown one in the x-face Zou/He
+    conditions.  D3Q19 pairs true opposites (boundaries3d.py:14-19); the D3Q27
+    tables pair x-mirrors, e.g. 7 (1,1,0) with 8 (-1,1,0)
+    (boundaries_d3q27.py:36-41), and that pairing is what TensorLBM computes."""
+    if q != 27:
+        return opposite(q)
+    c = C[27]
+    idx = {tuple(r): i for i, r in enumerate(c.tolist())}
+    return np.array([idx[(-int(r[0]), int(r[1]), int(r[2]))] for r in c], dtype=np.int64)
+
+
+def weights(q: int, dtype) -> np.ndarray:
+    """D2Q9 keeps float32 weights for every field dtype (d2q9.py:22-36);
+    D3Q19/D3Q27 cast the binary64 weights (d3q19.py:58-80)."""
+    if q == 9:
+        return W64[9].astype(np.float32).astype(dtype)
+    return W64[q].astype(dtype)
+
+
+def _view(v: np.ndarray, ndim: int) -> np.ndarray:
+    return v.reshape((-1,) + (1,) * ndim)
+
+
+# ---------------------------------------------------------------------------
+# moments and equilibrium
+# ---------------------------------------------------------------------------
+
+
+def macroscopic(f: np.ndarray):
+    """d2q9.py:61-74, d3q19.py:165-186, d3q27.py:395-420."""
+    q = f.shape[0]
+    nd = f.ndim - 1
+    c = C[q].astype(f.dtype)
+    rho = f.sum(axis=0)
+    rs = np.maximum(rho, f.dtype.type(1e-12))
+    ux = (f * _view(c[:, 0], nd)).sum(axis=0) / rs
+    uy = (f * _view(c[:, 1], nd)).sum(axis=0) / rs
+    if q == 9:
+        return rho, ux, uy, None
+    uz = (f * _view(c[:, 2], nd)).sum(axis=0) / rs
+    return rho, ux, uy, uz
+
+
+def equilibrium(q: int, rho, ux, uy, uz=None) -> np.ndarray:
+    """d2q9.py:39-58, d3q19.py:83-125, d3q27.py:353-392."""
+    nd = rho.ndim
+    dt = rho.dtype
+    c = C[q]
+    w = _view(weights(q, dt), nd)
+    if q == 9:
+        usq = ux * ux + uy * uy
+        cu = _view(c[:, 0].astype(dt), nd) * ux + _view(c[:, 1].astype(dt), nd) * uy
+    else:
+        usq = ux * ux + uy * uy + uz * uz
+        cu = (_view(c[:, 0].astype(dt), nd) * ux + _view(c[:, 1].astype(dt), nd) * uy
+              + _view(c[:, 2].astype(dt), nd) * uz)
+    return w * rho[None] * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq[None])
+
+
+# ---------------------------------------------------------------------------
+# collisions
+# ---------------------------------------------------------------------------
+
+
+def collide_bgk(f: np.ndarray, tau: float) -> np.ndarray:
+    """solver.py:67-71, solver3d.py:100-104, d3q27.py:423-437."""
+    rho, ux, uy, uz = macroscopic(f)
+    feq = equilibrium(f.shape[0], rho, ux, uy, uz)
+    return f - (f - feq) / f.dtype.type(tau)
+
+
+def mrt_matrix(q: int) -> np.ndarray:
+    """Moment bases: solver.py:24-34 (D2Q9), solver3d.py:24-55 (D3Q19),
+    d3q27.py:545-635 (D3Q27 Gram-Schmidt)."""
+    c = C[q].astype(np.float64)
+    if q == 9:
+        cx, cy = c[:, 0], c[:, 1]
+        c2 = cx**2 + cy**2
+        return np.array([np.ones(9), 3 * c2 - 4, (9 * c2**2 - 21 * c2 + 8) / 2, cx, (3 * c2 - 5) * cx, cy,
+                         (3 * c2 - 5) * cy, cx**2 - cy**2, cx * cy])
+    cx, cy, cz = c[:, 0], c[:, 1], c[:, 2]
+    e2 = cx**2 + cy**2 + cz**2
+    if q == 19:
+        return np.array([np.ones(19), 19 * e2 - 30, (21 * e2**2 - 53 * e2 + 24) / 2, cx,
+                         cx * e2 * (5 * e2 - 9) / 2, cy, cy * e2 * (5 * e2 - 9) / 2, cz,
+                         cz * e2 * (5 * e2 - 9) / 2, 3 * cx**2 - e2, cx**2 - cy**2, cx * cy, cx * cz, cy * cz,
+                         (3 * e2 - 5) * (3 * cx**2 - e2) / 2, (3 * e2 - 5) * (cx**2 - cy**2) / 2, cx**2 * cy,
+                         cx**2 * cz, cy**2 * cx])
+    raw = [np.ones(27), cx, cy, cz, e2, 3 * cx**2 - e2, cy**2 - cz**2, cx * cy, cx * cz, cy * cz,
+           cx * e2, cy * e2, cz * e2, cx**2 * cy, cx**2 * cz, cy**2 * cx, cy**2 * cz, cz**2 * cx, cz**2 * cy,
+           e2**2, cx**2 * e2, cy**2 * e2, cz**2 * e2, cx**2 * cy**2, cx**2 * cz**2, cy**2 * cz**2,
+           cx * cy * cz]
+    rows: list[np.ndarray] = []
+    for r in raw:
+        v = r.copy()
+        for p in rows:
+            v = v - (v @ p) / (p @ p) * p
+        if np.sqrt(v @ v) < 1e-14:
+            for i in range(27):
+                u = np.zeros(27)
+                u[i] = 1.0
+                for p in rows:
+                    u = u - (u @ p) / (p @ p) * p
+                if np.sqrt(u @ u) > 1e-10:
+                    v = u
+                    break
+        rows.append(v)
+    return np.array(rows)
+
+
+def _mrt_rates(q: int, tau: float, s_e, s_eps, s_q, s_pi) -> list[float]:
+    s_nu = 1.0 / tau
+    if q == 9:
+        return [0.0, s_e, s_eps, 0.0, s_q, 0.0, s_q, s_nu, s_nu]
+    if s_pi is None:
+        s_pi = s_e
+    if q == 19:
+        return [0.0, s_e, s_eps, 0.0, s_q, 0.0, s_q, 0.0, s_q] + [s_nu] * 5 + [s_pi, s_pi, 1.0, 1.0, 1.0]
+    return [0.0] * 4 + [s_e] + [s_nu] * 5 + [s_q] * 9 + [s_eps] + [s_pi] * 7
+
+
+def collide_mrt(f: np.ndarray, tau: float, s_e=None, s_eps=None, s_q=None, s_pi=None, tau_field=None):
+    """m = M f, m* = m - s (m - M feq), f' = M^-1 m* (solver.py:249-331,
+    solver3d.py:107-160, d3q27.py:643-727).  D3Q19/D3Q27 matrices are float32
+    in the reference whatever the field dtype (solver3d.py:93-97)."""
+    q = f.shape[0]
+    defaults = {9: (1.64, 1.54, 1.7), 19: (1.19, 1.4, 1.2), 27: (1.19, 1.4, 1.2)}[q]
+    s_e = defaults[0] if s_e is None else s_e
+    s_eps = defaults[1] if s_eps is None else s_eps
+    s_q = defaults[2] if s_q is None else s_q
+    m64 = mrt_matrix(q)
+    mat_dt = f.dtype if q == 9 else np.float32
+    m = m64.astype(mat_dt)
+    minv = np.linalg.inv(m64).astype(mat_dt)
+    spatial = f.shape[1:]
+    ff = f.reshape(q, -1)
+    rho, ux, uy, uz = macroscopic(f)
+    feq = equilibrium(q, rho, ux, uy, uz).reshape(q, -1)
+    mom = m @ ff
+    meq = m @ feq
+    s = np.array(_mrt_rates(q, tau, s_e, s_eps, s_q, s_pi), dtype=f.dtype)[:, None]
+    if tau_field is not None:
+        s = np.repeat(s, ff.shape[1], axis=1)
+        inv = (1.0 / tau_field.astype(f.dtype)).reshape(-1)
+        s[7] = inv
+        s[8] = inv
+    mstar = mom - s * (mom - meq)
+    return (minv @ mstar).reshape((q,) + spatial).astype(f.dtype)
+
+
+def neq_stress(fneq: np.ndarray):
+    q = fneq.shape[0]
+    nd = fneq.ndim - 1
+    c = C[q].astype(fneq.dtype)
+    cx = _view(c[:, 0], nd)
+    cy = _view(c[:, 1], nd)
+    pxx = (cx * cx * fneq).sum(0)
+    pyy = (cy * cy * fneq).sum(0)
+    pxy = (cx * cy * fneq).sum(0)
+    if q == 9:
+        return pxx, pyy, None, pxy, None, None
+    cz = _view(c[:, 2], nd)
+    return pxx, pyy, (cz * cz * fneq).sum(0), pxy, (cx * cz * fneq).sum(0), (cy * cz * fneq).sum(0)
+
+
+def smagorinsky_tau(tau: float, pi_norm, rho, c_s: float):
+    """turbulence.py:183-208 with the clamps of :77-100."""
+    rs = np.maximum(rho, rho.dtype.type(1e-12))
+    disc = tau**2 + 18.0 * c_s**2 * pi_norm / rs
+    te = 0.5 * (tau + np.sqrt(np.maximum(disc, 0.0)))
+    return np.clip(te, 0.5001, max(1.0, tau + 0.5)).astype(rho.dtype)
+
+
+def collide_smagorinsky(f: np.ndarray, tau: float, c_s: float = 0.1) -> np.ndarray:
+    """turbulence.py:216 (D2Q9), :245 (D3Q19), :472 (D3Q27)."""
+    q = f.shape[0]
+    rho, ux, uy, uz = macroscopic(f)
+    fneq = f - equilibrium(q, rho, ux, uy, uz)
+    pxx, pyy, pzz, pxy, pxz, pyz = neq_stress(fneq)
+    if q == 9:
+        rad = pxx**2 + pyy**2 + 2.0 * pxy**2
+    else:
+        rad = pxx**2 + pyy**2 + pzz**2 + 2.0 * (pxy**2 + pxz**2 + pyz**2)
+    pn = np.sqrt(np.maximum(rad, rad.dtype.type(1e-30)))
+    te = smagorinsky_tau(tau, pn, rho, c_s)
+    return f - fneq / te[None]
+
+
+def collide_cumulant_d3q19(f: np.ndarray, tau: float, omega_b=1.0, omega_odd=1.0, omega_even=1.0, c_s=0.0):
+    """Hermite-regularised stress relaxation, cumulant.py:1159-1420 (Smagorinsky branch only)."""
+    rho, ux, uy, uz = macroscopic(f)
+    feq = equilibrium(19, rho, ux, uy, uz)
+    fneq = f - feq
+    pxx, pyy, pzz, pxy, pxz, pyz = neq_stress(fneq)
+    if c_s > 0.0:
+        pn = np.sqrt(pxx**2 + pyy**2 + pzz**2 + 2.0 * (pxy**2 + pxz**2 + pyz**2))
+        rs = np.maximum(rho, rho.dtype.type(1e-12))
+        te = 0.5 * (tau + np.sqrt(tau * tau + 18.0 * c_s * c_s * pn / rs))
+        omega = (1.0 / te).astype(f.dtype)
+    else:
+        omega = 1.0 / tau
+    tr = pxx + pyy + pzz
+    sxx = pxx - omega * pxx - (omega_b - omega) * tr / 3.0
+    syy = pyy - omega * pyy - (omega_b - omega) * tr / 3.0
+    szz = pzz - omega * pzz - (omega_b - omega) * tr / 3.0
+    sxy = pxy - omega * pxy
+    sxz = pxz - omega * pxz
+    syz = pyz - omega * pyz
+    c = C[19].astype(f.dtype)
+    cx, cy, cz = (_view(c[:, k], 3) for k in range(3))
+    w = _view(np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=f.dtype), 3)
+    cs2 = 1.0 / 3.0
+    hxx, hyy, hzz = cx * cx - cs2, cy * cy - cs2, cz * cz - cs2
+    reg = 4.5 * w * (hxx * sxx + hyy * syy + hzz * szz + 2.0 * cx * cy * sxy + 2.0 * cx * cz * sxz
+                     + 2.0 * cy * cz * syz)
+    ho = fneq - 4.5 * w * (hxx * pxx + hyy * pyy + hzz * pzz + 2.0 * cx * cy * pxy + 2.0 * cx * cz * pxz
+                           + 2.0 * cy * cz * pyz)
+    return (feq + reg + (1.0 - omega_even) * ho).astype(f.dtype)
+
+
+# D3Q27 cumulant machinery (cumulant.py:321-457, 904-919)
+DEGREES = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (0, 2, 0), (0, 0, 2), (1, 1, 0), (1, 0, 1),
+           (0, 1, 1), (2, 1, 0), (2, 0, 1), (1, 2, 0), (0, 2, 1), (1, 0, 2), (0, 1, 2), (1, 1, 1), (2, 2, 0),
+           (2, 0, 2), (0, 2, 2), (2, 1, 1), (1, 2, 1), (1, 1, 2), (2, 2, 1), (2, 1, 2), (1, 2, 2), (2, 2, 2)]
+
+
+def _shift_groups():
+    out = []
+    for axis in range(3):
+        others = [a for a in range(3) if a != axis]
+        bucket: dict = {}
+        for k, d in enumerate(DEGREES):
+            bucket.setdefault((d[others[0]], d[others[1]]), {})[d[axis]] = k
+        out.append([(b[0], b[1], b[2]) for key, b in sorted(bucket.items()) if len(b) == 3])
+    return out
+
+
+_GROUPS = _shift_groups()
+
+
+def monomial_matrix() -> np.ndarray:
+    c = C[27].astype(np.float64)
+    return np.array([c[:, 0] ** a * c[:, 1] ** b * c[:, 2] ** d for a, b, d in DEGREES])
+
+
+def _shift(m, groups, u, sign):
+    out = m.copy()
+    for i0, i1, i2 in groups:
+        out[i1] = m[i1] + sign * u * m[i0]
+        out[i2] = m[i2] + sign * 2.0 * u * m[i1] + u * u * m[i0]
+    return out
+
+
+def to_central(m, ux, uy, uz):
+    m = _shift(m, _GROUPS[0], ux, -1.0)
+    m = _shift(m, _GROUPS[1], uy, -1.0)
+    return _shift(m, _GROUPS[2], uz, -1.0)
+
+
+def to_raw(k, ux, uy, uz):
+    k = _shift(k, _GROUPS[2], uz, 1.0)
+    k = _shift(k, _GROUPS[1], uy, 1.0)
+    return _shift(k, _GROUPS[0], ux, 1.0)
+
+
+def legacy_forward(k):
+    """cumulant.py:470-577"""
+    C_ = k.copy()
+    k200, k020, k002, k110, k101, k011 = k[4], k[5], k[6], k[7], k[8], k[9]
+    C_[17] = k[17] - k200 * k020 - 2.0 * k110 * k110
+    C_[18] = k[18] - k200 * k002 - 2.0 * k101 * k101
+    C_[19] = k[19] - k020 * k002 - 2.0 * k011 * k011
+    C_[20] = k[20] - k200 * k011 - 2.0 * k101 * k110
+    C_[21] = k[21] - k020 * k101 - 2.0 * k110 * k011
+    C_[22] = k[22] - k002 * k110 - 2.0 * k101 * k011
+    C_[23] = k[23] - k200 * k[13] - 2.0 * k110 * k[16]
+    C_[24] = k[24] - k200 * k[15] - 2.0 * k101 * k[16]
+    C_[25] = k[25] - k020 * k[14] - 2.0 * k011 * k[16]
+    C_[26] = (k[26] - k200 * C_[19] - k020 * C_[18] - k002 * C_[17]
+              - 2.0 * (k110 * C_[22] + k101 * C_[21] + k011 * C_[20]) + 2.0 * k200 * k020 * k002
+              + 4.0 * k110 * k101 * k011 + 2.0 * k110 * k110 * k002 + 2.0 * k101 * k101 * k020
+              + 2.0 * k011 * k011 * k200)
+    return C_
+
+
+def legacy_inverse(C_):
+    """cumulant.py:580-651"""
+    k = C_.copy()
+    c200, c020, c002, c110, c101, c011 = C_[4], C_[5], C_[6], C_[7], C_[8], C_[9]
+    k[17] = C_[17] + c200 * c020 + 2.0 * c110 * c110
+    k[18] = C_[18] + c200 * c002 + 2.0 * c101 * c101
+    k[19] = C_[19] + c020 * c002 + 2.0 * c011 * c011
+    k[20] = C_[20] + c200 * c011 + 2.0 * c101 * c110
+    k[21] = C_[21] + c020 * c101 + 2.0 * c110 * c011
+    k[22] = C_[22] + c002 * c110 + 2.0 * c101 * c011
+    k[23] = C_[23] + c200 * C_[13] + 2.0 * c110 * C_[16]
+    k[24] = C_[24] + c200 * C_[15] + 2.0 * c101 * C_[16]
+    k[25] = C_[25] + c020 * C_[14] + 2.0 * c011 * C_[16]
+    k[26] = (C_[26] + c200 * C_[19] + c020 * C_[18] + c002 * C_[17]
+             + 2.0 * (c110 * C_[22] + c101 * C_[21] + c011 * C_[20]) - 2.0 * c200 * c020 * c002
+             - 4.0 * c110 * c101 * c011 - 2.0 * c110 * c110 * c002 - 2.0 * c101 * c101 * c020
+             - 2.0 * c011 * c011 * c200)
+    return k
+
+
+def collide_cumulant_d3q27(f: np.ndarray, tau: float, omega_b=1.0, omega_odd=1.0, omega_even=1.0):
+    """cumulant.py:935-1047 (C_s = 0)."""
+    om = 1.0 / tau
+    rho, ux, uy, uz = macroscopic(f)
+    feq = equilibrium(27, rho, ux, uy, uz)
+    fneq = f - feq
+    m64 = monomial_matrix()
+    M = m64.astype(f.dtype)
+    Minv = np.linalg.inv(m64).astype(f.dtype)
+    sp = f.shape[1:]
+    m = (M @ fneq.reshape(27, -1)).reshape((27,) + sp)
+    Cn = legacy_forward(to_central(m, ux, uy, uz))
+    out = Cn.copy()
+    tr = Cn[4] + Cn[5] + Cn[6]
+    trs = (1.0 - omega_b) * tr
+    for i in range(3):
+        out[4 + i] = (1.0 - om) * (Cn[4 + i] - tr / 3.0) + trs / 3.0
+    for i in (7, 8, 9):
+        out[i] = (1.0 - om) * Cn[i]
+    out[10:17] = (1.0 - omega_odd) * Cn[10:17]
+    out[17:27] = (1.0 - omega_even) * Cn[17:27]
+    ms = to_raw(legacy_inverse(out), ux, uy, uz)
+    return (feq + (Minv @ ms.reshape(27, -1)).reshape((27,) + sp)).astype(f.dtype)
+
+
+def geier_forward(k):
+    """cumulant.py:674-745"""
+    rho = k[0]
+    t = k / rho
+    c = t.copy()
+    c[17] = t[17] - (t[5] * t[4] + 2.0 * t[7] ** 2)
+    c[18] = t[18] - (t[6] * t[4] + 2.0 * t[8] ** 2)
+    c[19] = t[19] - (t[6] * t[5] + 2.0 * t[9] ** 2)
+    c[20] = t[20] - (t[9] * t[4] + 2.0 * t[8] * t[7])
+    c[21] = t[21] - (2.0 * t[9] * t[7] + t[5] * t[8])
+    c[22] = t[22] - (t[6] * t[7] + 2.0 * t[9] * t[8])
+    c[23] = t[23] - (2.0 * t[9] * t[10] + t[5] * t[11] + t[13] * t[4] + 2.0 * t[8] * t[12] + 4.0 * t[7] * t[16])
+    c[24] = t[24] - (t[6] * t[10] + 2.0 * t[9] * t[11] + t[15] * t[4] + 4.0 * t[8] * t[16] + 2.0 * t[14] * t[7])
+    c[25] = t[25] - (t[6] * t[12] + 4.0 * t[9] * t[16] + 2.0 * t[15] * t[7] + t[5] * t[14] + 2.0 * t[13] * t[8])
+    c[26] = t[26] - (-2.0 * t[6] * t[5] * t[4] - 4.0 * t[6] * t[7] ** 2 + t[6] * t[17] - 4.0 * t[9] ** 2 * t[4]
+                     - 16.0 * t[9] * t[8] * t[7] + 4.0 * t[9] * t[20] + 2.0 * t[15] * t[10]
+                     - 4.0 * t[5] * t[8] ** 2 + t[5] * t[18] + 2.0 * t[13] * t[11] + t[19] * t[4]
+                     + 4.0 * t[8] * t[21] + 2.0 * t[14] * t[12] + 4.0 * t[7] * t[22] + 4.0 * t[16] ** 2)
+    out = c * rho
+    out[0] = rho
+    return out
+
+
+def geier_inverse(c):
+    """cumulant.py:748-815"""
+    rho = c[0]
+    t = c / rho
+    k = t.copy()
+    k[17] = t[5] * t[4] + 2.0 * t[7] ** 2 + t[17]
+    k[18] = t[6] * t[4] + 2.0 * t[8] ** 2 + t[18]
+    k[19] = t[6] * t[5] + 2.0 * t[9] ** 2 + t[19]
+    k[20] = t[9] * t[4] + 2.0 * t[8] * t[7] + t[20]
+    k[21] = 2.0 * t[9] * t[7] + t[5] * t[8] + t[21]
+    k[22] = t[6] * t[7] + 2.0 * t[9] * t[8] + t[22]
+    k[23] = 2.0 * t[9] * t[10] + t[5] * t[11] + t[13] * t[4] + 2.0 * t[8] * t[12] + 4.0 * t[7] * t[16] + t[23]
+    k[24] = t[6] * t[10] + 2.0 * t[9] * t[11] + t[15] * t[4] + 4.0 * t[8] * t[16] + 2.0 * t[14] * t[7] + t[24]
+    k[25] = t[6] * t[12] + 4.0 * t[9] * t[16] + 2.0 * t[15] * t[7] + t[5] * t[14] + 2.0 * t[13] * t[8] + t[25]
+    k[26] = (t[6] * t[5] * t[4] + 2.0 * t[6] * t[7] ** 2 + t[6] * t[17] + 2.0 * t[9] ** 2 * t[4]
+             + 8.0 * t[9] * t[8] * t[7] + 4.0 * t[9] * t[20] + 2.0 * t[15] * t[10] + 2.0 * t[5] * t[8] ** 2
+             + t[5] * t[18] + 2.0 * t[13] * t[11] + t[19] * t[4] + 4.0 * t[8] * t[21] + 2.0 * t[14] * t[12]
+             + 4.0 * t[7] * t[22] + 4.0 * t[16] ** 2 + t[26])
+    out = k * rho
+    out[0] = rho
+    return out
+
+
+def collide_cumulant_geier_d3q27(f: np.ndarray, tau: float, omega_b=1.0, omega_odd=1.0, omega_even=1.0):
+    """cumulant.py:1050-1156 (C_s = 0)."""
+    om = 1.0 / tau
+    rho, ux, uy, uz = macroscopic(f)
+    feq = equilibrium(27, rho, ux, uy, uz)
+    m64 = monomial_matrix()
+    M = m64.astype(f.dtype)
+    Minv = np.linalg.inv(m64).astype(f.dtype)
+    sp = f.shape[1:]
+    m = (M @ f.reshape(27, -1)).reshape((27,) + sp)
+    meq = (M @ feq.reshape(27, -1)).reshape((27,) + sp)
+    Cc = geier_forward(to_central(m, ux, uy, uz))
+    Ce = geier_forward(to_central(meq, ux, uy, uz))
+    D = Cc - Ce
+    out = Cc.copy()
+    tr = D[4] + D[5] + D[6]
+    for i in range(3):
+        out[4 + i] = Cc[4 + i] - (om * (D[4 + i] - tr / 3.0) + omega_b * tr / 3.0)
+    for i in (7, 8, 9):
+        out[i] = Cc[i] - om * D[i]
+    out[10:17] = Cc[10:17] - omega_odd * D[10:17]
+    out[17:27] = Cc[17:27] - omega_even * D[17:27]
+    ms = to_raw(geier_inverse(out), ux, uy, uz)
+    return (Minv @ ms.reshape(27, -1)).reshape((27,) + sp).astype(f.dtype)
+
+
+COLLIDERS = {
+    "bgk": collide_bgk,
+    "mrt": collide_mrt,
+    "smagorinsky": collide_smagorinsky,
+    "cumulant_d3q19": collide_cumulant_d3q19,
+    "cumulant": collide_cumulant_d3q27,
+    "cumulant_geier": collide_cumulant_geier_d3q27,
+}
+
+
+# ---------------------------------------------------------------------------
+# streaming and boundaries
+# ---------------------------------------------------------------------------
+
+
+def stream(f: np.ndarray) -> np.ndarray:
+    """Periodic pull f'[q, x] = f[q, x - c_q] (solver.py:396, solver3d.py:210, d3q27.py:766)."""
+    q = f.shape[0]
+    out = np.empty_like(f)
+    for i in range(q):
+        c = C[q][i]
+        if q == 9:
+            out[i] = np.roll(f[i], shift=(int(c[1]), int(c[0])), axis=(0, 1))
+        else:
+            out[i] = np.roll(f[i], shift=(int(c[2]), int(c[1]), int(c[0])), axis=(0, 1, 2))
+    return out
+
+
+def bounce_back(f: np.ndarray, mask: np.ndarray) -> np.ndarray:
+    """where(mask, f[opp], f): boundaries.py:39, boundaries3d.py:112, boundaries_d3q27.py:45."""
+    return np.where(mask[None], f[opposite(f.shape[0])], f)
+
+
+def zou_he_inlet(f: np.ndarray, u_in: float, uy_in: float = 0.0, uz_in: float = 0.0) -> np.ndarray:
+    """x = 0 velocity inlet: boundaries.py:50 (D2Q9), boundaries3d.py:205, boundaries_d3q27.py:107."""
+    q = f.shape[0]
+    f = f.copy()
+    if q == 9:
+        f0, f2, f3, f4, f6, f7 = (f[i][:, 0] for i in (0, 2, 3, 4, 6, 7))
+        rho = (f0 + f2 + f4 + 2.0 * (f3 + f6 + f7)) / (1.0 - u_in)
+        f[1][:, 0] = f3 + (2.0 / 3.0) * rho * u_in
+        f[5][:, 0] = f7 - 0.5 * (f2 - f4) + (1.0 / 6.0) * rho * u_in + 0.5 * rho * uy_in
+        f[8][:, 0] = f6 + 0.5 * (f2 - f4) + (1.0 / 6.0) * rho * u_in - 0.5 * rho * uy_in
+        return f
+    c = C[q]
+    zero = [i for i in range(q) if c[i, 0] == 0]
+    neg = [i for i in range(q) if c[i, 0] < 0]
+    pos = [i for i in range(q) if c[i, 0] > 0]
+    opp = zou_he_partner(q)
+    s0 = f[zero[0]][:, :, 0].copy()
+    for i in zero[1:]:
+        s0 = s0 + f[i][:, :, 0]
+    sn = f[neg[0]][:, :, 0].copy()
+    for i in neg[1:]:
+        sn = sn + f[i][:, :, 0]
+    rho = (s0 + 2.0 * sn) / (1.0 - u_in)
+    r3 = rho[..., None]
+    dt = f.dtype
+    feq = equilibrium(q, r3, np.full_like(r3, u_in, dtype=dt), np.full_like(r3, uy_in, dtype=dt),
+                      np.full_like(r3, uz_in, dtype=dt))
+    for k in pos:
+        f[k][:, :, 0] = feq[k][:, :, 0] - feq[opp[k]][:, :, 0] + f[opp[k]][:, :, 0]
+    return f
+
+
+def zou_he_outlet(f: np.ndarray, rho_out: float = 1.0) -> np.ndarray:
+    """x = nx-1 pressure outlet: boundaries.py:102, boundaries3d.py:269, boundaries_d3q27.py:179."""
+    q = f.shape[0]
+    f = f.copy()
+    if q == 9:
+        f1, f2, f4, f5, f8 = (f[i][:, -1] for i in (1, 2, 4, 5, 8))
+        ux = -1.0 + (f[0][:, -1] + f2 + f4 + 2.0 * (f1 + f5 + f8)) / rho_out
+        f[3][:, -1] = f1 - (2.0 / 3.0) * rho_out * ux
+        f[7][:, -1] = f5 + 0.5 * (f2 - f4) - (1.0 / 6.0) * rho_out * ux
+        f[6][:, -1] = f8 - 0.5 * (f2 - f4) - (1.0 / 6.0) * rho_out * ux
+        return f
+    c = C[q]
+    zero = [i for i in range(q) if c[i, 0] == 0]
+    pos = [i for i in range(q) if c[i, 0] > 0]
+    neg = [i for i in range(q) if c[i, 0] < 0]
+    opp = zou_he_partner(q)
+    s0 = f[zero[0]][:, :, -1].copy()
+    for i in zero[1:]:
+        s0 = s0 + f[i][:, :, -1]
+    sp = f[pos[0]][:, :, -1].copy()
+    for i in pos[1:]:
+        sp = sp + f[i][:, :, -1]
+    ux = -1.0 + (s0 + 2.0 * sp) / rho_out
+    r3 = np.full_like(ux, rho_out)[..., None]
+    feq = equilibrium(q, r3, ux[..., None], np.zeros_like(r3), np.zeros_like(r3))
+    for k in neg:
+        f[k][:, :, -1] = feq[k][:, :, 0] - feq[opp[k]][:, :, 0] + f[opp[k]][:, :, -1]
+    return f
+
+
+def moving_lid(f: np.ndarray, u_lid: float) -> np.ndarray:
+    """Zou/He lid on the whole y = ny-1 plane: lid_driven_cavity.py:431 (D2Q9),
+    boundaries3d.py:324 (D3Q19)."""
+    f = f.copy()
+    if f.shape[0] == 9:
+        f0, f1, f2, f3, f5, f6 = (f[i][-1, :].copy() for i in (0, 1, 2, 3, 5, 6))
+        rho = f0 + f1 + 2.0 * f2 + f3 + 2.0 * f5 + 2.0 * f6
+        f[4][-1, :] = f2
+        f[7][-1, :] = f5 + 0.5 * (f1 - f3) - 0.5 * rho * u_lid
+        f[8][-1, :] = f6 - 0.5 * (f1 - f3) + 0.5 * rho * u_lid
+        return f
+    fl = {i: f[i][:, -1, :].copy() for i in range(19)}
+    s0 = fl[0] + fl[1] + fl[2] + fl[5] + fl[6] + fl[11] + fl[12] + fl[13] + fl[14]
+    sp = fl[3] + fl[7] + fl[10] + fl[15] + fl[17]
+    rho = s0 + 2.0 * sp
+    sx0 = fl[1] - fl[2] + fl[11] - fl[12] + fl[13] - fl[14]
+    dx = rho * u_lid - (sx0 + (fl[7] - fl[10]))
+    sz0 = fl[5] - fl[6] + fl[11] - fl[12] - fl[13] + fl[14]
+    f[4][:, -1, :] = fl[3]
+    f[8][:, -1, :] = 0.5 * (fl[7] + fl[10]) - 0.5 * dx
+    f[9][:, -1, :] = 0.5 * (fl[7] + fl[10]) + 0.5 * dx
+    f[16][:, -1, :] = fl[15] + 0.5 * sz0
+    f[18][:, -1, :] = fl[17] - 0.5 * sz0
+    return f
+
+
+def obstacle_force(f: np.ndarray, mask: np.ndarray) -> np.ndarray:
+    """2 sum_solid sum_q c_q f_q in float64: boundaries.py:162, obstacles.py:91, :197."""
+    q = f.shape[0]
+    fs = f.astype(np.float64)[:, mask]
+    c = C[q].astype(np.float64)
+    return np.array([2.0 * (c[:, k] @ fs.sum(axis=1)) for k in range(2 if q == 9 else 3)] + ([0.0] if q == 9 else []))
+
+
+# ---------------------------------------------------------------------------
+# masks
+# ---------------------------------------------------------------------------
+
+
+def sphere_mask(nx, ny, nz, cx, cy, cz, radius) -> np.ndarray:
+    """float32 (x-cx)^2+(y-cy)^2+(z-cz)^2 <= r^2, boundaries3d.py:29."""
+    zz, yy, xx = np.meshgrid(np.arange(nz, dtype=np.float32), np.arange(ny, dtype=np.float32),
+                             np.arange(nx, dtype=np.float32), indexing="ij")
+    f32 = np.float32
+    d = (xx - f32(cx)) ** 2 + (yy - f32(cy)) ** 2 + (zz - f32(cz)) ** 2
+    return d <= f32(radius**2)
+
+
+def cylinder_mask(nx, ny, cx, cy, radius) -> np.ndarray:
+    """boundaries.py:8"""
+    yy, xx = np.meshgrid(np.arange(ny, dtype=np.float32), np.arange(nx, dtype=np.float32), indexing="ij")
+    f32 = np.float32
+    return (xx - f32(cx)) ** 2 + (yy - f32(cy)) ** 2 <= f32(radius**2)
+
+
+def missing_mask(q: int, shape, solid=None, periodic=(False, False, False)) -> np.ndarray:
+    """boundary_registry.py:488-575; shape (nz, ny, nx), periodic (z, y, x)."""
+    nz, ny, nx = shape
+    blocked = np.zeros(shape, dtype=bool) if solid is None else solid.astype(bool)
+    out = np.zeros((q,) + tuple(shape), dtype=bool)
+    zi, yi, xi = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    for i in range(q):
+        cx, cy, cz = (int(v) for v in C[q][i])
+        sz, sy, sx = zi - cz, yi - cy, xi - cx
+        oob = np.zeros(shape, dtype=bool)
+        for src, n, per in ((sz, nz, periodic[0]), (sy, ny, periodic[1]), (sx, nx, periodic[2])):
+            if per:
+                src %= n
+            else:
+                oob |= (src < 0) | (src >= n)
+                np.clip(src, 0, n - 1, out=src)
+        out[i] = oob | blocked[sz, sy, sx]
+    return out
+
+
+def cavity_walls_3d(n_z, n_y, n_x) -> np.ndarray:
+    """Five no-slip walls of benchmarks/verified/cavity_3d_full/run.py:85-89."""
+    wall = np.zeros((n_z, n_y, n_x), dtype=bool)
+    wall[:, :, 0] = True
+    wall[:, :, -1] = True
+    wall[:, 0, :] = True
+    wall[0, :, :] = True
+    wall[-1, :, :] = True
+    return wall
+
+
+# ---------------------------------------------------------------------------
+# time-step chains
+# ---------------------------------------------------------------------------
+
+
+def cavity_step(f: np.ndarray, tau: float, wall: np.ndarray, u_lid: float, collision="bgk", mode="fullway",
+                **kw) -> np.ndarray:
+    """mode "fullway": collide -> stream -> bounce-back on the walls -> Zou/He lid.
+    mode "halfway": collide -> where(wall, f_pre[opp], f) -> stream -> lid
+    (benchmarks/verified/cavity_3d_full/run.py:58, :95-104)."""
+    fc = COLLIDERS[collision](f, tau, **kw)
+    if mode == "halfway":
+        fc = np.where(wall[None], f[opposite(f.shape[0])], fc)
+    f = stream(fc)
+    if mode == "fullway":
+        f = bounce_back(f, wall)
+    return moving_lid(f, u_lid)
+
+
+def channel_step(f, tau, u_in, rho_out, wall, obstacle, collision="bgk", **kw):
+    """collide -> stream -> force -> Zou/He inlet -> outlet -> bounce-back(wall)
+    -> bounce-back(obstacle): d3q27_sphere_flow.py:246-256, cylinder_flow.py:854-899."""
+    f = COLLIDERS[collision](f, tau, **kw)
+    f = stream(f)
+    force = obstacle_force(f, obstacle) if obstacle is not None else None
+    if u_in is not None:
+        f = zou_he_inlet(f, u_in)
+    if rho_out is not None:
+        f = zou_he_outlet(f, rho_out)
+    if wall is not None:
+        f = bounce_back(f, wall)
+    if obstacle is not None:
+        f = bounce_back(f, obstacle)
+    return f, force

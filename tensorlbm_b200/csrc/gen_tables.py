@@ -1,0 +1,150 @@
+"""Generate the CUDA lattice headers from ``tensorlbm_b200.lattice``.
+
+Run ``python -m tensorlbm_b200.csrc.gen_tables`` after changing a velocity set
+or a moment basis; the build calls it too, so the headers under
+``csrc/generated/`` always match the Python tables.
+
+Two headers come out:
+
+* ``lattice_tables.cuh`` - one struct per lattice with Q, the velocity
+  components, opposite directions and weights as compile-time constants.
+* ``mrt_tables.cuh`` - the MRT collision written out as straight-line code:
+  the non-equilibrium moments ``d_k = sum_j M[k][j] * fneq_j`` of every
+  relaxed row and the back-projection ``f_i -= sum_k Minv[i][k] * s_k * d_k``.
+  Terms are grouped by coefficient so each multiply happens once per distinct
+  value; rows with a zero relaxation rate (mass, momentum) are skipped.
+"""
+
+from __future__ import annotations
+
+import pathlib
+from collections import defaultdict
+
+import numpy as np
+
+from tensorlbm_b200 import lattice as lat
+
+OUT = pathlib.Path(__file__).resolve().parent / "generated"
+
+
+def _lit(v: float) -> str:
+    """C double literal that round-trips exactly."""
+    r = repr(float(v))
+    if "e" not in r and "." not in r and "inf" not in r and "nan" not in r:
+        r += ".0"
+    return r
+
+
+def gen_lattice_tables() -> str:
+    lines = [
+        "// Generated by tensorlbm_b200/csrc/gen_tables.py - do not edit.",
+        "#pragma once",
+        "",
+    ]
+    for L in (lat.D2Q9, lat.D3Q19, lat.D3Q27):
+        cx = ", ".join(str(int(v)) for v in L.c[:, 0])
+        cy = ", ".join(str(int(v)) for v in L.c[:, 1])
+        cz = ", ".join(str(int(v)) for v in L.c[:, 2])
+        opp = ", ".join(str(int(v)) for v in L.opp)
+        w = ", ".join(_lit(float(v)) for v in L.w)
+        lines += [
+            f"struct {L.name} {{",
+            f"  static constexpr int Q = {L.q};",
+            f"  static constexpr int DIM = {L.dim};",
+            f"  __host__ __device__ static constexpr int cx(int q) {{ constexpr int t[{L.q}] = {{{cx}}}; return t[q]; }}",
+            f"  __host__ __device__ static constexpr int cy(int q) {{ constexpr int t[{L.q}] = {{{cy}}}; return t[q]; }}",
+            f"  __host__ __device__ static constexpr int cz(int q) {{ constexpr int t[{L.q}] = {{{cz}}}; return t[q]; }}",
+            f"  __host__ __device__ static constexpr int opp(int q) {{ constexpr int t[{L.q}] = {{{opp}}}; return t[q]; }}",
+            f"  __host__ __device__ static constexpr double w(int q) {{ constexpr double t[{L.q}] = {{{w}}}; return t[q]; }}",
+            "};",
+            "",
+        ]
+    return "\n".join(lines)
+
+
+# relaxation-rate symbol per MRT row (None = conserved, skipped)
+_RATES = {
+    9: [None, "s_e", "s_eps", None, "s_q", None, "s_q", "s_nu", "s_nu"],
+    19: [None, "s_e", "s_eps", None, "s_q", None, "s_q", None, "s_q",
+         "s_nu", "s_nu", "s_nu", "s_nu", "s_nu", "s_pi", "s_pi", "one", "one", "one"],
+    27: [None, None, None, None, "s_e", "s_nu", "s_nu", "s_nu", "s_nu", "s_nu"]
+    + ["s_q"] * 9 + ["s_eps"] + ["s_pi"] * 7,
+}
+
+
+def _grouped_sum(terms: list[tuple[float, str]]) -> str:
+    """sum c_j * x_j with equal coefficients factored: c*(x_a + x_b + ...)."""
+    groups: dict[float, list[str]] = defaultdict(list)
+    for c, x in terms:
+        if c != 0.0:
+            groups[c].append(x)
+    parts = []
+    for c in sorted(groups, key=lambda v: (abs(v), v)):
+        xs = groups[c]
+        s = xs[0] if len(xs) == 1 else "(" + " + ".join(xs) + ")"
+        if c == 1.0:
+            parts.append(s)
+        elif c == -1.0:
+            parts.append(f"-{s}")
+        else:
+            parts.append(f"T({_lit(c)}) * {s}")
+    if not parts:
+        return "T(0)"
+    expr = parts[0]
+    for p in parts[1:]:
+        expr += f" - {p[1:]}" if p.startswith("-") else f" + {p}"
+    return expr
+
+
+def gen_mrt(q: int) -> str:
+    m, minv = lat.mrt_matrices(q)
+    rates = _RATES[q]
+    name = {9: "d2q9", 19: "d3q19", 27: "d3q27"}[q]
+    out = [
+        f"// MRT relaxation for {name}: f_i -= sum_k Minv[i][k] * s_k * (M (f - feq))_k",
+        "template <typename T>",
+        f"__device__ __forceinline__ void mrt_relax_{name}(T (&f)[{q}], const T (&fn)[{q}], const MrtRates<T>& r) {{",
+        "  const T one = T(1);",
+    ]
+    relaxed = [k for k in range(q) if rates[k] is not None]
+    for k in relaxed:
+        # the Gram-Schmidt D3Q27 rows carry round-off of the same kind
+        terms = [(float(m[k, j]), f"fn[{j}]") for j in range(q) if abs(m[k, j]) > 1e-10]
+        rate = "one" if rates[k] == "one" else f"r.{rates[k]}"
+        out.append(f"  const T e{k} = {rate} * ({_grouped_sum(terms)});")
+    for i in range(q):
+        # entries below 1e-10 are round-off of the float64 inverse (the exact
+        # inverse has a zero there); dropping them changes results far below
+        # float32 resolution and saves an FMA each
+        terms = [(float(minv[i, k]), f"e{k}") for k in relaxed if abs(minv[i, k]) > 1e-10]
+        out.append(f"  f[{i}] -= {_grouped_sum(terms)};")
+    out.append("}")
+    out.append("")
+    return "\n".join(out)
+
+
+def gen_mrt_header() -> str:
+    parts = [
+        "// Generated by tensorlbm_b200/csrc/gen_tables.py - do not edit.",
+        "#pragma once",
+        "",
+        "template <typename T> struct MrtRates {",
+        "  T s_e, s_eps, s_q, s_nu, s_pi;",
+        "};",
+        "",
+    ]
+    for q in (9, 19, 27):
+        parts.append(gen_mrt(q))
+    return "\n".join(parts)
+
+
+def main() -> None:
+    OUT.mkdir(parents=True, exist_ok=True)
+    for name, text in (("lattice_tables.cuh", gen_lattice_tables()), ("mrt_tables.cuh", gen_mrt_header())):
+        path = OUT / name
+        if not path.exists() or path.read_text() != text:
+            path.write_text(text)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,556 @@
+// Per-cell collision operators on populations held in registers.
+//
+// Every function here takes the Q populations of ONE cell in a register array
+// and overwrites them with the post-collision populations.  Loops over q are
+// fully unrolled, so q (and every lattice constant looked up with it) is a
+// compile-time constant: terms with a zero velocity component are never
+// emitted, and no work depends on data layout.
+#pragma once
+
+#include "tlbm_common.cuh"
+
+namespace tlbm {
+
+template <typename T> struct CollideParams {
+  T tau, inv_tau;
+  MrtRates<T> mrt;          // s_nu = 1/tau unless a tau field overrides it per cell
+  T omega_b, omega_odd, omega_even;
+  T c_smag;
+  T smag_coef;              // 18 * C_s^2
+  T tau_sq;                 // tau^2
+  T tau_eff_max;            // max(1, tau + 0.5), turbulence.py:88-99
+};
+
+// sum of +-x, +-y, +-z terms for compile-time components a, b, c in {-1, 0, 1}
+template <typename T>
+__device__ __forceinline__ T signed_sum(int a, int b, int c, T x, T y, T z) {
+  T r = T(0);
+  bool any = false;
+  if (a != 0) { r = (a > 0) ? x : -x; any = true; }
+  if (b != 0) { r = any ? ((b > 0) ? r + y : r - y) : ((b > 0) ? y : -y); any = true; }
+  if (c != 0) { r = any ? ((c > 0) ? r + z : r - z) : ((c > 0) ? z : -z); any = true; }
+  return r;
+}
+
+// rho = sum f, u = sum c f / max(rho, 1e-12): d2q9.py:61-74, d3q19.py:165-186,
+// d3q27.py:395-420.  Sums run in direction order like torch's dim-0 sum.
+template <class L, typename T>
+__device__ __forceinline__ void macroscopic(const T (&f)[L::Q], T& rho, T& ux, T& uy, T& uz) {
+  rho = f[0];
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) rho += f[q];
+  T jx = T(0), jy = T(0), jz = T(0);
+  bool bx = false, by = false, bz = false;
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) {
+    if (L::cx(q) != 0) { jx = bx ? (L::cx(q) > 0 ? jx + f[q] : jx - f[q]) : (L::cx(q) > 0 ? f[q] : -f[q]); bx = true; }
+    if (L::cy(q) != 0) { jy = by ? (L::cy(q) > 0 ? jy + f[q] : jy - f[q]) : (L::cy(q) > 0 ? f[q] : -f[q]); by = true; }
+    if (L::cz(q) != 0) { jz = bz ? (L::cz(q) > 0 ? jz + f[q] : jz - f[q]) : (L::cz(q) > 0 ? f[q] : -f[q]); bz = true; }
+  }
+  const T rs = rho > T(1e-12) ? rho : T(1e-12);
+  const T ir = T(1) / rs;
+  ux = jx * ir;
+  uy = jy * ir;
+  uz = (L::DIM == 3) ? jz * ir : T(0);
+}
+
+// f_eq = w rho (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u.u): d2q9.py:39-58,
+// d3q19.py:83-125, d3q27.py:353-392.
+template <class L, typename T>
+__device__ __forceinline__ T usq_of(T ux, T uy, T uz) {
+  return (L::DIM == 3) ? ux * ux + uy * uy + uz * uz : ux * ux + uy * uy;
+}
+
+template <class L, typename T>
+__device__ __forceinline__ T feq_q(int q, T rho, T ux, T uy, T uz, T usq) {
+  const T wr = weight<L, T>(q) * rho;
+  if (L::cx(q) == 0 && L::cy(q) == 0 && L::cz(q) == 0) return wr * (T(1) - T(1.5) * usq);
+  const T cu = signed_sum(L::cx(q), L::cy(q), L::cz(q), ux, uy, uz);
+  return wr * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+}
+
+template <class L, typename T>
+__device__ __forceinline__ void equilibrium(T rho, T ux, T uy, T uz, T (&fe)[L::Q]) {
+  const T usq = usq_of<L>(ux, uy, uz);
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
+}
+
+// ---------------------------------------------------------------------------
+// BGK: f - (f - feq)/tau (solver.py:67-71, solver3d.py:100-104, d3q27.py:423-437)
+// ---------------------------------------------------------------------------
+template <class L, typename T>
+__device__ __forceinline__ void collide_bgk(T (&f)[L::Q], T inv_tau) {
+  T rho, ux, uy, uz;
+  macroscopic<L>(f, rho, ux, uy, uz);
+  const T usq = usq_of<L>(ux, uy, uz);
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    const T fe = feq_q<L>(q, rho, ux, uy, uz, usq);
+    f[q] = f[q] - (f[q] - fe) * inv_tau;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MRT: m* = m - S (m - m_eq), f = M^-1 m*  (solver.py:249-331, solver3d.py:107-160,
+// d3q27.py:643-727), written as f -= M^-1 S M (f - feq) over the relaxed rows.
+// ---------------------------------------------------------------------------
+template <class L, typename T>
+__device__ __forceinline__ void collide_mrt(T (&f)[L::Q], const MrtRates<T>& r) {
+  T rho, ux, uy, uz;
+  macroscopic<L>(f, rho, ux, uy, uz);
+  const T usq = usq_of<L>(ux, uy, uz);
+  T fn[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) fn[q] = f[q] - feq_q<L>(q, rho, ux, uy, uz, usq);
+  if constexpr (L::Q == 9) mrt_relax_d2q9<T>(f, fn, r);
+  else if constexpr (L::Q == 19) mrt_relax_d3q19<T>(f, fn, r);
+  else mrt_relax_d3q27<T>(f, fn, r);
+}
+
+// ---------------------------------------------------------------------------
+// Second moment of the non-equilibrium part, Pi_ab = sum c_a c_b fneq
+// ---------------------------------------------------------------------------
+template <typename T> struct Pi6 { T xx, yy, zz, xy, xz, yz; };
+
+template <class L, typename T>
+__device__ __forceinline__ Pi6<T> neq_stress(const T (&fn)[L::Q]) {
+  Pi6<T> p{T(0), T(0), T(0), T(0), T(0), T(0)};
+  bool bxx = false, byy = false, bzz = false, bxy = false, bxz = false, byz = false;
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    const int a = L::cx(q), b = L::cy(q), c = L::cz(q);
+    if (a != 0) { p.xx = bxx ? p.xx + fn[q] : fn[q]; bxx = true; }
+    if (b != 0) { p.yy = byy ? p.yy + fn[q] : fn[q]; byy = true; }
+    if (c != 0) { p.zz = bzz ? p.zz + fn[q] : fn[q]; bzz = true; }
+    if (a * b != 0) { p.xy = bxy ? (a * b > 0 ? p.xy + fn[q] : p.xy - fn[q]) : (a * b > 0 ? fn[q] : -fn[q]); bxy = true; }
+    if (a * c != 0) { p.xz = bxz ? (a * c > 0 ? p.xz + fn[q] : p.xz - fn[q]) : (a * c > 0 ? fn[q] : -fn[q]); bxz = true; }
+    if (b * c != 0) { p.yz = byz ? (b * c > 0 ? p.yz + fn[q] : p.yz - fn[q]) : (b * c > 0 ? fn[q] : -fn[q]); byz = true; }
+  }
+  return p;
+}
+
+// Hou-1994 tau_eff with the clamps of turbulence.py:183-208 (norm clamp of
+// :128-140 / :170-181).
+template <class L, typename T>
+__device__ __forceinline__ T smagorinsky_tau(const Pi6<T>& p, T rho, const CollideParams<T>& cp) {
+  T rad = (L::DIM == 3)
+              ? p.xx * p.xx + p.yy * p.yy + p.zz * p.zz + T(2) * (p.xy * p.xy + p.xz * p.xz + p.yz * p.yz)
+              : p.xx * p.xx + p.yy * p.yy + T(2) * p.xy * p.xy;
+  rad = rad > T(1e-30) ? rad : T(1e-30);
+  const T pi_norm = sqrt(rad);
+  const T rs = rho > T(1e-12) ? rho : T(1e-12);
+  T disc = cp.tau_sq + cp.smag_coef * pi_norm / rs;
+  disc = disc > T(0) ? disc : T(0);
+  T te = T(0.5) * (cp.tau + sqrt(disc));
+  te = te < T(0.5001) ? T(0.5001) : te;
+  te = te > cp.tau_eff_max ? cp.tau_eff_max : te;
+  return te;
+}
+
+// BGK with per-cell Smagorinsky tau_eff: turbulence.py:216-230 (D2Q9),
+// :245-261 (D3Q19), :472 (D3Q27).
+template <class L, typename T>
+__device__ __forceinline__ void collide_smagorinsky(T (&f)[L::Q], const CollideParams<T>& cp) {
+  T rho, ux, uy, uz;
+  macroscopic<L>(f, rho, ux, uy, uz);
+  const T usq = usq_of<L>(ux, uy, uz);
+  T fn[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) fn[q] = f[q] - feq_q<L>(q, rho, ux, uy, uz, usq);
+  const Pi6<T> p = neq_stress<L>(fn);
+  const T inv_te = T(1) / smagorinsky_tau<L>(p, rho, cp);
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) f[q] = f[q] - fn[q] * inv_te;
+}
+
+// ---------------------------------------------------------------------------
+// D3Q19 "cumulant": Hermite-regularised relaxation of the stress with a
+// separate bulk rate and a damped higher-order remainder (cumulant.py:1159-1420).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void collide_cumulant_d3q19(T (&f)[19], const CollideParams<T>& cp) {
+  using L = D3Q19;
+  T rho, ux, uy, uz;
+  macroscopic<L>(f, rho, ux, uy, uz);
+  const T usq = usq_of<L>(ux, uy, uz);
+  T fe[19], fn[19];
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
+    fn[q] = f[q] - fe[q];
+  }
+  const Pi6<T> p = neq_stress<L>(fn);
+  T omega = cp.inv_tau;
+  if (cp.c_smag > T(0)) {
+    // cumulant.py:1349-1353: no norm or tau clamps on this path
+    const T pn = sqrt(p.xx * p.xx + p.yy * p.yy + p.zz * p.zz + T(2) * (p.xy * p.xy + p.xz * p.xz + p.yz * p.yz));
+    const T rs = rho > T(1e-12) ? rho : T(1e-12);
+    const T te = T(0.5) * (cp.tau + sqrt(cp.tau * cp.tau + cp.smag_coef * pn / rs));
+    omega = T(1) / te;
+  }
+  const T tr = p.xx + p.yy + p.zz;
+  const T bulk = (cp.omega_b - omega) * tr / T(3);
+  const Pi6<T> s{p.xx - omega * p.xx - bulk, p.yy - omega * p.yy - bulk, p.zz - omega * p.zz - bulk,
+                 p.xy - omega * p.xy, p.xz - omega * p.xz, p.yz - omega * p.yz};
+  const T cs2 = T(1) / T(3);
+  const T keep = T(1) - cp.omega_even;
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    const int a = L::cx(q), b = L::cy(q), c = L::cz(q);
+    const T hxx = T(a * a) - cs2, hyy = T(b * b) - cs2, hzz = T(c * c) - cs2;
+    const T w45 = T(4.5) * weight<L, T>(q);
+    T hs = hxx * s.xx + hyy * s.yy + hzz * s.zz;
+    T hp = hxx * p.xx + hyy * p.yy + hzz * p.zz;
+    if (a * b != 0) { hs += T(2 * a * b) * s.xy; hp += T(2 * a * b) * p.xy; }
+    if (a * c != 0) { hs += T(2 * a * c) * s.xz; hp += T(2 * a * c) * p.xz; }
+    if (b * c != 0) { hs += T(2 * b * c) * s.yz; hp += T(2 * b * c) * p.yz; }
+    const T reg = w45 * hs;
+    const T ho = fn[q] - w45 * hp;
+    f[q] = fe[q] + reg + keep * ho;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// D3Q27 cumulant operators.  Moments live in a 3x3x3 array g[a][b][c] indexed
+// by the exponents of cx^a cy^b cz^c; because D3Q27 is the full tensor
+// product {-1,0,1}^3, the raw-moment transform M (cumulant.py:904-919) factors
+// into three 1-D transforms, and the central shift (cumulant.py:390-457) is
+// the 1-D binomial shift along each axis.
+// ---------------------------------------------------------------------------
+template <typename T> using Cube = T[3][3][3];
+
+// populations -> g[ix][iy][iz] with i = c + 1
+template <typename T>
+__device__ __forceinline__ void to_cube(const T (&f)[27], Cube<T>& g) {
+#pragma unroll
+  for (int q = 0; q < 27; ++q) g[D3Q27::cx(q) + 1][D3Q27::cy(q) + 1][D3Q27::cz(q) + 1] = f[q];
+}
+template <typename T>
+__device__ __forceinline__ void from_cube(const Cube<T>& g, T (&f)[27]) {
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = g[D3Q27::cx(q) + 1][D3Q27::cy(q) + 1][D3Q27::cz(q) + 1];
+}
+
+// element accessor along an axis: axis 0 -> g[i][j][k], 1 -> g[j][i][k], 2 -> g[j][k][i]
+template <int AX, typename T>
+__device__ __forceinline__ T& at(Cube<T>& g, int i, int j, int k) {
+  if constexpr (AX == 0) return g[i][j][k];
+  else if constexpr (AX == 1) return g[j][i][k];
+  else return g[j][k][i];
+}
+
+// values at c = -1, 0, +1 -> moments of degree 0, 1, 2 along AX
+template <int AX, typename T>
+__device__ __forceinline__ void raw_1d(Cube<T>& g) {
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T vm = at<AX>(g, 0, j, k), v0 = at<AX>(g, 1, j, k), vp = at<AX>(g, 2, j, k);
+      at<AX>(g, 0, j, k) = vm + v0 + vp;
+      at<AX>(g, 1, j, k) = vp - vm;
+      at<AX>(g, 2, j, k) = vp + vm;
+    }
+}
+template <int AX, typename T>
+__device__ __forceinline__ void pop_1d(Cube<T>& g) {
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T m0 = at<AX>(g, 0, j, k), m1 = at<AX>(g, 1, j, k), m2 = at<AX>(g, 2, j, k);
+      at<AX>(g, 0, j, k) = (m2 - m1) * T(0.5);
+      at<AX>(g, 1, j, k) = m0 - m2;
+      at<AX>(g, 2, j, k) = (m1 + m2) * T(0.5);
+    }
+}
+// forward binomial shift (cumulant.py:390-412) and its inverse (:415-434)
+template <int AX, typename T>
+__device__ __forceinline__ void shift_1d(Cube<T>& g, T u) {
+  const T tu = T(2) * u, uu = u * u;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T m0 = at<AX>(g, 0, j, k), m1 = at<AX>(g, 1, j, k), m2 = at<AX>(g, 2, j, k);
+      at<AX>(g, 1, j, k) = m1 - u * m0;
+      at<AX>(g, 2, j, k) = m2 - tu * m1 + uu * m0;
+    }
+}
+template <int AX, typename T>
+__device__ __forceinline__ void unshift_1d(Cube<T>& g, T u) {
+  const T tu = T(2) * u, uu = u * u;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T m0 = at<AX>(g, 0, j, k), m1 = at<AX>(g, 1, j, k), m2 = at<AX>(g, 2, j, k);
+      at<AX>(g, 1, j, k) = m1 + u * m0;
+      at<AX>(g, 2, j, k) = m2 + tu * m1 + uu * m0;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void central_moments(const T (&f)[27], T ux, T uy, T uz, Cube<T>& g) {
+  to_cube(f, g);
+  raw_1d<0>(g);
+  raw_1d<1>(g);
+  raw_1d<2>(g);
+  shift_1d<0>(g, ux);
+  shift_1d<1>(g, uy);
+  shift_1d<2>(g, uz);
+}
+template <typename T>
+__device__ __forceinline__ void populations(Cube<T>& g, T ux, T uy, T uz, T (&f)[27]) {
+  unshift_1d<2>(g, uz);
+  unshift_1d<1>(g, uy);
+  unshift_1d<0>(g, ux);
+  pop_1d<0>(g);
+  pop_1d<1>(g);
+  pop_1d<2>(g);
+  from_cube(g, f);
+}
+
+// moment index k (cumulant.py:321-349 ordering) <-> cube exponents
+__host__ __device__ constexpr int kdeg(int k, int axis) {
+  constexpr int t[27][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {0, 2, 0}, {0, 0, 2},
+                            {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {2, 1, 0}, {2, 0, 1}, {1, 2, 0}, {0, 2, 1},
+                            {1, 0, 2}, {0, 1, 2}, {1, 1, 1}, {2, 2, 0}, {2, 0, 2}, {0, 2, 2}, {2, 1, 1},
+                            {1, 2, 1}, {1, 1, 2}, {2, 2, 1}, {2, 1, 2}, {1, 2, 2}, {2, 2, 2}};
+  return t[k][axis];
+}
+template <typename T>
+__device__ __forceinline__ void cube_to_k(const Cube<T>& g, T (&k)[27]) {
+#pragma unroll
+  for (int i = 0; i < 27; ++i) k[i] = g[kdeg(i, 0)][kdeg(i, 1)][kdeg(i, 2)];
+}
+template <typename T>
+__device__ __forceinline__ void k_to_cube(const T (&k)[27], Cube<T>& g) {
+#pragma unroll
+  for (int i = 0; i < 27; ++i) g[kdeg(i, 0)][kdeg(i, 1)][kdeg(i, 2)] = k[i];
+}
+
+// Legacy pseudo-cumulant transform on central moments of f_neq
+// (cumulant.py:470-577), in place.
+template <typename T>
+__device__ __forceinline__ void legacy_forward(T (&c)[27]) {
+  const T k200 = c[4], k020 = c[5], k002 = c[6], k110 = c[7], k101 = c[8], k011 = c[9];
+  c[17] = c[17] - k200 * k020 - T(2) * k110 * k110;
+  c[18] = c[18] - k200 * k002 - T(2) * k101 * k101;
+  c[19] = c[19] - k020 * k002 - T(2) * k011 * k011;
+  c[20] = c[20] - k200 * k011 - T(2) * k101 * k110;
+  c[21] = c[21] - k020 * k101 - T(2) * k110 * k011;
+  c[22] = c[22] - k002 * k110 - T(2) * k101 * k011;
+  c[23] = c[23] - k200 * c[13] - T(2) * k110 * c[16];
+  c[24] = c[24] - k200 * c[15] - T(2) * k101 * c[16];
+  c[25] = c[25] - k020 * c[14] - T(2) * k011 * c[16];
+  c[26] = c[26] - k200 * c[19] - k020 * c[18] - k002 * c[17] -
+          T(2) * (k110 * c[22] + k101 * c[21] + k011 * c[20]) + T(2) * k200 * k020 * k002 +
+          T(4) * k110 * k101 * k011 + T(2) * k110 * k110 * k002 + T(2) * k101 * k101 * k020 +
+          T(2) * k011 * k011 * k200;
+}
+// inverse (cumulant.py:580-651), in place
+template <typename T>
+__device__ __forceinline__ void legacy_inverse(T (&c)[27]) {
+  const T c200 = c[4], c020 = c[5], c002 = c[6], c110 = c[7], c101 = c[8], c011 = c[9];
+  const T c220 = c[17], c202 = c[18], c022 = c[19], c211 = c[20], c121 = c[21], c112 = c[22];
+  c[17] = c220 + c200 * c020 + T(2) * c110 * c110;
+  c[18] = c202 + c200 * c002 + T(2) * c101 * c101;
+  c[19] = c022 + c020 * c002 + T(2) * c011 * c011;
+  c[20] = c211 + c200 * c011 + T(2) * c101 * c110;
+  c[21] = c121 + c020 * c101 + T(2) * c110 * c011;
+  c[22] = c112 + c002 * c110 + T(2) * c101 * c011;
+  c[23] = c[23] + c200 * c[13] + T(2) * c110 * c[16];
+  c[24] = c[24] + c200 * c[15] + T(2) * c101 * c[16];
+  c[25] = c[25] + c020 * c[14] + T(2) * c011 * c[16];
+  c[26] = c[26] + c200 * c022 + c020 * c202 + c002 * c220 + T(2) * (c110 * c112 + c101 * c121 + c011 * c211) -
+          T(2) * c200 * c020 * c002 - T(4) * c110 * c101 * c011 - T(2) * c110 * c110 * c002 -
+          T(2) * c101 * c101 * c020 - T(2) * c011 * c011 * c200;
+}
+
+// D3Q27 legacy cumulant collision (cumulant.py:935-1047)
+template <typename T>
+__device__ __forceinline__ void collide_cumulant_legacy(T (&f)[27], const CollideParams<T>& cp) {
+  using L = D3Q27;
+  T rho, ux, uy, uz;
+  macroscopic<L>(f, rho, ux, uy, uz);
+  const T usq = usq_of<L>(ux, uy, uz);
+  T fe[27], fn[27];
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
+    fn[q] = f[q] - fe[q];
+  }
+  Cube<T> g;
+  central_moments(fn, ux, uy, uz, g);
+  T c[27];
+  cube_to_k(g, c);
+  legacy_forward(c);
+  // relaxation (cumulant.py:654-740): trace / deviatoric split at 2nd order
+  const T om = cp.inv_tau;
+  const T tr = c[4] + c[5] + c[6];
+  const T dxx = c[4] - tr / T(3), dyy = c[5] - tr / T(3), dzz = c[6] - tr / T(3);
+  const T trs = (T(1) - cp.omega_b) * tr;
+  const T ks = T(1) - om;
+  c[4] = ks * dxx + trs / T(3);
+  c[5] = ks * dyy + trs / T(3);
+  c[6] = ks * dzz + trs / T(3);
+  c[7] = ks * c[7];
+  c[8] = ks * c[8];
+  c[9] = ks * c[9];
+  const T k3 = T(1) - cp.omega_odd, k4 = T(1) - cp.omega_even;
+#pragma unroll
+  for (int i = 10; i < 17; ++i) c[i] = k3 * c[i];
+#pragma unroll
+  for (int i = 17; i < 27; ++i) c[i] = k4 * c[i];
+  legacy_inverse(c);
+  k_to_cube(c, g);
+  T fns[27];
+  populations(g, ux, uy, uz, fns);
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = fe[q] + fns[q];
+}
+
+// Geier-2015 cumulants of the full distribution (cumulant.py:674-815), using
+// normalised central moments kt = k / rho.  Input/outputs in k ordering.
+template <typename T>
+__device__ __forceinline__ void geier_forward(T (&k)[27]) {
+  const T rho = k[0];
+  const T ir = T(1) / rho;
+  T t[27];
+#pragma unroll
+  for (int i = 0; i < 27; ++i) t[i] = k[i] * ir;
+  T c[27];
+#pragma unroll
+  for (int i = 0; i < 27; ++i) c[i] = t[i];
+  c[17] = t[17] - (t[5] * t[4] + T(2) * t[7] * t[7]);
+  c[18] = t[18] - (t[6] * t[4] + T(2) * t[8] * t[8]);
+  c[19] = t[19] - (t[6] * t[5] + T(2) * t[9] * t[9]);
+  c[20] = t[20] - (t[9] * t[4] + T(2) * t[8] * t[7]);
+  c[21] = t[21] - (T(2) * t[9] * t[7] + t[5] * t[8]);
+  c[22] = t[22] - (t[6] * t[7] + T(2) * t[9] * t[8]);
+  c[23] = t[23] - (T(2) * t[9] * t[10] + t[5] * t[11] + t[13] * t[4] + T(2) * t[8] * t[12] + T(4) * t[7] * t[16]);
+  c[24] = t[24] - (t[6] * t[10] + T(2) * t[9] * t[11] + t[15] * t[4] + T(4) * t[8] * t[16] + T(2) * t[14] * t[7]);
+  c[25] = t[25] - (t[6] * t[12] + T(4) * t[9] * t[16] + T(2) * t[15] * t[7] + t[5] * t[14] + T(2) * t[13] * t[8]);
+  c[26] = t[26] - (-T(2) * t[6] * t[5] * t[4] - T(4) * t[6] * t[7] * t[7] + t[6] * t[17] -
+                   T(4) * t[9] * t[9] * t[4] - T(16) * t[9] * t[8] * t[7] + T(4) * t[9] * t[20] +
+                   T(2) * t[15] * t[10] - T(4) * t[5] * t[8] * t[8] + t[5] * t[18] + T(2) * t[13] * t[11] +
+                   t[19] * t[4] + T(4) * t[8] * t[21] + T(2) * t[14] * t[12] + T(4) * t[7] * t[22] +
+                   T(4) * t[16] * t[16]);
+#pragma unroll
+  for (int i = 1; i < 27; ++i) k[i] = c[i] * rho;
+  k[0] = rho;
+}
+template <typename T>
+__device__ __forceinline__ void geier_inverse(T (&c)[27]) {
+  const T rho = c[0];
+  const T ir = T(1) / rho;
+  T t[27];
+#pragma unroll
+  for (int i = 0; i < 27; ++i) t[i] = c[i] * ir;
+  T k[27];
+#pragma unroll
+  for (int i = 0; i < 27; ++i) k[i] = t[i];
+  k[17] = t[5] * t[4] + T(2) * t[7] * t[7] + t[17];
+  k[18] = t[6] * t[4] + T(2) * t[8] * t[8] + t[18];
+  k[19] = t[6] * t[5] + T(2) * t[9] * t[9] + t[19];
+  k[20] = t[9] * t[4] + T(2) * t[8] * t[7] + t[20];
+  k[21] = T(2) * t[9] * t[7] + t[5] * t[8] + t[21];
+  k[22] = t[6] * t[7] + T(2) * t[9] * t[8] + t[22];
+  k[23] = T(2) * t[9] * t[10] + t[5] * t[11] + t[13] * t[4] + T(2) * t[8] * t[12] + T(4) * t[7] * t[16] + t[23];
+  k[24] = t[6] * t[10] + T(2) * t[9] * t[11] + t[15] * t[4] + T(4) * t[8] * t[16] + T(2) * t[14] * t[7] + t[24];
+  k[25] = t[6] * t[12] + T(4) * t[9] * t[16] + T(2) * t[15] * t[7] + t[5] * t[14] + T(2) * t[13] * t[8] + t[25];
+  k[26] = t[6] * t[5] * t[4] + T(2) * t[6] * t[7] * t[7] + t[6] * t[17] + T(2) * t[9] * t[9] * t[4] +
+          T(8) * t[9] * t[8] * t[7] + T(4) * t[9] * t[20] + T(2) * t[15] * t[10] + T(2) * t[5] * t[8] * t[8] +
+          t[5] * t[18] + T(2) * t[13] * t[11] + t[19] * t[4] + T(4) * t[8] * t[21] + T(2) * t[14] * t[12] +
+          T(4) * t[7] * t[22] + T(4) * t[16] * t[16] + t[26];
+#pragma unroll
+  for (int i = 1; i < 27; ++i) c[i] = k[i] * rho;
+  c[0] = rho;
+}
+
+// D3Q27 Geier cumulant collision (cumulant.py:1050-1156)
+template <typename T>
+__device__ __forceinline__ void collide_cumulant_geier(T (&f)[27], const CollideParams<T>& cp) {
+  using L = D3Q27;
+  T rho, ux, uy, uz;
+  macroscopic<L>(f, rho, ux, uy, uz);
+  const T usq = usq_of<L>(ux, uy, uz);
+  T fe[27];
+#pragma unroll
+  for (int q = 0; q < 27; ++q) fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
+  Cube<T> g;
+  T c[27], ce[27];
+  central_moments(fe, ux, uy, uz, g);
+  cube_to_k(g, ce);
+  geier_forward(ce);
+  central_moments(f, ux, uy, uz, g);
+  cube_to_k(g, c);
+  geier_forward(c);
+  const T om = cp.inv_tau;
+  const T dxx = c[4] - ce[4], dyy = c[5] - ce[5], dzz = c[6] - ce[6];
+  const T tr = dxx + dyy + dzz;
+  const T tr3 = tr / T(3);
+  c[4] = c[4] - (om * (dxx - tr3) + cp.omega_b * tr3);
+  c[5] = c[5] - (om * (dyy - tr3) + cp.omega_b * tr3);
+  c[6] = c[6] - (om * (dzz - tr3) + cp.omega_b * tr3);
+  c[7] = c[7] - om * (c[7] - ce[7]);
+  c[8] = c[8] - om * (c[8] - ce[8]);
+  c[9] = c[9] - om * (c[9] - ce[9]);
+#pragma unroll
+  for (int i = 10; i < 17; ++i) c[i] = c[i] - cp.omega_odd * (c[i] - ce[i]);
+#pragma unroll
+  for (int i = 17; i < 27; ++i) c[i] = c[i] - cp.omega_even * (c[i] - ce[i]);
+  geier_inverse(c);
+  k_to_cube(c, g);
+  populations(g, ux, uy, uz, f);
+}
+
+// ---------------------------------------------------------------------------
+// dispatch
+// ---------------------------------------------------------------------------
+template <class L, int COLL, typename T>
+__device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp, T tau_cell, bool has_tau_cell) {
+  if constexpr (COLL == TLBM_COLL_BGK) {
+    collide_bgk<L>(f, has_tau_cell ? T(1) / tau_cell : cp.inv_tau);
+  } else if constexpr (COLL == TLBM_COLL_MRT) {
+    MrtRates<T> r = cp.mrt;
+    if (has_tau_cell) r.s_nu = T(1) / tau_cell;
+    collide_mrt<L>(f, r);
+  } else if constexpr (COLL == TLBM_COLL_SMAGORINSKY) {
+    collide_smagorinsky<L>(f, cp);
+  } else if constexpr (COLL == TLBM_COLL_CUMULANT_D3Q19) {
+    static_assert(L::Q == 19, "D3Q19 only");
+    collide_cumulant_d3q19(f, cp);
+  } else if constexpr (COLL == TLBM_COLL_CUMULANT) {
+    static_assert(L::Q == 27, "D3Q27 only");
+    collide_cumulant_legacy(f, cp);
+  } else if constexpr (COLL == TLBM_COLL_CUMULANT_GEIER) {
+    static_assert(L::Q == 27, "D3Q27 only");
+    collide_cumulant_geier(f, cp);
+  }
+}
+
+template <typename T>
+CollideParams<T> make_collide_params(double tau, double s_e, double s_eps, double s_q, double s_pi,
+                                     double omega_b, double omega_odd, double omega_even, double c_smag) {
+  CollideParams<T> cp;
+  cp.tau = T(tau);
+  cp.inv_tau = T(1.0 / tau);
+  cp.mrt.s_e = T(s_e);
+  cp.mrt.s_eps = T(s_eps);
+  cp.mrt.s_q = T(s_q);
+  cp.mrt.s_pi = T(s_pi < 0 ? s_e : s_pi);
+  cp.mrt.s_nu = T(1.0 / tau);
+  cp.omega_b = T(omega_b);
+  cp.omega_odd = T(omega_odd);
+  cp.omega_even = T(omega_even);
+  cp.c_smag = T(c_smag);
+  cp.smag_coef = T(18.0 * c_smag * c_smag);
+  cp.tau_sq = T(tau * tau);
+  cp.tau_eff_max = T(tau + 0.5 > 1.0 ? tau + 0.5 : 1.0);
+  return cp;
+}
+
+}  // namespace tlbm

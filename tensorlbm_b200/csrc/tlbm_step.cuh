@@ -1,0 +1,139 @@
+// The fused time-step kernel: pull -> boundary conditions -> collision -> store.
+//
+// One thread owns one cell.  It gathers the Q populations that stream into
+// its cell (f_in[q, x - c_q], periodic wrap on every axis exactly like
+// torch.roll / the cached index gather of stream3d), applies the boundary
+// conditions in TensorLBM's order, collides, and writes the Q results at its
+// own cell.  Every population of f_in is read by exactly one thread, so the
+// kernel moves 2*Q*sizeof(S) bytes per cell and nothing else except the flag
+// byte.  Warps span consecutive x, so each direction is one coalesced
+// 128-byte row access (shifted by one element for c_x = +-1).
+#pragma once
+
+#include "tlbm_bc.cuh"
+
+namespace tlbm {
+
+// Warp-reduce one cell's momentum in float64 and add 2x it to force[0..2].
+// Blocks are at least 32 wide in x, so a warp is 32 consecutive x of one row.
+template <typename T>
+__device__ __forceinline__ void accumulate_force(double* force, bool any_in_warp, T mx, T my, T mz) {
+  if (!any_in_warp) return;
+  const double sx = warp_sum(double(mx)), sy = warp_sum(double(my)), sz = warp_sum(double(mz));
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(force + 0, 2.0 * sx);
+    atomicAdd(force + 1, 2.0 * sy);
+    atomicAdd(force + 2, 2.0 * sz);
+  }
+}
+
+// PULL = true : gather from neighbours, boundaries, collide (COLL may be NONE)
+// PULL = false: local collide / format conversion only (no boundaries)
+template <class L, typename SI, typename SO, int COLL, bool PULL>
+__global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typename Storage<SI>::T> cp,
+                                              BcParams<typename Storage<SI>::T> bp) {
+  using T = typename Storage<SI>::T;
+  constexpr int Q = L::Q;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool active = (x < p.nx) && (y < p.ny);
+  const long long N = p.n;
+  const long long cell = (long long)z * p.plane + (long long)y * p.nx + x;
+  const SI* __restrict__ fin = static_cast<const SI*>(p.f_in);
+  SO* __restrict__ fout = static_cast<SO*>(p.f_out);
+
+  T f[Q];
+  uint8_t fl = 0;
+  if (active) {
+    if constexpr (PULL) {
+      const int xm = (x == 0) ? p.nx - 1 : x - 1;
+      const int xp = (x == p.nx - 1) ? 0 : x + 1;
+      const int ym = (y == 0) ? p.ny - 1 : y - 1;
+      const int yp = (y == p.ny - 1) ? 0 : y + 1;
+      const int zm = (z == 0) ? p.nz - 1 : z - 1;
+      const int zp = (z == p.nz - 1) ? 0 : z + 1;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        // source = cell - c_q
+        const int sx = L::cx(q) > 0 ? xm : (L::cx(q) < 0 ? xp : x);
+        const int sy = L::cy(q) > 0 ? ym : (L::cy(q) < 0 ? yp : y);
+        const int sz = L::cz(q) > 0 ? zm : (L::cz(q) < 0 ? zp : z);
+        const long long src = (long long)sz * p.plane + (long long)sy * p.nx + sx;
+        f[q] = Storage<SI>::load(__ldg(fin + (long long)q * N + src), weight<L, T>(q));
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) f[q] = Storage<SI>::load(fin[(long long)q * N + cell], weight<L, T>(q));
+    }
+    if (p.flags) fl = p.flags[cell];
+  }
+
+  if constexpr (PULL) {
+    // 1. momentum-exchange force sample (post-stream, pre-bounce-back)
+    if (p.force) {
+      const bool ob = active && (fl & TLBM_FLAG_OBSTACLE);
+      T mx = T(0), my = T(0), mz = T(0);
+      if (ob) cell_momentum<L>(f, mx, my, mz);
+      accumulate_force(p.force, __any_sync(0xffffffffu, ob), mx, my, mz);
+    }
+    if (active) {
+      // 2. Zou/He inlet / outlet planes
+      if ((p.bc & TLBM_BC_ZH_INLET) && x == 0) {
+        if constexpr (Q == 9) zou_he_inlet_d2q9(f, bp.u_in, bp.uy_in, bp.one_minus_u);
+        else zou_he_inlet_3d<L>(f, bp.u_in, bp.uy_in, bp.uz_in, bp.one_minus_u);
+      }
+      if ((p.bc & TLBM_BC_ZH_OUTLET) && x == p.nx - 1) {
+        if constexpr (Q == 9) zou_he_outlet_d2q9(f, bp.rho_out, bp.two_thirds_rho_out, bp.sixth_rho_out);
+        else zou_he_outlet_3d<L>(f, bp.rho_out);
+      }
+      // 3. full-way bounce-back
+      if (fl & TLBM_FLAG_SOLID) bounce_back<L>(f);
+      // 4. moving lid
+      if ((p.bc & TLBM_BC_LID) && y == p.ny - 1) {
+        if constexpr (Q == 9) moving_lid_d2q9(f, bp.u_lid);
+        else if constexpr (Q == 19) moving_lid_d3q19(f, bp.u_lid);
+      }
+    }
+  }
+
+  if (!active) return;
+  if constexpr (COLL != TLBM_COLL_NONE) {
+    if (fl & TLBM_FLAG_HALFWAY) {
+      // pre-stream half-way wall: keep the populations, reversed, uncollided
+      bounce_back<L>(f);
+    } else {
+      const bool has_tau = p.tau_field != nullptr;
+      const T tau_cell = has_tau ? T(p.tau_field[cell]) : T(0);
+      collide<L, COLL>(f, cp, tau_cell, has_tau);
+      if (p.status) {
+        const T r = f[0];
+        if (!(r == r) || r - r != T(0)) atomicOr(p.status, 1u);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) fout[(long long)q * N + cell] = Storage<SO>::store(f[q], weight<L, T>(q));
+}
+
+inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block) {
+  int bx = 32;
+  while (bx < nx && bx < 256) bx <<= 1;
+  int by = 256 / bx;
+  block = dim3(bx, by, 1);
+  grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
+}
+
+template <class L, typename SI, typename SO, int COLL, bool PULL>
+int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
+  using T = typename Storage<SI>::T;
+  dim3 grid, block;
+  step_launch_shape(p.nx, p.ny, p.nz, grid, block);
+  const CollideParams<T> cp = make_collide_params<T>(d.tau, d.s_e, d.s_eps, d.s_q, d.s_pi, d.omega_b,
+                                                     d.omega_odd, d.omega_even, d.c_smag);
+  const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
+  k_step<L, SI, SO, COLL, PULL><<<grid, block, 0, s>>>(p, cp, bp);
+  return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
+}
+
+}  // namespace tlbm

@@ -1,0 +1,365 @@
+"""Time-step drivers: the "solvers' step()" of TensorLBM on the fused kernel.
+
+Three entry points, all running the sm_100a kernels through the C ABI:
+
+* :class:`LBMSolver` - stateful, one fused kernel per step (the fast path).
+  TensorLBM's runners advance ``S_{n+1} = BC(stream(collide(S_n)))``
+  (``cases/base.py:270-289``, ``d3q27_sphere_flow.py:246-256``).  The fused
+  kernel pulls, applies the boundaries and collides in one pass, so what it
+  stores is the post-collision state ``P_n = collide(S_n)``.  The solver keeps
+  the previous buffer, so ``solver.f`` returns the TensorLBM-phase ``S_n``
+  with one extra pass (boundaries without collision) whenever it is asked for.
+* :func:`make_step` - the functional ``step(f) -> f`` closure of
+  ``CaseBase.make_step`` with TensorLBM's phase on both sides: a collision
+  pass followed by a pull + boundary pass (two passes per step).
+* :class:`FusedSolver3D` - same surface as ``TritonFusedSolver3D``
+  (``triton_fused.py:676-865``): periodic D3Q19 BGK, ``step(f)`` returns
+  ``collide(stream(f))`` in one of two persistent ping-pong buffers.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib, _ops
+
+COLLISIONS = {
+    "none": _lib.COLL_NONE,
+    "bgk": _lib.COLL_BGK,
+    "mrt": _lib.COLL_MRT,
+    "cumulant": _lib.COLL_CUMULANT,
+    "cumulant_geier": _lib.COLL_CUMULANT_GEIER,
+    "cumulant_d3q19": _lib.COLL_CUMULANT_D3Q19,
+    "smagorinsky": _lib.COLL_SMAGORINSKY,
+}
+_LATTICES = {"D2Q9": 9, "D3Q19": 19, "D3Q27": 27, 9: 9, 19: 19, 27: 27}
+# storage dtype -> (C code, torch dtype of the buffer)
+STORAGE = {
+    "f32": (_lib.F32, torch.float32),
+    "f64": (_lib.F64, torch.float64),
+    "f16": (_lib.F16_SHIFTED, torch.float16),
+    "bf16": (_lib.BF16_SHIFTED, torch.bfloat16),
+}
+_TORCH_STORAGE = {torch.float32: "f32", torch.float64: "f64", torch.float16: "f16", torch.bfloat16: "bf16"}
+
+# default relaxation rates per lattice (solver.py:249, solver3d.py:107, d3q27.py:643)
+_MRT_DEFAULTS = {9: (1.64, 1.54, 1.7), 19: (1.19, 1.4, 1.2), 27: (1.19, 1.4, 1.2)}
+
+
+@dataclass
+class StepConfig:
+    """Everything one fused step needs besides the buffers."""
+
+    lattice: int
+    shape: tuple[int, ...]          # (ny, nx) or (nz, ny, nx)
+    tau: float
+    collision: str = "bgk"
+    s_e: float | None = None
+    s_eps: float | None = None
+    s_q: float | None = None
+    s_pi: float | None = None
+    omega_b: float = 1.0
+    omega_odd: float = 1.0
+    omega_even: float = 1.0
+    c_smag: float = 0.0
+    u_lid: float | None = None       # moving lid at y = ny-1
+    u_in: tuple[float, float, float] | float | None = None  # Zou/He inlet at x = 0
+    rho_out: float | None = None     # Zou/He outlet at x = nx-1
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def grid(self) -> tuple[int, int, int]:
+        if self.lattice == 9:
+            ny, nx = self.shape
+            return nx, ny, 1
+        nz, ny, nx = self.shape
+        return nx, ny, nz
+
+    def desc(self, dtype_code: int, collision: str | None = None) -> _lib.Desc:
+        q = self.lattice
+        d_se, d_seps, d_sq = _MRT_DEFAULTS[q]
+        bc = 0
+        u_in = (0.0, 0.0, 0.0)
+        if self.u_lid is not None:
+            bc |= _lib.BC_LID
+        if self.u_in is not None:
+            bc |= _lib.BC_ZH_INLET
+            u_in = (float(self.u_in), 0.0, 0.0) if isinstance(self.u_in, (int, float)) else tuple(self.u_in)
+        if self.rho_out is not None:
+            bc |= _lib.BC_ZH_OUTLET
+        coll = COLLISIONS[collision or self.collision]
+        return _ops.make_desc(
+            q, self.grid, dtype_code, coll, self.tau,
+            s_e=d_se if self.s_e is None else self.s_e,
+            s_eps=d_seps if self.s_eps is None else self.s_eps,
+            s_q=d_sq if self.s_q is None else self.s_q,
+            s_pi=self.s_pi, omega_b=self.omega_b, omega_odd=self.omega_odd, omega_even=self.omega_even,
+            c_smag=self.c_smag, bc=bc, u_lid=self.u_lid or 0.0, u_in=u_in,
+            rho_out=1.0 if self.rho_out is None else self.rho_out,
+        )
+
+
+class LBMSolver:
+    """Fused single-GPU LBM time stepper (one kernel pass per step).
+
+    Args:
+        lattice: "D2Q9", "D3Q19" or "D3Q27" (or 9 / 19 / 27).
+        shape: (ny, nx) or (nz, ny, nx).
+        tau: shear relaxation time.
+        collision: "bgk", "mrt", "smagorinsky", "cumulant" (D3Q27 legacy),
+            "cumulant_geier" (D3Q27), "cumulant_d3q19".
+        storage: "f32", "f64", "f16" or "bf16" (half formats hold f - w).
+        wall_mask, obstacle_mask: bool fields; both bounce back, only the
+            obstacle enters the momentum-exchange force.
+        u_lid, u_in, rho_out: enable the lid / Zou-He inlet / outlet planes.
+        tau_field: optional per-cell tau (BGK and MRT shear rate).
+        track_force: record the float64 force of every step.
+    """
+
+    def __init__(self, lattice, shape, tau: float, collision: str = "bgk", *, device=None, storage="f32",
+                 wall_mask=None, obstacle_mask=None, wall_mode: str = "fullway", tau_field=None,
+                 track_force: bool = False, **cfg):
+        q = _LATTICES[lattice]
+        if isinstance(storage, torch.dtype):
+            storage = _TORCH_STORAGE[storage]
+        if storage not in STORAGE:
+            raise ValueError(f"unknown storage {storage!r}; expected one of {sorted(STORAGE)}")
+        if collision not in COLLISIONS:
+            raise ValueError(f"unknown collision {collision!r}; expected one of {sorted(COLLISIONS)}")
+        shape = tuple(int(s) for s in shape)
+        if len(shape) != (2 if q == 9 else 3):
+            raise ValueError(f"shape {shape} does not fit lattice D{'2' if q == 9 else '3'}Q{q}")
+        self.cfg = StepConfig(q, shape, float(tau), collision, **cfg)
+        self.device = _ops.cuda_device(device)
+        self.q = q
+        self.storage = storage
+        self.code, self.buf_dtype = STORAGE[storage]
+        self.compute_dtype = torch.float64 if storage == "f64" else torch.float32
+        self.flags = None
+        if wall_mask is not None or obstacle_mask is not None:
+            self.flags = _ops.build_flags(shape, self.device, wall_mask, obstacle_mask, wall_mode)
+        self.tau_field = None
+        if tau_field is not None:
+            if tuple(tau_field.shape) != shape:
+                raise ValueError(f"tau_field shape {tuple(tau_field.shape)} != {shape}")
+            self.tau_field = tau_field.to(device=self.device, dtype=torch.float32).contiguous()
+        self.track_force = track_force
+        full = (q,) + shape
+        self._buf = [torch.empty(full, dtype=self.buf_dtype, device=self.device) for _ in range(2)]
+        self._cur = 0
+        self.steps_done = 0
+        self._f0: torch.Tensor | None = None
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.forces: list[torch.Tensor] = []
+        self._desc = self.cfg.desc(self.code)
+        self._desc_none = self.cfg.desc(self.code, "none")
+        self._graph = None
+
+    # -- state -----------------------------------------------------------------
+
+    @property
+    def n_cells(self) -> int:
+        n = 1
+        for s in self.cfg.shape:
+            n *= s
+        return n
+
+    def _stream(self) -> int:
+        return _lib.stream_of(self.device)
+
+    def load(self, f: torch.Tensor) -> "LBMSolver":
+        """Set the state to a TensorLBM-phase population field S_0."""
+        if tuple(f.shape) != (self.q,) + self.cfg.shape:
+            raise ValueError(f"f shape {tuple(f.shape)} != {(self.q,) + self.cfg.shape}")
+        f = f.to(device=self.device, dtype=self.compute_dtype).contiguous()
+        self._f0 = f.clone()
+        lib = _lib.load()
+        dc = self.cfg.desc(_lib.F64 if self.storage == "f64" else _lib.F32)
+        if self.storage in ("f32", "f64"):
+            _lib.check(lib.tlbm_collide(ctypes.byref(dc), dc.dtype, f.data_ptr(), self._buf[0].data_ptr(), _lib.ptr(self.flags),
+                                        _lib.ptr(self.tau_field), self._stream()), "collide")
+        else:
+            tmp = torch.empty_like(f)
+            _lib.check(lib.tlbm_collide(ctypes.byref(dc), _lib.F32, f.data_ptr(), tmp.data_ptr(), _lib.ptr(self.flags),
+                                        _lib.ptr(self.tau_field), self._stream()), "collide")
+            conv = self.cfg.desc(_lib.F32, "none")
+            _lib.check(lib.tlbm_collide(ctypes.byref(conv), self.code, tmp.data_ptr(), self._buf[0].data_ptr(), None,
+                                        None, self._stream()), "convert")
+        self._cur = 0
+        self.steps_done = 0
+        self.forces = []
+        self._graph = None
+        return self
+
+    def _launch(self, src: torch.Tensor, dst: torch.Tensor, force: torch.Tensor | None) -> None:
+        st = _lib.load().tlbm_step(ctypes.byref(self._desc), src.data_ptr(), dst.data_ptr(), _lib.ptr(self.flags),
+                                   _lib.ptr(self.tau_field), _lib.ptr(force), self.status.data_ptr(),
+                                   self._stream())
+        _lib.check(st, "tlbm_step")
+
+    def step(self, n: int = 1) -> "LBMSolver":
+        """Advance n time steps (n fused kernel launches)."""
+        if self._f0 is None:
+            raise RuntimeError("LBMSolver.step() before load(f)")
+        for _ in range(n):
+            force = None
+            if self.track_force:
+                force = torch.zeros(3, dtype=torch.float64, device=self.device)
+                self.forces.append(force)
+            self._launch(self._buf[self._cur], self._buf[1 - self._cur], force)
+            self._cur ^= 1
+            self.steps_done += 1
+        return self
+
+    def run(self, n: int, *, graph: bool = True, chunk: int = 50) -> "LBMSolver":
+        """Advance n steps, replaying a CUDA graph of `chunk` launches when graph=True.
+
+        Force tracking records one force per step, so it runs eagerly."""
+        if not graph or self.track_force or n < chunk:
+            return self.step(n)
+        if self._graph is None or self._graph[1] != chunk or self._graph[2] != self._cur:
+            # capture `chunk` (even) steps starting from the current buffer parity
+            chunk = chunk + (chunk & 1)
+            cur0 = self._cur
+            s = torch.cuda.Stream(self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    c = cur0
+                    for _ in range(chunk):
+                        self._launch(self._buf[c], self._buf[1 - c], None)
+                        c ^= 1
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            self._graph = (g, chunk, cur0)
+        g, chunk, _ = self._graph
+        reps, rest = divmod(n, chunk)
+        for _ in range(reps):
+            g.replay()
+        self.steps_done += reps * chunk
+        if rest:
+            self.step(rest)
+        return self
+
+    @property
+    def state(self) -> torch.Tensor:
+        """Stored post-collision populations P_n (storage format, f - w for half formats)."""
+        return self._buf[self._cur]
+
+    @property
+    def f(self) -> torch.Tensor:
+        """TensorLBM-phase populations S_n = BC(stream(P_{n-1})) as float32/float64."""
+        if self._f0 is None:
+            raise RuntimeError("LBMSolver.f before load(f)")
+        if self.steps_done == 0:
+            return self._f0.clone()
+        out = torch.empty((self.q,) + self.cfg.shape, dtype=self.compute_dtype, device=self.device)
+        prev = self._buf[1 - self._cur]
+        if self.storage in ("f32", "f64"):
+            st = _lib.load().tlbm_step(ctypes.byref(self._desc_none), prev.data_ptr(), out.data_ptr(),
+                                       _lib.ptr(self.flags), None, None, None, self._stream())
+            _lib.check(st, "tlbm_step(stream+bc)")
+        else:
+            # boundaries in the storage format, then widen to float32 locally
+            tmp = torch.empty_like(prev)
+            st = _lib.load().tlbm_step(ctypes.byref(self._desc_none), prev.data_ptr(), tmp.data_ptr(),
+                                       _lib.ptr(self.flags), None, None, None, self._stream())
+            _lib.check(st, "tlbm_step(stream+bc)")
+            conv = self.cfg.desc(self.code, "none")
+            _lib.check(_lib.load().tlbm_collide(ctypes.byref(conv), _lib.F32, tmp.data_ptr(), out.data_ptr(), None,
+                                                None, self._stream()), "convert")
+        return out
+
+    def moment_sums(self) -> torch.Tensor:
+        """float64 (mass, jx, jy, jz) of the stored post-collision state."""
+        return _ops.moment_sums(self.q, self.state, self.code)
+
+    def nonfinite_seen(self) -> bool:
+        """True if any step produced a non-finite density (reads one int)."""
+        return bool(self.status.item() != 0)
+
+    def force_history(self) -> torch.Tensor:
+        if not self.forces:
+            return torch.zeros((0, 3), dtype=torch.float64, device=self.device)
+        return torch.stack(self.forces)
+
+
+def make_step(lattice, shape, tau: float, collision: str = "bgk", *, device=None, wall_mask=None,
+              obstacle_mask=None, wall_mode: str = "fullway", tau_field=None, dtype=torch.float32, **cfg):
+    """Functional ``step(f) -> f`` with TensorLBM's chain collide -> stream -> boundaries.
+
+    Two passes per call: collision (local) then pull + boundaries.  Returns a new
+    tensor; the input is not modified.  ``step.last_force`` holds the float64
+    momentum-exchange force of the latest call when an obstacle is given."""
+    q = _LATTICES[lattice]
+    shape = tuple(int(s) for s in shape)
+    scfg = StepConfig(q, shape, float(tau), collision, **cfg)
+    dev = _ops.cuda_device(device)
+    code = _lib.real_dtype(torch.empty(0, dtype=dtype))
+    flags = None
+    if wall_mask is not None or obstacle_mask is not None:
+        flags = _ops.build_flags(shape, dev, wall_mask, obstacle_mask, wall_mode)
+    tf = None if tau_field is None else tau_field.to(device=dev, dtype=torch.float32).contiguous()
+    d_coll = scfg.desc(code)
+    d_bc = scfg.desc(code, "none")
+    track = obstacle_mask is not None
+
+    def step(f: torch.Tensor) -> torch.Tensor:
+        if tuple(f.shape) != (q,) + shape or f.dtype != dtype:
+            raise ValueError(f"step expects {(q,) + shape} {dtype}, got {tuple(f.shape)} {f.dtype}")
+        _lib.require_cuda(f)
+        f = f.contiguous()
+        tmp = torch.empty_like(f)
+        out = torch.empty_like(f)
+        s = _lib.stream_of(dev)
+        lib = _lib.load()
+        _lib.check(lib.tlbm_collide(ctypes.byref(d_coll), code, f.data_ptr(), tmp.data_ptr(), _lib.ptr(flags), _lib.ptr(tf), s),
+                   "collide")
+        force = torch.zeros(3, dtype=torch.float64, device=dev) if track else None
+        _lib.check(lib.tlbm_step(ctypes.byref(d_bc), tmp.data_ptr(), out.data_ptr(), _lib.ptr(flags), None,
+                                 _lib.ptr(force), None, s), "stream+boundaries")
+        step.last_force = force
+        return out
+
+    step.last_force = None
+    return step
+
+
+class FusedSolver3D:
+    """Periodic D3Q19 BGK step with the surface of ``TritonFusedSolver3D``
+    (``triton_fused.py:676-865``): ``step(f)`` returns ``collide(stream(f))``.
+
+    fp32 is the drop-in format.  For float16 / bfloat16 storage use
+    :class:`LBMSolver` with ``storage="f16"`` / ``"bf16"``, which keeps the
+    shifted deviations f - w instead of plain half values."""
+
+    def __init__(self, nz: int, ny: int, nx: int, tau: float, device="cuda:0", dtype=None, **_unused):
+        dtype = torch.float32 if dtype is None else dtype
+        if dtype != torch.float32:
+            raise NotImplementedError("FusedSolver3D is the float32 drop-in; use LBMSolver(storage='f16'|'bf16')")
+        self.nz, self.ny, self.nx = int(nz), int(ny), int(nx)
+        self.tau = float(tau)
+        self.device = _ops.cuda_device(device)
+        self.dtype = dtype
+        self._desc = _ops.make_desc(19, (self.nx, self.ny, self.nz), _lib.F32, _lib.COLL_BGK, self.tau)
+        self._buf_a: torch.Tensor | None = None
+        self._buf_b: torch.Tensor | None = None
+
+    def step(self, f: torch.Tensor) -> torch.Tensor:
+        if f.dtype != self.dtype:
+            raise ValueError(f"step() input dtype {f.dtype} does not match the solver's storage dtype {self.dtype}")
+        if tuple(f.shape) != (19, self.nz, self.ny, self.nx):
+            raise ValueError(f"f shape {tuple(f.shape)} != {(19, self.nz, self.ny, self.nx)}")
+        _lib.require_cuda(f)
+        f = f.contiguous()
+        if self._buf_a is None or self._buf_a.shape != f.shape:
+            self._buf_a = torch.empty_like(f)
+            self._buf_b = torch.empty_like(f)
+        out = self._buf_b if f.data_ptr() == self._buf_a.data_ptr() else self._buf_a
+        st = _lib.load().tlbm_step(ctypes.byref(self._desc), f.data_ptr(), out.data_ptr(), None, None, None, None,
+                                   _lib.stream_of(self.device))
+        _lib.check(st, "FusedSolver3D.step")
+        return out

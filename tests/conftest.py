@@ -1,0 +1,43 @@
+"""Shared fixtures.  Tests marked ``gpu`` need a CUDA device and the built
+libtlbm.so; everything else runs on the CPU."""
+
+from __future__ import annotations
+
+import pathlib
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+GOLDEN = ROOT / "tests" / "golden"
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libtlbm.so")
+    config.addinivalue_line("markers", "slow: long-running")
+
+
+def golden(name: str) -> dict:
+    with np.load(GOLDEN / f"{name}.npz") as d:
+        return {k: d[k] for k in d.files}
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import tensorlbm_b200._lib as lib
+
+    lib.load()  # raises if the CUDA library is missing on a GPU machine
+    return torch.device("cuda", 0)
+
+
+def rel_err(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-30))

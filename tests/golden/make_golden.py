@@ -1,0 +1,320 @@
+"""Generate golden vectors from the unmodified TensorLBM reference.
+
+Run from the repository root in a checkout that has the reference source:
+
+    python tests/golden/make_golden.py [--reference /path/to/TensorLBM/src]
+
+It imports TensorLBM's torch operators on the CPU (a stub ``matplotlib``
+package is put on sys.path first, because TensorLBM's package ``__init__``
+imports matplotlib for plotting and matplotlib is not installed here), runs
+each hot-path function on small seeded inputs and writes the inputs and
+outputs to ``tests/golden/*.npz``.  The tests load these files; nothing at
+test time needs the reference.
+"""
+
+from __future__ import annotations
+
+import argparse
+import pathlib
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+
+_STUB = '''
+import sys, types, importlib.abc, importlib.machinery
+class _Dummy:
+    def __getattr__(self, name): return _Dummy()
+    def __call__(self, *a, **k): return _Dummy()
+    def __iter__(self): return iter(())
+def use(*a, **k): pass
+class _Finder(importlib.abc.MetaPathFinder, importlib.abc.Loader):
+    def find_spec(self, name, path, target=None):
+        if name.startswith("matplotlib.") or name.startswith("mpl_toolkits"):
+            return importlib.machinery.ModuleSpec(name, self, is_package=True)
+        return None
+    def create_module(self, spec):
+        m = types.ModuleType(spec.name); m.__path__ = []
+        m.__getattr__ = lambda n: _Dummy(); return m
+    def exec_module(self, module): pass
+sys.meta_path.insert(0, _Finder())
+def __getattr__(name): return _Dummy()
+'''
+
+
+def import_reference(src: str):
+    stub_dir = pathlib.Path(tempfile.mkdtemp(prefix="tlbm_stub_"))
+    (stub_dir / "matplotlib").mkdir()
+    (stub_dir / "matplotlib" / "__init__.py").write_text(_STUB)
+    sys.path[:0] = [str(stub_dir), src]
+    import tensorlbm  # noqa: F401
+
+    return tensorlbm
+
+
+def near_eq_field(torch, q, spatial, dtype, seed, amp=0.05, noise=0.01):
+    """Random rho ~ 1 +- amp, |u| ~ amp, plus a non-equilibrium perturbation."""
+    from tensorlbm.d2q9 import equilibrium
+    from tensorlbm.d3q19 import equilibrium3d
+    from tensorlbm.d3q27 import equilibrium27
+
+    g = torch.Generator().manual_seed(seed)
+    rho = 1.0 + amp * (2 * torch.rand(spatial, generator=g, dtype=torch.float64) - 1)
+    u = [amp * (2 * torch.rand(spatial, generator=g, dtype=torch.float64) - 1) for _ in range(3)]
+    rho, u = rho.to(dtype), [v.to(dtype) for v in u]
+    if q == 9:
+        feq = equilibrium(rho, u[0], u[1])
+    elif q == 19:
+        feq = equilibrium3d(rho, *u)
+    else:
+        feq = equilibrium27(rho, *u)
+    pert = noise * (2 * torch.rand(feq.shape, generator=g, dtype=torch.float64) - 1).to(dtype)
+    return rho, u, feq * (1 + pert)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference/src")
+    ap.add_argument("--skip-long", action="store_true", help="skip the 64^3 x 1000-step cavity run")
+    args = ap.parse_args()
+    import_reference(args.reference)
+    import torch
+
+    torch.set_num_threads(8)
+    from tensorlbm import boundaries as b2
+    from tensorlbm import boundaries3d as b3
+    from tensorlbm import boundaries_d3q27 as b27
+    from tensorlbm import cumulant, obstacles, turbulence
+    from tensorlbm.boundary_registry import derive_missing_mask
+    from tensorlbm.d2q9 import equilibrium, macroscopic
+    from tensorlbm.d3q19 import equilibrium3d, macroscopic3d
+    from tensorlbm.d3q27 import collide_bgk27, collide_mrt27, equilibrium27, macroscopic27, stream27
+    from tensorlbm.lid_driven_cavity import zou_he_moving_lid
+    from tensorlbm.solver import collide_bgk, collide_mrt, stream
+    from tensorlbm.solver3d import collide_bgk3d, collide_mrt3d, stream3d
+
+    def save(name, **arrays):
+        out = {k: (v.detach().cpu().numpy() if isinstance(v, torch.Tensor) else np.asarray(v)) for k, v in arrays.items()}
+        np.savez_compressed(HERE / f"{name}.npz", **out)
+        print(f"  {name}.npz  ({(HERE / f'{name}.npz').stat().st_size / 1024:.0f} KB)")
+
+    sp2 = (6, 7)            # (ny, nx)
+    sp3 = (4, 5, 6)         # (nz, ny, nx)
+    tau = 0.6
+
+    print("moments / equilibrium")
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        rho, u, f = near_eq_field(torch, 9, sp2, dt, 1)
+        r, ux, uy = macroscopic(f)
+        save(f"moments_d2q9_{tag}", f=f, rho_in=rho, ux_in=u[0], uy_in=u[1], feq=equilibrium(rho, u[0], u[1]),
+             rho=r, ux=ux, uy=uy)
+        for q, eqf, macf in ((19, equilibrium3d, macroscopic3d), (27, equilibrium27, macroscopic27)):
+            rho, u, f = near_eq_field(torch, q, sp3, dt, q)
+            r, ux, uy, uz = macf(f)
+            save(f"moments_d3q{q}_{tag}", f=f, rho_in=rho, ux_in=u[0], uy_in=u[1], uz_in=u[2],
+                 feq=eqf(rho, *u), rho=r, ux=ux, uy=uy, uz=uz)
+
+    print("collisions")
+    _, _, f9 = near_eq_field(torch, 9, sp2, torch.float32, 11)
+    tf = 0.55 + 0.2 * torch.rand(sp2, generator=torch.Generator().manual_seed(5))
+    save("collide_d2q9_f32", f=f9, tau=tau, tau_field=tf, bgk=collide_bgk(f9, tau), mrt=collide_mrt(f9, tau),
+         mrt_field=collide_mrt(f9, tau, tau_field=tf), smag=turbulence.collide_smagorinsky_bgk(f9, tau, C_s=0.17))
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        _, _, f19 = near_eq_field(torch, 19, sp3, dt, 21)
+        kw19 = dict(f=f19, tau=tau, bgk=collide_bgk3d(f19, tau),
+                    smag=turbulence.collide_smagorinsky_bgk3d(f19, tau, C_s=0.17),
+                    cum19=cumulant.collide_cumulant_d3q19(f19, tau, omega_b=1.2, omega_even=0.8),
+                    cum19_smag=cumulant.collide_cumulant_d3q19(f19, tau, omega_b=1.2, omega_even=0.8, C_s=0.17))
+        if dt == torch.float32:  # the reference MRT matrices are float32 only
+            kw19["mrt"] = collide_mrt3d(f19, tau)
+            kw19["mrt_custom"] = collide_mrt3d(f19, tau, s_e=1.3, s_eps=1.5, s_q=1.1, s_pi=1.25)
+        save(f"collide_d3q19_{tag}", **kw19)
+        _, _, f27 = near_eq_field(torch, 27, sp3, dt, 31)
+        kw27 = dict(f=f27, tau=tau, bgk=collide_bgk27(f27, tau),
+                    smag=turbulence.collide_smagorinsky_bgk27(f27, tau, C_s=0.17),
+                    cum=cumulant.collide_cumulant_d3q27(f27, tau, omega_b=1.1, omega_odd=1.2, omega_even=0.9),
+                    geier=cumulant.collide_cumulant_geier_d3q27(f27, tau, omega_b=1.1, omega_odd=1.2, omega_even=0.9))
+        if dt == torch.float32:
+            kw27["mrt"] = collide_mrt27(f27, tau)
+        save(f"collide_d3q27_{tag}", **kw27)
+
+    print("streaming (integer canary: every value identifies its source)")
+    def canary(q, spatial):
+        n = int(np.prod(spatial))
+        return torch.arange(q * n, dtype=torch.float32).reshape((q,) + spatial)
+    c9 = canary(9, (5, 7))
+    c19 = canary(19, (3, 4, 5))
+    c27 = canary(27, (3, 4, 5))
+    save("stream", f9=c9, s9=stream(c9), f19=c19, s19=stream3d(c19), f27=c27, s27=stream27(c27))
+
+    print("boundaries")
+    g = torch.Generator().manual_seed(7)
+    m2 = torch.rand(sp2, generator=g) < 0.3
+    m3 = torch.rand(sp3, generator=g) < 0.3
+    _, _, f19 = near_eq_field(torch, 19, sp3, torch.float32, 41)
+    _, _, f27 = near_eq_field(torch, 27, sp3, torch.float32, 42)
+    _, _, f9 = near_eq_field(torch, 9, sp2, torch.float32, 43)
+    prof = 0.05 + 0.01 * torch.rand(sp2[0], generator=g)
+    save("bc_d2q9", f=f9, mask=m2, bb=b2.bounce_back_cells(f9, m2), inlet=b2.zou_he_inlet_velocity(f9, 0.05, 0.01),
+         inlet_profile=b2.zou_he_inlet_velocity(f9, prof), profile=prof,
+         outlet=b2.zou_he_outlet_pressure(f9, 1.02), lid=zou_he_moving_lid(f9, 0.07),
+         force=torch.stack(b2.compute_obstacle_forces(f9, m2)))
+    save("bc_d3q19", f=f19, mask=m3, bb=b3.bounce_back_cells_3d(f19, m3),
+         inlet=b3.zou_he_inlet_velocity_3d(f19.clone(), 0.04, 0.01, -0.005),
+         outlet=b3.zou_he_outlet_pressure_3d(f19.clone(), 0.98), lid=b3.zou_he_moving_lid_3d(f19, 0.05),
+         force=torch.stack(obstacles.compute_obstacle_forces_3d(f19, m3)))
+    save("bc_d3q27", f=f27, mask=m3, bb=b27.bounce_back_cells_27(f27, m3),
+         inlet=b27.zou_he_inlet_velocity_27(f27, 0.04, 0.01, -0.005),
+         outlet=b27.zou_he_outlet_pressure_27(f27, 0.98),
+         force=torch.stack(obstacles.compute_obstacle_forces_27(f27, m3)))
+
+    print("masks and links")
+    cpu = torch.device("cpu")
+    sph = b3.sphere_mask(32, 16, 16, 12.0, 8.0, 8.0, 4.5, cpu)
+    sph_odd = b3.sphere_mask(40, 24, 20, 17.3, 11.7, 9.1, 6.35, cpu)
+    big = b3.sphere_mask(512, 256, 256, 128, 128, 128, 16, cpu)  # sphere of D = 32 in the 512x256x256 channel
+    cyl = b2.cylinder_mask(200, 50, 25.0, 25.0, 3.125, cpu)
+    cyl_odd = b2.cylinder_mask(97, 31, 20.4, 15.5, 4.7, cpu)
+    miss19 = derive_missing_mask((16, 16, 32), solid_mask=sph, periodic={"y": True, "z": True, "x": False},
+                                 lattice="D3Q19")
+    miss27 = derive_missing_mask((16, 16, 32), solid_mask=sph, periodic=False, lattice="D3Q27")
+    links19 = torch.nonzero(miss19)
+    save("masks", sphere=sph, sphere_odd=sph_odd, big_index=torch.nonzero(big.reshape(-1))[:, 0].to(torch.int64),
+         big_count=big.sum(), cylinder=cyl, cylinder_odd=cyl_odd, missing19=np.packbits(miss19.numpy()),
+         missing19_shape=np.array(miss19.shape), missing27=np.packbits(miss27.numpy()),
+         missing27_shape=np.array(miss27.shape), links19=links19)
+
+    print("step chains")
+    from tensorlbm.d3q19 import OPPOSITE as OPP19
+
+    def cavity_walls(n):
+        wall = torch.zeros((n, n, n), dtype=torch.bool)
+        wall[:, :, 0] = wall[:, :, -1] = wall[:, 0, :] = wall[0, :, :] = wall[-1, :, :] = True
+        return wall
+
+    def cavity_run(n, coll, mode, steps, tau_c, u_lid=0.05, stop_at_nan=False):
+        """mode "fullway": collide -> stream -> bounce_back_cells_3d(walls) -> lid.
+        mode "halfway": collide -> where(wall, f_pre[opp], f) -> stream -> lid
+        (benchmarks/verified/cavity_3d_full/run.py:58 and :95-104)."""
+        wall = cavity_walls(n)
+        z = torch.zeros((n, n, n))
+        f = equilibrium3d(torch.ones((n, n, n)), z, z, z)
+        nan_step = -1
+        for s in range(1, steps + 1):
+            f_pre = f
+            f = collide_bgk3d(f, tau_c) if coll == "bgk" else collide_mrt3d(f, tau_c)
+            if mode == "halfway":
+                f = torch.where(wall.unsqueeze(0), f_pre[OPP19], f)
+            f = stream3d(f)
+            if mode == "fullway":
+                f = b3.bounce_back_cells_3d(f, wall)
+            f = b3.zou_he_moving_lid_3d(f, u_lid)
+            if nan_step < 0 and not bool(torch.isfinite(f).all()):
+                nan_step = s
+                if stop_at_nan:
+                    break
+        return f, wall, nan_step
+
+    # 12^3 cavity, 150 steps: the literal full-way chain diverges (NaN) inside the
+    # window for BGK and MRT; the production half-way chain stays finite
+    n = 12
+    tau_c = 3 * 0.05 * n / 100 + 0.5
+    for coll in ("bgk", "mrt"):
+        for mode in ("fullway", "halfway"):
+            f, wall, nan_step = cavity_run(n, coll, mode, 150, tau_c)
+            z = torch.zeros((n, n, n))
+            save(f"chain_cavity_d3q19_{coll}_{mode}", f0=equilibrium3d(torch.ones((n, n, n)), z, z, z), f=f,
+                 wall=wall, tau=tau_c, u_lid=0.05, steps=150, nan_step=nan_step)
+        # finite window of the literal chain, compared element-wise
+        f, wall, _ = cavity_run(n, coll, "fullway", 12, tau_c)
+        z = torch.zeros((n, n, n))
+        save(f"chain_cavity_d3q19_{coll}_fullway_window", f0=equilibrium3d(torch.ones((n, n, n)), z, z, z), f=f,
+             wall=wall, tau=tau_c, u_lid=0.05, steps=12)
+
+    # sphere channel: collide -> stream -> force -> ZH in -> ZH out -> BB(wall) -> BB(obstacle)
+    nz, ny, nx = 12, 12, 24
+    obst = b3.sphere_mask(nx, ny, nz, 8.0, 6.0, 6.0, 2.5, cpu)
+    empty = torch.zeros_like(obst)
+    u_in = 0.04
+    for q, coll in ((19, "mrt"), (19, "bgk"), (27, "cumulant"), (27, "geier"), (27, "bgk")):
+        ones, zz = torch.ones((nz, ny, nx)), torch.zeros((nz, ny, nx))
+        ux0 = torch.full((nz, ny, nx), u_in)
+        ux0[obst] = 0.0
+        f = (equilibrium3d if q == 19 else equilibrium27)(ones, ux0, zz, zz)
+        f0 = f.clone()
+        tau_s = 3 * u_in * 5 / 30 + 0.5
+        forces = []
+        for _ in range(60):
+            if q == 19:
+                f = collide_mrt3d(f, tau_s) if coll == "mrt" else collide_bgk3d(f, tau_s)
+                f = stream3d(f)
+                forces.append(torch.stack(obstacles.compute_obstacle_forces_3d(f, obst)))
+                f = b3.apply_zou_he_channel_boundaries_3d(f, u_in, empty, obst)
+            else:
+                if coll == "cumulant":
+                    f = cumulant.collide_cumulant_d3q27(f, tau_s)
+                elif coll == "geier":
+                    f = cumulant.collide_cumulant_geier_d3q27(f, tau_s)
+                else:
+                    f = collide_bgk27(f, tau_s)
+                f = stream27(f)
+                forces.append(torch.stack(obstacles.compute_obstacle_forces_27(f, obst)))
+                f = b27.apply_zou_he_channel_boundaries_27(f, u_in, empty, obst)
+        save(f"chain_sphere_d3q{q}_{coll}", f0=f0, f=f, obstacle=obst, tau=tau_s, u_in=u_in, steps=60,
+             forces=torch.stack(forces))
+
+    # D2Q9 cylinder channel with walls: cylinder_flow.py:854-899 (zou_he outlet mode)
+    ny2, nx2 = 20, 60
+    obst2 = b2.cylinder_mask(nx2, ny2, 10.0, 10.0, 2.5, cpu)
+    wall2 = b2.make_channel_wall_mask(ny2, nx2, obst2, cpu)
+    ux0 = torch.full((ny2, nx2), 0.05)
+    ux0[obst2] = 0.0
+    f = equilibrium(torch.ones((ny2, nx2)), ux0, torch.zeros((ny2, nx2)))
+    f0 = f.clone()
+    tau2 = 3 * 0.05 * 5 / 20 + 0.5  # Re = u D / nu = 20
+    forces = []
+    for _ in range(200):
+        f = collide_bgk(f, tau2)
+        f = stream(f)
+        forces.append(torch.stack(b2.compute_obstacle_forces(f, obst2)))
+        f = b2.zou_he_inlet_velocity(f, 0.05)
+        f = b2.zou_he_outlet_pressure(f, rho_out=1.0)
+        f = b2.bounce_back_cells(f, wall2)
+        f = b2.bounce_back_cells(f, obst2)
+    save("chain_cylinder_d2q9_bgk", f0=f0, f=f, obstacle=obst2, wall=wall2, tau=tau2, u_in=0.05, steps=200,
+         forces=torch.stack(forces))
+
+    if not args.skip_long:
+        # the 64^3, Re=400, lid 0.05 cavity (tau = 3 u N / Re + 0.5)
+        n = 64
+        tau_c = 3 * 0.05 * n / 400 + 0.5
+        mid = n // 2
+
+        def summary(f):
+            rho, ux, uy, uz = macroscopic3d(f)
+            return dict(rho_mid=rho[mid], ux_mid=ux[mid], uy_mid=uy[mid], uz_mid=uz[mid],
+                        ux_center_line=ux[mid, :, mid], uy_center_line=uy[mid, mid, :],
+                        sums=torch.stack([rho.double().sum(), ux.double().sum(), uy.double().sum(),
+                                          uz.double().sum(), (ux.double() ** 2 + uy.double() ** 2
+                                                              + uz.double() ** 2).sum()]),
+                        f_sum_per_q=f.double().sum(dim=(1, 2, 3)))
+
+        # literal BGK full-way chain: 20 finite steps, then the step where it turns NaN
+        f, _, _ = cavity_run(n, "bgk", "fullway", 20, tau_c)
+        _, _, nan_step = cavity_run(n, "bgk", "fullway", 1000, tau_c, stop_at_nan=True)
+        save("chain_cavity64_d3q19_bgk_fullway", tau=tau_c, u_lid=0.05, steps=20, nan_step=nan_step, **summary(f))
+        print(f"  64^3 BGK full-way cavity: NaN from step {nan_step}")
+        # production half-way walls, MRT, 1000 steps (finite)
+        t0 = time.time()
+        f, _, nan_step = cavity_run(n, "mrt", "halfway", 1000, tau_c)
+        dt = time.time() - t0
+        save("chain_cavity64_d3q19_mrt_halfway_1000", tau=tau_c, u_lid=0.05, steps=1000, seconds=dt,
+             nan_step=nan_step, **summary(f))
+        print(f"  64^3 MRT half-way cavity, 1000 steps: {dt:.1f} s ({n**3 * 1000 / dt / 1e6:.2f} MLUPS)")
+
+
+if __name__ == "__main__":
+    main()

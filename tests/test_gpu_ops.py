@@ -1,0 +1,227 @@
+"""GPU parity of the stand-alone operators against TensorLBM's outputs (golden
+vectors) and the numpy oracle.  Every call goes through libtlbm.so."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lbm as O
+from tests.conftest import golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+F32_TOL = 2e-6
+F64_TOL = 1e-12
+
+
+def T(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def N(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+@pytest.mark.parametrize("q", [9, 19, 27])
+def test_moments_equilibrium(cuda, q, tag):
+    from tensorlbm_b200 import d2q9, d3q19, d3q27
+
+    g = golden(f"moments_d{'2' if q == 9 else '3'}q{q}_{tag}")
+    tol = F32_TOL if tag == "f32" else F64_TOL
+    f = T(g["f"], cuda)
+    if q == 9:
+        rho, ux, uy = d2q9.macroscopic(f)
+        feq = d2q9.equilibrium(T(g["rho_in"], cuda), T(g["ux_in"], cuda), T(g["uy_in"], cuda))
+    else:
+        mod = d3q19 if q == 19 else d3q27
+        mac = mod.macroscopic3d if q == 19 else mod.macroscopic27
+        eqf = mod.equilibrium3d if q == 19 else mod.equilibrium27
+        rho, ux, uy, uz = mac(f)
+        assert np.max(np.abs(N(uz) - g["uz"])) < 10 * tol
+        feq = eqf(*(T(g[k], cuda) for k in ("rho_in", "ux_in", "uy_in", "uz_in")))
+    assert feq.dtype == f.dtype
+    assert rel_err(N(rho), g["rho"]) < tol
+    assert np.max(np.abs(N(ux) - g["ux"])) < 10 * tol
+    assert np.max(np.abs(N(uy) - g["uy"])) < 10 * tol
+    assert rel_err(N(feq), g["feq"]) < tol
+
+
+def test_collide_d2q9(cuda):
+    from tensorlbm_b200 import solver, turbulence
+
+    g = golden("collide_d2q9_f32")
+    f, tau = T(g["f"], cuda), float(g["tau"])
+    assert rel_err(N(solver.collide_bgk(f, tau)), g["bgk"]) < F32_TOL
+    assert rel_err(N(solver.collide_mrt(f, tau)), g["mrt"]) < F32_TOL
+    assert rel_err(N(solver.collide_mrt(f, tau, tau_field=T(g["tau_field"], cuda))), g["mrt_field"]) < F32_TOL
+    assert rel_err(N(turbulence.collide_smagorinsky_bgk(f, tau, C_s=0.17)), g["smag"]) < F32_TOL
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_collide_d3q19(cuda, tag):
+    from tensorlbm_b200 import cumulant, solver3d, turbulence
+
+    g = golden(f"collide_d3q19_{tag}")
+    tol = F32_TOL if tag == "f32" else F64_TOL
+    f, tau = T(g["f"], cuda), float(g["tau"])
+    assert rel_err(N(solver3d.collide_bgk3d(f, tau)), g["bgk"]) < tol
+    assert rel_err(N(turbulence.collide_smagorinsky_bgk3d(f, tau, C_s=0.17)), g["smag"]) < tol
+    assert rel_err(N(cumulant.collide_cumulant_d3q19(f, tau, omega_b=1.2, omega_even=0.8)), g["cum19"]) < tol
+    assert rel_err(N(cumulant.collide_cumulant_d3q19(f, tau, omega_b=1.2, omega_even=0.8, C_s=0.17)),
+                   g["cum19_smag"]) < tol
+    if "mrt" in g:
+        assert rel_err(N(solver3d.collide_mrt3d(f, tau)), g["mrt"]) < F32_TOL
+        assert rel_err(N(solver3d.collide_mrt3d(f, tau, s_e=1.3, s_eps=1.5, s_q=1.1, s_pi=1.25)),
+                       g["mrt_custom"]) < F32_TOL
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_collide_d3q27(cuda, tag):
+    from tensorlbm_b200 import cumulant, d3q27, turbulence
+
+    g = golden(f"collide_d3q27_{tag}")
+    tol = F32_TOL if tag == "f32" else F64_TOL
+    f, tau = T(g["f"], cuda), float(g["tau"])
+    assert rel_err(N(d3q27.collide_bgk27(f, tau)), g["bgk"]) < tol
+    assert rel_err(N(turbulence.collide_smagorinsky_bgk27(f, tau, C_s=0.17)), g["smag"]) < tol
+    assert rel_err(N(cumulant.collide_cumulant_d3q27(f, tau, 1.1, 1.2, 0.9)), g["cum"]) < 5 * tol
+    assert rel_err(N(cumulant.collide_cumulant_geier_d3q27(f, tau, 1.1, 1.2, 0.9)), g["geier"]) < 5 * tol
+    if "mrt" in g:
+        assert rel_err(N(d3q27.collide_mrt27(f, tau)), g["mrt"]) < 5 * F32_TOL
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_collisions_vs_oracle_larger(cuda, seed):
+    """Seeded 12x10x8 fields (beyond the golden sizes) against the oracle."""
+    from tensorlbm_b200 import cumulant, d3q27, solver3d
+
+    rng = np.random.default_rng(seed)
+    for q, fns in ((19, [(solver3d.collide_bgk3d, O.collide_bgk), (solver3d.collide_mrt3d, O.collide_mrt)]),
+                   (27, [(cumulant.collide_cumulant_d3q27, O.collide_cumulant_d3q27),
+                         (cumulant.collide_cumulant_geier_d3q27, O.collide_cumulant_geier_d3q27),
+                         (d3q27.collide_mrt27, O.collide_mrt)])):
+        sp = (8, 10, 12)
+        rho = (1 + 0.05 * rng.uniform(-1, 1, sp)).astype(np.float32)
+        u = [(0.08 * rng.uniform(-1, 1, sp)).astype(np.float32) for _ in range(3)]
+        f = O.equilibrium(q, rho, *u) * (1 + 0.02 * rng.uniform(-1, 1, (q,) + sp)).astype(np.float32)
+        f = f.astype(np.float32)
+        for ours, ref in fns:
+            assert rel_err(N(ours(T(f, cuda), 0.57)), ref(f, 0.57)) < 5 * F32_TOL, ours.__name__
+
+
+def test_stream_canary_bitwise(cuda):
+    from tensorlbm_b200 import d3q27, solver, solver3d
+
+    g = golden("stream")
+    assert np.array_equal(N(solver.stream(T(g["f9"], cuda))), g["s9"])
+    assert np.array_equal(N(solver3d.stream3d(T(g["f19"], cuda))), g["s19"])
+    assert np.array_equal(N(d3q27.stream27(T(g["f27"], cuda))), g["s27"])
+
+
+def test_stream_full_size_roundtrip(cuda):
+    """Size-independent: streaming then streaming the reversed directions is the identity."""
+    from tensorlbm_b200 import solver3d
+    from tensorlbm_b200.d3q19 import OPPOSITE
+
+    f = torch.rand((19, 64, 96, 128), device=cuda)
+    s = solver3d.stream3d(f)
+    back = solver3d.stream3d(s[OPPOSITE.to(cuda)])[OPPOSITE.to(cuda)]
+    assert torch.equal(back, f)
+
+
+@pytest.mark.parametrize("q", [9, 19, 27])
+def test_boundaries(cuda, q):
+    from tensorlbm_b200 import boundaries, boundaries3d, boundaries_d3q27, lid_driven_cavity, obstacles
+
+    g = golden(f"bc_d{'2' if q == 9 else '3'}q{q}")
+    f, m = T(g["f"], cuda), T(g["mask"], cuda)
+    if q == 9:
+        assert np.array_equal(N(boundaries.bounce_back_cells(f, m)), g["bb"])
+        assert rel_err(N(boundaries.zou_he_inlet_velocity(f, 0.05, 0.01)), g["inlet"]) < F32_TOL
+        assert rel_err(N(boundaries.zou_he_inlet_velocity(f, T(g["profile"], cuda))), g["inlet_profile"]) < F32_TOL
+        assert rel_err(N(boundaries.zou_he_outlet_pressure(f, 1.02)), g["outlet"]) < F32_TOL
+        assert rel_err(N(lid_driven_cavity.zou_he_moving_lid(f, 0.07)), g["lid"]) < F32_TOL
+        force = torch.stack(boundaries.compute_obstacle_forces(f, m))
+        assert np.array_equal(N(f), g["f"])  # functional: input untouched
+    elif q == 19:
+        assert np.array_equal(N(boundaries3d.bounce_back_cells_3d(f, m)), g["bb"])
+        fin = f.clone()
+        out = boundaries3d.zou_he_inlet_velocity_3d(fin, 0.04, 0.01, -0.005)
+        assert out.data_ptr() == fin.data_ptr()  # in place, like the reference
+        assert rel_err(N(out), g["inlet"]) < F32_TOL
+        assert rel_err(N(boundaries3d.zou_he_outlet_pressure_3d(f.clone(), 0.98)), g["outlet"]) < F32_TOL
+        assert rel_err(N(boundaries3d.zou_he_moving_lid_3d(f, 0.05)), g["lid"]) < F32_TOL
+        force = torch.stack(obstacles.compute_obstacle_forces_3d(f, m))
+    else:
+        assert np.array_equal(N(boundaries_d3q27.bounce_back_cells_27(f, m)), g["bb"])
+        assert rel_err(N(boundaries_d3q27.zou_he_inlet_velocity_27(f, 0.04, 0.01, -0.005)), g["inlet"]) < F32_TOL
+        assert rel_err(N(boundaries_d3q27.zou_he_outlet_pressure_27(f, 0.98)), g["outlet"]) < F32_TOL
+        force = torch.stack(obstacles.compute_obstacle_forces_27(f, m))
+    ref = g["force"].astype(np.float64)
+    assert force.dtype == torch.float64
+    assert np.max(np.abs(N(force) - ref)) < 1e-5 * max(np.max(np.abs(ref)), 1.0)
+
+
+def test_errors(cuda):
+    from tensorlbm_b200 import boundaries3d, d3q19, solver3d
+
+    f = torch.rand((19, 4, 5, 6), device=cuda)
+    with pytest.raises(ValueError):
+        solver3d.collide_bgk3d(torch.rand((18, 4, 5, 6), device=cuda), 0.6)
+    with pytest.raises(ValueError):
+        d3q19.equilibrium3d(*(torch.ones((4, 5, 6), device=cuda),) * 3, torch.ones((4, 5, 7), device=cuda))
+    with pytest.raises(ValueError):
+        solver3d.collide_bgk3d(f.half(), 0.6)
+    with pytest.raises(NotImplementedError):
+        boundaries3d.zou_he_moving_lid_3d(f, 0.05, uy_lid=0.01)
+    with pytest.raises(RuntimeError):
+        solver3d.collide_bgk3d(f.cpu(), 0.6)
+
+
+def test_masks_bitwise(cuda):
+    from tensorlbm_b200 import boundaries, boundaries3d
+
+    g = golden("masks")
+    assert np.array_equal(N(boundaries3d.sphere_mask(32, 16, 16, 12.0, 8.0, 8.0, 4.5, cuda)), g["sphere"])
+    assert np.array_equal(N(boundaries3d.sphere_mask(40, 24, 20, 17.3, 11.7, 9.1, 6.35, cuda)), g["sphere_odd"])
+    assert np.array_equal(N(boundaries.cylinder_mask(200, 50, 25.0, 25.0, 3.125, cuda)), g["cylinder"])
+    assert np.array_equal(N(boundaries.cylinder_mask(97, 31, 20.4, 15.5, 4.7, cuda)), g["cylinder_odd"])
+    big = boundaries3d.sphere_mask(512, 256, 256, 128, 128, 128, 16, cuda)
+    assert int(big.sum()) == int(g["big_count"])
+    assert np.array_equal(N(torch.nonzero(big.reshape(-1))[:, 0]), g["big_index"])
+
+
+def test_missing_mask_and_links(cuda):
+    from tensorlbm_b200 import boundary_registry as br
+
+    g = golden("masks")
+    sph = T(g["sphere"], cuda)
+    m19 = br.derive_missing_mask((16, 16, 32), solid_mask=sph, periodic={"y": True, "z": True, "x": False},
+                                 lattice="D3Q19")
+    ref19 = np.unpackbits(g["missing19"])[: int(np.prod(g["missing19_shape"]))].reshape(tuple(g["missing19_shape"]))
+    assert np.array_equal(N(m19), ref19.astype(bool))
+    links = br.link_list(m19)
+    assert np.array_equal(N(links), g["links19"])
+    m27 = br.derive_missing_mask((16, 16, 32), solid_mask=sph, periodic=False, lattice="D3Q27")
+    ref27 = np.unpackbits(g["missing27"])[: int(np.prod(g["missing27_shape"]))].reshape(tuple(g["missing27_shape"]))
+    assert np.array_equal(N(m27), ref27.astype(bool))
+
+
+def test_link_list_large_and_empty(cuda):
+    from tensorlbm_b200 import _ops
+
+    m = torch.rand((19, 40, 50, 60), device=cuda) < 0.01
+    assert torch.equal(_ops.link_list(m), torch.nonzero(m.reshape(-1))[:, 0])
+    assert _ops.link_list(torch.zeros(1000, dtype=torch.bool, device=cuda)).numel() == 0
+
+
+def test_correct_mass(cuda):
+    from tensorlbm_b200 import solver3d
+
+    f = torch.rand((19, 8, 9, 10), device=cuda, dtype=torch.float64)
+    out = solver3d.correct_mass3d(f, 123.0)
+    assert abs(float(out.sum()) - 123.0) < 1e-9
+    assert torch.equal(solver3d.correct_mass3d(torch.zeros_like(f), 5.0), torch.zeros_like(f))

@@ -1,0 +1,298 @@
+"""GPU parity of the fused time step (tlbm_step) and the step drivers against
+TensorLBM's chains (golden vectors) and the numpy oracle."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lbm as O
+from tests.conftest import golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+# float32 populations after tens to hundreds of steps: relative to max |f|
+CHAIN_TOL = 1e-5
+
+
+def T(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def N(t):
+    return t.detach().cpu().numpy()
+
+
+def _step_raw(q, f, out, flags=None, collision="none", **cfg):
+    from tensorlbm_b200 import _lib, _ops
+    from tensorlbm_b200.solvers import COLLISIONS
+
+    grid = _ops.grid_of(f, q)
+    d = _ops.make_desc(q, grid, _lib.real_dtype(f), COLLISIONS[collision], cfg.pop("tau", 1.0), **cfg)
+    st = _lib.load().tlbm_step(ctypes.byref(d), f.data_ptr(), out.data_ptr(), _lib.ptr(flags), None, None, None,
+                               _lib.stream_of(f.device))
+    _lib.check(st, "tlbm_step")
+    return out
+
+
+@pytest.mark.parametrize("q", [9, 19, 27])
+def test_pull_gather_canary_bitwise(cuda, q):
+    """Integer-coded f (every value names its source) through the fused pull
+    with full-way solids: must equal bounce_back(stream(f)) bit for bit."""
+    sp = (11, 13) if q == 9 else (6, 7, 9)
+    n = int(np.prod(sp))
+    f = np.arange(q * n, dtype=np.float32).reshape((q,) + sp)
+    solid = np.random.default_rng(3).random(sp) < 0.3
+    from tensorlbm_b200 import _ops
+
+    flags = _ops.build_flags(sp, cuda, T(solid, cuda), None)
+    out = _step_raw(q, T(f, cuda), torch.empty((q,) + sp, device=cuda), flags)
+    assert np.array_equal(N(out), O.bounce_back(O.stream(f), solid))
+
+
+def test_fused_solver3d_matches_collide_of_stream(cuda):
+    from tensorlbm_b200 import FusedSolver3D
+
+    rng = np.random.default_rng(0)
+    sp = (16, 20, 24)
+    f = O.equilibrium(19, (1 + 0.02 * rng.standard_normal(sp)).astype(np.float32),
+                      *(0.05 * rng.standard_normal(sp).astype(np.float32) for _ in range(3)))
+    s = FusedSolver3D(*sp, tau=0.6, device=cuda)
+    a = s.step(T(f, cuda))
+    b = s.step(a)
+    assert a.data_ptr() != b.data_ptr()
+    ref = O.collide_bgk(O.stream(O.collide_bgk(O.stream(f), 0.6)), 0.6)
+    assert rel_err(N(b), ref) < 2e-6
+
+
+def _cavity_solver(n, coll, mode, tau, cuda, storage="f32"):
+    from tensorlbm_b200 import LBMSolver
+
+    wall = O.cavity_walls_3d(n, n, n)
+    return LBMSolver("D3Q19", (n, n, n), tau, coll, device=cuda, wall_mask=T(wall, cuda), wall_mode=mode,
+                     u_lid=0.05, storage=storage)
+
+
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+@pytest.mark.parametrize("mode", ["halfway", "fullway_window", "fullway"])
+def test_cavity_chain_vs_reference(cuda, coll, mode):
+    g = golden(f"chain_cavity_d3q19_{coll}_{mode}")
+    n = g["f0"].shape[1]
+    s = _cavity_solver(n, coll, "halfway" if mode == "halfway" else "fullway", float(g["tau"]), cuda)
+    s.load(T(g["f0"], cuda))
+    nan_step = -1
+    for k in range(1, int(g["steps"]) + 1):
+        s.step()
+        if nan_step < 0 and not bool(torch.isfinite(s.state).all()):
+            nan_step = k  # P_k = collide(S_k) is non-finite exactly when S_k is
+    if int(g.get("nan_step", -1)) > 0:
+        assert nan_step > 0 and abs(nan_step - int(g["nan_step"])) <= 2, (nan_step, int(g["nan_step"]))
+    else:
+        assert rel_err(N(s.f), g["f"]) < CHAIN_TOL
+
+
+def test_cavity64_mrt_halfway_1000_steps(cuda):
+    """The 64^3 Re=400 lid-driven cavity, 1000 steps, against TensorLBM's run."""
+    g = golden("chain_cavity64_d3q19_mrt_halfway_1000")
+    n = 64
+    s = _cavity_solver(n, "mrt", "halfway", float(g["tau"]), cuda)
+    z = np.zeros((n, n, n), np.float32)
+    s.load(T(O.equilibrium(19, np.ones((n, n, n), np.float32), z, z, z), cuda))
+    s.run(1000)
+    from tensorlbm_b200.d3q19 import macroscopic3d
+
+    rho, ux, uy, uz = (N(t) for t in macroscopic3d(s.f))
+    mid = n // 2
+    umax = float(np.max(np.abs(g["ux_mid"])))
+    for got, key in ((ux[mid], "ux_mid"), (uy[mid], "uy_mid"), (uz[mid], "uz_mid")):
+        assert np.max(np.abs(got - g[key])) < CHAIN_TOL * umax * 10, key
+    assert rel_err(rho[mid], g["rho_mid"]) < CHAIN_TOL
+    assert np.max(np.abs(ux[mid, :, mid] - g["ux_center_line"])) < 1e-4 * umax
+
+
+def test_cavity64_bgk_fullway_diverges_like_reference(cuda):
+    g = golden("chain_cavity64_d3q19_bgk_fullway")
+    n = 64
+    s = _cavity_solver(n, "bgk", "fullway", float(g["tau"]), cuda)
+    z = np.zeros((n, n, n), np.float32)
+    s.load(T(O.equilibrium(19, np.ones((n, n, n), np.float32), z, z, z), cuda))
+    s.step(int(g["steps"]))
+    from tensorlbm_b200.d3q19 import macroscopic3d
+
+    rho, ux, uy, uz = (N(t) for t in macroscopic3d(s.f))
+    assert rel_err(rho[n // 2], g["rho_mid"]) < CHAIN_TOL
+    assert np.max(np.abs(ux[n // 2] - g["ux_mid"])) < 1e-5
+    nan_step = -1
+    for k in range(int(g["steps"]) + 1, 400):
+        s.step()
+        if not bool(torch.isfinite(s.state).all()):
+            nan_step = k
+            break
+    assert abs(nan_step - int(g["nan_step"])) <= 2, (nan_step, int(g["nan_step"]))
+
+
+@pytest.mark.parametrize("name,q,coll", [("d3q19_mrt", 19, "mrt"), ("d3q19_bgk", 19, "bgk"),
+                                         ("d3q27_cumulant", 27, "cumulant"), ("d3q27_geier", 27, "cumulant_geier"),
+                                         ("d3q27_bgk", 27, "bgk")])
+def test_sphere_channel_vs_reference(cuda, name, q, coll):
+    from tensorlbm_b200 import LBMSolver
+
+    g = golden(f"chain_sphere_{name}")
+    sp = g["obstacle"].shape
+    s = LBMSolver(q, sp, float(g["tau"]), coll, device=cuda, obstacle_mask=T(g["obstacle"], cuda),
+                  u_in=float(g["u_in"]), rho_out=1.0, track_force=True)
+    s.load(T(g["f0"], cuda))
+    s.step(int(g["steps"]))
+    assert rel_err(N(s.f), g["f"]) < CHAIN_TOL
+    ref = g["forces"].astype(np.float64)
+    got = N(s.force_history())
+    assert np.max(np.abs(got - ref)) < 1e-4 * np.max(np.abs(ref[:, 0]))
+
+
+def test_cylinder_d2q9_vs_reference(cuda):
+    from tensorlbm_b200 import LBMSolver
+
+    g = golden("chain_cylinder_d2q9_bgk")
+    s = LBMSolver("D2Q9", g["obstacle"].shape, float(g["tau"]), "bgk", device=cuda,
+                  wall_mask=T(g["wall"], cuda), obstacle_mask=T(g["obstacle"], cuda), u_in=float(g["u_in"]),
+                  rho_out=1.0, track_force=True)
+    s.load(T(g["f0"], cuda))
+    s.step(int(g["steps"]))
+    assert rel_err(N(s.f), g["f"]) < CHAIN_TOL
+    ref = g["forces"].astype(np.float64)
+    assert np.max(np.abs(N(s.force_history())[:, :2] - ref)) < 1e-4 * np.max(np.abs(ref))
+
+
+def test_make_step_matches_solver(cuda):
+    from tensorlbm_b200 import LBMSolver, make_step
+
+    g = golden("chain_sphere_d3q19_mrt")
+    sp = g["obstacle"].shape
+    kw = dict(device=cuda, obstacle_mask=T(g["obstacle"], cuda), u_in=float(g["u_in"]), rho_out=1.0)
+    step = make_step("D3Q19", sp, float(g["tau"]), "mrt", **kw)
+    f = T(g["f0"], cuda)
+    for _ in range(5):
+        f = step(f)
+    s = LBMSolver("D3Q19", sp, float(g["tau"]), "mrt", **kw).load(T(g["f0"], cuda)).step(5)
+    assert rel_err(N(f), N(s.f)) < 1e-6
+    ref = g["f0"]
+    for _ in range(5):
+        ref, _ = O.channel_step(ref, float(g["tau"]), float(g["u_in"]), 1.0, None, g["obstacle"], "mrt")
+    assert rel_err(N(f), ref) < 2e-6
+
+
+def test_cuda_graph_run_matches_eager(cuda):
+    from tensorlbm_b200 import LBMSolver
+
+    g = golden("chain_sphere_d3q27_cumulant")
+    sp = g["obstacle"].shape
+    kw = dict(device=cuda, obstacle_mask=T(g["obstacle"], cuda), u_in=float(g["u_in"]), rho_out=1.0)
+    a = LBMSolver(27, sp, float(g["tau"]), "cumulant", **kw).load(T(g["f0"], cuda)).step(60)
+    b = LBMSolver(27, sp, float(g["tau"]), "cumulant", **kw).load(T(g["f0"], cuda)).run(60, chunk=10)
+    assert torch.equal(a.f, b.f)
+
+
+def _tgv(n, u0=0.05):
+    k = 2 * np.pi / n
+    x = np.arange(n)
+    zz, yy, xx = np.meshgrid(x, x, x, indexing="ij")
+    ux = u0 * np.sin(k * xx) * np.cos(k * yy) * np.cos(k * zz)
+    uy = -u0 * np.cos(k * xx) * np.sin(k * yy) * np.cos(k * zz)
+    return ux, uy, np.zeros_like(ux)
+
+
+@pytest.mark.parametrize("storage,tol", [("f16", 1e-3), ("bf16", 1e-2)])
+def test_shifted_half_storage_vs_f64(cuda, storage, tol):
+    """Half storage of f - w against an FP64 run: relative velocity L2 error."""
+    from tensorlbm_b200 import LBMSolver
+    from tensorlbm_b200.d3q19 import macroscopic3d
+
+    n = 32
+    u = _tgv(n)
+    f64 = O.equilibrium(19, np.ones((n, n, n)), *u)
+    ref = LBMSolver("D3Q19", (n, n, n), 0.51, "bgk", device=cuda, storage="f64").load(T(f64, cuda)).step(200)
+    low = LBMSolver("D3Q19", (n, n, n), 0.51, "bgk", device=cuda, storage=storage).load(
+        T(f64.astype(np.float32), cuda)).step(200)
+    _, ax, ay, az = (N(t) for t in macroscopic3d(ref.f))
+    _, bx, by, bz = (N(t).astype(np.float64) for t in macroscopic3d(low.f))
+    num = np.sqrt(np.sum((ax - bx) ** 2 + (ay - by) ** 2 + (az - bz) ** 2))
+    den = np.sqrt(np.sum(ax**2 + ay**2 + az**2))
+    assert num / den < tol
+    m_ref = float(ref.moment_sums()[0])
+    m_low = float(low.moment_sums()[0])
+    assert abs(m_low - m_ref) / m_ref < 1e-4
+
+
+def test_f64_storage_matches_oracle(cuda):
+    from tensorlbm_b200 import LBMSolver
+
+    n = 12
+    u = _tgv(n)
+    f = O.equilibrium(19, np.ones((n, n, n)), *u)
+    s = LBMSolver("D3Q19", (n, n, n), 0.55, "bgk", device=cuda, storage="f64").load(T(f, cuda)).step(20)
+    ref = f
+    for _ in range(20):
+        ref = O.stream(O.collide_bgk(ref, 0.55))
+    assert rel_err(N(s.f), ref) < 1e-12
+
+
+def test_tau_field_in_fused_step(cuda):
+    from tensorlbm_b200 import LBMSolver
+
+    rng = np.random.default_rng(4)
+    sp = (40, 60)
+    f = O.equilibrium(9, np.ones(sp, np.float32), *(0.05 * rng.standard_normal(sp).astype(np.float32) for _ in range(2)))
+    tf = (0.55 + 0.3 * rng.random(sp)).astype(np.float32)
+    s = LBMSolver("D2Q9", sp, 0.6, "mrt", device=cuda, tau_field=T(tf, cuda)).load(T(f, cuda)).step(3)
+    ref = f
+    for _ in range(3):
+        ref = O.stream(O.collide_mrt(ref, 0.6, tau_field=tf))
+    assert rel_err(N(s.f), ref) < 2e-6
+
+
+def test_periodic_mass_conservation_full_size(cuda):
+    """Size-independent property at 256^3: a periodic box conserves mass (FP64 sum)."""
+    from tensorlbm_b200 import LBMSolver
+
+    n = 256
+    s = LBMSolver("D3Q19", (n, n, n), 0.52, "mrt", device=cuda)
+    ux, uy, uz = (torch.from_numpy(v.astype(np.float32)) for v in _tgv(n))
+    from tensorlbm_b200.d3q19 import equilibrium3d
+
+    f0 = equilibrium3d(torch.ones((n, n, n), device=cuda), ux.to(cuda), uy.to(cuda), uz.to(cuda))
+    s.load(f0)
+    m0 = float(s.moment_sums()[0])
+    s.step(10)
+    m1 = float(s.moment_sums()[0])
+    assert abs(m1 - m0) / m0 < 1e-6
+    assert not s.nonfinite_seen()
+
+
+def test_sphere_channel_full_size_forces_symmetric(cuda):
+    """512x256x256 D3Q19 MRT sphere channel (config size): drag positive, side
+    forces ~0 by symmetry, and the FP64 force of the fused step equals the
+    stand-alone force kernel on the same post-stream state."""
+    from tensorlbm_b200 import LBMSolver, boundaries3d, obstacles
+    from tensorlbm_b200.d3q19 import equilibrium3d
+
+    nz, ny, nx = 256, 256, 512
+    obst = boundaries3d.sphere_mask(nx, ny, nz, 128, 128, 128, 16, cuda)
+    s = LBMSolver("D3Q19", (nz, ny, nx), 3 * 0.04 * 32 / 300 + 0.5, "mrt", device=cuda, obstacle_mask=obst,
+                  u_in=0.04, rho_out=1.0, track_force=True)
+    ux = torch.full((nz, ny, nx), 0.04, device=cuda)
+    ux[obst] = 0.0
+    z = torch.zeros_like(ux)
+    s.load(equilibrium3d(torch.ones_like(ux), ux, z, z))
+    s.step(20)
+    fx, fy, fz = (float(v) for v in s.forces[-1])
+    assert fx > 0 and abs(fy) < 1e-6 * fx and abs(fz) < 1e-6 * fx
+    # stand-alone force on the same post-stream state: stream+BC output before bounce-back equals
+    # the pulled values; recompute from the previous buffer by one more pull without boundaries
+    from tensorlbm_b200 import solver3d
+
+    post = solver3d.stream3d(s._buf[1 - s._cur].float())
+    ref = torch.stack(obstacles.compute_obstacle_forces_3d(post, obst))
+    assert abs(float(ref[0]) - fx) < 1e-9 * abs(fx) + 1e-9

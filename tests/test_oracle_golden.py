@@ -1,0 +1,166 @@
+"""Pin the numpy oracle to TensorLBM: every oracle function against the golden
+vectors produced by the unmodified reference (tests/golden/make_golden.py).
+CPU only."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import lbm as O
+from tests.conftest import golden, rel_err
+
+F32_TOL = 2e-6   # float32 re-association / FMA noise on O(1) populations
+F64_TOL = 1e-12
+
+
+def _tol(dt):
+    return F32_TOL if dt == np.float32 else F64_TOL
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+@pytest.mark.parametrize("q", [9, 19, 27])
+def test_moments_and_equilibrium(q, tag):
+    g = golden(f"moments_d{'2' if q == 9 else '3'}q{q}_{tag}")
+    f = g["f"]
+    rho, ux, uy, uz = O.macroscopic(f)
+    assert rel_err(rho, g["rho"]) < _tol(f.dtype)
+    assert np.max(np.abs(ux - g["ux"])) < 10 * _tol(f.dtype)
+    assert np.max(np.abs(uy - g["uy"])) < 10 * _tol(f.dtype)
+    if q != 9:
+        assert np.max(np.abs(uz - g["uz"])) < 10 * _tol(f.dtype)
+    feq = O.equilibrium(q, g["rho_in"], g["ux_in"], g["uy_in"], None if q == 9 else g["uz_in"])
+    assert feq.dtype == f.dtype
+    assert rel_err(feq, g["feq"]) < _tol(f.dtype)
+
+
+def test_collide_d2q9():
+    g = golden("collide_d2q9_f32")
+    f, tau = g["f"], float(g["tau"])
+    assert rel_err(O.collide_bgk(f, tau), g["bgk"]) < F32_TOL
+    assert rel_err(O.collide_mrt(f, tau), g["mrt"]) < F32_TOL
+    assert rel_err(O.collide_mrt(f, tau, tau_field=g["tau_field"]), g["mrt_field"]) < F32_TOL
+    assert rel_err(O.collide_smagorinsky(f, tau, 0.17), g["smag"]) < F32_TOL
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_collide_d3q19(tag):
+    g = golden(f"collide_d3q19_{tag}")
+    f, tau = g["f"], float(g["tau"])
+    tol = _tol(f.dtype)
+    assert rel_err(O.collide_bgk(f, tau), g["bgk"]) < tol
+    assert rel_err(O.collide_smagorinsky(f, tau, 0.17), g["smag"]) < tol
+    assert rel_err(O.collide_cumulant_d3q19(f, tau, omega_b=1.2, omega_even=0.8), g["cum19"]) < tol
+    assert rel_err(O.collide_cumulant_d3q19(f, tau, omega_b=1.2, omega_even=0.8, c_s=0.17), g["cum19_smag"]) < tol
+    if "mrt" in g:
+        assert rel_err(O.collide_mrt(f, tau), g["mrt"]) < F32_TOL
+        assert rel_err(O.collide_mrt(f, tau, s_e=1.3, s_eps=1.5, s_q=1.1, s_pi=1.25), g["mrt_custom"]) < F32_TOL
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_collide_d3q27(tag):
+    g = golden(f"collide_d3q27_{tag}")
+    f, tau = g["f"], float(g["tau"])
+    tol = _tol(f.dtype)
+    assert rel_err(O.collide_bgk(f, tau), g["bgk"]) < tol
+    assert rel_err(O.collide_smagorinsky(f, tau, 0.17), g["smag"]) < tol
+    assert rel_err(O.collide_cumulant_d3q27(f, tau, 1.1, 1.2, 0.9), g["cum"]) < 5 * tol
+    assert rel_err(O.collide_cumulant_geier_d3q27(f, tau, 1.1, 1.2, 0.9), g["geier"]) < 5 * tol
+    if "mrt" in g:
+        assert rel_err(O.collide_mrt(f, tau), g["mrt"]) < 5 * F32_TOL
+
+
+def test_stream_canary_bitwise():
+    g = golden("stream")
+    for q in (9, 19, 27):
+        assert np.array_equal(O.stream(g[f"f{q}"]), g[f"s{q}"])
+
+
+@pytest.mark.parametrize("q", [9, 19, 27])
+def test_boundaries(q):
+    g = golden(f"bc_d{'2' if q == 9 else '3'}q{q}")
+    f, m = g["f"], g["mask"]
+    assert np.array_equal(O.bounce_back(f, m), g["bb"])
+    if q == 9:
+        assert rel_err(O.zou_he_inlet(f, 0.05, 0.01), g["inlet"]) < F32_TOL
+        assert rel_err(O.zou_he_outlet(f, 1.02), g["outlet"]) < F32_TOL
+        assert rel_err(O.moving_lid(f, 0.07), g["lid"]) < F32_TOL
+    else:
+        assert rel_err(O.zou_he_inlet(f, 0.04, 0.01, -0.005), g["inlet"]) < F32_TOL
+        assert rel_err(O.zou_he_outlet(f, 0.98), g["outlet"]) < F32_TOL
+        if q == 19:
+            assert rel_err(O.moving_lid(f, 0.05), g["lid"]) < F32_TOL
+    ref = g["force"].astype(np.float64)
+    got = O.obstacle_force(f, m)[: len(ref)]
+    assert np.max(np.abs(got - ref)) < 1e-5 * max(np.max(np.abs(ref)), 1.0)
+
+
+def test_masks_bitwise():
+    g = golden("masks")
+    assert np.array_equal(O.sphere_mask(32, 16, 16, 12.0, 8.0, 8.0, 4.5), g["sphere"])
+    assert np.array_equal(O.sphere_mask(40, 24, 20, 17.3, 11.7, 9.1, 6.35), g["sphere_odd"])
+    assert np.array_equal(O.cylinder_mask(200, 50, 25.0, 25.0, 3.125), g["cylinder"])
+    assert np.array_equal(O.cylinder_mask(97, 31, 20.4, 15.5, 4.7), g["cylinder_odd"])
+    big = O.sphere_mask(512, 256, 256, 128, 128, 128, 16)
+    assert int(big.sum()) == int(g["big_count"])
+    assert np.array_equal(np.flatnonzero(big), g["big_index"])
+
+
+def test_missing_mask_and_links():
+    g = golden("masks")
+    sph = g["sphere"]
+    m19 = O.missing_mask(19, sph.shape, sph, periodic=(True, True, False))
+    ref19 = np.unpackbits(g["missing19"])[: m19.size].reshape(tuple(g["missing19_shape"])).astype(bool)
+    assert np.array_equal(m19, ref19)
+    assert np.array_equal(np.argwhere(m19), g["links19"])
+    m27 = O.missing_mask(27, sph.shape, sph, periodic=(False, False, False))
+    ref27 = np.unpackbits(g["missing27"])[: m27.size].reshape(tuple(g["missing27_shape"])).astype(bool)
+    assert np.array_equal(m27, ref27)
+
+
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+@pytest.mark.parametrize("mode", ["fullway", "halfway", "fullway_window"])
+def test_chain_cavity(coll, mode):
+    g = golden(f"chain_cavity_d3q19_{coll}_{mode}")
+    f = g["f0"]
+    nan_step = -1
+    with np.errstate(all="ignore"):
+        for s in range(1, int(g["steps"]) + 1):
+            f = O.cavity_step(f, float(g["tau"]), g["wall"], float(g["u_lid"]), coll,
+                              mode="halfway" if mode == "halfway" else "fullway")
+            if nan_step < 0 and not np.isfinite(f).all():
+                nan_step = s
+    if "nan_step" in g and int(g["nan_step"]) > 0:
+        # the literal chain diverges inside the window: the oracle must blow up
+        # within a step or two of the reference
+        assert nan_step > 0 and abs(nan_step - int(g["nan_step"])) <= 2, (nan_step, int(g["nan_step"]))
+    else:
+        assert nan_step < 0
+        assert rel_err(f, g["f"]) < 1e-4
+
+
+def test_chain_cylinder_d2q9():
+    g = golden("chain_cylinder_d2q9_bgk")
+    f = g["f0"]
+    forces = []
+    for _ in range(int(g["steps"])):
+        f, fo = O.channel_step(f, float(g["tau"]), float(g["u_in"]), 1.0, g["wall"], g["obstacle"], "bgk")
+        forces.append(fo[:2])
+    assert rel_err(f, g["f"]) < 1e-4
+    ref = g["forces"].astype(np.float64)
+    assert np.max(np.abs(np.array(forces) - ref)) < 1e-3 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("name,coll", [("d3q19_mrt", "mrt"), ("d3q19_bgk", "bgk"), ("d3q27_cumulant", "cumulant"),
+                                       ("d3q27_geier", "cumulant_geier"), ("d3q27_bgk", "bgk")])
+def test_chain_sphere(name, coll):
+    g = golden(f"chain_sphere_{name}")
+    f = g["f0"]
+    forces = []
+    for _ in range(int(g["steps"])):
+        f, fo = O.channel_step(f, float(g["tau"]), float(g["u_in"]), 1.0, None, g["obstacle"], coll)
+        forces.append(fo)
+    assert rel_err(f, g["f"]) < 1e-4
+    ref = g["forces"].astype(np.float64)
+    scale = np.max(np.abs(ref[:, 0]))
+    assert np.max(np.abs(np.array(forces)[:, :3] - ref)) < 1e-3 * scale
