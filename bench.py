@@ -438,9 +438,16 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-slab", type=int, default=8, help="z-planes per CPU sample slab")
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--grid", default=None,
+                    help="nx,ny,nz of a smaller channel (profiling only; the sphere keeps its size, centred)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.grid:
+        global NX, NY, NZ, CX, CY, CZ, WORKLOAD
+        NX, NY, NZ = (int(v) for v in args.grid.split(","))
+        CX, CY, CZ = NY // 2, NY // 2, NZ // 2
+        WORKLOAD = f"d3q19_mrt_sphere_channel_{NX}x{NY}x{NZ}"
     if args.impl == "reference":
         run_reference(args)
     else:

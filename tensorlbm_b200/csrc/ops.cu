@@ -76,8 +76,7 @@ __global__ void k_zou_he_inlet(int nx, int ny, int nz, T* f, BcParams<T> bp, con
     const int y = (int)j;
     const T u = uxp ? uxp[y] : bp.u_in;
     const T uy = uyp ? uyp[y] : bp.uy_in;
-    const T omu = uxp ? T(1) - u : bp.one_minus_u;
-    zou_he_inlet_d2q9(v, u, uy, omu);
+    zou_he_inlet_d2q9(v, u, uy);
   } else {
     zou_he_inlet_3d<L>(v, bp.u_in, bp.uy_in, bp.uz_in, bp.one_minus_u);
   }

@@ -64,10 +64,13 @@ BcParams<T> make_bc_params(double u_in0, double u_in1, double u_in2, double rho_
 // the results follow that pairing.
 template <class L>
 __host__ __device__ constexpr int zh_partner(int q) {
-  if (L::Q != 27) return L::opp(q);
-  for (int k = 0; k < L::Q; ++k)
-    if (L::cx(k) == -L::cx(q) && L::cy(k) == L::cy(q) && L::cz(k) == L::cz(q)) return k;
-  return q;
+  if constexpr (L::Q != 27) {
+    return L::opp(q);
+  } else {
+    for (int k = 0; k < L::Q; ++k)
+      if (L::cx(k) == -L::cx(q) && L::cy(k) == L::cy(q) && L::cz(k) == L::cz(q)) return k;
+    return q;
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -118,23 +121,28 @@ __device__ __forceinline__ void zou_he_outlet_3d(T (&f)[L::Q], T rho_out) {
   }
 }
 
-// D2Q9 closed forms (boundaries.py:50-99, :102-125)
+// D2Q9 closed forms (boundaries.py:50-99, :102-125).  The inlet profile is a
+// float32 tensor there, so 1 - u is formed in the field dtype.
 template <typename T>
-__device__ __forceinline__ void zou_he_inlet_d2q9(T (&f)[9], T u, T uy, T one_minus_u) {
-  const T rho = (f[0] + f[2] + f[4] + T(2) * (f[3] + f[6] + f[7])) / one_minus_u;
-  const T d24 = f[2] - f[4];
-  f[1] = f[3] + T(2.0 / 3.0) * rho * u;
-  f[5] = f[7] - T(0.5) * d24 + T(1.0 / 6.0) * rho * u + T(0.5) * rho * uy;
-  f[8] = f[6] + T(0.5) * d24 + T(1.0 / 6.0) * rho * u - T(0.5) * rho * uy;
+__device__ __forceinline__ void zou_he_inlet_d2q9(T (&f)[9], T u, T uy) {
+  const T rho = xdiv(xadd(xadd(xadd(f[0], f[2]), f[4]), xmul(T(2), xadd(xadd(f[3], f[6]), f[7]))), xsub(T(1), u));
+  const T h24 = xmul(T(0.5), xsub(f[2], f[4]));
+  const T r6u = xmul(xmul(T(1.0 / 6.0), rho), u);
+  const T r2uy = xmul(xmul(T(0.5), rho), uy);
+  f[1] = xadd(f[3], xmul(xmul(T(2.0 / 3.0), rho), u));
+  f[5] = xadd(xadd(xsub(f[7], h24), r6u), r2uy);
+  f[8] = xsub(xadd(xadd(f[6], h24), r6u), r2uy);
 }
 template <typename T>
 __device__ __forceinline__ void zou_he_outlet_d2q9(T (&f)[9], T rho_out, T two_thirds_rho_out, T sixth_rho_out) {
-  const T ux = T(-1) + (f[0] + f[2] + f[4] + T(2) * (f[1] + f[5] + f[8])) / rho_out;
-  const T d24 = f[2] - f[4];
+  const T s = xadd(xadd(xadd(f[0], f[2]), f[4]), xmul(T(2), xadd(xadd(f[1], f[5]), f[8])));
+  const T ux = xadd(T(-1), xdiv(s, rho_out));
+  const T h24 = xmul(T(0.5), xsub(f[2], f[4]));
+  const T su = xmul(sixth_rho_out, ux);
   const T f1 = f[1], f5 = f[5], f8 = f[8];
-  f[3] = f1 - two_thirds_rho_out * ux;
-  f[7] = f5 + T(0.5) * d24 - sixth_rho_out * ux;
-  f[6] = f8 - T(0.5) * d24 - sixth_rho_out * ux;
+  f[3] = xsub(f1, xmul(two_thirds_rho_out, ux));
+  f[7] = xsub(xadd(f5, h24), su);
+  f[6] = xsub(xsub(f8, h24), su);
 }
 
 // --------------------------------------------------------------------------
@@ -143,12 +151,13 @@ __device__ __forceinline__ void zou_he_outlet_d2q9(T (&f)[9], T rho_out, T two_t
 // D2Q9: lid_driven_cavity.py:431-473
 template <typename T>
 __device__ __forceinline__ void moving_lid_d2q9(T (&f)[9], T u_lid) {
-  const T rho = f[0] + f[1] + T(2) * f[2] + f[3] + T(2) * f[5] + T(2) * f[6];
-  const T d13 = f[1] - f[3];
+  const T rho = xadd(xadd(xadd(xadd(xadd(f[0], f[1]), xmul(T(2), f[2])), f[3]), xmul(T(2), f[5])), xmul(T(2), f[6]));
+  const T h13 = xmul(T(0.5), xsub(f[1], f[3]));
+  const T ru = xmul(xmul(T(0.5), rho), u_lid);
   const T f2 = f[2], f5 = f[5], f6 = f[6];
   f[4] = f2;
-  f[7] = f5 + T(0.5) * d13 - T(0.5) * rho * u_lid;
-  f[8] = f6 - T(0.5) * d13 + T(0.5) * rho * u_lid;
+  f[7] = xsub(xadd(f5, h13), ru);
+  f[8] = xadd(xsub(f6, h13), ru);
 }
 // D3Q19: boundaries3d.py:324-404 (uy = uz = 0)
 template <typename T>
@@ -158,7 +167,7 @@ __device__ __forceinline__ void moving_lid_d3q19(T (&f)[19], T u_lid) {
   const T rho = sum0 + T(2) * sump;
   const T sx0 = f[1] - f[2] + f[11] - f[12] + f[13] - f[14];
   const T sxp = f[7] - f[10];
-  const T dx = rho * u_lid - (sx0 + sxp);
+  const T dx = xsub(xmul(rho, u_lid), xadd(sx0, sxp));
   const T sz0 = f[5] - f[6] + f[11] - f[12] - f[13] + f[14];
   const T h = T(0.5) * (f[7] + f[10]);
   f[4] = f[3];

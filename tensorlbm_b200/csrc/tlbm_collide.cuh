@@ -13,60 +13,99 @@ namespace tlbm {
 
 template <typename T> struct CollideParams {
   T tau, inv_tau;
+  double inv_tau64;         // RN64(1 / float(tau)) for the exact BGK quotient
   MrtRates<T> mrt;          // s_nu = 1/tau unless a tau field overrides it per cell
   T omega_b, omega_odd, omega_even;
   T c_smag;
-  T smag_coef;              // 18 * C_s^2
+  T smag_coef;              // 18.0 * C_s**2 (turbulence.py:206)
+  T smag_coef_cum;          // 18.0 * C_s * C_s (cumulant.py:1352), rounded differently in double
+  T omega_b_minus_omega;    // omega_b - 1/tau formed in double, as a python scalar
+  T keep_even;              // 1 - omega_even
   T tau_sq;                 // tau^2
   T tau_eff_max;            // max(1, tau + 0.5), turbulence.py:88-99
 };
 
+// ---------------------------------------------------------------------------
+// Reference-exact arithmetic.  TensorLBM evaluates its elementwise operators
+// as separate torch kernels: every +, -, *, / is rounded on its own (no fused
+// multiply-add) and divisions are IEEE divisions.  x* keep that rounding in
+// device code (the compiler may not contract them), so the elementwise
+// operators below reproduce the reference bit for bit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
 // sum of +-x, +-y, +-z terms for compile-time components a, b, c in {-1, 0, 1}
+// (c_x u_x + c_y u_y + c_z u_z with exact integer products; only additions round)
 template <typename T>
 __device__ __forceinline__ T signed_sum(int a, int b, int c, T x, T y, T z) {
   T r = T(0);
   bool any = false;
   if (a != 0) { r = (a > 0) ? x : -x; any = true; }
-  if (b != 0) { r = any ? ((b > 0) ? r + y : r - y) : ((b > 0) ? y : -y); any = true; }
-  if (c != 0) { r = any ? ((c > 0) ? r + z : r - z) : ((c > 0) ? z : -z); any = true; }
+  if (b != 0) { r = any ? ((b > 0) ? xadd(r, y) : xsub(r, y)) : ((b > 0) ? y : -y); any = true; }
+  if (c != 0) { r = any ? ((c > 0) ? xadd(r, z) : xsub(r, z)) : ((c > 0) ? z : -z); any = true; }
   return r;
 }
 
+// torch's CPU sum over the direction axis of a (Q, ...) tensor accumulates
+// directions 0..15 in order, directions 16..Q-1 in order, and adds the two
+// partial sums (a 16-row cascade; measured bit for bit against torch 2.11).
+// csum<L>(f, coeff) returns that sum of coeff(q) * f[q] for integer
+// coefficients in {-1, 0, 1}; zero terms are skipped (adding a zero product
+// does not change a non-zero sum).
+template <class L, typename T, typename Coef>
+__device__ __forceinline__ T csum(const T (&f)[L::Q], Coef coeff) {
+  T head = T(0), tail = T(0);
+  bool bh = false, bt = false;
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    const int c = coeff(q);
+    if (c == 0) continue;
+    const T v = c > 0 ? f[q] : -f[q];
+    if (q < 16) { head = bh ? xadd(head, v) : v; bh = true; }
+    else { tail = bt ? xadd(tail, v) : v; bt = true; }
+  }
+  if (bh && bt) return xadd(tail, head);
+  return bh ? head : tail;
+}
+
+struct OneCoef { __host__ __device__ constexpr int operator()(int) const { return 1; } };
+template <class L> struct CxCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cx(q); } };
+template <class L> struct CyCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cy(q); } };
+template <class L> struct CzCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cz(q); } };
+
 // rho = sum f, u = sum c f / max(rho, 1e-12): d2q9.py:61-74, d3q19.py:165-186,
-// d3q27.py:395-420.  Sums run in direction order like torch's dim-0 sum.
+// d3q27.py:395-420, in the reference's summation order and rounding.
 template <class L, typename T>
 __device__ __forceinline__ void macroscopic(const T (&f)[L::Q], T& rho, T& ux, T& uy, T& uz) {
-  rho = f[0];
-#pragma unroll
-  for (int q = 1; q < L::Q; ++q) rho += f[q];
-  T jx = T(0), jy = T(0), jz = T(0);
-  bool bx = false, by = false, bz = false;
-#pragma unroll
-  for (int q = 1; q < L::Q; ++q) {
-    if (L::cx(q) != 0) { jx = bx ? (L::cx(q) > 0 ? jx + f[q] : jx - f[q]) : (L::cx(q) > 0 ? f[q] : -f[q]); bx = true; }
-    if (L::cy(q) != 0) { jy = by ? (L::cy(q) > 0 ? jy + f[q] : jy - f[q]) : (L::cy(q) > 0 ? f[q] : -f[q]); by = true; }
-    if (L::cz(q) != 0) { jz = bz ? (L::cz(q) > 0 ? jz + f[q] : jz - f[q]) : (L::cz(q) > 0 ? f[q] : -f[q]); bz = true; }
-  }
+  rho = csum<L>(f, OneCoef{});
   const T rs = rho > T(1e-12) ? rho : T(1e-12);
-  const T ir = T(1) / rs;
-  ux = jx * ir;
-  uy = jy * ir;
-  uz = (L::DIM == 3) ? jz * ir : T(0);
+  ux = xdiv(csum<L>(f, CxCoef<L>{}), rs);
+  uy = xdiv(csum<L>(f, CyCoef<L>{}), rs);
+  uz = (L::DIM == 3) ? xdiv(csum<L>(f, CzCoef<L>{}), rs) : T(0);
 }
 
 // f_eq = w rho (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u.u): d2q9.py:39-58,
-// d3q19.py:83-125, d3q27.py:353-392.
+// d3q19.py:83-125, d3q27.py:353-392, evaluated as
+// (w*rho) * (((1 + 3*cu) + (4.5*cu)*cu) - 1.5*usq), one rounding per operation.
 template <class L, typename T>
 __device__ __forceinline__ T usq_of(T ux, T uy, T uz) {
-  return (L::DIM == 3) ? ux * ux + uy * uy + uz * uz : ux * ux + uy * uy;
+  return (L::DIM == 3) ? xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz)) : xadd(xmul(ux, ux), xmul(uy, uy));
 }
 
 template <class L, typename T>
 __device__ __forceinline__ T feq_q(int q, T rho, T ux, T uy, T uz, T usq) {
-  const T wr = weight<L, T>(q) * rho;
-  if (L::cx(q) == 0 && L::cy(q) == 0 && L::cz(q) == 0) return wr * (T(1) - T(1.5) * usq);
+  const T wr = xmul(weight<L, T>(q), rho);
+  if (L::cx(q) == 0 && L::cy(q) == 0 && L::cz(q) == 0) return xmul(wr, xsub(T(1), xmul(T(1.5), usq)));
   const T cu = signed_sum(L::cx(q), L::cy(q), L::cz(q), ux, uy, uz);
-  return wr * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+  const T inner = xsub(xadd(xadd(T(1), xmul(T(3), cu)), xmul(xmul(T(4.5), cu), cu)), xmul(T(1.5), usq));
+  return xmul(wr, inner);
 }
 
 template <class L, typename T>
@@ -76,18 +115,64 @@ __device__ __forceinline__ void equilibrium(T rho, T ux, T uy, T uz, T (&fe)[L::
   for (int q = 0; q < L::Q; ++q) fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
 }
 
+// Correctly rounded a / b for a float32 divisor used many times, from one
+// float64 reciprocal: RN32(RN64(a * RN64(1/b))).  The float64 product lies
+// within 2^-52 (relative) of a/b.  A quotient of two float32 numbers is never
+// a float32 rounding boundary (a boundary m has an odd 25-bit significand, so
+// m*b cannot fit in 24 bits) and lies at least 2^-49 (relative) from every
+// boundary, so the float64 product rounds to float32 exactly as a/b does.
+// For float64 fields the division itself is used.
+__device__ __forceinline__ float div_by(float a, float, double inv_b) { return __double2float_rn(__dmul_rn((double)a, inv_b)); }
+__device__ __forceinline__ double div_by(double a, double b, double) { return __ddiv_rn(a, b); }
+
+// Fused-arithmetic moments and equilibrium for the operators whose reference
+// goes through BLAS matrix products (MRT, D3Q27 cumulants): same operators,
+// rounding of a fused multiply-add pipeline, cheaper than the exact forms.
+template <class L, typename T>
+__device__ __forceinline__ void macroscopic_fused(const T (&f)[L::Q], T& rho, T& ux, T& uy, T& uz) {
+  rho = f[0];
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) rho += f[q];
+  T jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) {
+    if (L::cx(q) != 0) jx = (L::cx(q) > 0) ? jx + f[q] : jx - f[q];
+    if (L::cy(q) != 0) jy = (L::cy(q) > 0) ? jy + f[q] : jy - f[q];
+    if (L::cz(q) != 0) jz = (L::cz(q) > 0) ? jz + f[q] : jz - f[q];
+  }
+  const T ir = T(1) / (rho > T(1e-12) ? rho : T(1e-12));
+  ux = jx * ir;
+  uy = jy * ir;
+  uz = (L::DIM == 3) ? jz * ir : T(0);
+}
+template <class L, typename T>
+__device__ __forceinline__ T feq_fused(int q, T rho, T ux, T uy, T uz, T usq) {
+  const T wr = weight<L, T>(q) * rho;
+  if (L::cx(q) == 0 && L::cy(q) == 0 && L::cz(q) == 0) return wr * (T(1) - T(1.5) * usq);
+  T cu = T(0);
+  if (L::cx(q) != 0) cu = (L::cx(q) > 0) ? cu + ux : cu - ux;
+  if (L::cy(q) != 0) cu = (L::cy(q) > 0) ? cu + uy : cu - uy;
+  if (L::cz(q) != 0) cu = (L::cz(q) > 0) ? cu + uz : cu - uz;
+  return wr * (T(1) + cu * (T(3) + T(4.5) * cu) - T(1.5) * usq);
+}
+template <class L, typename T>
+__device__ __forceinline__ T usq_fused(T ux, T uy, T uz) {
+  return (L::DIM == 3) ? ux * ux + uy * uy + uz * uz : ux * ux + uy * uy;
+}
+
 // ---------------------------------------------------------------------------
-// BGK: f - (f - feq)/tau (solver.py:67-71, solver3d.py:100-104, d3q27.py:423-437)
+// BGK: f - (f - feq)/tau (solver.py:67-71, solver3d.py:100-104, d3q27.py:423-437),
+// bit-exact: (f - feq)/tau is the correctly rounded quotient, like torch's.
 // ---------------------------------------------------------------------------
 template <class L, typename T>
-__device__ __forceinline__ void collide_bgk(T (&f)[L::Q], T inv_tau) {
+__device__ __forceinline__ void collide_bgk(T (&f)[L::Q], T tau, double inv_tau64) {
   T rho, ux, uy, uz;
   macroscopic<L>(f, rho, ux, uy, uz);
   const T usq = usq_of<L>(ux, uy, uz);
 #pragma unroll
   for (int q = 0; q < L::Q; ++q) {
     const T fe = feq_q<L>(q, rho, ux, uy, uz, usq);
-    f[q] = f[q] - (f[q] - fe) * inv_tau;
+    f[q] = xsub(f[q], div_by(xsub(f[q], fe), tau, inv_tau64));
   }
 }
 
@@ -98,11 +183,11 @@ __device__ __forceinline__ void collide_bgk(T (&f)[L::Q], T inv_tau) {
 template <class L, typename T>
 __device__ __forceinline__ void collide_mrt(T (&f)[L::Q], const MrtRates<T>& r) {
   T rho, ux, uy, uz;
-  macroscopic<L>(f, rho, ux, uy, uz);
-  const T usq = usq_of<L>(ux, uy, uz);
+  macroscopic_fused<L>(f, rho, ux, uy, uz);
+  const T usq = usq_fused<L>(ux, uy, uz);
   T fn[L::Q];
 #pragma unroll
-  for (int q = 0; q < L::Q; ++q) fn[q] = f[q] - feq_q<L>(q, rho, ux, uy, uz, usq);
+  for (int q = 0; q < L::Q; ++q) fn[q] = f[q] - feq_fused<L>(q, rho, ux, uy, uz, usq);
   if constexpr (L::Q == 9) mrt_relax_d2q9<T>(f, fn, r);
   else if constexpr (L::Q == 19) mrt_relax_d3q19<T>(f, fn, r);
   else mrt_relax_d3q27<T>(f, fn, r);
@@ -113,43 +198,60 @@ __device__ __forceinline__ void collide_mrt(T (&f)[L::Q], const MrtRates<T>& r) 
 // ---------------------------------------------------------------------------
 template <typename T> struct Pi6 { T xx, yy, zz, xy, xz, yz; };
 
+template <class L> struct CxxCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cx(q) * L::cx(q); } };
+template <class L> struct CyyCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cy(q) * L::cy(q); } };
+template <class L> struct CzzCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cz(q) * L::cz(q); } };
+template <class L> struct CxyCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cx(q) * L::cy(q); } };
+template <class L> struct CxzCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cx(q) * L::cz(q); } };
+template <class L> struct CyzCoef { __host__ __device__ constexpr int operator()(int q) const { return L::cy(q) * L::cz(q); } };
+
+// (c_a c_b * fneq).sum(0) in the reference's summation order
 template <class L, typename T>
 __device__ __forceinline__ Pi6<T> neq_stress(const T (&fn)[L::Q]) {
-  Pi6<T> p{T(0), T(0), T(0), T(0), T(0), T(0)};
-  bool bxx = false, byy = false, bzz = false, bxy = false, bxz = false, byz = false;
-#pragma unroll
-  for (int q = 0; q < L::Q; ++q) {
-    const int a = L::cx(q), b = L::cy(q), c = L::cz(q);
-    if (a != 0) { p.xx = bxx ? p.xx + fn[q] : fn[q]; bxx = true; }
-    if (b != 0) { p.yy = byy ? p.yy + fn[q] : fn[q]; byy = true; }
-    if (c != 0) { p.zz = bzz ? p.zz + fn[q] : fn[q]; bzz = true; }
-    if (a * b != 0) { p.xy = bxy ? (a * b > 0 ? p.xy + fn[q] : p.xy - fn[q]) : (a * b > 0 ? fn[q] : -fn[q]); bxy = true; }
-    if (a * c != 0) { p.xz = bxz ? (a * c > 0 ? p.xz + fn[q] : p.xz - fn[q]) : (a * c > 0 ? fn[q] : -fn[q]); bxz = true; }
-    if (b * c != 0) { p.yz = byz ? (b * c > 0 ? p.yz + fn[q] : p.yz - fn[q]) : (b * c > 0 ? fn[q] : -fn[q]); byz = true; }
+  Pi6<T> p;
+  p.xx = csum<L>(fn, CxxCoef<L>{});
+  p.yy = csum<L>(fn, CyyCoef<L>{});
+  p.xy = csum<L>(fn, CxyCoef<L>{});
+  if constexpr (L::DIM == 3) {
+    p.zz = csum<L>(fn, CzzCoef<L>{});
+    p.xz = csum<L>(fn, CxzCoef<L>{});
+    p.yz = csum<L>(fn, CyzCoef<L>{});
+  } else {
+    p.zz = p.xz = p.yz = T(0);
   }
   return p;
+}
+
+// |Pi|_F^2: pxx^2 + pyy^2 [+ pzz^2] + 2 (pxy^2 [+ pxz^2 + pyz^2])
+template <class L, typename T>
+__device__ __forceinline__ T stress_radicand(const Pi6<T>& p) {
+  if constexpr (L::DIM == 3) {
+    const T diag = xadd(xadd(xmul(p.xx, p.xx), xmul(p.yy, p.yy)), xmul(p.zz, p.zz));
+    const T off = xadd(xadd(xmul(p.xy, p.xy), xmul(p.xz, p.xz)), xmul(p.yz, p.yz));
+    return xadd(diag, xmul(T(2), off));
+  } else {
+    return xadd(xadd(xmul(p.xx, p.xx), xmul(p.yy, p.yy)), xmul(T(2), xmul(p.xy, p.xy)));
+  }
 }
 
 // Hou-1994 tau_eff with the clamps of turbulence.py:183-208 (norm clamp of
 // :128-140 / :170-181).
 template <class L, typename T>
 __device__ __forceinline__ T smagorinsky_tau(const Pi6<T>& p, T rho, const CollideParams<T>& cp) {
-  T rad = (L::DIM == 3)
-              ? p.xx * p.xx + p.yy * p.yy + p.zz * p.zz + T(2) * (p.xy * p.xy + p.xz * p.xz + p.yz * p.yz)
-              : p.xx * p.xx + p.yy * p.yy + T(2) * p.xy * p.xy;
+  T rad = stress_radicand<L>(p);
   rad = rad > T(1e-30) ? rad : T(1e-30);
   const T pi_norm = sqrt(rad);
   const T rs = rho > T(1e-12) ? rho : T(1e-12);
-  T disc = cp.tau_sq + cp.smag_coef * pi_norm / rs;
+  T disc = xadd(cp.tau_sq, xdiv(xmul(cp.smag_coef, pi_norm), rs));
   disc = disc > T(0) ? disc : T(0);
-  T te = T(0.5) * (cp.tau + sqrt(disc));
+  T te = xmul(T(0.5), xadd(cp.tau, sqrt(disc)));
   te = te < T(0.5001) ? T(0.5001) : te;
   te = te > cp.tau_eff_max ? cp.tau_eff_max : te;
   return te;
 }
 
-// BGK with per-cell Smagorinsky tau_eff: turbulence.py:216-230 (D2Q9),
-// :245-261 (D3Q19), :472 (D3Q27).
+// BGK with per-cell Smagorinsky tau_eff, f - f_neq / tau_eff:
+// turbulence.py:216-230 (D2Q9), :245-261 (D3Q19), :472-494 (D3Q27).
 template <class L, typename T>
 __device__ __forceinline__ void collide_smagorinsky(T (&f)[L::Q], const CollideParams<T>& cp) {
   T rho, ux, uy, uz;
@@ -157,17 +259,30 @@ __device__ __forceinline__ void collide_smagorinsky(T (&f)[L::Q], const CollideP
   const T usq = usq_of<L>(ux, uy, uz);
   T fn[L::Q];
 #pragma unroll
-  for (int q = 0; q < L::Q; ++q) fn[q] = f[q] - feq_q<L>(q, rho, ux, uy, uz, usq);
+  for (int q = 0; q < L::Q; ++q) fn[q] = xsub(f[q], feq_q<L>(q, rho, ux, uy, uz, usq));
   const Pi6<T> p = neq_stress<L>(fn);
-  const T inv_te = T(1) / smagorinsky_tau<L>(p, rho, cp);
+  const T te = smagorinsky_tau<L>(p, rho, cp);
 #pragma unroll
-  for (int q = 0; q < L::Q; ++q) f[q] = f[q] - fn[q] * inv_te;
+  const double inv_te = 1.0 / double(te);
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) f[q] = xsub(f[q], div_by(fn[q], te, inv_te));
 }
 
 // ---------------------------------------------------------------------------
 // D3Q19 "cumulant": Hermite-regularised relaxation of the stress with a
-// separate bulk rate and a damped higher-order remainder (cumulant.py:1159-1420).
+// separate bulk rate and a damped higher-order remainder (cumulant.py:1159-1420),
+// with the reference's evaluation order.
 // ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T hermite_contract(int a, int b, int c, T hxx, T hyy, T hzz, const Pi6<T>& s) {
+  // h_xx s_xx + h_yy s_yy + h_zz s_zz + (2 h_xy) s_xy + (2 h_xz) s_xz + (2 h_yz) s_yz
+  T r = xadd(xadd(xmul(hxx, s.xx), xmul(hyy, s.yy)), xmul(hzz, s.zz));
+  if (a * b != 0) r = xadd(r, xmul(T(2 * a * b), s.xy));
+  if (a * c != 0) r = xadd(r, xmul(T(2 * a * c), s.xz));
+  if (b * c != 0) r = xadd(r, xmul(T(2 * b * c), s.yz));
+  return r;
+}
+
 template <typename T>
 __device__ __forceinline__ void collide_cumulant_d3q19(T (&f)[19], const CollideParams<T>& cp) {
   using L = D3Q19;
@@ -178,36 +293,37 @@ __device__ __forceinline__ void collide_cumulant_d3q19(T (&f)[19], const Collide
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
     fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
-    fn[q] = f[q] - fe[q];
+    fn[q] = xsub(f[q], fe[q]);
   }
   const Pi6<T> p = neq_stress<L>(fn);
   T omega = cp.inv_tau;
+  T omb_minus_om = cp.omega_b_minus_omega;
   if (cp.c_smag > T(0)) {
     // cumulant.py:1349-1353: no norm or tau clamps on this path
-    const T pn = sqrt(p.xx * p.xx + p.yy * p.yy + p.zz * p.zz + T(2) * (p.xy * p.xy + p.xz * p.xz + p.yz * p.yz));
+    const T pn = sqrt(stress_radicand<L>(p));
     const T rs = rho > T(1e-12) ? rho : T(1e-12);
-    const T te = T(0.5) * (cp.tau + sqrt(cp.tau * cp.tau + cp.smag_coef * pn / rs));
-    omega = T(1) / te;
+    const T te = xmul(T(0.5), xadd(cp.tau, sqrt(xadd(cp.tau_sq, xdiv(xmul(cp.smag_coef_cum, pn), rs)))));
+    omega = xdiv(T(1), te);
+    omb_minus_om = xsub(cp.omega_b, omega);
   }
-  const T tr = p.xx + p.yy + p.zz;
-  const T bulk = (cp.omega_b - omega) * tr / T(3);
-  const Pi6<T> s{p.xx - omega * p.xx - bulk, p.yy - omega * p.yy - bulk, p.zz - omega * p.zz - bulk,
-                 p.xy - omega * p.xy, p.xz - omega * p.xz, p.yz - omega * p.yz};
-  const T cs2 = T(1) / T(3);
-  const T keep = T(1) - cp.omega_even;
+  const T tr = xadd(xadd(p.xx, p.yy), p.zz);
+  const T bulk = xdiv(xmul(omb_minus_om, tr), T(3));
+  Pi6<T> s;
+  s.xx = xsub(xsub(p.xx, xmul(omega, p.xx)), bulk);
+  s.yy = xsub(xsub(p.yy, xmul(omega, p.yy)), bulk);
+  s.zz = xsub(xsub(p.zz, xmul(omega, p.zz)), bulk);
+  s.xy = xsub(p.xy, xmul(omega, p.xy));
+  s.xz = xsub(p.xz, xmul(omega, p.xz));
+  s.yz = xsub(p.yz, xmul(omega, p.yz));
+  const T cs2 = T(1.0 / 3.0);
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
     const int a = L::cx(q), b = L::cy(q), c = L::cz(q);
-    const T hxx = T(a * a) - cs2, hyy = T(b * b) - cs2, hzz = T(c * c) - cs2;
-    const T w45 = T(4.5) * weight<L, T>(q);
-    T hs = hxx * s.xx + hyy * s.yy + hzz * s.zz;
-    T hp = hxx * p.xx + hyy * p.yy + hzz * p.zz;
-    if (a * b != 0) { hs += T(2 * a * b) * s.xy; hp += T(2 * a * b) * p.xy; }
-    if (a * c != 0) { hs += T(2 * a * c) * s.xz; hp += T(2 * a * c) * p.xz; }
-    if (b * c != 0) { hs += T(2 * b * c) * s.yz; hp += T(2 * b * c) * p.yz; }
-    const T reg = w45 * hs;
-    const T ho = fn[q] - w45 * hp;
-    f[q] = fe[q] + reg + keep * ho;
+    const T hxx = xsub(T(a * a), cs2), hyy = xsub(T(b * b), cs2), hzz = xsub(T(c * c), cs2);
+    const T w45 = xmul(T(4.5), weight<L, T>(q));
+    const T reg = xmul(w45, hermite_contract(a, b, c, hxx, hyy, hzz, s));
+    const T ho = xsub(fn[q], xmul(w45, hermite_contract(a, b, c, hxx, hyy, hzz, p)));
+    f[q] = xadd(xadd(fe[q], reg), xmul(cp.keep_even, ho));
   }
 }
 
@@ -374,12 +490,12 @@ template <typename T>
 __device__ __forceinline__ void collide_cumulant_legacy(T (&f)[27], const CollideParams<T>& cp) {
   using L = D3Q27;
   T rho, ux, uy, uz;
-  macroscopic<L>(f, rho, ux, uy, uz);
-  const T usq = usq_of<L>(ux, uy, uz);
+  macroscopic_fused<L>(f, rho, ux, uy, uz);
+  const T usq = usq_fused<L>(ux, uy, uz);
   T fe[27], fn[27];
 #pragma unroll
   for (int q = 0; q < 27; ++q) {
-    fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
+    fe[q] = feq_fused<L>(q, rho, ux, uy, uz, usq);
     fn[q] = f[q] - fe[q];
   }
   Cube<T> g;
@@ -475,11 +591,11 @@ template <typename T>
 __device__ __forceinline__ void collide_cumulant_geier(T (&f)[27], const CollideParams<T>& cp) {
   using L = D3Q27;
   T rho, ux, uy, uz;
-  macroscopic<L>(f, rho, ux, uy, uz);
-  const T usq = usq_of<L>(ux, uy, uz);
+  macroscopic_fused<L>(f, rho, ux, uy, uz);
+  const T usq = usq_fused<L>(ux, uy, uz);
   T fe[27];
 #pragma unroll
-  for (int q = 0; q < 27; ++q) fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
+  for (int q = 0; q < 27; ++q) fe[q] = feq_fused<L>(q, rho, ux, uy, uz, usq);
   Cube<T> g;
   T c[27], ce[27];
   central_moments(fe, ux, uy, uz, g);
@@ -513,7 +629,8 @@ __device__ __forceinline__ void collide_cumulant_geier(T (&f)[27], const Collide
 template <class L, int COLL, typename T>
 __device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp, T tau_cell, bool has_tau_cell) {
   if constexpr (COLL == TLBM_COLL_BGK) {
-    collide_bgk<L>(f, has_tau_cell ? T(1) / tau_cell : cp.inv_tau);
+    if (has_tau_cell) collide_bgk<L>(f, tau_cell, 1.0 / double(tau_cell));
+    else collide_bgk<L>(f, cp.tau, cp.inv_tau64);
   } else if constexpr (COLL == TLBM_COLL_MRT) {
     MrtRates<T> r = cp.mrt;
     if (has_tau_cell) r.s_nu = T(1) / tau_cell;
@@ -538,6 +655,7 @@ CollideParams<T> make_collide_params(double tau, double s_e, double s_eps, doubl
   CollideParams<T> cp;
   cp.tau = T(tau);
   cp.inv_tau = T(1.0 / tau);
+  cp.inv_tau64 = 1.0 / double(T(tau));
   cp.mrt.s_e = T(s_e);
   cp.mrt.s_eps = T(s_eps);
   cp.mrt.s_q = T(s_q);
@@ -547,7 +665,10 @@ CollideParams<T> make_collide_params(double tau, double s_e, double s_eps, doubl
   cp.omega_odd = T(omega_odd);
   cp.omega_even = T(omega_even);
   cp.c_smag = T(c_smag);
-  cp.smag_coef = T(18.0 * c_smag * c_smag);
+  cp.smag_coef = T(18.0 * (c_smag * c_smag));
+  cp.smag_coef_cum = T(18.0 * c_smag * c_smag);
+  cp.omega_b_minus_omega = T(omega_b - 1.0 / tau);
+  cp.keep_even = T(1.0 - omega_even);
   cp.tau_sq = T(tau * tau);
   cp.tau_eff_max = T(tau + 0.5 > 1.0 ? tau + 0.5 : 1.0);
   return cp;

@@ -27,70 +27,83 @@ __device__ __forceinline__ void accumulate_force(double* force, bool any_in_warp
   }
 }
 
+// One domain as seen by the per-cell update.
+template <typename SI, typename SO> struct Domain {
+  const SI* fin;
+  SO* fout;
+  const uint8_t* flags;     // may be null
+  const float* tau_field;   // may be null
+  double* force;            // may be null
+  unsigned int* status;     // may be null
+  int nx, ny, nz;
+  long long plane, n;
+  uint32_t bc;
+};
+
+// The update of cell (x, y, z) of one domain.  Every thread of a warp must
+// call it (inactive ones with active = false) because the force reduction is
+// warp-wide.
 // PULL = true : gather from neighbours, boundaries, collide (COLL may be NONE)
 // PULL = false: local collide / format conversion only (no boundaries)
 template <class L, typename SI, typename SO, int COLL, bool PULL>
-__global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typename Storage<SI>::T> cp,
-                                              BcParams<typename Storage<SI>::T> bp) {
+__device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int y, int z, bool active,
+                                            const CollideParams<typename Storage<SI>::T>& cp,
+                                            const BcParams<typename Storage<SI>::T>& bp) {
   using T = typename Storage<SI>::T;
   constexpr int Q = L::Q;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  const bool active = (x < p.nx) && (y < p.ny);
-  const long long N = p.n;
-  const long long cell = (long long)z * p.plane + (long long)y * p.nx + x;
-  const SI* __restrict__ fin = static_cast<const SI*>(p.f_in);
-  SO* __restrict__ fout = static_cast<SO*>(p.f_out);
+  const long long N = d.n;
+  const long long cell = (long long)z * d.plane + (long long)y * d.nx + x;
+  const SI* __restrict__ fin = d.fin;
+  SO* __restrict__ fout = d.fout;
 
   T f[Q];
   uint8_t fl = 0;
   if (active) {
     if constexpr (PULL) {
-      const int xm = (x == 0) ? p.nx - 1 : x - 1;
-      const int xp = (x == p.nx - 1) ? 0 : x + 1;
-      const int ym = (y == 0) ? p.ny - 1 : y - 1;
-      const int yp = (y == p.ny - 1) ? 0 : y + 1;
-      const int zm = (z == 0) ? p.nz - 1 : z - 1;
-      const int zp = (z == p.nz - 1) ? 0 : z + 1;
+      const int xm = (x == 0) ? d.nx - 1 : x - 1;
+      const int xp = (x == d.nx - 1) ? 0 : x + 1;
+      const int ym = (y == 0) ? d.ny - 1 : y - 1;
+      const int yp = (y == d.ny - 1) ? 0 : y + 1;
+      const int zm = (z == 0) ? d.nz - 1 : z - 1;
+      const int zp = (z == d.nz - 1) ? 0 : z + 1;
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         // source = cell - c_q
         const int sx = L::cx(q) > 0 ? xm : (L::cx(q) < 0 ? xp : x);
         const int sy = L::cy(q) > 0 ? ym : (L::cy(q) < 0 ? yp : y);
         const int sz = L::cz(q) > 0 ? zm : (L::cz(q) < 0 ? zp : z);
-        const long long src = (long long)sz * p.plane + (long long)sy * p.nx + sx;
+        const long long src = (long long)sz * d.plane + (long long)sy * d.nx + sx;
         f[q] = Storage<SI>::load(__ldg(fin + (long long)q * N + src), weight<L, T>(q));
       }
     } else {
 #pragma unroll
       for (int q = 0; q < Q; ++q) f[q] = Storage<SI>::load(fin[(long long)q * N + cell], weight<L, T>(q));
     }
-    if (p.flags) fl = p.flags[cell];
+    if (d.flags) fl = d.flags[cell];
   }
 
   if constexpr (PULL) {
     // 1. momentum-exchange force sample (post-stream, pre-bounce-back)
-    if (p.force) {
+    if (d.force) {
       const bool ob = active && (fl & TLBM_FLAG_OBSTACLE);
       T mx = T(0), my = T(0), mz = T(0);
       if (ob) cell_momentum<L>(f, mx, my, mz);
-      accumulate_force(p.force, __any_sync(0xffffffffu, ob), mx, my, mz);
+      accumulate_force(d.force, __any_sync(0xffffffffu, ob), mx, my, mz);
     }
     if (active) {
       // 2. Zou/He inlet / outlet planes
-      if ((p.bc & TLBM_BC_ZH_INLET) && x == 0) {
-        if constexpr (Q == 9) zou_he_inlet_d2q9(f, bp.u_in, bp.uy_in, bp.one_minus_u);
+      if ((d.bc & TLBM_BC_ZH_INLET) && x == 0) {
+        if constexpr (Q == 9) zou_he_inlet_d2q9(f, bp.u_in, bp.uy_in);
         else zou_he_inlet_3d<L>(f, bp.u_in, bp.uy_in, bp.uz_in, bp.one_minus_u);
       }
-      if ((p.bc & TLBM_BC_ZH_OUTLET) && x == p.nx - 1) {
+      if ((d.bc & TLBM_BC_ZH_OUTLET) && x == d.nx - 1) {
         if constexpr (Q == 9) zou_he_outlet_d2q9(f, bp.rho_out, bp.two_thirds_rho_out, bp.sixth_rho_out);
         else zou_he_outlet_3d<L>(f, bp.rho_out);
       }
       // 3. full-way bounce-back
       if (fl & TLBM_FLAG_SOLID) bounce_back<L>(f);
       // 4. moving lid
-      if ((p.bc & TLBM_BC_LID) && y == p.ny - 1) {
+      if ((d.bc & TLBM_BC_LID) && y == d.ny - 1) {
         if constexpr (Q == 9) moving_lid_d2q9(f, bp.u_lid);
         else if constexpr (Q == 19) moving_lid_d3q19(f, bp.u_lid);
       }
@@ -103,17 +116,39 @@ __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typena
       // pre-stream half-way wall: keep the populations, reversed, uncollided
       bounce_back<L>(f);
     } else {
-      const bool has_tau = p.tau_field != nullptr;
-      const T tau_cell = has_tau ? T(p.tau_field[cell]) : T(0);
+      const bool has_tau = d.tau_field != nullptr;
+      const T tau_cell = has_tau ? T(d.tau_field[cell]) : T(0);
       collide<L, COLL>(f, cp, tau_cell, has_tau);
-      if (p.status) {
+      if (d.status) {
         const T r = f[0];
-        if (!(r == r) || r - r != T(0)) atomicOr(p.status, 1u);
+        if (!(r == r) || r - r != T(0)) atomicOr(d.status, 1u);
       }
     }
   }
 #pragma unroll
   for (int q = 0; q < Q; ++q) fout[(long long)q * N + cell] = Storage<SO>::store(f[q], weight<L, T>(q));
+}
+
+template <class L, typename SI, typename SO, int COLL, bool PULL>
+__global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typename Storage<SI>::T> cp,
+                                              BcParams<typename Storage<SI>::T> bp) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  Domain<SI, SO> d;
+  d.fin = static_cast<const SI*>(p.f_in);
+  d.fout = static_cast<SO*>(p.f_out);
+  d.flags = p.flags;
+  d.tau_field = p.tau_field;
+  d.force = p.force;
+  d.status = p.status;
+  d.nx = p.nx;
+  d.ny = p.ny;
+  d.nz = p.nz;
+  d.plane = p.plane;
+  d.n = p.n;
+  d.bc = p.bc;
+  cell_update<L, SI, SO, COLL, PULL>(d, x, y, z, (x < p.nx) && (y < p.ny), cp, bp);
 }
 
 inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block) {

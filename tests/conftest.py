@@ -37,6 +37,13 @@ def cuda():
     return torch.device("cuda", 0)
 
 
+def same(a, b) -> bool:
+    """Bitwise equality of two arrays (NaN == NaN), shapes and dtypes included."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return a.shape == b.shape and a.dtype == b.dtype and np.array_equal(a, b, equal_nan=True)
+
+
 def rel_err(a, b) -> float:
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)

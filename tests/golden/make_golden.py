@@ -101,8 +101,10 @@ def main() -> None:
         np.savez_compressed(HERE / f"{name}.npz", **out)
         print(f"  {name}.npz  ({(HERE / f'{name}.npz').stat().st_size / 1024:.0f} KB)")
 
-    sp2 = (6, 7)            # (ny, nx)
-    sp3 = (4, 5, 6)         # (nz, ny, nx)
+    # inner sizes are multiples of 32, where torch's CPU reduction over the
+    # direction axis follows one fixed order for every cell (see oracle.lbm.sum0)
+    sp2 = (8, 8)            # (ny, nx)
+    sp3 = (4, 4, 8)         # (nz, ny, nx)
     tau = 0.6
 
     print("moments / equilibrium")
@@ -267,8 +269,8 @@ def main() -> None:
              forces=torch.stack(forces))
 
     # D2Q9 cylinder channel with walls: cylinder_flow.py:854-899 (zou_he outlet mode)
-    ny2, nx2 = 20, 60
-    obst2 = b2.cylinder_mask(nx2, ny2, 10.0, 10.0, 2.5, cpu)
+    ny2, nx2 = 16, 64
+    obst2 = b2.cylinder_mask(nx2, ny2, 10.0, 8.0, 2.5, cpu)
     wall2 = b2.make_channel_wall_mask(ny2, nx2, obst2, cpu)
     ux0 = torch.full((ny2, nx2), 0.05)
     ux0[obst2] = 0.0

@@ -1,6 +1,10 @@
 """Pin the numpy oracle to TensorLBM: every oracle function against the golden
 vectors produced by the unmodified reference (tests/golden/make_golden.py).
-CPU only."""
+
+The oracle restates the reference's arithmetic order, including torch's CPU
+summation order over the direction axis (oracle.lbm.sum0), so on the golden
+shapes (inner sizes that are multiples of 32) it reproduces TensorLBM bit for
+bit: operators, boundary planes and whole multi-step chains.  CPU only."""
 
 from __future__ import annotations
 
@@ -8,91 +12,85 @@ import numpy as np
 import pytest
 
 from oracle import lbm as O
-from tests.conftest import golden, rel_err
-
-F32_TOL = 2e-6   # float32 re-association / FMA noise on O(1) populations
-F64_TOL = 1e-12
+from tests.conftest import golden
 
 
-def _tol(dt):
-    return F32_TOL if dt == np.float32 else F64_TOL
+def same(a, b):
+    """bitwise equality, NaN == NaN"""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return a.shape == b.shape and a.dtype == b.dtype and np.array_equal(a, b, equal_nan=True)
 
 
 @pytest.mark.parametrize("tag", ["f32", "f64"])
 @pytest.mark.parametrize("q", [9, 19, 27])
 def test_moments_and_equilibrium(q, tag):
     g = golden(f"moments_d{'2' if q == 9 else '3'}q{q}_{tag}")
-    f = g["f"]
-    rho, ux, uy, uz = O.macroscopic(f)
-    assert rel_err(rho, g["rho"]) < _tol(f.dtype)
-    assert np.max(np.abs(ux - g["ux"])) < 10 * _tol(f.dtype)
-    assert np.max(np.abs(uy - g["uy"])) < 10 * _tol(f.dtype)
+    rho, ux, uy, uz = O.macroscopic(g["f"])
+    assert same(rho, g["rho"]) and same(ux, g["ux"]) and same(uy, g["uy"])
     if q != 9:
-        assert np.max(np.abs(uz - g["uz"])) < 10 * _tol(f.dtype)
-    feq = O.equilibrium(q, g["rho_in"], g["ux_in"], g["uy_in"], None if q == 9 else g["uz_in"])
-    assert feq.dtype == f.dtype
-    assert rel_err(feq, g["feq"]) < _tol(f.dtype)
+        assert same(uz, g["uz"])
+    assert same(O.equilibrium(q, g["rho_in"], g["ux_in"], g["uy_in"], None if q == 9 else g["uz_in"]), g["feq"])
 
 
 def test_collide_d2q9():
     g = golden("collide_d2q9_f32")
     f, tau = g["f"], float(g["tau"])
-    assert rel_err(O.collide_bgk(f, tau), g["bgk"]) < F32_TOL
-    assert rel_err(O.collide_mrt(f, tau), g["mrt"]) < F32_TOL
-    assert rel_err(O.collide_mrt(f, tau, tau_field=g["tau_field"]), g["mrt_field"]) < F32_TOL
-    assert rel_err(O.collide_smagorinsky(f, tau, 0.17), g["smag"]) < F32_TOL
+    assert same(O.collide_bgk(f, tau), g["bgk"])
+    assert same(O.collide_mrt(f, tau), g["mrt"])
+    assert same(O.collide_mrt(f, tau, tau_field=g["tau_field"]), g["mrt_field"])
+    assert same(O.collide_smagorinsky(f, tau, 0.17), g["smag"])
 
 
 @pytest.mark.parametrize("tag", ["f32", "f64"])
 def test_collide_d3q19(tag):
     g = golden(f"collide_d3q19_{tag}")
     f, tau = g["f"], float(g["tau"])
-    tol = _tol(f.dtype)
-    assert rel_err(O.collide_bgk(f, tau), g["bgk"]) < tol
-    assert rel_err(O.collide_smagorinsky(f, tau, 0.17), g["smag"]) < tol
-    assert rel_err(O.collide_cumulant_d3q19(f, tau, omega_b=1.2, omega_even=0.8), g["cum19"]) < tol
-    assert rel_err(O.collide_cumulant_d3q19(f, tau, omega_b=1.2, omega_even=0.8, c_s=0.17), g["cum19_smag"]) < tol
+    assert same(O.collide_bgk(f, tau), g["bgk"])
+    assert same(O.collide_smagorinsky(f, tau, 0.17), g["smag"])
+    assert same(O.collide_cumulant_d3q19(f, tau, omega_b=1.2, omega_even=0.8), g["cum19"])
+    assert same(O.collide_cumulant_d3q19(f, tau, omega_b=1.2, omega_even=0.8, c_s=0.17), g["cum19_smag"])
     if "mrt" in g:
-        assert rel_err(O.collide_mrt(f, tau), g["mrt"]) < F32_TOL
-        assert rel_err(O.collide_mrt(f, tau, s_e=1.3, s_eps=1.5, s_q=1.1, s_pi=1.25), g["mrt_custom"]) < F32_TOL
+        assert same(O.collide_mrt(f, tau), g["mrt"])
+        assert same(O.collide_mrt(f, tau, s_e=1.3, s_eps=1.5, s_q=1.1, s_pi=1.25), g["mrt_custom"])
 
 
 @pytest.mark.parametrize("tag", ["f32", "f64"])
 def test_collide_d3q27(tag):
     g = golden(f"collide_d3q27_{tag}")
     f, tau = g["f"], float(g["tau"])
-    tol = _tol(f.dtype)
-    assert rel_err(O.collide_bgk(f, tau), g["bgk"]) < tol
-    assert rel_err(O.collide_smagorinsky(f, tau, 0.17), g["smag"]) < tol
-    assert rel_err(O.collide_cumulant_d3q27(f, tau, 1.1, 1.2, 0.9), g["cum"]) < 5 * tol
-    assert rel_err(O.collide_cumulant_geier_d3q27(f, tau, 1.1, 1.2, 0.9), g["geier"]) < 5 * tol
+    assert same(O.collide_bgk(f, tau), g["bgk"])
+    assert same(O.collide_smagorinsky(f, tau, 0.17), g["smag"])
+    assert same(O.collide_cumulant_d3q27(f, tau, 1.1, 1.2, 0.9), g["cum"])
+    assert same(O.collide_cumulant_geier_d3q27(f, tau, 1.1, 1.2, 0.9), g["geier"])
     if "mrt" in g:
-        assert rel_err(O.collide_mrt(f, tau), g["mrt"]) < 5 * F32_TOL
+        assert same(O.collide_mrt(f, tau), g["mrt"])
 
 
 def test_stream_canary_bitwise():
     g = golden("stream")
     for q in (9, 19, 27):
-        assert np.array_equal(O.stream(g[f"f{q}"]), g[f"s{q}"])
+        assert same(O.stream(g[f"f{q}"]), g[f"s{q}"])
 
 
 @pytest.mark.parametrize("q", [9, 19, 27])
 def test_boundaries(q):
     g = golden(f"bc_d{'2' if q == 9 else '3'}q{q}")
     f, m = g["f"], g["mask"]
-    assert np.array_equal(O.bounce_back(f, m), g["bb"])
+    assert same(O.bounce_back(f, m), g["bb"])
     if q == 9:
-        assert rel_err(O.zou_he_inlet(f, 0.05, 0.01), g["inlet"]) < F32_TOL
-        assert rel_err(O.zou_he_outlet(f, 1.02), g["outlet"]) < F32_TOL
-        assert rel_err(O.moving_lid(f, 0.07), g["lid"]) < F32_TOL
+        assert same(O.zou_he_inlet(f, 0.05, 0.01), g["inlet"])
+        assert same(O.zou_he_outlet(f, 1.02), g["outlet"])
+        assert same(O.moving_lid(f, 0.07), g["lid"])
     else:
-        assert rel_err(O.zou_he_inlet(f, 0.04, 0.01, -0.005), g["inlet"]) < F32_TOL
-        assert rel_err(O.zou_he_outlet(f, 0.98), g["outlet"]) < F32_TOL
+        assert same(O.zou_he_inlet(f, 0.04, 0.01, -0.005), g["inlet"])
+        assert same(O.zou_he_outlet(f, 0.98), g["outlet"])
         if q == 19:
-            assert rel_err(O.moving_lid(f, 0.05), g["lid"]) < F32_TOL
+            assert same(O.moving_lid(f, 0.05), g["lid"])
+    # the reference sums the force in float32, the oracle in float64
     ref = g["force"].astype(np.float64)
     got = O.obstacle_force(f, m)[: len(ref)]
-    assert np.max(np.abs(got - ref)) < 1e-5 * max(np.max(np.abs(ref)), 1.0)
+    assert np.max(np.abs(got - ref)) < 1e-6 * max(np.max(np.abs(ref)), 1.0)
 
 
 def test_masks_bitwise():
@@ -121,6 +119,8 @@ def test_missing_mask_and_links():
 @pytest.mark.parametrize("coll", ["bgk", "mrt"])
 @pytest.mark.parametrize("mode", ["fullway", "halfway", "fullway_window"])
 def test_chain_cavity(coll, mode):
+    """12^3 cavity chains.  Where the reference diverges (NaN) inside the
+    window the oracle must diverge at the same step."""
     g = golden(f"chain_cavity_d3q19_{coll}_{mode}")
     f = g["f0"]
     nan_step = -1
@@ -130,13 +130,8 @@ def test_chain_cavity(coll, mode):
                               mode="halfway" if mode == "halfway" else "fullway")
             if nan_step < 0 and not np.isfinite(f).all():
                 nan_step = s
-    if "nan_step" in g and int(g["nan_step"]) > 0:
-        # the literal chain diverges inside the window: the oracle must blow up
-        # within a step or two of the reference
-        assert nan_step > 0 and abs(nan_step - int(g["nan_step"])) <= 2, (nan_step, int(g["nan_step"]))
-    else:
-        assert nan_step < 0
-        assert rel_err(f, g["f"]) < 1e-4
+    assert nan_step == int(g.get("nan_step", -1))
+    assert same(f, g["f"])
 
 
 def test_chain_cylinder_d2q9():
@@ -146,9 +141,9 @@ def test_chain_cylinder_d2q9():
     for _ in range(int(g["steps"])):
         f, fo = O.channel_step(f, float(g["tau"]), float(g["u_in"]), 1.0, g["wall"], g["obstacle"], "bgk")
         forces.append(fo[:2])
-    assert rel_err(f, g["f"]) < 1e-4
+    assert same(f, g["f"])
     ref = g["forces"].astype(np.float64)
-    assert np.max(np.abs(np.array(forces) - ref)) < 1e-3 * np.max(np.abs(ref))
+    assert np.max(np.abs(np.array(forces) - ref)) < 1e-5 * np.max(np.abs(ref))
 
 
 @pytest.mark.parametrize("name,coll", [("d3q19_mrt", "mrt"), ("d3q19_bgk", "bgk"), ("d3q27_cumulant", "cumulant"),
@@ -160,7 +155,6 @@ def test_chain_sphere(name, coll):
     for _ in range(int(g["steps"])):
         f, fo = O.channel_step(f, float(g["tau"]), float(g["u_in"]), 1.0, None, g["obstacle"], coll)
         forces.append(fo)
-    assert rel_err(f, g["f"]) < 1e-4
+    assert same(f, g["f"])
     ref = g["forces"].astype(np.float64)
-    scale = np.max(np.abs(ref[:, 0]))
-    assert np.max(np.abs(np.array(forces)[:, :3] - ref)) < 1e-3 * scale
+    assert np.max(np.abs(np.array(forces)[:, :3] - ref)) < 1e-5 * np.max(np.abs(ref[:, 0]))
