@@ -262,7 +262,6 @@ __device__ __forceinline__ void collide_smagorinsky(T (&f)[L::Q], const CollideP
   for (int q = 0; q < L::Q; ++q) fn[q] = xsub(f[q], feq_q<L>(q, rho, ux, uy, uz, usq));
   const Pi6<T> p = neq_stress<L>(fn);
   const T te = smagorinsky_tau<L>(p, rho, cp);
-#pragma unroll
   const double inv_te = 1.0 / double(te);
 #pragma unroll
   for (int q = 0; q < L::Q; ++q) f[q] = xsub(f[q], div_by(fn[q], te, inv_te));
