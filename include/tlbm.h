@@ -35,7 +35,8 @@ typedef enum tlbm_status {
   TLBM_ERR_TIMEOUT = 5,     /* a bounded device-side wait expired */
   TLBM_ERR_NONFINITE = 6,   /* reported by callers that read the status word */
   TLBM_ERR_ARG = 7,         /* null pointer or invalid parameter */
-  TLBM_ERR_UNSUPPORTED = 8  /* lattice / collision / boundary combination not built */
+  TLBM_ERR_UNSUPPORTED = 8, /* lattice / collision / boundary combination not built */
+  TLBM_ERR_TOO_LARGE = 9    /* input larger than a fixed-size static scratch array */
 } tlbm_status;
 
 typedef enum tlbm_lattice { TLBM_D2Q9 = 9, TLBM_D3Q19 = 19, TLBM_D3Q27 = 27 } tlbm_lattice;
@@ -224,6 +225,27 @@ TLBM_API int tlbm_link_count(const uint8_t* mask, int64_t count, int64_t* block_
                              int64_t* count_out, void* stream);
 TLBM_API int tlbm_link_list(const uint8_t* mask, int64_t count, const int64_t* block_counts,
                             int64_t* out, void* stream);
+
+/* Allocation-free link list.  No counterpart in TensorLBM: it exists for host
+ * programs that reserve all device memory up front and may not call
+ * cudaMalloc/cudaFree (or any allocating library) while they run - a fixed
+ * memory budget owned by a solver framework or a caching allocator, where a
+ * new allocation can fail or stall the device mid-pipeline.
+ * Same result as tlbm_link_count + tlbm_link_list in one call, but the
+ * per-block scratch is a static device array inside the library (1 MiB on every
+ * device that loads it, kept until the process exits), so the mask may hold at
+ * most tlbm_link_list_static_capacity() bytes (128 Mi); larger masks return
+ * TLBM_ERR_TOO_LARGE before any work.  *count_out (device int64) receives the
+ * number of non-zero entries; the first min(count, out_capacity) indices are
+ * written to out.  The first call on each device looks the array up with
+ * cudaGetSymbolAddress (make it before any stream capture).  All calls share
+ * the array: calls whose kernels overlap on the GPU (different streams or
+ * devices sharing nothing but the array - it is per device) race and must be
+ * ordered by the caller.  Nothing in the array needs clearing between calls:
+ * each call writes every entry it reads. */
+TLBM_API int tlbm_link_list_noalloc(const uint8_t* mask, int64_t count, int64_t* out, int64_t out_capacity,
+                                    int64_t* count_out, void* stream);
+TLBM_API int64_t tlbm_link_list_static_capacity(void);
 
 TLBM_API const char* tlbm_status_string(int status);
 TLBM_API int tlbm_abi_version(void);

@@ -19,6 +19,7 @@ LIB_PATH = pathlib.Path(os.environ.get("TLBM_LIB", _HERE / "libtlbm.so"))
 
 # tlbm_status
 OK, ERR_SHAPE, ERR_DTYPE, ERR_ALIAS, ERR_LAUNCH, ERR_TIMEOUT, ERR_NONFINITE, ERR_ARG, ERR_UNSUPPORTED = range(9)
+ERR_TOO_LARGE = 9
 # tlbm_dtype
 F32, F64, F16_SHIFTED, BF16_SHIFTED = 0, 1, 2, 3
 # tlbm_collision
@@ -82,10 +83,12 @@ SIGNATURES: dict[str, list] = {
     "tlbm_link_blocks": [_I64],
     "tlbm_link_count": [_P, _I64, _P, _P, _P],
     "tlbm_link_list": [_P, _I64, _P, _P, _P],
+    "tlbm_link_list_noalloc": [_P, _I64, _P, _I64, _P, _P],
+    "tlbm_link_list_static_capacity": [],
     "tlbm_status_string": [ctypes.c_int],
     "tlbm_abi_version": [],
 }
-_RESTYPES = {"tlbm_link_blocks": _I64, "tlbm_status_string": ctypes.c_char_p}
+_RESTYPES = {"tlbm_link_blocks": _I64, "tlbm_link_list_static_capacity": _I64, "tlbm_status_string": ctypes.c_char_p}
 
 _lib: ctypes.CDLL | None = None
 
@@ -114,7 +117,7 @@ def check(status: int, what: str) -> None:
     if status == OK:
         return
     msg = f"{what}: {load().tlbm_status_string(status).decode()} (status {status})"
-    if status in (ERR_SHAPE, ERR_DTYPE, ERR_ALIAS, ERR_ARG):
+    if status in (ERR_SHAPE, ERR_DTYPE, ERR_ALIAS, ERR_ARG, ERR_TOO_LARGE):
         raise ValueError(msg)
     if status == ERR_UNSUPPORTED:
         raise NotImplementedError(msg)

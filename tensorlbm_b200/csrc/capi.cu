@@ -308,6 +308,7 @@ TLBM_API const char* tlbm_status_string(int status) {
     case TLBM_ERR_NONFINITE: return "non-finite values";
     case TLBM_ERR_ARG: return "invalid argument";
     case TLBM_ERR_UNSUPPORTED: return "unsupported combination";
+    case TLBM_ERR_TOO_LARGE: return "input exceeds the fixed static scratch of this allocation-free entry point";
     default: return "unknown status";
   }
 }
