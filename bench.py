@@ -87,6 +87,12 @@ class ClockSampler:
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # wait for the sampler to be running, then keep only samples taken
+            # from here on (the timed region starts when this returns)
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 3.0:
+                time.sleep(0.01)
+            self.rows.clear()
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -183,6 +189,53 @@ def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_c
             "roofline_frac": round(gbs / peak, 4), "bytes_per_cell": bytes_per_cell, "finite": finite}
 
 
+def _batched_variant(torch, dev, steps, peak):
+    """512 D2Q9 BGK cylinder channels (nx ~ U{128..1024}, ny = nx/4, D = ny/8,
+    Re ~ U(40, 300), seed 20261203) advanced together, against the same domains
+    run one after the other (TensorLBM's scan runner does points sequentially)."""
+    from tensorlbm_b200 import LBMSolver, batch
+
+    doms = batch.uniform_scan(512, seed=20261203, device=dev)
+    f0 = batch.equilibrium_start(doms, dev)
+    b = batch.BatchedSolver(doms, "bgk", device=dev)
+    b.load(f0)
+    tune = batch.autotune(b, steps=5)
+    b.load(f0)
+    t = b.timed_steps(steps)
+    cells = b.n_cells
+    mlups = cells * steps / t / 1e6
+    fin = b.finite_domains().cpu()
+    finite_domains = int(fin.sum())
+    # BGK at tau - 1/2 = 3 u D / Re (down to 0.002 on the coarsest, fastest
+    # domains) is unstable; those domains overflow exactly as a plain run would
+    unstable_tau = sorted(round(doms[i].tau, 4) for i in range(len(doms)) if not bool(fin[i]))
+    del b
+    # sequential plain runs on a sample of 32 domains (graph-replayed fused steps)
+    sample = doms[:32]
+    seq_cells, seq_t = 0, 0.0
+    cur = torch.cuda.current_stream(dev)
+    for d, f in zip(sample, f0[:32]):
+        s = LBMSolver("D2Q9", (d.ny, d.nx), d.tau, "bgk", device=dev, wall_mask=d.wall_mask,
+                      obstacle_mask=d.obstacle_mask, u_in=d.u_in, rho_out=d.rho_out).load(f)
+        s.run(64)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        s.run(steps)
+        e1.record(cur)
+        torch.cuda.synchronize(dev)
+        seq_t += e0.elapsed_time(e1) / 1e3
+        seq_cells += d.nx * d.ny
+    seq_mlups = seq_cells * steps / seq_t / 1e6
+    torch.cuda.empty_cache()
+    return {"mlups": round(mlups, 1), "ms_per_step": round(1e3 * t / steps, 4), "domains": 512, "cells": cells,
+            "roofline_frac": round(72 * cells / (t / steps) / 1e9 / peak, 4), "bytes_per_cell": 72,
+            "mode": tune["best"]["mode"], "tile": list(tune["best"]["tile"]),
+            "sequential_mlups_32_domain_sample": round(seq_mlups, 1),
+            "speedup_vs_sequential": round(mlups / seq_mlups, 2), "finite_domains": finite_domains,
+            "nonfinite_domains_tau_max": unstable_tau[-1] if unstable_tau else None}
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -273,12 +326,21 @@ def run_ours(args) -> None:
 
     # ---- variants on the same grid (rank 0 device only, N=1 semantics) ----
     variants = {}
-    if not args.no_variants:
-        variants["d3q27_cumulant_f32"] = _variant(torch, dev, "D3Q27", "cumulant", "f32", max(args.steps // 2, 5),
+    wanted = set(args.variants.split(",")) if args.variants != "all" else None
+
+    def want(name):
+        return not args.no_variants and (wanted is None or name in wanted)
+
+    if want("d3q27_cumulant_f32"):
+        variants["d3q27_cumulant_f32"] = _variant(torch, dev, "D3Q27", "cumulant", "f32", max(args.steps // 2, 3),
                                                   args.warmup, 2 * 27 * 4, peak)
+    if want("d3q19_mrt_f16_shifted"):
         variants["d3q19_mrt_f16_shifted"] = _variant(torch, dev, "D3Q19", "mrt", "f16", args.steps, args.warmup,
                                                      2 * 19 * 2, peak)
+    if want("d3q19_bgk_f32"):
         variants["d3q19_bgk_f32"] = _variant(torch, dev, "D3Q19", "bgk", "f32", args.steps, args.warmup, bpc, peak)
+    if want("d2q9_batched_512_cylinders"):
+        variants["d2q9_batched_512_cylinders"] = _batched_variant(torch, dev, args.steps, peak)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -431,10 +493,13 @@ def run_reference(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--variants", default="all",
+                    help="comma list of variants to run (d3q27_cumulant_f32, d3q19_mrt_f16_shifted, "
+                         "d3q19_bgk_f32, d2q9_batched_512_cylinders) or 'all'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-slab", type=int, default=8, help="z-planes per CPU sample slab")
     ap.add_argument("--cpu-steps", type=int, default=2)

@@ -76,10 +76,12 @@ typedef enum tlbm_flag_bits {
   TLBM_FLAG_SOLID = 1u,     /* post-stream full-way bounce-back (wall XOR obstacle, as two
                                successive swaps cancel): bounce_back_cells* after stream */
   TLBM_FLAG_OBSTACLE = 2u,  /* summed into the momentum-exchange force */
-  TLBM_FLAG_HALFWAY = 4u    /* pre-stream half-way wall: the cell is not collided, its
+  TLBM_FLAG_HALFWAY = 4u,   /* pre-stream half-way wall: the cell is not collided, its
                                populations are stored reversed (where(wall, f_pre[opp], f)
                                before stream: cases/base.py:270-289 pre-boundaries,
                                lbm_step_correct.py:62 "bb" mode) */
+  TLBM_FLAG_MOVING = 8u     /* Ladd moving wall (with SOLID): swap plus 2 w rho (c.u_w)/c_s^2,
+                               u_w from tlbm_desc.wall_velocity (propeller_benchmark.py:221) */
 } tlbm_flag_bits;
 
 typedef struct tlbm_desc {
@@ -95,6 +97,8 @@ typedef struct tlbm_desc {
   double u_lid;        /* lid x-velocity */
   double u_in[3];      /* Zou/He inlet velocity */
   double rho_out;      /* Zou/He outlet density */
+  const void* wall_velocity; /* (DIM, N) wall velocity of TLBM_FLAG_MOVING cells in the compute
+                                type (float32; float64 for TLBM_F64), x-component first; may be NULL */
 } tlbm_desc;
 
 /* ---- fused time step ------------------------------------------------------
@@ -150,6 +154,15 @@ TLBM_API int tlbm_macroscopic(int32_t lattice, int32_t dtype, int64_t ncells, co
  * (boundaries3d.py:112), bounce_back_cells_27 (boundaries_d3q27.py:45). */
 TLBM_API int tlbm_bounce_back(int32_t lattice, int32_t dtype, int64_t ncells, const void* f_in,
                               const uint8_t* mask, void* f_out, void* stream);
+
+/* Ladd moving-wall bounce-back: f_out = where(mask, bounce_back(f_in) +
+ * 2 w rho (c.u_w) / c_s^2, f_in) with rho = sum f_in and u_w given per cell as
+ * DIM consecutive arrays of ncells (x first).  D2Q9 / D3Q19, F32/F64.
+ * Replaces moving_wall_bounce_back (rotating_cylinder.py:140) and
+ * moving_wall_bounce_back_3d (propeller_benchmark.py:221). */
+TLBM_API int tlbm_moving_wall_bounce_back(int32_t lattice, int32_t dtype, int64_t ncells, const void* f_in,
+                                          const uint8_t* mask, const void* wall_velocity, void* f_out,
+                                          void* stream);
 
 /* Zou/He velocity inlet on the x = 0 plane, in place.  ux_profile / uy_profile
  * (D2Q9 only, length ny, may be NULL) override u_in / uy_in per row.
@@ -246,6 +259,57 @@ TLBM_API int tlbm_link_list(const uint8_t* mask, int64_t count, const int64_t* b
 TLBM_API int tlbm_link_list_noalloc(const uint8_t* mask, int64_t count, int64_t* out, int64_t out_capacity,
                                     int64_t* count_out, void* stream);
 TLBM_API int64_t tlbm_link_list_static_capacity(void);
+
+/* ---- batched runner: many independent small D2Q9 domains ----------------------
+ * Replaces the sequential per-point loop of the scan runner
+ * (scan_runner.py:697 run_scan_point, :979 ScanExecutor) for the cylinder-flow
+ * chain of cylinder_flow.py:854-899 (collide -> stream -> force -> Zou/He inlet
+ * -> outlet -> bounce-back).  Each domain is a (9, ny, nx) block at f_offset
+ * (elements) in one packed population buffer, with its ny*nx flag bytes at
+ * cell_offset in one packed flag buffer.  tiles holds ntiles triplets
+ * (domain, x0, y0) of tile_x x tile_y cells; every cell of every domain must be
+ * in exactly one tile.  Every domain evolves bit for bit as tlbm_step would
+ * advance it alone. */
+typedef struct tlbm_batch_domain {
+  int64_t f_offset;
+  int64_t cell_offset;
+  int32_t nx, ny;
+  double tau;
+  double u_in;      /* Zou/He inlet x-velocity (TLBM_BC_ZH_INLET) */
+  double rho_out;   /* Zou/He outlet density (TLBM_BC_ZH_OUTLET) */
+  uint32_t bc;
+  uint32_t reserved;
+} tlbm_batch_domain;
+
+typedef struct tlbm_batch_desc {
+  int32_t lattice;      /* TLBM_D2Q9 */
+  int32_t dtype;        /* TLBM_F32 */
+  int32_t collision;    /* TLBM_COLL_BGK or TLBM_COLL_MRT */
+  int32_t ndomains;
+  int32_t tile_x;       /* multiple of 32, tile_x * tile_y <= 256 */
+  int32_t tile_y;
+  int32_t ctas_per_sm;  /* persistent mode: CTAs per SM (0 = occupancy limit) */
+  int32_t reserved;
+} tlbm_batch_desc;
+
+/* One step of every domain, one launch (grid = tiles).  domains and tiles are
+ * device arrays.  forces (may be NULL): ndomains x 3 doubles, accumulated
+ * (zero before the step).  status bit 0: non-finite density. */
+TLBM_API int tlbm_batch_step(const tlbm_batch_desc* b, const tlbm_batch_domain* domains, const int32_t* tiles,
+                             int64_t ntiles, const void* f_in, void* f_out, const uint8_t* flags, double* forces,
+                             unsigned int* status, void* stream);
+
+/* nsteps steps in one persistent cooperative launch; the state ping-pongs
+ * f_a -> f_b -> f_a ..., so it ends in f_a when nsteps is even.  Step s with
+ * s % record_every == 0 accumulates its forces into
+ * force_history[(s / record_every) * ndomains * 3 ...] (zeroed by the caller).
+ * sync: 3 device words, zero before the first call (and after a timeout).
+ * The grid barrier between steps gives up after max_spins polls: status gets
+ * bit 1 and every CTA returns (no hang). */
+TLBM_API int tlbm_batch_run(const tlbm_batch_desc* b, const tlbm_batch_domain* domains, const int32_t* tiles,
+                            int64_t ntiles, void* f_a, void* f_b, const uint8_t* flags, int32_t nsteps,
+                            double* force_history, int32_t record_every, unsigned int* sync, unsigned int* status,
+                            int64_t max_spins, void* stream);
 
 TLBM_API const char* tlbm_status_string(int status);
 TLBM_API int tlbm_abi_version(void);

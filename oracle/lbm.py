@@ -501,6 +501,26 @@ def bounce_back(f: np.ndarray, mask: np.ndarray) -> np.ndarray:
     return np.where(mask[None], f[opposite(f.shape[0])], f)
 
 
+def moving_wall_bounce_back(f: np.ndarray, mask: np.ndarray, *wall_u: np.ndarray) -> np.ndarray:
+    """Ladd moving wall: where(mask, bounce_back(f) + ((2 w_q) rho) (c_q . u_w) 3, f),
+    rho = sum0(f), the float32 W tensor cast to f's dtype for both lattices and
+    c_q . u_w summed x, y, z in order: rotating_cylinder.py:140-190 (D2Q9),
+    propeller_benchmark.py:221-270 (D3Q19)."""
+    q = f.shape[0]
+    dt = f.dtype
+    nd = f.ndim - 1
+    rho = sum0(f)
+    fbb = bounce_back(f, mask)
+    c = C[q].astype(dt)
+    w = _view(W64[q].astype(np.float32).astype(dt), nd)
+    u = [np.asarray(v).astype(dt) for v in wall_u]
+    cu = _view(c[:, 0], nd) * u[0][None] + _view(c[:, 1], nd) * u[1][None]
+    if len(u) == 3:
+        cu = cu + _view(c[:, 2], nd) * u[2][None]
+    corr = dt.type(2.0) * w * rho[None] * cu * dt.type(3.0)
+    return np.where(mask[None], fbb + corr, fbb)
+
+
 def zou_he_inlet(f: np.ndarray, u_in: float, uy_in: float = 0.0, uz_in: float = 0.0) -> np.ndarray:
     """x = 0 velocity inlet: boundaries.py:50 (D2Q9), boundaries3d.py:205, boundaries_d3q27.py:107."""
     q = f.shape[0]
@@ -668,9 +688,11 @@ def cavity_step(f: np.ndarray, tau: float, wall: np.ndarray, u_lid: float, colli
     return moving_lid(f, u_lid)
 
 
-def channel_step(f, tau, u_in, rho_out, wall, obstacle, collision="bgk", **kw):
+def channel_step(f, tau, u_in, rho_out, wall, obstacle, collision="bgk", wall_u=None, **kw):
     """collide -> stream -> force -> Zou/He inlet -> outlet -> bounce-back(wall)
-    -> bounce-back(obstacle): d3q27_sphere_flow.py:246-256, cylinder_flow.py:854-899."""
+    -> bounce-back(obstacle): d3q27_sphere_flow.py:246-256, cylinder_flow.py:854-899.
+    With wall_u (the obstacle's wall velocity, one array per axis) the obstacle
+    pass is the Ladd moving wall instead, as rotating_cylinder.py:241-253 orders it."""
     f = COLLIDERS[collision](f, tau, **kw)
     f = stream(f)
     force = obstacle_force(f, obstacle) if obstacle is not None else None
@@ -681,5 +703,5 @@ def channel_step(f, tau, u_in, rho_out, wall, obstacle, collision="bgk", **kw):
     if wall is not None:
         f = bounce_back(f, wall)
     if obstacle is not None:
-        f = bounce_back(f, obstacle)
+        f = bounce_back(f, obstacle) if wall_u is None else moving_wall_bounce_back(f, obstacle, *wall_u)
     return f, force

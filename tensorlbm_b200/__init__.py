@@ -35,6 +35,8 @@ _PATCHES = {
     "lid_driven_cavity": ["zou_he_moving_lid"],
     "obstacles": ["compute_obstacle_forces_3d", "compute_obstacle_forces_27"],
     "boundary_registry": ["derive_missing_mask"],
+    "rotating_cylinder": ["moving_wall_bounce_back"],
+    "propeller_benchmark": ["moving_wall_bounce_back_3d"],
 }
 
 

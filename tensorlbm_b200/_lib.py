@@ -26,7 +26,7 @@ F32, F64, F16_SHIFTED, BF16_SHIFTED = 0, 1, 2, 3
 COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY = range(7)
 # tlbm_bc_bits / tlbm_flag_bits
 BC_LID, BC_ZH_INLET, BC_ZH_OUTLET = 1, 2, 4
-FLAG_SOLID, FLAG_OBSTACLE, FLAG_HALFWAY = 1, 2, 4
+FLAG_SOLID, FLAG_OBSTACLE, FLAG_HALFWAY, FLAG_MOVING = 1, 2, 4, 8
 
 TORCH_TO_DTYPE = {torch.float32: F32, torch.float64: F64}
 
@@ -54,7 +54,24 @@ class Desc(ctypes.Structure):
         ("u_lid", ctypes.c_double),
         ("u_in", ctypes.c_double * 3),
         ("rho_out", ctypes.c_double),
+        ("wall_velocity", ctypes.c_void_p),
     ]
+
+
+class BatchDomain(ctypes.Structure):
+    """struct tlbm_batch_domain"""
+
+    _fields_ = [("f_offset", ctypes.c_int64), ("cell_offset", ctypes.c_int64), ("nx", ctypes.c_int32),
+                ("ny", ctypes.c_int32), ("tau", ctypes.c_double), ("u_in", ctypes.c_double),
+                ("rho_out", ctypes.c_double), ("bc", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class BatchDesc(ctypes.Structure):
+    """struct tlbm_batch_desc"""
+
+    _fields_ = [("lattice", ctypes.c_int32), ("dtype", ctypes.c_int32), ("collision", ctypes.c_int32),
+                ("ndomains", ctypes.c_int32), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 _P = ctypes.c_void_p
@@ -70,6 +87,7 @@ SIGNATURES: dict[str, list] = {
     "tlbm_equilibrium": [_I32, _I32, _I64, _P, _P, _P, _P, _P, _P],
     "tlbm_macroscopic": [_I32, _I32, _I64, _P, _P, _P, _P, _P, _P],
     "tlbm_bounce_back": [_I32, _I32, _I64, _P, _P, _P, _P],
+    "tlbm_moving_wall_bounce_back": [_I32, _I32, _I64, _P, _P, _P, _P, _P],
     "tlbm_zou_he_inlet": [_I32, _I32, _I32, _I32, _I32, _P, _D, _D, _D, _P, _P, _P],
     "tlbm_zou_he_outlet": [_I32, _I32, _I32, _I32, _I32, _P, _D, _P],
     "tlbm_moving_lid": [_I32, _I32, _I32, _I32, _I32, _P, _D, _P],
@@ -83,6 +101,8 @@ SIGNATURES: dict[str, list] = {
     "tlbm_link_blocks": [_I64],
     "tlbm_link_count": [_P, _I64, _P, _P, _P],
     "tlbm_link_list": [_P, _I64, _P, _P, _P],
+    "tlbm_batch_step": [ctypes.POINTER(BatchDesc), _P, _P, _I64, _P, _P, _P, _P, _P, _P],
+    "tlbm_batch_run": [ctypes.POINTER(BatchDesc), _P, _P, _I64, _P, _P, _P, _I32, _P, _I32, _P, _P, _I64, _P],
     "tlbm_link_list_noalloc": [_P, _I64, _P, _I64, _P, _P],
     "tlbm_link_list_static_capacity": [],
     "tlbm_status_string": [ctypes.c_int],

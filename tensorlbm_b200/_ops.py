@@ -181,6 +181,30 @@ def bounce_back(q: int, f: torch.Tensor, mask: torch.Tensor) -> torch.Tensor:
     return out
 
 
+def moving_wall_bounce_back(q: int, f: torch.Tensor, mask: torch.Tensor, *wall_u: torch.Tensor) -> torch.Tensor:
+    """Ladd moving-wall bounce-back (out of place); wall_u = (ux_w, uy_w[, uz_w])."""
+    dev = _lib.require_cuda(f, mask, *wall_u)
+    grid_of(f, q)
+    code = _lib.real_dtype(f)
+    dim = 2 if q == 9 else 3
+    if len(wall_u) != dim:
+        raise ValueError(f"moving_wall_bounce_back on Q={q} needs {dim} wall-velocity fields")
+    f = _c(f)
+    shape = tuple(f.shape[1:])
+    m = _mask_u8(mask, shape)
+    for u in wall_u:
+        if tuple(u.shape) != shape:
+            raise ValueError(f"wall velocity shape {tuple(u.shape)} != grid {shape}")
+    uw = torch.stack([u.to(f.dtype) for u in wall_u]).contiguous()
+    out = torch.empty_like(f)
+    n = m.numel()
+    if n > 0:
+        st = _lib.load().tlbm_moving_wall_bounce_back(q, code, n, f.data_ptr(), m.data_ptr(), uw.data_ptr(),
+                                                      out.data_ptr(), _lib.stream_of(dev))
+        _lib.check(st, "moving_wall_bounce_back")
+    return out
+
+
 def zou_he_inlet_(q: int, f: torch.Tensor, u_in, uy_in=0.0, uz_in=0.0) -> torch.Tensor:
     """In place on f (which must be contiguous)."""
     dev = _lib.require_cuda(f)

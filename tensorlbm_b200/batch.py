@@ -1,0 +1,346 @@
+"""Batched runner: many independent small D2Q9 domains advanced together.
+
+TensorLBM's scan runner advances design points one after the other in worker
+processes (``scan_runner.py:697`` ``run_scan_point``, ``:979``
+``ScanExecutor``), each running the cylinder-flow chain of
+``cylinder_flow.py:854-899``.  :class:`BatchedSolver` packs all the domains
+of a scan into one population buffer.  It advances them with one kernel launch
+per step, replayed as a CUDA graph, or one persistent cooperative launch for
+many steps.  Every domain evolves bit for bit as it would alone.
+:func:`autotune` picks the tile shape and the execution mode by timing them on
+the actual domain set.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib, _ops
+
+
+BatchDomain = _lib.BatchDomain
+BatchDesc = _lib.BatchDesc
+
+
+def _fn(name):
+    return getattr(_lib.load(), name)
+
+
+@dataclass
+class DomainSpec:
+    """One channel domain: (ny, nx) grid, BGK/MRT relaxation time, Zou/He inlet
+    velocity and outlet density (None disables the plane), wall and obstacle masks."""
+
+    nx: int
+    ny: int
+    tau: float
+    u_in: float | None = None
+    rho_out: float | None = 1.0
+    wall_mask: torch.Tensor | None = None
+    obstacle_mask: torch.Tensor | None = None
+
+
+def cylinder_channel(nx: int, re: float, u_in: float = 0.05, device=None) -> DomainSpec:
+    """The batched-form case: ny = nx/4, cylinder of diameter D = ny/8 at
+    (ny/2, ny/2), channel walls top and bottom, tau = 3 u D / Re + 0.5
+    (cylinder_flow.py conventions; masks from cylinder_mask / make_channel_wall_mask)."""
+    from . import boundaries
+
+    ny = nx // 4
+    d = ny / 8.0
+    obst = boundaries.cylinder_mask(nx, ny, ny / 2.0, ny / 2.0, d / 2.0, device)
+    wall = boundaries.make_channel_wall_mask(ny, nx, obst, device)
+    return DomainSpec(nx, ny, 3.0 * u_in * d / re + 0.5, u_in, 1.0, wall, obst)
+
+
+class BatchedSolver:
+    """Packed multi-domain D2Q9 solver (float32).
+
+    State phase and API follow :class:`tensorlbm_b200.LBMSolver`: ``load``
+    takes TensorLBM-phase fields, ``f(i)`` returns domain i in that phase, and
+    ``forces`` holds the float64 momentum-exchange force per domain of every
+    recorded step."""
+
+    ALIGN = 32  # elements: every domain block starts on a 128-byte boundary
+
+    def __init__(self, domains: list[DomainSpec], collision: str = "bgk", *, device=None,
+                 tile: tuple[int, int] = (64, 4), mode: str = "graph", ctas_per_sm: int = 0):
+        if collision not in ("bgk", "mrt"):
+            raise ValueError("the batched runner supports 'bgk' and 'mrt'")
+        if mode not in ("graph", "launch", "persistent"):
+            raise ValueError("mode must be 'graph', 'launch' or 'persistent'")
+        self.device = _ops.cuda_device(device)
+        self.domains = list(domains)
+        self.collision = collision
+        self.mode = mode
+        n = len(self.domains)
+        doms = (BatchDomain * n)()
+        f_off, c_off = 0, 0
+        self.f_offsets, self.cell_offsets = [], []
+        for i, d in enumerate(self.domains):
+            cells = d.nx * d.ny
+            doms[i].f_offset, doms[i].cell_offset = f_off, c_off
+            doms[i].nx, doms[i].ny, doms[i].tau = d.nx, d.ny, float(d.tau)
+            doms[i].u_in = float(d.u_in or 0.0)
+            doms[i].rho_out = float(1.0 if d.rho_out is None else d.rho_out)
+            doms[i].bc = (_lib.BC_ZH_INLET if d.u_in is not None else 0) | (_lib.BC_ZH_OUTLET if d.rho_out is not None else 0)
+            self.f_offsets.append(f_off)
+            self.cell_offsets.append(c_off)
+            f_off += -(-9 * cells // self.ALIGN) * self.ALIGN
+            c_off += -(-cells // self.ALIGN) * self.ALIGN
+        self.n_cells = sum(d.nx * d.ny for d in self.domains)
+        self._host_domains = doms
+        self.domains_dev = torch.frombuffer(bytearray(doms), dtype=torch.uint8).to(self.device)
+        self.fa = torch.zeros(f_off, dtype=torch.float32, device=self.device)
+        self.fb = torch.zeros_like(self.fa)
+        self.flags = torch.zeros(c_off, dtype=torch.uint8, device=self.device)
+        for i, d in enumerate(self.domains):
+            if d.wall_mask is not None or d.obstacle_mask is not None:
+                fl = _ops.build_flags((d.ny, d.nx), self.device, d.wall_mask, d.obstacle_mask)
+                self.flags[self.cell_offsets[i]: self.cell_offsets[i] + d.nx * d.ny] = fl.reshape(-1)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.sync = torch.zeros(3, dtype=torch.int32, device=self.device)
+        self.ctas_per_sm = ctas_per_sm
+        self.set_tile(*tile)
+        self.steps_done = 0
+        self._cur = 0
+        self._graph = None
+        self.forces: list[torch.Tensor] = []
+
+    # -- layout -----------------------------------------------------------------
+
+    def set_tile(self, tx: int, ty: int) -> None:
+        if tx % 32 or tx * ty > 256 or ty < 1:
+            raise ValueError("tile_x must be a multiple of 32 and tile_x * tile_y <= 256")
+        self.tile = (tx, ty)
+        tiles = []
+        for i, d in enumerate(self.domains):
+            for y0 in range(0, d.ny, ty):
+                for x0 in range(0, d.nx, tx):
+                    tiles.append((i, x0, y0))
+        self.ntiles = len(tiles)
+        self.tiles_dev = torch.tensor(tiles, dtype=torch.int32, device=self.device).reshape(-1)
+        self._graph = None
+
+    def _desc(self) -> BatchDesc:
+        b = BatchDesc()
+        b.lattice, b.dtype = 9, _lib.F32
+        b.collision = _lib.COLL_BGK if self.collision == "bgk" else _lib.COLL_MRT
+        b.ndomains = len(self.domains)
+        b.tile_x, b.tile_y = self.tile
+        b.ctas_per_sm = self.ctas_per_sm
+        return b
+
+    def _view(self, buf: torch.Tensor, i: int) -> torch.Tensor:
+        d = self.domains[i]
+        o = self.f_offsets[i]
+        return buf[o: o + 9 * d.nx * d.ny].view(9, d.ny, d.nx)
+
+    def _flags_view(self, i: int) -> torch.Tensor:
+        d = self.domains[i]
+        o = self.cell_offsets[i]
+        return self.flags[o: o + d.nx * d.ny].view(d.ny, d.nx)
+
+    def _single_desc(self, i: int, collision: str):
+        from .solvers import COLLISIONS
+
+        d = self.domains[i]
+        bc = (_lib.BC_ZH_INLET if d.u_in is not None else 0) | (_lib.BC_ZH_OUTLET if d.rho_out is not None else 0)
+        return _ops.make_desc(9, (d.nx, d.ny, 1), _lib.F32, COLLISIONS[collision], d.tau, s_e=1.64, s_eps=1.54,
+                              s_q=1.7, bc=bc, u_in=(float(d.u_in or 0.0), 0.0, 0.0),
+                              rho_out=float(1.0 if d.rho_out is None else d.rho_out))
+
+    # -- state ----------------------------------------------------------------
+
+    def load(self, fields: list[torch.Tensor]) -> "BatchedSolver":
+        """TensorLBM-phase initial populations, one (9, ny, nx) tensor per domain."""
+        if len(fields) != len(self.domains):
+            raise ValueError(f"{len(fields)} fields for {len(self.domains)} domains")
+        lib = _lib.load()
+        s = _lib.stream_of(self.device)
+        for i, f in enumerate(fields):
+            d = self.domains[i]
+            if tuple(f.shape) != (9, d.ny, d.nx):
+                raise ValueError(f"domain {i}: expected {(9, d.ny, d.nx)}, got {tuple(f.shape)}")
+            src = f.to(device=self.device, dtype=torch.float32).contiguous()
+            desc = self._single_desc(i, self.collision)
+            _lib.check(lib.tlbm_collide(ctypes.byref(desc), _lib.F32, src.data_ptr(), self._view(self.fa, i).data_ptr(),
+                                        self._flags_view(i).data_ptr(), None, s), "collide")
+        self._cur = 0
+        self.steps_done = 0
+        self.forces = []
+        self._graph = None
+        self._f0 = [f.to(self.device, torch.float32).clone() for f in fields]
+        return self
+
+    def _bufs(self):
+        return (self.fa, self.fb) if self._cur == 0 else (self.fb, self.fa)
+
+    def _launch(self, src, dst, forces) -> None:
+        st = _fn("tlbm_batch_step")(ctypes.byref(self._desc()), self.domains_dev.data_ptr(), self.tiles_dev.data_ptr(),
+                                   self.ntiles, src.data_ptr(), dst.data_ptr(), self.flags.data_ptr(),
+                                   _lib.ptr(forces), self.status.data_ptr(), _lib.stream_of(self.device))
+        _lib.check(st, "tlbm_batch_step")
+
+    def step(self, n: int = 1, *, record_forces: bool = False) -> "BatchedSolver":
+        for _ in range(n):
+            src, dst = self._bufs()
+            forces = None
+            if record_forces:
+                forces = torch.zeros((len(self.domains), 3), dtype=torch.float64, device=self.device)
+                self.forces.append(forces)
+            self._launch(src, dst, forces)
+            self._cur ^= 1
+            self.steps_done += 1
+        return self
+
+    def run(self, n: int, *, record_every: int = 0, chunk: int = 64, max_spins: int = 1 << 24) -> torch.Tensor | None:
+        """Advance n steps in the configured mode.  With record_every > 0 returns
+        the float64 force history (n // record_every, ndomains, 3)."""
+        hist = None
+        if record_every > 0:
+            hist = torch.zeros((-(-n // record_every), len(self.domains), 3), dtype=torch.float64, device=self.device)
+        if self.mode == "persistent":
+            a, b = self._bufs()
+            st = _fn("tlbm_batch_run")(ctypes.byref(self._desc()), self.domains_dev.data_ptr(),
+                                      self.tiles_dev.data_ptr(), self.ntiles, a.data_ptr(), b.data_ptr(),
+                                      self.flags.data_ptr(), n, _lib.ptr(hist), record_every,
+                                      self.sync.data_ptr(), self.status.data_ptr(), max_spins,
+                                      _lib.stream_of(self.device))
+            _lib.check(st, "tlbm_batch_run")
+            self._cur ^= n & 1
+            self.steps_done += n
+            return hist
+        if record_every > 0 or self.mode == "launch" or n < chunk:
+            for k in range(n):
+                src, dst = self._bufs()
+                forces = hist[k // record_every] if record_every > 0 and k % record_every == 0 else None
+                self._launch(src, dst, forces)
+                self._cur ^= 1
+                self.steps_done += 1
+            return hist
+        chunk += chunk & 1
+        if self._graph is None or self._graph[1] != chunk or self._graph[2] != self._cur:
+            s = torch.cuda.Stream(self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            g = torch.cuda.CUDAGraph()
+            cur0 = self._cur
+            with torch.cuda.stream(s), torch.cuda.graph(g, stream=s):
+                c = cur0
+                for _ in range(chunk):
+                    src, dst = (self.fa, self.fb) if c == 0 else (self.fb, self.fa)
+                    self._launch(src, dst, None)
+                    c ^= 1
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            self._graph = (g, chunk, cur0)
+        g = self._graph[0]
+        reps, rest = divmod(n, chunk)
+        for _ in range(reps):
+            g.replay()
+        self.steps_done += reps * chunk
+        if rest:
+            self.step(rest)
+        return hist
+
+    def f(self, i: int) -> torch.Tensor:
+        """Domain i in TensorLBM's phase (one extra pull + boundary pass)."""
+        if self.steps_done == 0:
+            return self._f0[i].clone()
+        prev = self.fb if self._cur == 0 else self.fa
+        d = self.domains[i]
+        out = torch.empty((9, d.ny, d.nx), dtype=torch.float32, device=self.device)
+        desc = self._single_desc(i, "none")
+        st = _lib.load().tlbm_step(ctypes.byref(desc), self._view(prev, i).data_ptr(), out.data_ptr(),
+                                   self._flags_view(i).data_ptr(), None, None, None, _lib.stream_of(self.device))
+        _lib.check(st, "tlbm_step(stream+bc)")
+        return out
+
+    def finite_domains(self) -> torch.Tensor:
+        """Bool per domain: every stored population of the current state finite.
+        (The status word only says that some domain produced a non-finite value.)"""
+        cur = self.fa if self._cur == 0 else self.fb
+        return torch.stack([torch.isfinite(self._view(cur, i)).all() for i in range(len(self.domains))])
+
+    def timed_steps(self, n: int) -> float:
+        """Seconds for n steps in the current mode (CUDA events, after one warm-up step)."""
+        self.run(1)
+        cur = torch.cuda.current_stream(self.device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(self.device)
+        e0.record(cur)
+        self.run(n)
+        e1.record(cur)
+        torch.cuda.synchronize(self.device)
+        return e0.elapsed_time(e1) / 1e3
+
+
+def autotune(solver: BatchedSolver, steps: int = 20,
+             tiles=((32, 8), (64, 4), (128, 2), (256, 1), (32, 4), (64, 2), (128, 1)),
+             modes=("graph", "persistent")) -> dict:
+    """Time every (tile, mode) candidate on the solver's own domains and keep the
+    fastest.  The state is advanced by the trials; reload it afterwards."""
+    results = []
+    for mode in modes:
+        for tx, ty in tiles:
+            solver.mode = mode
+            solver.set_tile(tx, ty)
+            try:
+                t = solver.timed_steps(steps)
+            except (RuntimeError, NotImplementedError):
+                continue
+            results.append({"mode": mode, "tile": (tx, ty), "seconds": t,
+                            "mlups": solver.n_cells * steps / t / 1e6})
+    best = max(results, key=lambda r: r["mlups"])
+    solver.mode = best["mode"]
+    solver.set_tile(*best["tile"])
+    return {"best": best, "trials": results}
+
+
+def uniform_scan(n_domains: int, seed: int, device=None, nx_range=(128, 1024), re_range=(40.0, 300.0),
+                 u_in: float = 0.05) -> list[DomainSpec]:
+    """Seeded design of the batched-form case: nx ~ U{nx_range} (multiple of 8 so
+    that ny = nx/4 and D = ny/8 stay whole), Re ~ U(re_range)."""
+    g = torch.Generator().manual_seed(seed)
+    nxs = torch.randint(nx_range[0] // 8, nx_range[1] // 8 + 1, (n_domains,), generator=g) * 8
+    res = re_range[0] + (re_range[1] - re_range[0]) * torch.rand(n_domains, generator=g, dtype=torch.float64)
+    return [cylinder_channel(int(nx), float(re), u_in, device) for nx, re in zip(nxs.tolist(), res.tolist())]
+
+
+def equilibrium_start(domains: list[DomainSpec], device=None) -> list[torch.Tensor]:
+    """Uniform inlet flow with zero velocity in the obstacle (cylinder_flow.py start state)."""
+    from .d2q9 import equilibrium
+
+    out = []
+    for d in domains:
+        ux = torch.full((d.ny, d.nx), float(d.u_in or 0.0), device=device)
+        if d.obstacle_mask is not None:
+            ux[d.obstacle_mask.to(ux.device)] = 0.0
+        out.append(equilibrium(torch.ones_like(ux), ux, torch.zeros_like(ux)))
+    return out
+
+
+def strouhal(lift: torch.Tensor, length_ref: float, u_ref: float, sample_every: int = 1,
+             st_band=(0.05, 0.35)) -> float | None:
+    """Dominant shedding frequency of a lift history as St = f D / U: Hann
+    window, band-limited FFT peak (the FFT branch of postprocess.py:646)."""
+    x = lift.detach().double().cpu()
+    x = x - x.mean()
+    n = x.numel()
+    if n < 32:
+        return None
+    w = torch.hann_window(n, periodic=False, dtype=torch.float64)
+    spec = torch.fft.rfft(x * w).abs()
+    freq = torch.fft.rfftfreq(n, d=float(sample_every), dtype=torch.float64)
+    st = freq * length_ref / u_ref
+    band = (st >= st_band[0]) & (st <= st_band[1])
+    if not bool(band.any()):
+        return None
+    k = int(torch.argmax(torch.where(band, spec, torch.zeros_like(spec))))
+    return float(st[k])
+
+
+__all__ = ["DomainSpec", "BatchedSolver", "autotune", "cylinder_channel", "uniform_scan", "equilibrium_start",
+           "strouhal"]

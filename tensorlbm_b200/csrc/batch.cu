@@ -1,0 +1,219 @@
+// Batched runner: many independent small domains advanced together.
+//
+// The domains (each its own (Q, ny, nx) block at f_offset in one packed
+// population buffer, its flag bytes at cell_offset in one packed flag buffer)
+// are cut into tiles of tile_x x tile_y cells.  A step is the fused per-cell
+// update (cell_update, identical arithmetic to tlbm_step) over every tile, so
+// each domain evolves exactly as it would alone.
+//
+// Two execution modes:
+//  * tlbm_batch_step: one launch per step, grid = tiles (the caller replays a
+//    CUDA graph of these launches);
+//  * tlbm_batch_run: one persistent cooperative launch that runs nsteps steps,
+//    each CTA striding over the tile list, with a grid barrier between steps.
+//    The barrier spins a bounded number of times; on expiry the kernel records
+//    TLBM_ERR_TIMEOUT in *status and every CTA returns.
+#include <cooperative_groups.h>
+
+#include "tlbm_step.cuh"
+
+namespace tlbm {
+namespace {
+
+template <typename T>
+__device__ __forceinline__ void domain_params(const tlbm_batch_domain& dm, int collision, CollideParams<T>& cp,
+                                              BcParams<T>& bp) {
+  // per-domain relaxation time; the other rates are TensorLBM's D2Q9 defaults
+  cp = make_collide_params<T>(dm.tau, 1.64, 1.54, 1.7, -1.0, 1.0, 1.0, 1.0, 0.0);
+  bp = make_bc_params<T>(dm.u_in, 0.0, 0.0, dm.rho_out, 0.0);
+  (void)collision;
+}
+
+template <class L, typename S, int COLL>
+__device__ __forceinline__ void process_tile(const tlbm_batch_domain* __restrict__ doms, const int* __restrict__ tiles,
+                                             long long t, const S* fin, S* fout, const uint8_t* flags,
+                                             double* forces, unsigned int* status) {
+  using T = typename Storage<S>::T;
+  const int di = tiles[3 * t + 0];
+  const int x = tiles[3 * t + 1] + threadIdx.x;
+  const int y = tiles[3 * t + 2] + threadIdx.y;
+  const tlbm_batch_domain dm = doms[di];
+  CollideParams<T> cp;
+  BcParams<T> bp;
+  domain_params<T>(dm, COLL, cp, bp);
+  Domain<S, S> d;
+  d.fin = fin + dm.f_offset;
+  d.fout = fout + dm.f_offset;
+  d.flags = flags ? flags + dm.cell_offset : nullptr;
+  d.tau_field = nullptr;
+  d.force = forces ? forces + 3 * (long long)di : nullptr;
+  d.status = status;
+  d.wall_u = nullptr;
+  d.nx = dm.nx;
+  d.ny = dm.ny;
+  d.nz = 1;
+  d.plane = (long long)dm.nx * dm.ny;
+  d.n = d.plane;
+  d.bc = dm.bc;
+  cell_update<L, S, S, COLL, true>(d, x, y, 0, x < dm.nx && y < dm.ny, cp, bp);
+}
+
+template <class L, typename S, int COLL>
+__global__ void __launch_bounds__(256) k_batch_step(const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
+                                                    const S* fin, S* fout, const uint8_t* flags, double* forces,
+                                                    unsigned int* status) {
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x)
+    process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status);
+}
+
+// Grid barrier over a cooperative launch, bounded: sync[0] counts arrivals,
+// sync[1] is the generation, sync[2] the error flag.  Returns false if the wait
+// gave up (or another CTA already did); the caller then returns.
+__device__ bool grid_barrier(unsigned int* sync, unsigned long long max_spins) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    volatile unsigned int* gen = sync + 1;
+    volatile unsigned int* err = sync + 2;
+    const unsigned int g = *gen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(sync, 1u);
+    if (arrived == gridDim.x - 1) {
+      sync[0] = 0u;
+      __threadfence();
+      atomicAdd(sync + 1, 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (*gen == g && *err == 0u) {
+        if (++spins > max_spins) {
+          atomicExch(sync + 2, 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok = (*err == 0u);
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+template <class L, typename S, int COLL>
+__global__ void __launch_bounds__(256) k_batch_run(const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
+                                                   S* fa, S* fb, const uint8_t* flags, int nsteps, double* force_hist,
+                                                   int ndomains, int record_every, unsigned int* sync,
+                                                   unsigned int* status, unsigned long long max_spins) {
+  for (int s = 0; s < nsteps; ++s) {
+    const S* fin = (s & 1) ? fb : fa;
+    S* fout = (s & 1) ? fa : fb;
+    double* forces = nullptr;
+    if (force_hist && record_every > 0 && (s % record_every) == 0)
+      forces = force_hist + 3 * (long long)ndomains * (s / record_every);
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x)
+      process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status);
+    if (!grid_barrier(sync, max_spins)) {
+      if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x == 0) atomicOr(status, 2u);
+      return;
+    }
+  }
+}
+
+template <class L, typename S, int COLL>
+int launch_batch(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
+                 const void* fin, void* fout, const uint8_t* flags, double* forces, unsigned int* status,
+                 cudaStream_t s) {
+  const dim3 block(b.tile_x, b.tile_y);
+  const long long grid = ntiles < 0x7fffffffLL ? ntiles : 0x7fffffffLL;
+  k_batch_step<L, S, COLL><<<(unsigned)grid, block, 0, s>>>(doms, tiles, ntiles, (const S*)fin, (S*)fout, flags,
+                                                           forces, status);
+  return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
+}
+
+template <class L, typename S, int COLL>
+int launch_batch_run(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
+                     void* fa, void* fb, const uint8_t* flags, int nsteps, double* force_hist, int record_every,
+                     unsigned int* sync, unsigned int* status, long long max_spins, cudaStream_t s) {
+  const dim3 block(b.tile_x, b.tile_y);
+  int dev = 0, sms = 0, per_sm = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+    return TLBM_ERR_UNSUPPORTED;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
+  auto kern = k_batch_run<L, S, COLL>;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)(block.x * block.y), 0) != cudaSuccess)
+    return TLBM_ERR_LAUNCH;
+  if (per_sm < 1) return TLBM_ERR_UNSUPPORTED;
+  if (b.ctas_per_sm > 0 && b.ctas_per_sm < per_sm) per_sm = b.ctas_per_sm;
+  long long grid = (long long)sms * per_sm;
+  if (grid > ntiles) grid = ntiles;
+  if (grid < 1) return TLBM_OK;
+  const tlbm_batch_domain* a0 = doms;
+  const int* a1 = tiles;
+  long long a2 = ntiles;
+  S* a3 = (S*)fa;
+  S* a4 = (S*)fb;
+  const uint8_t* a5 = flags;
+  int a6 = nsteps;
+  double* a7 = force_hist;
+  int a8 = b.ndomains;
+  int a9 = record_every;
+  unsigned int* a10 = sync;
+  unsigned int* a11 = status;
+  unsigned long long a12 = (unsigned long long)max_spins;
+  void* args[] = {&a0, &a1, &a2, &a3, &a4, &a5, &a6, &a7, &a8, &a9, &a10, &a11, &a12};
+  if (cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)grid), block, args, 0, s) != cudaSuccess)
+    return TLBM_ERR_LAUNCH;
+  return TLBM_OK;
+}
+
+int check_batch(const tlbm_batch_desc* b, const tlbm_batch_domain* doms, const int* tiles, long long ntiles) {
+  if (!b || !doms || !tiles) return TLBM_ERR_ARG;
+  if (b->lattice != TLBM_D2Q9) return TLBM_ERR_UNSUPPORTED;
+  if (b->dtype != TLBM_F32) return TLBM_ERR_DTYPE;
+  if (b->collision != TLBM_COLL_BGK && b->collision != TLBM_COLL_MRT) return TLBM_ERR_UNSUPPORTED;
+  if (b->tile_x < 32 || (b->tile_x % 32) != 0 || b->tile_y < 1 || b->tile_x * b->tile_y > 256) return TLBM_ERR_ARG;
+  if (ntiles < 0 || b->ndomains < 1) return TLBM_ERR_SHAPE;
+  return TLBM_OK;
+}
+
+}  // namespace
+}  // namespace tlbm
+
+using namespace tlbm;
+
+extern "C" {
+
+TLBM_API int tlbm_batch_step(const tlbm_batch_desc* b, const tlbm_batch_domain* domains, const int32_t* tiles,
+                             int64_t ntiles, const void* f_in, void* f_out, const uint8_t* flags, double* forces,
+                             unsigned int* status, void* stream) {
+  int st = check_batch(b, domains, tiles, ntiles);
+  if (st != TLBM_OK) return st;
+  if (!f_in || !f_out) return TLBM_ERR_ARG;
+  if (f_in == f_out) return TLBM_ERR_ALIAS;
+  if (ntiles == 0) return TLBM_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (b->collision == TLBM_COLL_BGK)
+    return launch_batch<D2Q9, float, TLBM_COLL_BGK>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces, status, s);
+  return launch_batch<D2Q9, float, TLBM_COLL_MRT>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces, status, s);
+}
+
+TLBM_API int tlbm_batch_run(const tlbm_batch_desc* b, const tlbm_batch_domain* domains, const int32_t* tiles,
+                            int64_t ntiles, void* f_a, void* f_b, const uint8_t* flags, int32_t nsteps,
+                            double* force_history, int32_t record_every, unsigned int* sync, unsigned int* status,
+                            int64_t max_spins, void* stream) {
+  int st = check_batch(b, domains, tiles, ntiles);
+  if (st != TLBM_OK) return st;
+  if (!f_a || !f_b || !sync || !status) return TLBM_ERR_ARG;
+  if (f_a == f_b) return TLBM_ERR_ALIAS;
+  if (nsteps < 0 || max_spins < 1) return TLBM_ERR_ARG;
+  if (ntiles == 0 || nsteps == 0) return TLBM_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (b->collision == TLBM_COLL_BGK)
+    return launch_batch_run<D2Q9, float, TLBM_COLL_BGK>(*b, domains, tiles, ntiles, f_a, f_b, flags, nsteps,
+                                                        force_history, record_every, sync, status, max_spins, s);
+  return launch_batch_run<D2Q9, float, TLBM_COLL_MRT>(*b, domains, tiles, ntiles, f_a, f_b, flags, nsteps,
+                                                     force_history, record_every, sync, status, max_spins, s);
+}
+
+}  // extern "C"

@@ -72,6 +72,7 @@ StepParams make_params(const tlbm_desc& d, const void* fin, void* fout, const ui
   p.tau_field = tau_field;
   p.force = force;
   p.status = status;
+  p.wall_velocity = d.wall_velocity;
   p.nx = d.nx;
   p.ny = d.ny;
   p.nz = d.nz;
@@ -173,6 +174,22 @@ TLBM_API int tlbm_bounce_back(int32_t lattice, int32_t dtype, int64_t ncells, co
   if (ncells <= 0) return TLBM_ERR_SHAPE;
   if (!f_in || !mask || !f_out) return TLBM_ERR_ARG;
   return by_lattice_real<BbFn>(lattice, dtype, (long long)ncells, f_in, mask, f_out, as_stream(stream));
+}
+
+TLBM_API int tlbm_moving_wall_bounce_back(int32_t lattice, int32_t dtype, int64_t ncells, const void* f_in,
+                                          const uint8_t* mask, const void* wall_velocity, void* f_out,
+                                          void* stream) {
+  if (lattice != TLBM_D2Q9 && lattice != TLBM_D3Q19) return TLBM_ERR_UNSUPPORTED;
+  if (ncells <= 0) return TLBM_ERR_SHAPE;
+  if (!f_in || !mask || !wall_velocity || !f_out) return TLBM_ERR_ARG;
+  if (dtype != TLBM_F32 && dtype != TLBM_F64) return TLBM_ERR_DTYPE;
+  const bool f64 = dtype == TLBM_F64;
+  cudaStream_t s = as_stream(stream);
+  if (lattice == TLBM_D2Q9)
+    return f64 ? op_moving_wall<D2Q9, double>(ncells, f_in, mask, wall_velocity, f_out, s)
+               : op_moving_wall<D2Q9, float>(ncells, f_in, mask, wall_velocity, f_out, s);
+  return f64 ? op_moving_wall<D3Q19, double>(ncells, f_in, mask, wall_velocity, f_out, s)
+             : op_moving_wall<D3Q19, float>(ncells, f_in, mask, wall_velocity, f_out, s);
 }
 
 TLBM_API int tlbm_zou_he_inlet(int32_t lattice, int32_t dtype, int32_t nx, int32_t ny, int32_t nz, void* f,

@@ -96,28 +96,75 @@ def _grouped_sum(terms: list[tuple[float, str]]) -> str:
     return expr
 
 
+def _clean(v: float) -> float:
+    # entries below 1e-10 are round-off of the float64 Gram-Schmidt / inverse
+    # (the exact matrices have a zero there); dropping them changes results far
+    # below float32 resolution and saves an FMA each
+    return 0.0 if abs(v) <= 1e-10 else float(v)
+
+
 def gen_mrt(q: int) -> str:
+    """Straight-line MRT relaxation using opposite-direction pairs.
+
+    Every basis row is even (M[k][opp q] = M[k][q]) or odd (= -M[k][q]), so an
+    even moment only sees s = fn[q] + fn[opp q] and an odd one only
+    a = fn[q] - fn[opp q]; the back-projection splits the same way into an even
+    part E and an odd part O with f[q] -= E + O and f[opp q] -= E - O.  This is
+    the same operator with half the multiply-adds of the dense form."""
+    L = lat.LATTICES[q]
     m, minv = lat.mrt_matrices(q)
     rates = _RATES[q]
     name = {9: "d2q9", 19: "d3q19", 27: "d3q27"}[q]
+    opp = [int(v) for v in L.opp]
+    pairs = [(i, opp[i]) for i in range(1, q) if i < opp[i]]
+    rest = [i for i in range(q) if opp[i] == i]
+    # rows TensorLBM's D3Q27 Gram-Schmidt replaced by unit vectors (dependent
+    # monomials, d3q27.py:614-625) have no parity and stay dense
+    parity = {}
+    for k in range(q):
+        ev = all(abs(m[k, i] - m[k, opp[i]]) < 1e-9 for i in range(q))
+        od = all(abs(m[k, i] + m[k, opp[i]]) < 1e-9 for i in range(q))
+        parity[k] = "even" if ev else ("odd" if od else "none")
+        if parity[k] != "none":
+            sgn = 1.0 if ev else -1.0
+            for i in range(q):  # the inverse inherits the parity
+                assert abs(minv[opp[i], k] - sgn * minv[i, k]) < 1e-9, (q, k, i)
     out = [
-        f"// MRT relaxation for {name}: f_i -= sum_k Minv[i][k] * s_k * (M (f - feq))_k",
+        f"// MRT relaxation for {name}: f_i -= sum_k Minv[i][k] * s_k * (M (f - feq))_k, paired form",
         "template <typename T>",
         f"__device__ __forceinline__ void mrt_relax_{name}(T (&f)[{q}], const T (&fn)[{q}], const MrtRates<T>& r) {{",
         "  const T one = T(1);",
     ]
+    for a, b in pairs:
+        out.append(f"  const T s{a} = fn[{a}] + fn[{b}], a{a} = fn[{a}] - fn[{b}];")
     relaxed = [k for k in range(q) if rates[k] is not None]
     for k in relaxed:
-        # the Gram-Schmidt D3Q27 rows carry round-off of the same kind
-        terms = [(float(m[k, j]), f"fn[{j}]") for j in range(q) if abs(m[k, j]) > 1e-10]
+        if parity[k] == "even":
+            terms = [(_clean(m[k, i]), f"fn[{i}]") for i in rest] + [(_clean(m[k, a]), f"s{a}") for a, _ in pairs]
+        elif parity[k] == "odd":
+            terms = [(_clean(m[k, a]), f"a{a}") for a, _ in pairs]
+        else:
+            terms = [(_clean(m[k, i]), f"fn[{i}]") for i in range(q)]
         rate = "one" if rates[k] == "one" else f"r.{rates[k]}"
         out.append(f"  const T e{k} = {rate} * ({_grouped_sum(terms)});")
-    for i in range(q):
-        # entries below 1e-10 are round-off of the float64 inverse (the exact
-        # inverse has a zero there); dropping them changes results far below
-        # float32 resolution and saves an FMA each
-        terms = [(float(minv[i, k]), f"e{k}") for k in relaxed if abs(minv[i, k]) > 1e-10]
+    even = [k for k in relaxed if parity[k] == "even"]
+    odd = [k for k in relaxed if parity[k] == "odd"]
+    dense = [k for k in relaxed if parity[k] == "none"]
+
+    def nsum(i):
+        return _grouped_sum([(_clean(minv[i, k]), f"e{k}") for k in dense]) if dense else "T(0)"
+
+    for i in rest:
+        terms = [(_clean(minv[i, k]), f"e{k}") for k in even + dense]
         out.append(f"  f[{i}] -= {_grouped_sum(terms)};")
+    for a, b in pairs:
+        ev = _grouped_sum([(_clean(minv[a, k]), f"e{k}") for k in even])
+        od = _grouped_sum([(_clean(minv[a, k]), f"e{k}") for k in odd])
+        if dense:
+            out.append(f"  {{ const T E = {ev}; const T O = {od}; f[{a}] -= E + O + ({nsum(a)}); "
+                       f"f[{b}] -= E - O + ({nsum(b)}); }}")
+        else:
+            out.append(f"  {{ const T E = {ev}; const T O = {od}; f[{a}] -= E + O; f[{b}] -= E - O; }}")
     out.append("}")
     out.append("")
     return "\n".join(out)

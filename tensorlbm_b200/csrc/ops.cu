@@ -61,6 +61,18 @@ __global__ void k_bounce_back(long long n, const T* fin, const uint8_t* mask, T*
   for (int q = 0; q < L::Q; ++q) fout[(long long)q * n + i] = v[q];
 }
 
+template <class L, typename T>
+__global__ void k_moving_wall(long long n, const T* fin, const uint8_t* mask, const T* uw, T* fout) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  T v[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) v[q] = fin[(long long)q * n + i];
+  if (mask[i]) moving_wall_bounce_back<L>(v, uw[i], uw[n + i], L::DIM == 3 ? uw[2 * n + i] : T(0));
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) fout[(long long)q * n + i] = v[q];
+}
+
 // ---- boundary planes (in place) -------------------------------------------
 
 template <class L, typename T>
@@ -363,6 +375,11 @@ int op_bounce_back(long long n, const void* fin, const uint8_t* mask, void* fout
   return launch_status();
 }
 template <class L, typename T>
+int op_moving_wall(long long n, const void* fin, const uint8_t* mask, const void* uw, void* fout, cudaStream_t s) {
+  k_moving_wall<L, T><<<blocks_for(n), kThreads, 0, s>>>(n, (const T*)fin, mask, (const T*)uw, (T*)fout);
+  return launch_status();
+}
+template <class L, typename T>
 int op_zou_he_inlet(int nx, int ny, int nz, void* f, double u, double uy, double uz, const void* uxp, const void* uyp, cudaStream_t s) {
   const BcParams<T> bp = make_bc_params<T>(u, uy, uz, 1.0, 0.0);
   k_zou_he_inlet<L, T><<<blocks_for((long long)ny * nz), kThreads, 0, s>>>(nx, ny, nz, (T*)f, bp, (const T*)uxp, (const T*)uyp);
@@ -457,6 +474,10 @@ TLBM_INST_LT(D3Q19, float)
 TLBM_INST_LT(D3Q19, double)
 TLBM_INST_LT(D3Q27, float)
 TLBM_INST_LT(D3Q27, double)
+template int op_moving_wall<D2Q9, float>(long long, const void*, const uint8_t*, const void*, void*, cudaStream_t);
+template int op_moving_wall<D2Q9, double>(long long, const void*, const uint8_t*, const void*, void*, cudaStream_t);
+template int op_moving_wall<D3Q19, float>(long long, const void*, const uint8_t*, const void*, void*, cudaStream_t);
+template int op_moving_wall<D3Q19, double>(long long, const void*, const uint8_t*, const void*, void*, cudaStream_t);
 template int op_moving_lid<D2Q9, float>(int, int, int, void*, double, cudaStream_t);
 template int op_moving_lid<D2Q9, double>(int, int, int, void*, double, cudaStream_t);
 template int op_moving_lid<D3Q19, float>(int, int, int, void*, double, cudaStream_t);

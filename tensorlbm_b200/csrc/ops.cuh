@@ -12,6 +12,8 @@ int op_macroscopic(long long n, const void* f, void* rho, void* ux, void* uy, vo
 template <class L, typename T>
 int op_bounce_back(long long n, const void* fin, const uint8_t* mask, void* fout, cudaStream_t s);
 template <class L, typename T>
+int op_moving_wall(long long n, const void* fin, const uint8_t* mask, const void* uw, void* fout, cudaStream_t s);
+template <class L, typename T>
 int op_zou_he_inlet(int nx, int ny, int nz, void* f, double u, double uy, double uz, const void* uxp, const void* uyp,
                     cudaStream_t s);
 template <class L, typename T>

@@ -22,6 +22,23 @@ __device__ __forceinline__ void bounce_back(T (&f)[L::Q]) {
   }
 }
 
+// Ladd moving-wall bounce-back (propeller_benchmark.py:221-270 for D3Q19,
+// rotating_cylinder.py:140-192 for D2Q9): swap, then add
+// 2 w_q rho (c_q . u_w) / c_s^2 with rho the density before the swap,
+// evaluated as (((2 w) rho) cu) 3 like the reference, whose weights there are
+// the float32 W tensors of d2q9.py / d3q19.py cast to the field dtype.
+template <class L, typename T>
+__device__ __forceinline__ void moving_wall_bounce_back(T (&f)[L::Q], T uwx, T uwy, T uwz) {
+  const T rho = csum<L>(f, OneCoef{});
+  bounce_back<L>(f);
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) {
+    const T cu = signed_sum(L::cx(q), L::cy(q), L::cz(q), uwx, uwy, uwz);
+    const T corr = xmul(xmul(xmul(xmul(T(2), T(float(L::w(q)))), rho), cu), T(3));
+    f[q] = xadd(f[q], corr);
+  }
+}
+
 // momentum carried by the post-stream populations of one cell: sum_q c_q f_q
 template <class L, typename T>
 __device__ __forceinline__ void cell_momentum(const T (&f)[L::Q], T& mx, T& my, T& mz) {
@@ -45,7 +62,7 @@ template <typename T> struct BcParams {
 };
 
 template <typename T>
-BcParams<T> make_bc_params(double u_in0, double u_in1, double u_in2, double rho_out, double u_lid) {
+__host__ __device__ BcParams<T> make_bc_params(double u_in0, double u_in1, double u_in2, double rho_out, double u_lid) {
   BcParams<T> b;
   b.u_in = T(u_in0);
   b.uy_in = T(u_in1);

@@ -649,7 +649,7 @@ __device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp
 }
 
 template <typename T>
-CollideParams<T> make_collide_params(double tau, double s_e, double s_eps, double s_q, double s_pi,
+__host__ __device__ CollideParams<T> make_collide_params(double tau, double s_e, double s_eps, double s_q, double s_pi,
                                      double omega_b, double omega_odd, double omega_even, double c_smag) {
   CollideParams<T> cp;
   cp.tau = T(tau);

@@ -64,6 +64,7 @@ struct StepParams {
   const float* tau_field;   // per cell relaxation time, may be null
   double* force;            // [3] accumulated momentum-exchange force, may be null
   unsigned int* status;     // bit0: non-finite density seen, may be null
+  const void* wall_velocity;  // (DIM, n) moving-wall velocity, compute type, may be null
   int nx, ny, nz;
   long long plane;          // nx*ny
   long long n;              // nx*ny*nz

@@ -35,6 +35,7 @@ template <typename SI, typename SO> struct Domain {
   const float* tau_field;   // may be null
   double* force;            // may be null
   unsigned int* status;     // may be null
+  const void* wall_u;       // (DIM, n) wall velocity of TLBM_FLAG_MOVING cells, compute type; may be null
   int nx, ny, nz;
   long long plane, n;
   uint32_t bc;
@@ -100,8 +101,17 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
         if constexpr (Q == 9) zou_he_outlet_d2q9(f, bp.rho_out, bp.two_thirds_rho_out, bp.sixth_rho_out);
         else zou_he_outlet_3d<L>(f, bp.rho_out);
       }
-      // 3. full-way bounce-back
-      if (fl & TLBM_FLAG_SOLID) bounce_back<L>(f);
+      // 3. full-way bounce-back; Ladd moving wall where flagged.  A moving
+      //    obstacle cell that is also a wall cell has SOLID cleared (wall XOR
+      //    obstacle): it takes the wall swap first, then the moving-wall pass,
+      //    as bounce_back(wall) followed by moving_wall_bounce_back(obstacle).
+      if ((fl & TLBM_FLAG_MOVING) && d.wall_u) {
+        const T* uw = static_cast<const T*>(d.wall_u);
+        if (!(fl & TLBM_FLAG_SOLID)) bounce_back<L>(f);
+        moving_wall_bounce_back<L>(f, uw[cell], uw[N + cell], L::DIM == 3 ? uw[2 * N + cell] : T(0));
+      } else if (fl & TLBM_FLAG_SOLID) {
+        bounce_back<L>(f);
+      }
       // 4. moving lid
       if ((d.bc & TLBM_BC_LID) && y == d.ny - 1) {
         if constexpr (Q == 9) moving_lid_d2q9(f, bp.u_lid);
@@ -142,6 +152,7 @@ __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typena
   d.tau_field = p.tau_field;
   d.force = p.force;
   d.status = p.status;
+  d.wall_u = p.wall_velocity;
   d.nx = p.nx;
   d.ny = p.ny;
   d.nz = p.nz;

@@ -121,7 +121,7 @@ class LBMSolver:
 
     def __init__(self, lattice, shape, tau: float, collision: str = "bgk", *, device=None, storage="f32",
                  wall_mask=None, obstacle_mask=None, wall_mode: str = "fullway", tau_field=None,
-                 track_force: bool = False, **cfg):
+                 track_force: bool = False, wall_velocity=None, **cfg):
         q = _LATTICES[lattice]
         if isinstance(storage, torch.dtype):
             storage = _TORCH_STORAGE[storage]
@@ -141,6 +141,17 @@ class LBMSolver:
         self.flags = None
         if wall_mask is not None or obstacle_mask is not None:
             self.flags = _ops.build_flags(shape, self.device, wall_mask, obstacle_mask, wall_mode)
+        self.wall_u = None
+        if wall_velocity is not None:
+            # the obstacle becomes a Ladd moving wall with this velocity field
+            if obstacle_mask is None:
+                raise ValueError("wall_velocity needs an obstacle_mask (the moving surface)")
+            if len(wall_velocity) != len(shape) or any(tuple(u.shape) != shape for u in wall_velocity):
+                raise ValueError(f"wall_velocity must be {len(shape)} fields of shape {shape}")
+            moving = _ops._mask_u8(obstacle_mask.to(self.device), shape)
+            self.flags.bitwise_or_(moving * _lib.FLAG_MOVING)
+            self.wall_u = torch.stack([u.to(device=self.device, dtype=self.compute_dtype)
+                                       for u in wall_velocity]).contiguous()
         self.tau_field = None
         if tau_field is not None:
             if tuple(tau_field.shape) != shape:
@@ -156,6 +167,9 @@ class LBMSolver:
         self.forces: list[torch.Tensor] = []
         self._desc = self.cfg.desc(self.code)
         self._desc_none = self.cfg.desc(self.code, "none")
+        if self.wall_u is not None:
+            self._desc.wall_velocity = self.wall_u.data_ptr()
+            self._desc_none.wall_velocity = self.wall_u.data_ptr()
         self._graph = None
 
     # -- state -----------------------------------------------------------------

@@ -75,15 +75,46 @@ def near_eq_field(torch, q, spatial, dtype, seed, amp=0.05, noise=0.01):
     return rho, u, feq * (1 + pert)
 
 
+def moving_wall(torch) -> None:
+    """Ladd moving-wall bounce-back (rotating_cylinder.py / propeller_benchmark.py)
+    on a rotating disc / rotor-like cylinder, float32 and float64."""
+    from tensorlbm.propeller_benchmark import moving_wall_bounce_back_3d, rotating_wall_velocity_3d
+    from tensorlbm.rotating_cylinder import moving_wall_bounce_back, rotating_wall_velocity
+
+    out = {}
+    sp2, sp3 = (32, 64), (8, 12, 32)
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        _, _, f9 = near_eq_field(torch, 9, sp2, dt, 51)
+        _, _, f19 = near_eq_field(torch, 19, sp3, dt, 52)
+        yy, xx = torch.meshgrid(torch.arange(sp2[0]), torch.arange(sp2[1]), indexing="ij")
+        disc = (xx - 30.3) ** 2 + (yy - 15.6) ** 2 <= 9.5 ** 2
+        ux2, uy2 = rotating_wall_velocity(disc, 30.3, 15.6, 0.004)
+        zz, yy3, xx3 = torch.meshgrid(torch.arange(sp3[0]), torch.arange(sp3[1]), torch.arange(sp3[2]), indexing="ij")
+        rotor = ((yy3 - 5.6) ** 2 + (zz - 3.8) ** 2 <= 3.2 ** 2) & (xx3 >= 9) & (xx3 < 21)
+        ux3, uy3, uz3 = rotating_wall_velocity_3d(rotor, 15.0, 5.6, 3.8, 0.006)
+        out.update({f"f9_{tag}": f9, f"f19_{tag}": f19,
+                    # outputs on the masked cells only; the others must equal the input
+                    f"mw9_{tag}": moving_wall_bounce_back(f9, disc, ux2, uy2)[:, disc],
+                    f"mw19_{tag}": moving_wall_bounce_back_3d(f19, rotor, ux3, uy3, uz3)[:, rotor]})
+        out.update({"disc": disc, "rotor": rotor, "ux2": ux2, "uy2": uy2, "ux3": ux3, "uy3": uy3, "uz3": uz3})
+    arrays = {k: (v.detach().cpu().numpy() if isinstance(v, torch.Tensor) else np.asarray(v)) for k, v in out.items()}
+    np.savez_compressed(HERE / "moving_wall.npz", **arrays)
+    print("wrote moving_wall.npz")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
     ap.add_argument("--skip-long", action="store_true", help="skip the 64^3 x 1000-step cavity run")
+    ap.add_argument("--only", default=None, help="write only this group of fixtures (e.g. moving_wall)")
     args = ap.parse_args()
     import_reference(args.reference)
     import torch
 
     torch.set_num_threads(8)
+    if args.only == "moving_wall":
+        moving_wall(torch)
+        return
     from tensorlbm import boundaries as b2
     from tensorlbm import boundaries3d as b3
     from tensorlbm import boundaries_d3q27 as b27

@@ -225,3 +225,26 @@ def test_correct_mass(cuda):
     out = solver3d.correct_mass3d(f, 123.0)
     assert abs(float(out.sum()) - 123.0) < 1e-9
     assert torch.equal(solver3d.correct_mass3d(torch.zeros_like(f), 5.0), torch.zeros_like(f))
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_moving_wall_bounce_back(cuda, tag):
+    """Ladd moving wall (rotating_cylinder.py:140, propeller_benchmark.py:221),
+    bit for bit against the reference on a rotating disc and rotor."""
+    from tensorlbm_b200 import propeller_benchmark, rotating_cylinder
+
+    g = golden("moving_wall")
+    disc, rotor = T(g["disc"], cuda), T(g["rotor"], cuda)
+    f9, f19 = T(g[f"f9_{tag}"], cuda), T(g[f"f19_{tag}"], cuda)
+    ux2, uy2 = rotating_cylinder.rotating_wall_velocity(disc, 30.3, 15.6, 0.004)
+    assert same(N(ux2), g["ux2"]) and same(N(uy2), g["uy2"])
+    out9 = N(rotating_cylinder.moving_wall_bounce_back(f9, disc, ux2, uy2))
+    assert same(out9[:, g["disc"]], g[f"mw9_{tag}"])
+    assert same(out9[:, ~g["disc"]], g[f"f9_{tag}"][:, ~g["disc"]])
+    ux3, uy3, uz3 = propeller_benchmark.rotating_wall_velocity_3d(rotor, 15.0, 5.6, 3.8, 0.006)
+    assert same(N(uy3), g["uy3"]) and same(N(uz3), g["uz3"])
+    out19 = N(propeller_benchmark.moving_wall_bounce_back_3d(f19, rotor, ux3, uy3, uz3))
+    assert same(out19[:, g["rotor"]], g[f"mw19_{tag}"])
+    assert same(out19[:, ~g["rotor"]], g[f"f19_{tag}"][:, ~g["rotor"]])
+    with pytest.raises(ValueError):
+        rotating_cylinder.moving_wall_bounce_back(f9, disc, ux2, uy2[:-1])

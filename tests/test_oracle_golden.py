@@ -93,6 +93,16 @@ def test_boundaries(q):
     assert np.max(np.abs(got - ref)) < 1e-6 * max(np.max(np.abs(ref)), 1.0)
 
 
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_moving_wall(tag):
+    g = golden("moving_wall")
+    for f, m, uw, key in ((g[f"f9_{tag}"], g["disc"], (g["ux2"], g["uy2"]), f"mw9_{tag}"),
+                          (g[f"f19_{tag}"], g["rotor"], (g["ux3"], g["uy3"], g["uz3"]), f"mw19_{tag}")):
+        out = O.moving_wall_bounce_back(f, m, *uw)
+        assert same(out[:, m], g[key])
+        assert same(out[:, ~m], f[:, ~m])
+
+
 def test_masks_bitwise():
     g = golden("masks")
     assert np.array_equal(O.sphere_mask(32, 16, 16, 12.0, 8.0, 8.0, 4.5), g["sphere"])
