@@ -99,6 +99,11 @@ typedef struct tlbm_desc {
   double rho_out;      /* Zou/He outlet density */
   const void* wall_velocity; /* (DIM, N) wall velocity of TLBM_FLAG_MOVING cells in the compute
                                 type (float32; float64 for TLBM_F64), x-component first; may be NULL */
+  double force_lin;    /* linear body force F = force_lin * rho * u (Lundgren forcing of forced
+                          isotropic turbulence), exact-difference scheme: after the collision
+                          f += feq(rho, (1 + A) u) - feq(rho, u); 0 = none.  BGK and
+                          Smagorinsky collisions only (else TLBM_ERR_UNSUPPORTED); |A| < 1.
+                          New in this library. */
 } tlbm_desc;
 
 /* ---- fused time step ------------------------------------------------------
@@ -310,6 +315,80 @@ TLBM_API int tlbm_batch_run(const tlbm_batch_desc* b, const tlbm_batch_domain* d
                             int64_t ntiles, void* f_a, void* f_b, const uint8_t* flags, int32_t nsteps,
                             double* force_history, int32_t record_every, unsigned int* sync, unsigned int* status,
                             int64_t max_spins, void* stream);
+
+/* ---- learned LES closure (D3Q19) ---------------------------------------------
+ * TensorLBM's closure is 2-D (ai/model.py:40-92 EddyViscosityMLP, 3 strain
+ * inputs -> 2x16 tanh -> softplus nu_t; ai/inference.py:68-92
+ * collide_ai_les_bgk, tau + 3 nu_t; ai/train.py:310 Adam/MSE).  These entry
+ * points are its 3-D replacement: 9 invariants of Pi_neq -> 3 x 64 SiLU ->
+ * nu_t = nu_scale softplus(y); tau_eff = tau0 + 3 nu_t, Smagorinsky tau_s
+ * (turbulence.py:183-208) outside the training range of any feature.
+ *
+ * Training vector theta (float32, tlbm_mlp_param_count() entries):
+ * W1 (64x9, row = output), b1, W2 (64x64), b2, W3, b3, w4 (64), b4.
+ * Features are normalised as (x - mean) * istd before the first layer. */
+
+/* Block means over factor^3 cells of rho, u, u_iu_j from D3Q19 float32
+ * populations (Q, nz, ny, nx); out: (10, nz/f, ny/f, nx/f) float32 in the order
+ * rho, ux, uy, uz, uxux, uyuy, uzuz, uxuy, uxuz, uyuz.  u includes half the
+ * linear force, m / rho (1 + A/2).  Extends ai/pipeline.py:93 (_coarsen_mean)
+ * to 3-D and to the velocity products. */
+TLBM_API int tlbm_les_filter_moments(const float* f, int32_t nx, int32_t ny, int32_t nz, int32_t factor,
+                                     double a_lin, float* out, void* stream);
+
+/* Training samples of one filtered field (nx, ny, nz are the filtered sizes):
+ * features (N, 9) of Pi = -(2/3) rho tau_eff S (S by periodic central
+ * differences; tau_eff = tau0 + 3 nu_hat if nu_hat != NULL, else the
+ * Smagorinsky tau of c_s), target nu* = -(tau_sgs_dev : S) / (2 S:S),
+ * weight S:S.  No reference counterpart. */
+TLBM_API int tlbm_les_samples(const float* moments, int32_t nx, int32_t ny, int32_t nz, double tau0, double c_s,
+                              const float* nu_hat, float* features, float* target, float* weight, void* stream);
+
+TLBM_API int32_t tlbm_mlp_param_count(void);
+TLBM_API int32_t tlbm_mlp_blob_bytes(void);
+/* number of gradient partial blocks (rows of N_PARAMS + 1 floats) for a batch */
+TLBM_API int64_t tlbm_mlp_grad_blocks(int64_t batch);
+
+/* Gradient of L = sum_s w_s (softplus(y_s) - t_s)^2 / count over the rows
+ * idx[0..count) (idx NULL: rows 0..count-1) of x (.., 9), t, w (w NULL: 1).
+ * Writes per-block partial gradients and block losses to
+ * partial[tlbm_mlp_grad_blocks(count)][N_PARAMS + 1].  Replaces the autograd
+ * backward of ai/train.py:310 (train_eddy_viscosity_model). */
+TLBM_API int tlbm_mlp_grad(const float* theta, const float* mean, const float* istd, const float* x,
+                           const float* target, const float* weight, const int64_t* idx, int64_t count,
+                           float* partial, void* stream);
+
+/* Sum the partials in block order; Adam step number `step` (from 1) on theta
+ * with moments m, v (lr = 0: no update).  grad_out (N_PARAMS) and loss_out
+ * (1 float) may be NULL. */
+TLBM_API int tlbm_mlp_adam(float* theta, float* m, float* v, const float* partial, int64_t nblocks, double lr,
+                           double beta1, double beta2, double eps, int64_t step, float* grad_out, float* loss_out,
+                           void* stream);
+
+/* float32 forward: y (count) of raw features x (count, 9). */
+TLBM_API int tlbm_mlp_eval(const float* theta, const float* mean, const float* istd, const float* x, int64_t count,
+                           float* y, void* stream);
+
+/* Pack theta, the feature statistics (mean, std) and the training range
+ * (lo, hi) into the inference blob (tlbm_mlp_blob_bytes(), 16-byte aligned):
+ * bf16 weight tiles in the tensor cores' 128-byte-swizzled K-major layout. */
+TLBM_API int tlbm_mlp_pack(const float* theta, const float* mean, const float* std, const float* lo, const float* hi,
+                           double nu_scale, void* blob, void* stream);
+
+/* Tensor-core inference (tcgen05, bf16 weights and layer inputs, fp32
+ * accumulation): y (count) of raw features x (count, 9).  status bit 2: a
+ * bounded tensor-core wait expired. */
+TLBM_API int tlbm_mlp_infer(const void* blob, const float* x, int64_t count, float* y, unsigned int* status,
+                            void* stream);
+
+/* One fused D3Q19 LES step on a periodic box (float32 populations, pull):
+ * BGK with the learned tau_eff and exact-difference linear forcing
+ * F = force_lin rho u.  tau_out (per cell), fallback_count (cells that used the
+ * Smagorinsky tau of c_s) and status may be NULL.  Replaces
+ * collide_ai_les_bgk (ai/inference.py:68-92) + stream for 3-D. */
+TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, double c_s, double force_lin,
+                           const void* blob, const float* f_in, float* f_out, float* tau_out,
+                           unsigned int* fallback_count, unsigned int* status, void* stream);
 
 TLBM_API const char* tlbm_status_string(int status);
 TLBM_API int tlbm_abi_version(void);

@@ -55,6 +55,7 @@ class Desc(ctypes.Structure):
         ("u_in", ctypes.c_double * 3),
         ("rho_out", ctypes.c_double),
         ("wall_velocity", ctypes.c_void_p),
+        ("force_lin", ctypes.c_double),
     ]
 
 
@@ -105,10 +106,22 @@ SIGNATURES: dict[str, list] = {
     "tlbm_batch_run": [ctypes.POINTER(BatchDesc), _P, _P, _I64, _P, _P, _P, _I32, _P, _I32, _P, _P, _I64, _P],
     "tlbm_link_list_noalloc": [_P, _I64, _P, _I64, _P, _P],
     "tlbm_link_list_static_capacity": [],
+    "tlbm_les_filter_moments": [_P, _I32, _I32, _I32, _I32, _D, _P, _P],
+    "tlbm_les_samples": [_P, _I32, _I32, _I32, _D, _D, _P, _P, _P, _P, _P],
+    "tlbm_mlp_param_count": [],
+    "tlbm_mlp_blob_bytes": [],
+    "tlbm_mlp_grad_blocks": [_I64],
+    "tlbm_mlp_grad": [_P, _P, _P, _P, _P, _P, _P, _I64, _P, _P],
+    "tlbm_mlp_adam": [_P, _P, _P, _P, _I64, _D, _D, _D, _D, _I64, _P, _P, _P],
+    "tlbm_mlp_eval": [_P, _P, _P, _P, _I64, _P, _P],
+    "tlbm_mlp_pack": [_P, _P, _P, _P, _P, _D, _P, _P],
+    "tlbm_mlp_infer": [_P, _P, _I64, _P, _P, _P],
+    "tlbm_les_step": [_I32, _I32, _I32, _D, _D, _D, _P, _P, _P, _P, _P, _P, _P],
     "tlbm_status_string": [ctypes.c_int],
     "tlbm_abi_version": [],
 }
-_RESTYPES = {"tlbm_link_blocks": _I64, "tlbm_link_list_static_capacity": _I64, "tlbm_status_string": ctypes.c_char_p}
+_RESTYPES = {"tlbm_link_blocks": _I64, "tlbm_link_list_static_capacity": _I64, "tlbm_status_string": ctypes.c_char_p,
+             "tlbm_mlp_param_count": _I32, "tlbm_mlp_blob_bytes": _I32, "tlbm_mlp_grad_blocks": _I64}
 
 _lib: ctypes.CDLL | None = None
 

@@ -1,0 +1,179 @@
+// Fused D3Q19 LES step with the learned eddy-viscosity closure.
+//
+// Persistent kernel: each CTA loads the packed network once (shared memory),
+// allocates 128 TMEM columns, then walks tiles of 256 consecutive cells:
+//   pull (periodic) -> rho, u -> Pi_neq = sum_q c c (f - feq) -> 9 features
+//   -> tcgen05 MLP (three 64-wide layers, bf16 x bf16 -> fp32 in TMEM)
+//   -> nu_t = nu_scale softplus(y), tau_eff = tau0 + 3 nu_t
+//      (Smagorinsky tau_s where a feature leaves the training range)
+//   -> BGK with tau_eff + exact-difference linear forcing -> store.
+// The populations stay in registers across the tensor-core pass, so the
+// kernel moves 2 x 19 x 4 bytes per cell like the plain fused step.
+#include "tlbm_collide.cuh"
+#include "tlbm_mlp.cuh"
+
+namespace tlbm {
+namespace {
+
+struct LesStep {
+  const float* fin;
+  float* fout;
+  int nx, ny, nz;
+  long long plane, n;
+  float tau0, c_s, a_lin;
+  const uint8_t* blob;
+  float* tau_out;                // per-cell tau_eff, may be null
+  unsigned int* fallback_count;  // cells that took the Smagorinsky fallback, may be null
+  unsigned int* status;          // bit0 non-finite, bit2 tensor-core wait timeout; may be null
+};
+
+__global__ void __launch_bounds__(mlp::TILE, 3) k_step_les(LesStep p) {
+  using L = D3Q19;
+  constexpr int Q = L::Q;
+  extern __shared__ uint8_t raw[];
+  mlp::Engine e;
+  e.setup(raw, p.blob);
+  const float* P = e.params();
+  const float tmax = p.tau0 + 0.5f > 1.0f ? p.tau0 + 0.5f : 1.0f;
+  const long long ntiles = (p.n + mlp::TILE - 1) / mlp::TILE;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const long long cell = t * mlp::TILE + threadIdx.x;
+    const bool active = cell < p.n;
+    float f[Q];
+    float z[mlp::NF];
+    float rho = 1.0f, ux = 0.0f, uy = 0.0f, uz = 0.0f, tau_s = p.tau0;
+    bool inrange = false;
+    if (active) {
+      const int x = int(cell % p.nx);
+      const int y = int((cell / p.nx) % p.ny);
+      const int zc = int(cell / p.plane);
+      const int xm = x == 0 ? p.nx - 1 : x - 1, xp = x == p.nx - 1 ? 0 : x + 1;
+      const int ym = y == 0 ? p.ny - 1 : y - 1, yp = y == p.ny - 1 ? 0 : y + 1;
+      const int zm = zc == 0 ? p.nz - 1 : zc - 1, zp = zc == p.nz - 1 ? 0 : zc + 1;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int sx = L::cx(q) > 0 ? xm : (L::cx(q) < 0 ? xp : x);
+        const int sy = L::cy(q) > 0 ? ym : (L::cy(q) < 0 ? yp : y);
+        const int sz = L::cz(q) > 0 ? zm : (L::cz(q) < 0 ? zp : zc);
+        f[q] = __ldg(p.fin + (long long)q * p.n + (long long)sz * p.plane + (long long)sy * p.nx + sx);
+      }
+      macroscopic_fused<L>(f, rho, ux, uy, uz);
+      const float usq = ux * ux + uy * uy + uz * uz;
+      float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const float fn = f[q] - feq_fused<L>(q, rho, ux, uy, uz, usq);
+        if (L::cx(q) != 0) pxx += fn;
+        if (L::cy(q) != 0) pyy += fn;
+        if (L::cz(q) != 0) pzz += fn;
+        if (L::cx(q) * L::cy(q) != 0) pxy += float(L::cx(q) * L::cy(q)) * fn;
+        if (L::cx(q) * L::cz(q) != 0) pxz += float(L::cx(q) * L::cz(q)) * fn;
+        if (L::cy(q) * L::cz(q) != 0) pyz += float(L::cy(q) * L::cz(q)) * fn;
+      }
+      float feat[mlp::NF];
+      mlp::features<float>(pxx, pyy, pzz, pxy, pxz, pyz, rho, p.tau0, p.c_s, feat);
+      tau_s = feat[6] + p.tau0;
+      inrange = true;
+#pragma unroll
+      for (int k = 0; k < mlp::NF; ++k) {
+        inrange = inrange && feat[k] >= P[mlp::P_LO + k] && feat[k] <= P[mlp::P_HI + k];
+        z[k] = (feat[k] - P[mlp::P_MEAN + k]) * P[mlp::P_ISTD + k];
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) f[q] = 0.0f;
+#pragma unroll
+      for (int k = 0; k < mlp::NF; ++k) z[k] = 0.0f;
+    }
+    bool ok = true;
+    const float y = e.run(z, ok);
+    if (active) {
+      float tau = tau_s;
+      if (inrange) {
+        tau = p.tau0 + 3.0f * P[mlp::P_NUS] * mlp::softplus(y);
+        tau = tau < 0.5001f ? 0.5001f : (tau > tmax ? tmax : tau);
+      }
+      const float inv = 1.0f / tau;
+      const float usq = ux * ux + uy * uy + uz * uz;
+      const float k = 1.0f + p.a_lin;
+      const float usq_k = usq * k * k;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const float feq = feq_fused<L>(q, rho, ux, uy, uz, usq);
+        float fo = f[q] - (f[q] - feq) * inv;
+        if (p.a_lin != 0.0f) fo += feq_fused<L>(q, rho, ux * k, uy * k, uz * k, usq_k) - feq;
+        p.fout[(long long)q * p.n + cell] = fo;
+      }
+      if (p.tau_out) p.tau_out[cell] = tau;
+      if (p.status && !(rho == rho && rho - rho == 0.0f)) atomicOr(p.status, 1u);
+    }
+    if (p.fallback_count) {
+      const unsigned int fb = __ballot_sync(0xffffffffu, active && !inrange);
+      if ((threadIdx.x & 31) == 0 && fb) atomicAdd(p.fallback_count, __popc(fb));
+    }
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0 && p.status) atomicOr(p.status, 4u);
+      break;
+    }
+  }
+  e.teardown();
+}
+
+int les_grid(long long n, int& grid) {
+  static int per_sm = -1, sms = 0;
+  if (per_sm < 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
+    if (cudaFuncSetAttribute(k_step_les, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::SM_BYTES) != cudaSuccess)
+      return TLBM_ERR_LAUNCH;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_les, mlp::TILE, mlp::SM_BYTES) != cudaSuccess)
+      return TLBM_ERR_LAUNCH;
+    const int tmem_cap = 512 / int(mlp::TMEM_COLS);
+    if (per_sm > tmem_cap) per_sm = tmem_cap;
+  }
+  if (per_sm < 1) return TLBM_ERR_UNSUPPORTED;
+  const long long ntiles = (n + mlp::TILE - 1) / mlp::TILE;
+  const long long g = (long long)sms * per_sm;
+  grid = int(g < ntiles ? g : ntiles);
+  return TLBM_OK;
+}
+
+}  // namespace
+}  // namespace tlbm
+
+using namespace tlbm;
+
+extern "C" {
+
+TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, double c_s, double force_lin,
+                           const void* blob, const float* f_in, float* f_out, float* tau_out,
+                           unsigned int* fallback_count, unsigned int* status, void* stream) {
+  if (!blob || !f_in || !f_out) return TLBM_ERR_ARG;
+  if (f_in == f_out) return TLBM_ERR_ALIAS;
+  if (reinterpret_cast<uintptr_t>(blob) % 16) return TLBM_ERR_ARG;
+  if (nx < 1 || ny < 1 || nz < 1) return TLBM_ERR_SHAPE;
+  if (!(tau0 > 0.5) || !(force_lin > -1.0 && force_lin < 1.0) || !(c_s >= 0.0)) return TLBM_ERR_ARG;
+  LesStep p;
+  p.fin = f_in;
+  p.fout = f_out;
+  p.nx = nx;
+  p.ny = ny;
+  p.nz = nz;
+  p.plane = (long long)nx * ny;
+  p.n = p.plane * nz;
+  p.tau0 = float(tau0);
+  p.c_s = float(c_s);
+  p.a_lin = float(force_lin);
+  p.blob = static_cast<const uint8_t*>(blob);
+  p.tau_out = tau_out;
+  p.fallback_count = fallback_count;
+  p.status = status;
+  int grid = 0;
+  const int st = les_grid(p.n, grid);
+  if (st != TLBM_OK) return st;
+  k_step_les<<<grid, mlp::TILE, mlp::SM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
+  return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
+}
+
+}  // extern "C"

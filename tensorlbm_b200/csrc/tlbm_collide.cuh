@@ -23,6 +23,7 @@ template <typename T> struct CollideParams {
   T keep_even;              // 1 - omega_even
   T tau_sq;                 // tau^2
   T tau_eff_max;            // max(1, tau + 0.5), turbulence.py:88-99
+  T force_a;                // linear body force F = A rho u (exact-difference forcing); 0 = none
 };
 
 // ---------------------------------------------------------------------------
@@ -670,6 +671,7 @@ __host__ __device__ CollideParams<T> make_collide_params(double tau, double s_e,
   cp.keep_even = T(1.0 - omega_even);
   cp.tau_sq = T(tau * tau);
   cp.tau_eff_max = T(tau + 0.5 > 1.0 ? tau + 0.5 : 1.0);
+  cp.force_a = T(0);
   return cp;
 }
 

@@ -128,7 +128,23 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
     } else {
       const bool has_tau = d.tau_field != nullptr;
       const T tau_cell = has_tau ? T(d.tau_field[cell]) : T(0);
-      collide<L, COLL>(f, cp, tau_cell, has_tau);
+      constexpr bool kForced = COLL == TLBM_COLL_BGK || COLL == TLBM_COLL_SMAGORINSKY;
+      if (kForced && cp.force_a != T(0)) {
+        // exact-difference forcing of F = A rho u (BGK and Smagorinsky only):
+        // collide, then add feq(rho, (1 + A) u) - feq(rho, u) with the
+        // pre-collision moments
+        T rho, ux, uy, uz;
+        macroscopic_fused<L>(f, rho, ux, uy, uz);
+        collide<L, COLL>(f, cp, tau_cell, has_tau);
+        const T k = T(1) + cp.force_a;
+        const T usq = ux * ux + uy * uy + uz * uz;
+        const T usq_k = usq * k * k;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+          f[q] += feq_fused<L>(q, rho, ux * k, uy * k, uz * k, usq_k) - feq_fused<L>(q, rho, ux, uy, uz, usq);
+      } else {
+        collide<L, COLL>(f, cp, tau_cell, has_tau);
+      }
       if (d.status) {
         const T r = f[0];
         if (!(r == r) || r - r != T(0)) atomicOr(d.status, 1u);
@@ -175,8 +191,9 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   using T = typename Storage<SI>::T;
   dim3 grid, block;
   step_launch_shape(p.nx, p.ny, p.nz, grid, block);
-  const CollideParams<T> cp = make_collide_params<T>(d.tau, d.s_e, d.s_eps, d.s_q, d.s_pi, d.omega_b,
-                                                     d.omega_odd, d.omega_even, d.c_smag);
+  CollideParams<T> cp = make_collide_params<T>(d.tau, d.s_e, d.s_eps, d.s_q, d.s_pi, d.omega_b, d.omega_odd,
+                                               d.omega_even, d.c_smag);
+  cp.force_a = T(d.force_lin);
   const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
   k_step<L, SI, SO, COLL, PULL><<<grid, block, 0, s>>>(p, cp, bp);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;

@@ -68,6 +68,7 @@ class StepConfig:
     u_lid: float | None = None       # moving lid at y = ny-1
     u_in: tuple[float, float, float] | float | None = None  # Zou/He inlet at x = 0
     rho_out: float | None = None     # Zou/He outlet at x = nx-1
+    force_lin: float = 0.0           # linear body force F = A rho u (BGK / Smagorinsky)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -91,7 +92,7 @@ class StepConfig:
         if self.rho_out is not None:
             bc |= _lib.BC_ZH_OUTLET
         coll = COLLISIONS[collision or self.collision]
-        return _ops.make_desc(
+        d = _ops.make_desc(
             q, self.grid, dtype_code, coll, self.tau,
             s_e=d_se if self.s_e is None else self.s_e,
             s_eps=d_seps if self.s_eps is None else self.s_eps,
@@ -100,6 +101,11 @@ class StepConfig:
             c_smag=self.c_smag, bc=bc, u_lid=self.u_lid or 0.0, u_in=u_in,
             rho_out=1.0 if self.rho_out is None else self.rho_out,
         )
+        if coll in (_lib.COLL_BGK, _lib.COLL_SMAGORINSKY):
+            d.force_lin = float(self.force_lin)
+        elif self.force_lin and coll != _lib.COLL_NONE:
+            raise NotImplementedError("force_lin is implemented for the bgk and smagorinsky collisions")
+        return d
 
 
 class LBMSolver:

@@ -1,0 +1,49 @@
+"""End to end at small scale: forced DNS 128^3 -> block-filtered (factor 4)
+training data -> the library's training kernels -> LES 32^3 with the fused
+learned-closure step.  Shows what the trained network gains over the method
+without it (Smagorinsky, the fallback and judge) on the filtered DNS."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def test_hit_pipeline_small(cuda, tmp_path):
+    from tensorlbm_b200.ai import pipeline as P
+
+    cfg = P.HITConfig(dns=128, les=(32,), re_lambda=40.0, spinup_turnovers=3.0, snapshots=2,
+                      snapshot_gap_turnovers=0.5, window_turnovers=1.0, spectra_per_window=4, train_epochs=8,
+                      train_batch=4096, max_samples_per_grid=200_000, chunk=20)
+    res = P.run(cfg, tmp_path, device=cuda, log=lambda *_: None)
+    ap = res["a_priori"]
+    # the learned closure fits the subgrid eddy viscosity better than Smagorinsky
+    assert ap["mse_mlp"] < 0.9 * ap["mse_smagorinsky"], ap
+    assert 0.5 < ap["dissipation_ratio_mlp"] < 1.5, ap
+    les = res["les"]
+    assert les["mlp_32"]["finite"] and les["smagorinsky_32"]["finite"]
+    for k in ("mlp_32", "smagorinsky_32"):
+        assert math.isfinite(les[k]["spectrum_error_all"])
+    assert les["mlp_32"]["fallback_cells_per_step"] < 0.5 * 32 ** 3
+    assert (tmp_path / "closure.npz").exists() and (tmp_path / "hit_les.json").exists()
+
+
+def test_random_solenoidal_field_is_divergence_free(cuda):
+    from tensorlbm_b200.ai import pipeline as P
+
+    u = P.random_solenoidal_field(32, 4.0, 0.05, 11, cuda).double()
+    uh = [torch.fft.fftn(c) for c in u]
+    k = torch.fft.fftfreq(32, d=1.0 / 32, device=cuda).double()
+    KZ, KY, KX = torch.meshgrid(k, k, k, indexing="ij")
+    div = KX * uh[0] + KY * uh[1] + KZ * uh[2]
+    assert float(div.abs().max()) <= 1e-5 * float(uh[0].abs().max())  # float32 field
+    assert abs(float(torch.sqrt((u ** 2).mean())) - 0.05) < 1e-6
+    e = P.energy_spectrum(u.float())
+    assert abs(float(e.sum()) - 0.5 * float((u ** 2).sum(0).mean())) < 1e-6 * float(e.sum())
+    assert int(torch.argmax(e)) in (3, 4, 5)
+    np.testing.assert_allclose(float(e.sum()), 1.5 * 0.05 ** 2, rtol=1e-5)

@@ -348,5 +348,5 @@ def test_rotating_obstacle_fused_chain(cuda, q):
         assert rel_err(N(s.f), ref) < 2e-6
     got = N(s.force_history())
     want = np.array(forces)
-    tol = 1e-9 if coll == "bgk" else 1e-4
+    tol = 1e-6 if coll == "bgk" else 1e-4  # per-cell momenta are float32, as in TensorLBM
     assert np.max(np.abs(got[:, :want.shape[1]] - want)) <= tol * max(np.max(np.abs(want)), 1e-30)
