@@ -189,6 +189,52 @@ def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_c
             "roofline_frac": round(gbs / peak, 4), "bytes_per_cell": bytes_per_cell, "finite": finite}
 
 
+def _les_variant(torch, dev, steps, warmup, peak, n_mlp=128, n_smag=256):
+    """Forced-turbulence LES steps: the fused learned-closure step (tensor-core
+    MLP per cell) at n_mlp^3 against the fused Smagorinsky step at n_smag^3,
+    both from a seeded random solenoidal field.  The network has random
+    weights and an unbounded training range (no cell takes the fallback): its
+    cost does not depend on the weight values."""
+    from tensorlbm_b200 import LBMSolver
+    from tensorlbm_b200.ai import EddyViscosityMLP3D, LearnedLESSolver
+    from tensorlbm_b200.ai.pipeline import equilibrium_field, random_solenoidal_field
+
+    def timed(run):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / 1e3
+
+    out = {}
+    model = EddyViscosityMLP3D(dev, seed=7)
+    model.nu_scale = 1e-3
+    f0 = equilibrium_field(random_solenoidal_field(n_mlp, 4.0, 0.05, 3, dev))
+    s = LearnedLESSolver((n_mlp,) * 3, 0.51, model, force_lin=1e-4, device=dev).load(f0)
+    s.step(warmup)
+    t = timed(lambda: s.step(steps))
+    cells = n_mlp ** 3
+    out["mlp"] = {"grid": n_mlp, "mlups": round(cells * steps / t / 1e6, 1), "ms_per_step": round(1e3 * t / steps, 4),
+                  "roofline_frac": round(152 * cells / (t / steps) / 1e9 / peak, 4),
+                  "finite": not s.nonfinite_seen(), "fallback_cells": int(s.fallback.item())}
+    del s, f0
+    f0 = equilibrium_field(random_solenoidal_field(n_smag, 4.0, 0.05, 3, dev))
+    s = LBMSolver("D3Q19", (n_smag,) * 3, 0.52, "smagorinsky", device=dev, c_smag=0.17, force_lin=1e-4).load(f0)
+    s.step(warmup)
+    t2 = timed(lambda: s.step(steps))
+    cells2 = n_smag ** 3
+    out["smagorinsky"] = {"grid": n_smag, "mlups": round(cells2 * steps / t2 / 1e6, 1),
+                          "ms_per_step": round(1e3 * t2 / steps, 4),
+                          "roofline_frac": round(152 * cells2 / (t2 / steps) / 1e9 / peak, 4)}
+    # the same physical time: one n_mlp step covers n_smag / n_mlp steps of the finer grid
+    out["wall_time_ratio_same_physical_time"] = round((t2 / steps) * (n_smag / n_mlp) / (t / steps), 2)
+    del s, f0
+    torch.cuda.empty_cache()
+    return out
+
+
 def _batched_variant(torch, dev, steps, peak):
     """512 D2Q9 BGK cylinder channels (nx ~ U{128..1024}, ny = nx/4, D = ny/8,
     Re ~ U(40, 300), seed 20261203) advanced together, against the same domains
@@ -339,6 +385,8 @@ def run_ours(args) -> None:
                                                      2 * 19 * 2, peak)
     if want("d3q19_bgk_f32"):
         variants["d3q19_bgk_f32"] = _variant(torch, dev, "D3Q19", "bgk", "f32", args.steps, args.warmup, bpc, peak)
+    if want("les_mlp_128_vs_smagorinsky_256"):
+        variants["les_mlp_128_vs_smagorinsky_256"] = _les_variant(torch, dev, args.steps, args.warmup, peak)
     if want("d2q9_batched_512_cylinders"):
         variants["d2q9_batched_512_cylinders"] = _batched_variant(torch, dev, args.steps, peak)
 
@@ -499,7 +547,7 @@ def main() -> None:
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--variants", default="all",
                     help="comma list of variants to run (d3q27_cumulant_f32, d3q19_mrt_f16_shifted, "
-                         "d3q19_bgk_f32, d2q9_batched_512_cylinders) or 'all'")
+                         "d3q19_bgk_f32, les_mlp_128_vs_smagorinsky_256, d2q9_batched_512_cylinders) or 'all'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-slab", type=int, default=8, help="z-planes per CPU sample slab")
     ap.add_argument("--cpu-steps", type=int, default=2)

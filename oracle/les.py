@@ -132,18 +132,18 @@ def bf16(a):
 
 
 def forward_bf16(theta, z):
-    """The inference arithmetic of the fused kernel: bf16 weights and bf16
-    layer inputs, float32 accumulation and activations, float32 output layer
-    with the bf16-rounded w4."""
+    """The inference arithmetic of the tensor-core kernels: bf16 inputs and
+    weights with float32 accumulation in every layer (the output layer too);
+    between layers h = bf16(0.5 (acc + b)) and SiLU = bf16(h + h bf16(tanh h))."""
     p = unpack(np.asarray(theta, np.float32))
     h = bf16(np.asarray(z, np.float32))
     for wn, bn in (("W1", "b1"), ("W2", "b2"), ("W3", "b3")):
-        a = h.astype(np.float64) @ bf16(p[wn]).astype(np.float64).T
-        a = a.astype(np.float32) + p[bn]
-        h = (a / (1.0 + np.exp(-a.astype(np.float64)))).astype(np.float32)
-        if wn != "W3":
-            h = bf16(h)
-    return (h.astype(np.float64) @ bf16(p["w4"]).astype(np.float64) + float(p["b4"][0])).astype(np.float32)
+        acc = (h.astype(np.float64) @ bf16(p[wn]).astype(np.float64).T).astype(np.float32)
+        hh = bf16(np.float32(0.5) * (acc + p[bn]))
+        t = bf16(np.tanh(hh.astype(np.float64)).astype(np.float32))
+        h = bf16((hh.astype(np.float64) + hh.astype(np.float64) * t.astype(np.float64)).astype(np.float32))
+    y = (h.astype(np.float64) @ bf16(p["w4"]).astype(np.float64)).astype(np.float32)
+    return (y + p["b4"][0]).astype(np.float32)
 
 
 # ---------------------------------------------------------------------------

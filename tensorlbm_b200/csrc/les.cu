@@ -340,12 +340,15 @@ __global__ void k_mlp_pack(const float* __restrict__ theta, const float* __restr
     *reinterpret_cast<__nv_bfloat16*>(blob + mlp::OFF_W + l * mlp::W_TILE_BYTES + umma::sw128_offset(n, k)) =
         __float2bfloat16_rn(v);
   }
+  if (i < H)  // output layer: row 0 of a 16-row tile (rows 1..15 stay zero)
+    *reinterpret_cast<__nv_bfloat16*>(blob + mlp::OFF_W4 + umma::sw128_offset(0, i)) =
+        __float2bfloat16_rn(theta[O_W4 + i]);
   if (i < mlp::P_COUNT) {
     float* p = reinterpret_cast<float*>(blob + mlp::OFF_P);
     float v = 0.0f;
-    if (i < mlp::P_B2) v = theta[O_B1 + i];
-    else if (i < mlp::P_B3) v = theta[O_B2 + i - mlp::P_B2];
-    else if (i < mlp::P_W4) v = theta[O_B3 + i - mlp::P_B3];
+    if (i < mlp::P_HB2) v = 0.5f * theta[O_B1 + i];  // hidden biases are stored halved
+    else if (i < mlp::P_HB3) v = 0.5f * theta[O_B2 + i - mlp::P_HB2];
+    else if (i < mlp::P_W4) v = 0.5f * theta[O_B3 + i - mlp::P_HB3];
     else if (i < mlp::P_B4) v = __bfloat162float(__float2bfloat16_rn(theta[O_W4 + i - mlp::P_W4]));
     else if (i == mlp::P_B4) v = theta[O_B4];
     else if (i == mlp::P_NUS) v = nu_scale;
@@ -374,8 +377,8 @@ __global__ void __launch_bounds__(mlp::TILE) k_mlp_infer(const uint8_t* __restri
     bool ok = true;
     const float y = e.run(z, ok);
     if (i < count) y_out[i] = y;
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0 && status) atomicOr(status, 4u);
+    if (!ok) {  // uniform across the half
+      if (e.lt == 0 && status) atomicOr(status, 4u);
       break;
     }
   }
@@ -389,6 +392,9 @@ int infer_grid(long long count, int& grid) {
     if (cudaGetDevice(&dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
     if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::SM_BYTES) !=
         cudaSuccess)
+      return TLBM_ERR_LAUNCH;
+    if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
       return TLBM_ERR_LAUNCH;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer, mlp::TILE, mlp::SM_BYTES) !=

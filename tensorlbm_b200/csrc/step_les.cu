@@ -1,9 +1,11 @@
 // Fused D3Q19 LES step with the learned eddy-viscosity closure.
 //
 // Persistent kernel: each CTA loads the packed network once (shared memory),
-// allocates 128 TMEM columns, then walks tiles of 256 consecutive cells:
+// allocates 128 TMEM columns, then walks tiles of 256 consecutive cells as two
+// independent halves of 128 (see tlbm_mlp.cuh):
 //   pull (periodic) -> rho, u -> Pi_neq = sum_q c c (f - feq) -> 9 features
-//   -> tcgen05 MLP (three 64-wide layers, bf16 x bf16 -> fp32 in TMEM)
+//   -> tcgen05 MLP (three 64-wide layers and the output layer, bf16 x bf16 ->
+//      fp32 in TMEM)
 //   -> nu_t = nu_scale softplus(y), tau_eff = tau0 + 3 nu_t
 //      (Smagorinsky tau_s where a feature leaves the training range)
 //   -> BGK with tau_eff + exact-difference linear forcing -> store.
@@ -95,14 +97,21 @@ __global__ void __launch_bounds__(mlp::TILE, 3) k_step_les(LesStep p) {
       }
       const float inv = 1.0f / tau;
       const float usq = ux * ux + uy * uy + uz * uz;
-      const float k = 1.0f + p.a_lin;
-      const float usq_k = usq * k * k;
+      // exact-difference force term feq(rho, (1+A) u) - feq(rho, u)
+      //   = w rho [3 A (c.u) + ((1+A)^2 - 1) (4.5 (c.u)^2 - 1.5 u^2)]
+      const float a3 = 3.0f * p.a_lin;
+      const float k2m1 = p.a_lin * (2.0f + p.a_lin);
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
-        const float feq = feq_fused<L>(q, rho, ux, uy, uz, usq);
-        float fo = f[q] - (f[q] - feq) * inv;
-        if (p.a_lin != 0.0f) fo += feq_fused<L>(q, rho, ux * k, uy * k, uz * k, usq_k) - feq;
-        p.fout[(long long)q * p.n + cell] = fo;
+        float cu = 0.0f;
+        if (L::cx(q) != 0) cu = L::cx(q) > 0 ? cu + ux : cu - ux;
+        if (L::cy(q) != 0) cu = L::cy(q) > 0 ? cu + uy : cu - uy;
+        if (L::cz(q) != 0) cu = L::cz(q) > 0 ? cu + uz : cu - uz;
+        const float wr = weight<L, float>(q) * rho;
+        const float quad = fmaf(4.5f * cu, cu, -1.5f * usq);
+        const float feq = wr * (1.0f + fmaf(3.0f, cu, quad));
+        const float force = wr * fmaf(a3, cu, k2m1 * quad);
+        p.fout[(long long)q * p.n + cell] = fmaf(feq - f[q], inv, f[q]) + force;
       }
       if (p.tau_out) p.tau_out[cell] = tau;
       if (p.status && !(rho == rho && rho - rho == 0.0f)) atomicOr(p.status, 1u);
@@ -111,8 +120,8 @@ __global__ void __launch_bounds__(mlp::TILE, 3) k_step_les(LesStep p) {
       const unsigned int fb = __ballot_sync(0xffffffffu, active && !inrange);
       if ((threadIdx.x & 31) == 0 && fb) atomicAdd(p.fallback_count, __popc(fb));
     }
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0 && p.status) atomicOr(p.status, 4u);
+    if (!ok) {  // uniform across the half
+      if (e.lt == 0 && p.status) atomicOr(p.status, 4u);
       break;
     }
   }
@@ -125,6 +134,11 @@ int les_grid(long long n, int& grid) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
     if (cudaFuncSetAttribute(k_step_les, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::SM_BYTES) != cudaSuccess)
+      return TLBM_ERR_LAUNCH;
+    // ask for the largest shared-memory carveout, or the occupancy query plans
+    // for the default split and finds room for a single CTA
+    if (cudaFuncSetAttribute(k_step_les, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
       return TLBM_ERR_LAUNCH;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_les, mlp::TILE, mlp::SM_BYTES) != cudaSuccess)

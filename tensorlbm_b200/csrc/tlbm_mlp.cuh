@@ -1,11 +1,18 @@
 // Eddy-viscosity MLP of the learned LES closure: feature map, packed model
-// blob, and the per-CTA tensor-core inference engine.
+// blob, and the tensor-core inference engine.
 //
 // Network: 9 invariant features -> 64 -> 64 -> 64 (SiLU) -> 1,
-// nu_t = nu_scale * softplus(y), tau_eff = tau0 + 3 nu_t.  The three hidden
-// layers run on tcgen05 (bf16 operands from shared memory, fp32 accumulators in
-// TMEM, M = 128 cells per MMA, N = 64, K = 16 per instruction); the output layer
-// and the activations run in fp32 on the CUDA cores, one cell per thread.
+// nu_t = nu_scale * softplus(y), tau_eff = tau0 + 3 nu_t.  All four layers run
+// on tcgen05 (bf16 operands from shared memory, fp32 accumulators in TMEM,
+// M = 128 cells per MMA, K = 16 per instruction; N = 64 for the hidden layers,
+// N = 16 for the output layer whose B tile holds w4 in row 0).  Between layers
+// each thread turns its cell's accumulator row into the next A row:
+// h = bf16(0.5 (acc + b)), SiLU = h + h tanh(h) in packed bf16x2 arithmetic.
+//
+// A CTA of 256 threads is two independent halves of 128 rows.  Each half has
+// its own A tile, 64 TMEM columns, mbarrier and named barrier, so the halves
+// drift apart and one half's MMA round trip overlaps the other half's CUDA-core
+// work.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -17,28 +24,34 @@ namespace mlp {
 
 constexpr int NF = 9;        // input features
 constexpr int H = 64;        // hidden width
-constexpr int TILE = 256;    // cells per CTA pass (two M = 128 MMA tiles)
+constexpr int TILE = 256;    // cells per CTA pass (two halves of M = 128)
+constexpr int HALF = 128;
 constexpr int N_PARAMS = H * NF + H + H * H + H + H * H + H + H + 1;  // 9025, flat training vector
 
 // ---- packed inference blob (global memory) --------------------------------
 // [0, 24576): W1, W2, W3 as SW128 K-major bf16 64x64 tiles (W1 zero beyond column 9)
-// [24576, ..): float block
+// [24576, 26624): w4 as a 16-row SW128 tile (row 0 = w4, rows 1..15 zero)
+// [26624, ..): float block (biases b1..b3 stored halved)
 constexpr int W_TILE_BYTES = H * H * 2;  // 8192
+constexpr int W4_TILE_BYTES = 16 * 128;  // 2048
 constexpr int OFF_W = 0;
-constexpr int OFF_P = 3 * W_TILE_BYTES;  // 24576
-constexpr int P_B1 = 0, P_B2 = 64, P_B3 = 128, P_W4 = 192, P_B4 = 256, P_NUS = 257, P_MEAN = 260,
+constexpr int OFF_W4 = 3 * W_TILE_BYTES;             // 24576
+constexpr int OFF_P = OFF_W4 + W4_TILE_BYTES;        // 26624
+constexpr int P_HB1 = 0, P_HB2 = 64, P_HB3 = 128, P_W4 = 192, P_B4 = 256, P_NUS = 257, P_MEAN = 260,
               P_ISTD = P_MEAN + NF, P_LO = P_ISTD + NF, P_HI = P_LO + NF, P_COUNT = P_HI + NF;  // 296
-constexpr int BLOB_BYTES = OFF_P + ((P_COUNT * 4 + 127) / 128) * 128;                    // 25856
+constexpr int P_BYTES = ((P_COUNT * 4 + 127) / 128) * 128;                               // 1280
+constexpr int BLOB_BYTES = OFF_P + P_BYTES;                                              // 27904
 
 // ---- shared memory of one CTA (offsets from a 1024-byte aligned base) -------
-constexpr int SM_A = 0;                          // 2 x (128 rows x 128 B) activations
-constexpr int SM_W = SM_A + 2 * 128 * 128;       // 32768: three weight tiles
-constexpr int SM_P = SM_W + 3 * W_TILE_BYTES;    // 57344: float block
-constexpr int SM_BAR = SM_P + ((P_COUNT * 4 + 127) / 128) * 128;  // 58624
-constexpr int SM_SLOT = SM_BAR + 8;
-constexpr int SM_FLAG = SM_SLOT + 4;
-constexpr int SM_BYTES = SM_FLAG + 4 + 1024;     // with alignment slack
-constexpr uint32_t TMEM_COLS = 128;              // two 64-column accumulators
+constexpr int A_TILE_BYTES = HALF * 128;         // 16384: one half's activations
+constexpr int SM_A = 0;                          // 2 A tiles
+constexpr int SM_W = SM_A + 2 * A_TILE_BYTES;    // 32768: the blob
+constexpr int SM_P = SM_W + OFF_P;               // 59392: float block
+constexpr int SM_BAR = SM_P + P_BYTES;           // 60672: one mbarrier per half
+constexpr int SM_SLOT = SM_BAR + 16;             // TMEM base address
+constexpr int SM_FLAG = SM_SLOT + 4;             // one timeout flag per half
+constexpr int SM_BYTES = SM_FLAG + 8 + 1024;     // with alignment slack
+constexpr uint32_t TMEM_COLS = 128;              // 64 accumulator columns per half
 constexpr uint32_t MAX_WAIT = 1u << 20;          // mbarrier polls before giving up
 
 // ---- features --------------------------------------------------------------
@@ -80,7 +93,6 @@ __host__ __device__ inline void features(T xx, T yy, T zz, T xy, T xz, T yz, T r
   x[8] = sqrt(m);
 }
 
-__device__ __forceinline__ float silu(float a) { return a / (1.0f + __expf(-a)); }
 __device__ __forceinline__ float softplus(float y) { return y > 20.0f ? y : log1pf(__expf(y)); }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -88,127 +100,143 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// The tensor-core pass of one CTA over TILE rows (threads 0..TILE-1, one row each).
+// SiLU of two pre-activations given as h = a/2 (already rounded to bf16x2):
+// a sigmoid(a) = h + h tanh(h), with the hardware bf16x2 tanh and one bf16x2 fma
+__device__ __forceinline__ uint32_t silu_half_bf16x2(uint32_t h) {
+  uint32_t t, r;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(h));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(r) : "r"(h), "r"(t));
+  return r;
+}
+
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// The tensor-core pass of one half-CTA (128 threads, one row each).
 struct Engine {
   uint8_t* sm;
-  uint32_t tmem;
-  uint32_t mbar;
+  uint32_t tmem;   // this half's first accumulator column
+  uint32_t mbar;   // this half's mbarrier
   uint32_t phase;
+  int half;        // 0 or 1
+  int lt;          // thread index within the half
 
-  // copy the blob to shared memory, allocate TMEM, initialise the mbarrier
+  // CTA-wide: copy the blob to shared memory, allocate TMEM, initialise the mbarriers
   __device__ void setup(uint8_t* raw_smem, const uint8_t* __restrict__ blob) {
     sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(raw_smem) + 1023) & ~uintptr_t(1023));
     const int4* src = reinterpret_cast<const int4*>(blob);
     int4* dst = reinterpret_cast<int4*>(sm + SM_W);
     for (int i = threadIdx.x; i < (BLOB_BYTES / 16); i += blockDim.x) dst[i] = src[i];
-    mbar = umma::smem_addr(sm + SM_BAR);
     if (threadIdx.x < 32) umma::tmem_alloc(umma::smem_addr(sm + SM_SLOT), TMEM_COLS);
     if (threadIdx.x == 0) {
-      umma::mbar_init(mbar, 1);
-      *reinterpret_cast<volatile int*>(sm + SM_FLAG) = 0;
+      umma::mbar_init(umma::smem_addr(sm + SM_BAR), 1);
+      umma::mbar_init(umma::smem_addr(sm + SM_BAR + 8), 1);
+      reinterpret_cast<volatile int*>(sm + SM_FLAG)[0] = 0;
+      reinterpret_cast<volatile int*>(sm + SM_FLAG)[1] = 0;
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
-    tmem = *reinterpret_cast<volatile uint32_t*>(sm + SM_SLOT);
+    half = threadIdx.x / HALF;
+    lt = threadIdx.x % HALF;
+    tmem = *reinterpret_cast<volatile uint32_t*>(sm + SM_SLOT) + uint32_t(half * H);
+    mbar = umma::smem_addr(sm + SM_BAR + 8 * half);
     phase = 0;
   }
 
+  // CTA-wide
   __device__ void teardown() {
     umma::fence_before_sync();
     __syncthreads();
     if (threadIdx.x < 32) {
       umma::fence_after_sync();
-      umma::tmem_dealloc(tmem, TMEM_COLS);
+      umma::tmem_dealloc(*reinterpret_cast<volatile uint32_t*>(sm + SM_SLOT), TMEM_COLS);
     }
   }
 
   __device__ const float* params() const { return reinterpret_cast<const float*>(sm + SM_P); }
+  __device__ void sync_half() const { named_sync(1 + half, HALF); }
 
-  // A row of this thread: 16-byte chunk c (8 bf16) <- w[0..3]
+  // this thread's A row: 16-byte chunk c (8 bf16)
   __device__ void put_chunk(int c, uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3) {
-    const int t = threadIdx.x;
-    uint8_t* a = sm + SM_A + (t >> 7) * (128 * 128) + umma::sw128_offset(t & 127, c * 8);
+    uint8_t* a = sm + SM_A + half * A_TILE_BYTES + umma::sw128_offset(lt, c * 8);
     *reinterpret_cast<uint4*>(a) = make_uint4(w0, w1, w2, w3);
   }
 
-  // issue D = A W_l^T over k_slices slices of 16, wait for it; false on timeout
-  __device__ bool mma_layer(int l, int k_slices) {
+  // D = A B^T over k_slices slices of 16 (B = the tile at blob offset b_off,
+  // N = 64, or N = 16 for the output layer).  Warp 0 of the half issues and
+  // polls the mbarrier; the half meets at its named barrier.  False on timeout.
+  template <int N>
+  __device__ bool mma(int b_off, int k_slices) {
+    volatile int* flag = reinterpret_cast<volatile int*>(sm + SM_FLAG) + half;
     umma::fence_proxy_async_smem();
     umma::fence_before_sync();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      umma::fence_after_sync();
-      const uint32_t b0 = umma::smem_addr(sm + SM_W + l * W_TILE_BYTES);
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
-        const uint32_t a0 = umma::smem_addr(sm + SM_A + mt * 128 * 128);
+    sync_half();
+    if (lt < 32) {
+      if (lt == 0) {
+        umma::fence_after_sync();
+        const uint32_t a0 = umma::smem_addr(sm + SM_A + half * A_TILE_BYTES);
+        const uint32_t b0 = umma::smem_addr(sm + SM_W + b_off);
         for (int ks = 0; ks < k_slices; ++ks)
-          umma::mma_bf16(tmem + uint32_t(mt * H), umma::sw128_desc(a0 + 32u * ks), umma::sw128_desc(b0 + 32u * ks),
-                         umma::IdescBf16<128, H>::value, ks > 0 ? 1u : 0u);
+          umma::mma_bf16(tmem, umma::sw128_desc(a0 + 32u * ks), umma::sw128_desc(b0 + 32u * ks),
+                         umma::IdescBf16<128, N>::value, ks > 0 ? 1u : 0u);
+        umma::commit(mbar);
       }
-      umma::commit(mbar);
+      __syncwarp();
+      const bool done = umma::mbar_wait(mbar, phase, MAX_WAIT);
+      if (lt == 0 && !done) *flag = 1;
     }
-    const bool ok = umma::mbar_wait(mbar, phase, MAX_WAIT);
     phase ^= 1u;
+    sync_half();
     umma::fence_after_sync();
-    return ok;
+    return *flag == 0;
   }
 
-  // TMEM address of this thread's row, column 0 of its tile's accumulator
+  // TMEM address of this thread's row (lane) at this half's first column
   __device__ uint32_t row_taddr() const {
     const int w = threadIdx.x >> 5;
-    return tmem + (uint32_t((w & 3) * 32) << 16) + uint32_t((w >> 2) * H);
+    return tmem + (uint32_t((w & 3) * 32) << 16);
   }
 
-  // accumulator -> bias -> SiLU -> bf16 -> next A row
-  __device__ void hidden_to_a(const float* bias) {
+  // accumulator row -> bf16(0.5 (acc + b)) -> SiLU (bf16x2) -> next A row
+  __device__ void hidden_to_a(const float* hb) {
     const uint32_t ta = row_taddr();
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
+    for (int part = 0; part < 2; ++part) {
       float v[32];
-      umma::tmem_ld32(ta + uint32_t(32 * half), v);
+      umma::tmem_ld32(ta + uint32_t(32 * part), v);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        uint32_t w[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int k = 32 * half + 8 * c + 2 * j;
-          w[j] = pack_bf16x2(silu(v[8 * c + 2 * j] + bias[k]), silu(v[8 * c + 2 * j + 1] + bias[k + 1]));
-        }
-        put_chunk(4 * half + c, w[0], w[1], w[2], w[3]);
+        const float4 b0 = *reinterpret_cast<const float4*>(hb + 32 * part + 8 * c);
+        const float4 b1 = *reinterpret_cast<const float4*>(hb + 32 * part + 8 * c + 4);
+        const float* u = v + 8 * c;
+        put_chunk(4 * part + c, silu_half_bf16x2(pack_bf16x2(fmaf(u[0], 0.5f, b0.x), fmaf(u[1], 0.5f, b0.y))),
+                  silu_half_bf16x2(pack_bf16x2(fmaf(u[2], 0.5f, b0.z), fmaf(u[3], 0.5f, b0.w))),
+                  silu_half_bf16x2(pack_bf16x2(fmaf(u[4], 0.5f, b1.x), fmaf(u[5], 0.5f, b1.y))),
+                  silu_half_bf16x2(pack_bf16x2(fmaf(u[6], 0.5f, b1.z), fmaf(u[7], 0.5f, b1.w))));
       }
     }
   }
 
-  // y = w4 . SiLU(acc + b3) + b4 for this thread's row
-  __device__ float output_layer() const {
-    const float* p = params();
-    const uint32_t ta = row_taddr();
-    float y = p[P_B4];
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      float v[32];
-      umma::tmem_ld32(ta + uint32_t(32 * half), v);
-#pragma unroll
-      for (int i = 0; i < 32; ++i) y = fmaf(silu(v[i] + p[P_B3 + 32 * half + i]), p[P_W4 + 32 * half + i], y);
-    }
-    return y;
-  }
-
-  // Full pass.  z: normalised features of this thread's row (zeros for idle
-  // rows).  Returns y; *ok false if a tensor-core wait gave up.
+  // Full pass of this half.  z: normalised features of this thread's row
+  // (zeros for idle rows).  Returns y; ok false if a tensor-core wait gave up.
   __device__ float run(const float (&z)[NF], bool& ok) {
     const float* p = params();
     put_chunk(0, pack_bf16x2(z[0], z[1]), pack_bf16x2(z[2], z[3]), pack_bf16x2(z[4], z[5]), pack_bf16x2(z[6], z[7]));
     put_chunk(1, pack_bf16x2(z[8], 0.0f), 0u, 0u, 0u);
-    ok = mma_layer(0, 1);
-    hidden_to_a(p + P_B1);
-    ok = mma_layer(1, H / 16) && ok;
-    hidden_to_a(p + P_B2);
-    ok = mma_layer(2, H / 16) && ok;
-    return output_layer();
+    ok = mma<H>(OFF_W, 1);
+    hidden_to_a(p + P_HB1);
+    ok = mma<H>(OFF_W + W_TILE_BYTES, H / 16) && ok;
+    hidden_to_a(p + P_HB2);
+    ok = mma<H>(OFF_W + 2 * W_TILE_BYTES, H / 16) && ok;
+    hidden_to_a(p + P_HB3);
+    ok = mma<16>(OFF_W4, H / 16) && ok;
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(row_taddr()) : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    return __uint_as_float(r) + p[P_B4];
   }
 };
 
