@@ -396,13 +396,7 @@ int infer_grid(long long count, int& grid) {
     if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared) != cudaSuccess)
       return TLBM_ERR_LAUNCH;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer, mlp::TILE, mlp::SM_BYTES) !=
-        cudaSuccess)
-      return TLBM_ERR_LAUNCH;
-    // TMEM: each resident CTA holds TMEM_COLS of the SM's 512 columns
-    const int tmem_cap = 512 / int(mlp::TMEM_COLS);
-    if (per_sm > tmem_cap) per_sm = tmem_cap;
+    per_sm = mlp::resident_ctas(k_mlp_infer, sms);
   }
   if (per_sm < 1) return TLBM_ERR_UNSUPPORTED;
   const long long ntiles = (count + mlp::TILE - 1) / mlp::TILE;

@@ -135,16 +135,11 @@ int les_grid(long long n, int& grid) {
     if (cudaGetDevice(&dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
     if (cudaFuncSetAttribute(k_step_les, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::SM_BYTES) != cudaSuccess)
       return TLBM_ERR_LAUNCH;
-    // ask for the largest shared-memory carveout, or the occupancy query plans
-    // for the default split and finds room for a single CTA
+    // the largest shared-memory carveout, so that several CTAs fit per SM
     if (cudaFuncSetAttribute(k_step_les, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared) != cudaSuccess)
       return TLBM_ERR_LAUNCH;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_les, mlp::TILE, mlp::SM_BYTES) != cudaSuccess)
-      return TLBM_ERR_LAUNCH;
-    const int tmem_cap = 512 / int(mlp::TMEM_COLS);
-    if (per_sm > tmem_cap) per_sm = tmem_cap;
+    per_sm = mlp::resident_ctas(k_step_les, sms);
   }
   if (per_sm < 1) return TLBM_ERR_UNSUPPORTED;
   const long long ntiles = (n + mlp::TILE - 1) / mlp::TILE;

@@ -240,5 +240,32 @@ struct Engine {
   }
 };
 
+// CTAs of a persistent tensor-core kernel (TILE threads, SM_BYTES dynamic
+// shared memory) that fit on one SM at once, from the device's limits and the
+// kernel's register count; the TMEM columns bound it too.  (The occupancy
+// query of the runtime plans for the default shared-memory split and answers 1.)
+// Also returns the SM count.  0 on a runtime error.
+template <typename Kernel>
+inline int resident_ctas(Kernel kern, int& sms) {
+  int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 0, threads_sm = 0;
+  cudaFuncAttributes fa;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess)
+    return 0;
+  const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;  // allocation unit: 256 registers per warp
+  int n = smem_sm / (SM_BYTES + reserved);
+  const int by_regs = regs_sm / (regs_warp * (TILE / 32));
+  const int by_threads = threads_sm / TILE;
+  const int by_tmem = 512 / int(TMEM_COLS);
+  n = n < by_regs ? n : by_regs;
+  n = n < by_threads ? n : by_threads;
+  n = n < by_tmem ? n : by_tmem;
+  return n;
+}
+
 }  // namespace mlp
 }  // namespace tlbm
