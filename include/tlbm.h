@@ -101,9 +101,9 @@ typedef struct tlbm_desc {
                                 type (float32; float64 for TLBM_F64), x-component first; may be NULL */
   double force_lin;    /* linear body force F = force_lin * rho * u (Lundgren forcing of forced
                           isotropic turbulence), exact-difference scheme: after the collision
-                          f += feq(rho, (1 + A) u) - feq(rho, u); 0 = none.  BGK and
-                          Smagorinsky collisions only (else TLBM_ERR_UNSUPPORTED); |A| < 1.
-                          New in this library. */
+                          f += feq(rho, (1 + A) u) - feq(rho, u); 0 = none.  BGK, MRT and
+                          Smagorinsky collisions (else TLBM_ERR_UNSUPPORTED) on float32
+                          populations (else TLBM_ERR_DTYPE); |A| < 1.  New in this library. */
 } tlbm_desc;
 
 /* ---- fused time step ------------------------------------------------------

@@ -35,6 +35,12 @@ class LearnedLESSolver:
         self.tau = torch.empty((nz, ny, nx), dtype=torch.float32, device=self.device) if track_tau else None
         self._graph = None
 
+    def set_force_lin(self, a: float) -> "LearnedLESSolver":
+        """Change the linear body force A (drops the captured graph)."""
+        self.force_lin = float(a)
+        self._graph = None
+        return self
+
     def load(self, f: torch.Tensor) -> "LearnedLESSolver":
         """Set the post-collision state (19, nz, ny, nx)."""
         if tuple(f.shape) != (19,) + self.shape:

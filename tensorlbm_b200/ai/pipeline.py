@@ -2,10 +2,14 @@
 closure -> LES comparisons (ai/pipeline.py:222 run_ai_les_pipeline is the 2-D
 original).
 
-Everything is in lattice units of the DNS grid (dx = dt = 1), D3Q19 BGK with
-the exact-difference linear (Lundgren) forcing F = A rho u.  A grid filtered by
-a factor r uses dx_r = dt_r = r (acoustic scaling): nu_r = nu / r, A_r = A r,
-and one filtered step covers r DNS steps.  ``HITConfig.les`` lists the LES
+Everything is in lattice units of the DNS grid (dx = dt = 1), D3Q19 MRT (the
+DNS) or BGK with tau_eff (the LES) with the exact-difference linear (Lundgren)
+forcing F = A rho u at constant power: every `force_every` steps
+A = epsilon / (2 K) from the current kinetic energy K, so that the injection
+rate is the target dissipation whatever the integral scale does (Carroll &
+Blanquart 2013).  A grid filtered by a factor r uses dx_r = dt_r = r (acoustic
+scaling): nu_r = nu / r, epsilon_r = epsilon r, and one filtered step covers r
+DNS steps.  ``HITConfig.les`` lists the LES
 grids; the first one runs the learned closure.
 
 Run as a module for the full experiment:
@@ -120,30 +124,41 @@ class HITConfig:
     k0: float = 4.0                 # initial spectrum peak
     re_lambda: float = 100.0        # target Taylor Reynolds number
     seed: int = 20261203
-    spinup_turnovers: float = 6.0   # DNS turnovers before the first training snapshot
-    snapshots: int = 3              # training snapshots
-    snapshot_gap_turnovers: float = 0.5
-    window_turnovers: float = 2.0   # LES / DNS comparison window
+    spinup_turnovers: float = 15.0  # DNS turnovers before the first training snapshot
+    snapshots: int = 4              # training snapshots
+    snapshot_gap_turnovers: float = 1.0
+    window_turnovers: float = 3.0   # LES / DNS comparison window
     spectra_per_window: int = 8
     train_epochs: int = 12
     train_batch: int = 16384
     max_samples_per_grid: int = 3_000_000
     chunk: int = 50                 # steps per CUDA graph replay
+    dns_collision: str = "mrt"      # BGK diverges at the DNS's tau ~ 0.515
+    calibration: tuple = (1.0, 0.7, 0.5, 0.35, 0.25, 0.15)  # candidate nu_t scale factors
+
+    force_every: int = 100          # steps between updates of the constant-power force
 
     @property
     def integral_scale(self) -> float:
-        # linear forcing settles at L ~ 0.19 of the box (Rosales & Meneveau 2005)
-        return 0.19 * self.dns
+        # integral scale assumed when choosing epsilon: 0.1 of the box (between
+        # the 0.066 measured after 6 turnovers from the k0 = 4 start and the
+        # asymptotic 0.19 of linear forcing, Rosales & Meneveau 2005)
+        return 0.1 * self.dns
+
+    @property
+    def eps(self) -> float:
+        # target dissipation = injected power, epsilon ~ 0.5 u'^3 / L
+        return 0.5 * self.u_rms ** 3 / self.integral_scale
 
     @property
     def force_lin(self) -> float:
-        # stationary balance u' ~ 6 A L (epsilon = 3 A u'^2, epsilon ~ 0.5 u'^3 / L)
-        return self.u_rms / (6.0 * self.integral_scale)
+        # initial A = epsilon / (2 K), K = 1.5 u'^2
+        return self.eps / (3.0 * self.u_rms ** 2)
 
     @property
     def nu(self) -> float:
-        # Re_lambda = u' sqrt(5 / (A nu))  (lambda^2 = 15 nu u'^2 / epsilon)
-        return 5.0 * self.u_rms ** 2 / (self.force_lin * self.re_lambda ** 2)
+        # Re_lambda = u' lambda / nu with lambda^2 = 15 nu u'^2 / epsilon
+        return 15.0 * self.u_rms ** 4 / (self.re_lambda ** 2 * self.eps)
 
     @property
     def tau(self) -> float:
@@ -157,6 +172,29 @@ class HITConfig:
 def tau_on(cfg: HITConfig, factor: int) -> float:
     """Molecular tau on a grid filtered by `factor` (nu_r = nu / r)."""
     return 3.0 * cfg.nu / factor + 0.5
+
+
+def kinetic_energy(state: torch.Tensor) -> float:
+    """K = <|u|^2> / 2 of D3Q19 populations."""
+    _, ux, uy, uz = macroscopic3d(state)
+    return 0.5 * float((ux.double() ** 2 + uy.double() ** 2 + uz.double() ** 2).mean())
+
+
+def run_forced(solver, steps: int, eps: float, every: int, chunk: int) -> float:
+    """Advance `steps` steps at constant injected power eps (grid units): the
+    force is reset to A = eps / (2 K) every `every` steps.  Returns the last A."""
+    a = 0.0
+    done = 0
+    while done < steps:
+        k = kinetic_energy(solver.state)
+        if not (math.isfinite(k) and k > 0.0):
+            raise RuntimeError("the flow diverged")
+        a = min(eps / (2.0 * k), 0.05)
+        solver.set_force_lin(a)
+        m = min(every, steps - done)
+        solver.run(m, chunk=chunk)
+        done += m
+    return a
 
 
 # ---------------------------------------------------------------------------
@@ -226,23 +264,29 @@ def run(cfg: HITConfig, out_dir: pathlib.Path, device="cuda:0", log=print) -> di
     dev = torch.device(device)
     out_dir = pathlib.Path(out_dir)
     out_dir.mkdir(parents=True, exist_ok=True)
-    res: dict = {"config": asdict(cfg), "derived": {"force_lin": cfg.force_lin, "nu": cfg.nu, "tau": cfg.tau,
+    res: dict = {"config": asdict(cfg), "derived": {"eps_target": cfg.eps, "force_lin_initial": cfg.force_lin,
+                                                    "nu": cfg.nu, "tau": cfg.tau,
                                                     "turnover_steps": cfg.turnover_steps}}
     n = cfg.dns
     # ---- DNS spin-up ----------------------------------------------------
     u0 = random_solenoidal_field(n, cfg.k0, cfg.u_rms, cfg.seed, dev)
-    dns = LBMSolver("D3Q19", (n, n, n), cfg.tau, "bgk", device=dev, force_lin=cfg.force_lin)
+    dns = LBMSolver("D3Q19", (n, n, n), cfg.tau, cfg.dns_collision, device=dev, force_lin=cfg.force_lin)
     dns.load(equilibrium_field(u0))
     del u0
     torch.cuda.empty_cache()
     spin = int(cfg.spinup_turnovers * cfg.turnover_steps)
-    t_spin = _timed(lambda: dns.run(spin, chunk=cfg.chunk), dev)
+    a_now = [cfg.force_lin]
+
+    def advance(steps):
+        a_now[0] = run_forced(dns, steps, cfg.eps, cfg.force_every, cfg.chunk)
+
+    t_spin = _timed(lambda: advance(spin), dev)
     res["dns_mlups"] = n ** 3 * spin / t_spin / 1e6
     log(f"DNS {n}^3 spin-up {spin} steps in {t_spin:.1f} s ({res['dns_mlups']:.0f} MLUPS)")
 
     def dns_stats():
         f = dns.f
-        u = velocity_of(f, cfg.force_lin)
+        u = velocity_of(f, a_now[0])
         e = energy_spectrum(u)
         del u
         eps = dissipation_from_spectrum(e, n, cfg.nu)
@@ -250,7 +294,8 @@ def run(cfg: HITConfig, out_dir: pathlib.Path, device="cuda:0", log=print) -> di
         up = math.sqrt(2.0 * k_e / 3.0)
         lam = math.sqrt(15.0 * cfg.nu * up * up / max(eps, 1e-300))
         return f, e, {"kinetic_energy": k_e, "u_prime": up, "epsilon": eps, "lambda": lam,
-                      "re_lambda": up * lam / cfg.nu, "eta": (cfg.nu ** 3 / max(eps, 1e-300)) ** 0.25}
+                      "re_lambda": up * lam / cfg.nu, "eta": (cfg.nu ** 3 / max(eps, 1e-300)) ** 0.25,
+                      "force_lin": a_now[0]}
 
     # ---- training snapshots ------------------------------------------------
     moms: dict = {g: [] for g in cfg.les}
@@ -259,11 +304,11 @@ def run(cfg: HITConfig, out_dir: pathlib.Path, device="cuda:0", log=print) -> di
     e = None
     for s in range(cfg.snapshots):
         if s:
-            dns.run(gap, chunk=cfg.chunk)
+            advance(gap)
         f, e, st = dns_stats()
         stats.append(st)
         for g in cfg.les:
-            moms[g].append(filtered_moments(f, n // g, cfg.force_lin))
+            moms[g].append(filtered_moments(f, n // g, a_now[0]))
         del f
         torch.cuda.empty_cache()
         log(f"snapshot {s}: Re_lambda {st['re_lambda']:.1f}, u' {st['u_prime']:.4f}, eps {st['epsilon']:.3e}")
@@ -286,7 +331,6 @@ def run(cfg: HITConfig, out_dir: pathlib.Path, device="cuda:0", log=print) -> di
     res["training"] = {"samples": int(x.shape[0]), "seconds": time.time() - t0, "pass1": h1, "pass2": h2,
                        "nu_scale": model.nu_scale}
     res["a_priori"] = a_priori(model, x, t, w)
-    model.save(out_dir / "closure.npz")
     del x, t, w
     log(f"trained on {res['training']['samples']} samples: a-priori {res['a_priori']}")
 
@@ -297,11 +341,11 @@ def run(cfg: HITConfig, out_dir: pathlib.Path, device="cuda:0", log=print) -> di
     dns_spec = {g: [] for g in cfg.les}
     dns_eps = []
     for _ in range(cfg.spectra_per_window):
-        dns.run(every, chunk=cfg.chunk)
+        advance(every)
         f, _e, st = dns_stats()
         dns_eps.append(st["epsilon"])
         for g in cfg.les:
-            mom = filtered_moments(f, n // g, cfg.force_lin)
+            mom = filtered_moments(f, n // g, a_now[0])
             dns_spec[g].append(energy_spectrum(mom[1:4]).cpu().numpy())
         del f
     del dns
@@ -309,49 +353,101 @@ def run(cfg: HITConfig, out_dir: pathlib.Path, device="cuda:0", log=print) -> di
     res["dns_window"] = {"epsilon_mean": float(np.mean(dns_eps))}
 
     # ---- LES runs ------------------------------------------------------------
-    runs: dict = {}
-    for name, m, kind in (("mlp", cfg.les[0], "mlp"), ("smagorinsky", cfg.les[0], "smag"),
-                          ("smagorinsky", cfg.les[-1], "smag"), ("no_model", cfg.les[0], "bgk")):
-        if f"{name}_{m}" in runs:
-            continue
+    def les_run(kind, m, mom, nsamples, steps_per):
+        """One LES from the filtered state `mom`; spectra after every steps_per
+        steps.  Returns (spectra, device seconds, finite, fallback cells per step)."""
         r = n // m
         tau0 = tau_on(cfg, r)
-        a_r = cfg.force_lin * r
-        mom = init[m]
-        f0 = equilibrium_field(mom[1:4] / (1.0 + 0.5 * cfg.force_lin), mom[0])
+        eps_r = cfg.eps * r
+        a_r = [a_now[0] * r]
+        f0 = equilibrium_field(mom[1:4] / (1.0 + 0.5 * a_now[0]), mom[0])
         if kind == "mlp":
-            sol = LearnedLESSolver((m, m, m), tau0, model, force_lin=a_r, c_s=C_SMAG, device=dev).load(f0)
+            sol = LearnedLESSolver((m, m, m), tau0, model, force_lin=a_r[0], c_s=C_SMAG, device=dev).load(f0)
         else:
             sol = LBMSolver("D3Q19", (m, m, m), tau0, "smagorinsky" if kind == "smag" else "bgk", device=dev,
-                            c_smag=C_SMAG, force_lin=a_r).load(f0)
-        steps_per = max(1, every // r)
-        specs, secs = [], 0.0
-        for _ in range(cfg.spectra_per_window):
-            secs += _timed(lambda: sol.run(steps_per, chunk=cfg.chunk), dev)
+                            c_smag=C_SMAG, force_lin=a_r[0]).load(f0)
+        every_r = max(10, cfg.force_every // r)
+        specs, secs, finite = [], 0.0, True
+
+        def advance_les():
+            a_r[0] = run_forced(sol, steps_per, eps_r, every_r, cfg.chunk)
+
+        for _ in range(nsamples):
+            try:
+                secs += _timed(advance_les, dev)
+            except RuntimeError:
+                finite = False
+                break
             state = sol.state if kind == "mlp" else sol.f
-            specs.append(energy_spectrum(velocity_of(state, a_r)).cpu().numpy())
-        finite = not sol.nonfinite_seen()
+            specs.append(energy_spectrum(velocity_of(state, a_r[0])).cpu().numpy())
+        finite = finite and not sol.nonfinite_seen() and len(specs) > 0
+        fb = int(sol.fallback.item()) / max(sol.steps_done, 1) if kind == "mlp" else None
+        del sol
+        torch.cuda.empty_cache()
+        return specs, secs, finite, fb
+
+    # in-the-loop calibration of the network's scale on the TRAINING window:
+    # the LES starts from the first training snapshot and is compared with the
+    # filtered spectra of the later training snapshots (not the comparison window)
+    m0 = cfg.les[0]
+    r0 = n // m0
+    train_ref = np.mean([energy_spectrum(mm[1:4]).cpu().numpy() for mm in moms[m0][1:]], axis=0)
+    base_scale = model.nu_scale
+    calib = {}
+    if cfg.snapshots > 1:
+        for alpha in cfg.calibration:
+            model.nu_scale = base_scale * alpha
+            model.invalidate()
+            specs, _, fin, _ = les_run("mlp", m0, moms[m0][0], cfg.snapshots - 1, max(1, gap // r0))
+            err = _spec_error(np.mean(specs, axis=0), train_ref, min(m0 // 2, 21)) if fin else float("inf")
+            calib[str(alpha)] = err
+            log(f"calibration alpha {alpha}: error {err:.4f}")
+    alpha_best = float(min(calib, key=calib.get)) if calib else 1.0
+    res["calibration"] = {"errors": calib, "alpha": alpha_best}
+    model.nu_scale = base_scale * alpha_best
+    model.invalidate()
+    model.save(out_dir / "closure.npz")
+
+    runs: dict = {}
+    for name, m, kind, alpha in (("mlp", cfg.les[0], "mlp", alpha_best), ("mlp_uncalibrated", cfg.les[0], "mlp", 1.0),
+                                 ("smagorinsky", cfg.les[0], "smag", None),
+                                 ("smagorinsky", cfg.les[-1], "smag", None), ("no_model", cfg.les[0], "bgk", None)):
+        if f"{name}_{m}" in runs:
+            continue
+        if kind == "mlp":
+            model.nu_scale = base_scale * alpha
+            model.invalidate()
+        r = n // m
+        steps_per = max(1, every // r)
+        specs, secs, finite, fb = les_run(kind, m, init[m], cfg.spectra_per_window, steps_per)
+        if not specs:
+            specs = [np.full(len(dns_spec[m][0]), np.nan)]
         e_mean = np.mean(specs, axis=0)
         e_ref = np.mean(dns_spec[m], axis=0)
         kc = m // 2
-        entry = {"grid": m, "tau0": tau0, "steps": steps_per * cfg.spectra_per_window, "seconds": secs,
+        entry = {"grid": m, "tau0": tau_on(cfg, r), "steps": steps_per * cfg.spectra_per_window, "seconds": secs,
                  "mlups": m ** 3 * steps_per * cfg.spectra_per_window / max(secs, 1e-12) / 1e6,
                  "finite": finite, "spectrum": e_mean.tolist(), "filtered_dns_spectrum": e_ref.tolist(),
                  "spectrum_error_all": _spec_error(e_mean, e_ref, kc),
                  "spectrum_error_k_le_21": _spec_error(e_mean, e_ref, min(kc, 21)),
                  "kinetic_energy": float(e_mean.sum()), "filtered_dns_kinetic_energy": float(e_ref.sum())}
         if kind == "mlp":
-            entry["fallback_cells_per_step"] = int(sol.fallback.item()) / max(sol.steps_done, 1)
+            entry["fallback_cells_per_step"] = fb
+            entry["nu_scale_factor"] = alpha
         runs[f"{name}_{m}"] = entry
         log(f"LES {name} {m}^3: err {entry['spectrum_error_all']:.4f} (k<=21 {entry['spectrum_error_k_le_21']:.4f}),"
             f" {secs:.3f} s, finite {finite}")
-        del sol
-        torch.cuda.empty_cache()
+    model.nu_scale = base_scale * alpha_best
+    model.invalidate()
     res["les"] = runs
     mlp_key, big_key = f"mlp_{cfg.les[0]}", f"smagorinsky_{cfg.les[-1]}"
     res["summary"] = {
         "mlp_les_error": runs[mlp_key]["spectrum_error_k_le_21"],
+        "mlp_uncalibrated_les_error": runs[f"mlp_uncalibrated_{cfg.les[0]}"]["spectrum_error_k_le_21"],
+        "smagorinsky_coarse_error": runs[f"smagorinsky_{cfg.les[0]}"]["spectrum_error_k_le_21"],
         "smagorinsky_fine_error": runs[big_key]["spectrum_error_k_le_21"],
+        "no_model_coarse_error": runs[f"no_model_{cfg.les[0]}"]["spectrum_error_k_le_21"],
+        "calibration_alpha": alpha_best,
         "wall_time_ratio_smagorinsky_fine_over_mlp": runs[big_key]["seconds"] / max(runs[mlp_key]["seconds"], 1e-12),
     }
     (out_dir / "hit_les.json").write_text(json.dumps(res))
@@ -364,10 +460,10 @@ def main(argv=None) -> None:
     ap.add_argument("--les", type=int, nargs="+", default=[128, 256])
     ap.add_argument("--out", default="hit_les_out")
     ap.add_argument("--re-lambda", type=float, default=100.0)
-    ap.add_argument("--spinup", type=float, default=6.0, help="turnovers")
-    ap.add_argument("--window", type=float, default=2.0, help="turnovers")
+    ap.add_argument("--spinup", type=float, default=15.0, help="turnovers")
+    ap.add_argument("--window", type=float, default=3.0, help="turnovers")
     ap.add_argument("--epochs", type=int, default=12)
-    ap.add_argument("--snapshots", type=int, default=3)
+    ap.add_argument("--snapshots", type=int, default=4)
     args = ap.parse_args(argv)
     cfg = HITConfig(dns=args.dns, les=tuple(args.les), re_lambda=args.re_lambda, spinup_turnovers=args.spinup,
                     window_turnovers=args.window, train_epochs=args.epochs, snapshots=args.snapshots)

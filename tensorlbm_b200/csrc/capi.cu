@@ -106,7 +106,8 @@ int check_desc(const tlbm_desc* d) {
   if (d->bc & ~(uint32_t)(TLBM_BC_LID | TLBM_BC_ZH_INLET | TLBM_BC_ZH_OUTLET)) return TLBM_ERR_ARG;
   if (d->force_lin != 0.0) {
     if (!(d->force_lin == d->force_lin) || d->force_lin <= -1.0 || d->force_lin >= 1.0) return TLBM_ERR_ARG;
-    if (d->collision != TLBM_COLL_BGK && d->collision != TLBM_COLL_SMAGORINSKY && d->collision != TLBM_COLL_NONE)
+    if (d->collision != TLBM_COLL_BGK && d->collision != TLBM_COLL_MRT && d->collision != TLBM_COLL_SMAGORINSKY &&
+        d->collision != TLBM_COLL_NONE)
       return TLBM_ERR_UNSUPPORTED;
   }
   return TLBM_OK;

@@ -3,12 +3,30 @@
 // three lattices compile in parallel.
 #pragma once
 
+#include <type_traits>
+
 #include "tlbm_step.cuh"
 
 namespace tlbm {
 
+// linear forcing: float32 populations, BGK / MRT / Smagorinsky
+template <class L, typename S, bool PULL>
+int dispatch_forced(const tlbm_desc& d, const StepParams& p, cudaStream_t s) {
+  if constexpr (std::is_same<S, float>::value) {
+    switch (d.collision) {
+      case TLBM_COLL_BGK: return launch_step<L, S, S, TLBM_COLL_BGK, PULL, true>(p, d, s);
+      case TLBM_COLL_MRT: return launch_step<L, S, S, TLBM_COLL_MRT, PULL, true>(p, d, s);
+      case TLBM_COLL_SMAGORINSKY: return launch_step<L, S, S, TLBM_COLL_SMAGORINSKY, PULL, true>(p, d, s);
+      default: return TLBM_ERR_UNSUPPORTED;
+    }
+  } else {
+    return TLBM_ERR_DTYPE;
+  }
+}
+
 template <class L, typename S, bool PULL>
 int dispatch_collision(const tlbm_desc& d, const StepParams& p, cudaStream_t s) {
+  if (d.force_lin != 0.0 && d.collision != TLBM_COLL_NONE) return dispatch_forced<L, S, PULL>(d, p, s);
   switch (d.collision) {
     case TLBM_COLL_NONE: return launch_step<L, S, S, TLBM_COLL_NONE, PULL>(p, d, s);
     case TLBM_COLL_BGK: return launch_step<L, S, S, TLBM_COLL_BGK, PULL>(p, d, s);

@@ -46,7 +46,9 @@ template <typename SI, typename SO> struct Domain {
 // warp-wide.
 // PULL = true : gather from neighbours, boundaries, collide (COLL may be NONE)
 // PULL = false: local collide / format conversion only (no boundaries)
-template <class L, typename SI, typename SO, int COLL, bool PULL>
+// FORCED: add the exact-difference linear force after the collision (a
+// separate instantiation, so that the unforced kernels carry none of it)
+template <class L, typename SI, typename SO, int COLL, bool PULL, bool FORCED = false>
 __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int y, int z, bool active,
                                             const CollideParams<typename Storage<SI>::T>& cp,
                                             const BcParams<typename Storage<SI>::T>& bp) {
@@ -128,11 +130,9 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
     } else {
       const bool has_tau = d.tau_field != nullptr;
       const T tau_cell = has_tau ? T(d.tau_field[cell]) : T(0);
-      constexpr bool kForced = COLL == TLBM_COLL_BGK || COLL == TLBM_COLL_SMAGORINSKY;
-      if (kForced && cp.force_a != T(0)) {
-        // exact-difference forcing of F = A rho u (BGK and Smagorinsky only):
-        // collide, then add feq(rho, (1 + A) u) - feq(rho, u) with the
-        // pre-collision moments
+      if constexpr (FORCED) {
+        // exact-difference forcing of F = A rho u: collide, then add
+        // feq(rho, (1 + A) u) - feq(rho, u) with the pre-collision moments
         T rho, ux, uy, uz;
         macroscopic_fused<L>(f, rho, ux, uy, uz);
         collide<L, COLL>(f, cp, tau_cell, has_tau);
@@ -155,7 +155,7 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
   for (int q = 0; q < Q; ++q) fout[(long long)q * N + cell] = Storage<SO>::store(f[q], weight<L, T>(q));
 }
 
-template <class L, typename SI, typename SO, int COLL, bool PULL>
+template <class L, typename SI, typename SO, int COLL, bool PULL, bool FORCED = false>
 __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typename Storage<SI>::T> cp,
                                               BcParams<typename Storage<SI>::T> bp) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typena
   d.plane = p.plane;
   d.n = p.n;
   d.bc = p.bc;
-  cell_update<L, SI, SO, COLL, PULL>(d, x, y, z, (x < p.nx) && (y < p.ny), cp, bp);
+  cell_update<L, SI, SO, COLL, PULL, FORCED>(d, x, y, z, (x < p.nx) && (y < p.ny), cp, bp);
 }
 
 inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block) {
@@ -186,7 +186,7 @@ inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block) {
   grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
 }
 
-template <class L, typename SI, typename SO, int COLL, bool PULL>
+template <class L, typename SI, typename SO, int COLL, bool PULL, bool FORCED = false>
 int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   using T = typename Storage<SI>::T;
   dim3 grid, block;
@@ -195,7 +195,7 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
                                                d.omega_even, d.c_smag);
   cp.force_a = T(d.force_lin);
   const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
-  k_step<L, SI, SO, COLL, PULL><<<grid, block, 0, s>>>(p, cp, bp);
+  k_step<L, SI, SO, COLL, PULL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }
 

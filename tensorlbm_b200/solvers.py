@@ -68,7 +68,7 @@ class StepConfig:
     u_lid: float | None = None       # moving lid at y = ny-1
     u_in: tuple[float, float, float] | float | None = None  # Zou/He inlet at x = 0
     rho_out: float | None = None     # Zou/He outlet at x = nx-1
-    force_lin: float = 0.0           # linear body force F = A rho u (BGK / Smagorinsky)
+    force_lin: float = 0.0           # linear body force F = A rho u (BGK / MRT / Smagorinsky, float32)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -101,10 +101,10 @@ class StepConfig:
             c_smag=self.c_smag, bc=bc, u_lid=self.u_lid or 0.0, u_in=u_in,
             rho_out=1.0 if self.rho_out is None else self.rho_out,
         )
-        if coll in (_lib.COLL_BGK, _lib.COLL_SMAGORINSKY):
+        if coll in (_lib.COLL_BGK, _lib.COLL_MRT, _lib.COLL_SMAGORINSKY):
             d.force_lin = float(self.force_lin)
         elif self.force_lin and coll != _lib.COLL_NONE:
-            raise NotImplementedError("force_lin is implemented for the bgk and smagorinsky collisions")
+            raise NotImplementedError("force_lin is implemented for the bgk, mrt and smagorinsky collisions")
         return d
 
 
@@ -232,6 +232,15 @@ class LBMSolver:
             self._launch(self._buf[self._cur], self._buf[1 - self._cur], force)
             self._cur ^= 1
             self.steps_done += 1
+        return self
+
+    def set_force_lin(self, a: float) -> "LBMSolver":
+        """Change the linear body force A of F = A rho u (drops the captured graph)."""
+        self.cfg.force_lin = float(a)
+        wall = self._desc.wall_velocity
+        self._desc = self.cfg.desc(self.code)
+        self._desc.wall_velocity = wall
+        self._graph = None
         return self
 
     def run(self, n: int, *, graph: bool = True, chunk: int = 50) -> "LBMSolver":

@@ -213,20 +213,31 @@ def test_fused_les_step_matches_oracle(cuda, cut):
     assert np.max(np.abs(got - want)) <= 2e-6 * np.max(np.abs(want))
 
 
-def test_forced_bgk_generic_step_matches_oracle(cuda):
+def _forced(f, coll, tau, a_lin):
+    """collide (oracle, float64) then the exact-difference force term"""
+    f = np.asarray(f, np.float64)
+    rho, ux, uy, uz = O.macroscopic(f)
+    k = 1.0 + a_lin
+    out = O.COLLIDERS[coll](f, tau)
+    return out + O.equilibrium(19, rho, ux * k, uy * k, uz * k) - O.equilibrium(19, rho, ux, uy, uz)
+
+
+@pytest.mark.parametrize("coll", ["bgk", "mrt", "smagorinsky"])
+def test_forced_generic_step_matches_oracle(cuda, coll):
     from tensorlbm_b200 import LBMSolver
 
     rng = np.random.default_rng(9)
     sp = (8, 16, 64)
     rho = (1.0 + 0.01 * rng.standard_normal(sp)).astype(np.float32)
     u = [(0.03 * rng.standard_normal(sp)).astype(np.float32) for _ in range(3)]
-    f0 = O.equilibrium(19, rho, *u)
-    a_lin = 2e-3
-    s = LBMSolver("D3Q19", sp, 0.6, "bgk", device=cuda, force_lin=a_lin)
+    f0 = O.equilibrium(19, rho, *u) * (1.0 + 0.002 * rng.standard_normal((19,) + sp)).astype(np.float32)
+    a_lin, tau = 2e-3, 0.56
+    kw = {"c_smag": 0.1} if coll == "smagorinsky" else {}
+    s = LBMSolver("D3Q19", sp, tau, coll, device=cuda, force_lin=a_lin, **kw)
     s.load(T(f0, cuda)).step(2)
-    ref = L.forced_bgk(f0, 0.6, a_lin)
+    ref = _forced(f0, coll, tau, a_lin)
     for _ in range(2):
-        ref = L.forced_bgk(O.stream(ref), 0.6, a_lin)
+        ref = _forced(O.stream(ref), coll, tau, a_lin)
     # the stored post-collision state P_2
     got = N(s._buf[s._cur]).astype(np.float64)
     assert np.max(np.abs(got - ref)) <= 2e-6 * np.max(np.abs(ref))
