@@ -41,8 +41,10 @@ typedef enum tlbm_status {
 
 typedef enum tlbm_lattice { TLBM_D2Q9 = 9, TLBM_D3Q19 = 19, TLBM_D3Q27 = 27 } tlbm_lattice;
 
-/* Storage / arithmetic formats.  The shifted half formats store f_q - w_q and
- * compute in float32. */
+/* Storage / arithmetic formats.  The shifted half formats store the deviation
+ * f_q - w_q (times 2^14 for float16, which keeps it out of the subnormal
+ * range), stochastically rounded (unbiased; the random bits hash the cell and
+ * the new value), and compute in float32. */
 typedef enum tlbm_dtype {
   TLBM_F32 = 0,
   TLBM_F64 = 1,

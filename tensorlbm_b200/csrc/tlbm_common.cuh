@@ -20,29 +20,63 @@ namespace tlbm {
 // ---------------------------------------------------------------------------
 template <typename S> struct Storage;
 
+// MurmurHash3's 32-bit finaliser (Appleby): a bijective mixer of the key bits
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85EBCA6Bu;
+  h ^= h >> 13;
+  h *= 0xC2B2AE35u;
+  h ^= h >> 16;
+  return h;
+}
+
+// Stochastic rounding of the float32 bit pattern to its `drop` low bits:
+// add uniform random bits below the kept mantissa, then truncate the
+// magnitude (round toward zero).  The result rounds up with probability equal
+// to the dropped fraction, so it is unbiased; non-finite values pass unchanged.
+template <int DROP>
+__device__ __forceinline__ float stochastic_truncate_bits(float d, uint32_t r) {
+  const uint32_t bits = __float_as_uint(d);
+  uint32_t mag = bits & 0x7FFFFFFFu;
+  if (mag < 0x7F800000u) mag += r >> (32 - DROP);
+  return __uint_as_float((bits & 0x80000000u) | mag);
+}
+
+// store(v, w, r): r is 32 random bits for the stochastic rounding of the
+// half formats (ignored by float and double).
 template <> struct Storage<float> {
   using T = float;
   static constexpr bool kShifted = false;
   __device__ __forceinline__ static float load(float v, float) { return v; }
-  __device__ __forceinline__ static float store(float v, float) { return v; }
+  __device__ __forceinline__ static float store(float v, float, uint32_t) { return v; }
 };
 template <> struct Storage<double> {
   using T = double;
   static constexpr bool kShifted = false;
   __device__ __forceinline__ static double load(double v, double) { return v; }
-  __device__ __forceinline__ static double store(double v, double) { return v; }
+  __device__ __forceinline__ static double store(double v, double, uint32_t) { return v; }
 };
+// float16: (f - w) * 2^14, stochastically rounded.  The scale keeps every
+// deviation |f - w| > 4e-9 out of the subnormal range (|f - w| < 4 stays finite).
 template <> struct Storage<__half> {
   using T = float;
   static constexpr bool kShifted = true;
-  __device__ __forceinline__ static float load(__half v, float w) { return __half2float(v) + w; }
-  __device__ __forceinline__ static __half store(float v, float w) { return __float2half_rn(v - w); }
+  static constexpr float kScale = 16384.0f;
+  __device__ __forceinline__ static float load(__half v, float w) {
+    return fmaf(__half2float(v), 1.0f / kScale, w);
+  }
+  __device__ __forceinline__ static __half store(float v, float w, uint32_t r) {
+    return __float2half_rz(stochastic_truncate_bits<13>((v - w) * kScale, r));
+  }
 };
+// bfloat16: f - w (float32 range), stochastically rounded
 template <> struct Storage<__nv_bfloat16> {
   using T = float;
   static constexpr bool kShifted = true;
   __device__ __forceinline__ static float load(__nv_bfloat16 v, float w) { return __bfloat162float(v) + w; }
-  __device__ __forceinline__ static __nv_bfloat16 store(float v, float w) { return __float2bfloat16_rn(v - w); }
+  __device__ __forceinline__ static __nv_bfloat16 store(float v, float w, uint32_t r) {
+    return __float2bfloat16_rz(stochastic_truncate_bits<16>(v - w, r));
+  }
 };
 
 // Lattice weight in compute type T.  TensorLBM's D2Q9 module keeps its weights

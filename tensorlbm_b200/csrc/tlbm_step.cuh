@@ -151,8 +151,14 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
       }
     }
   }
+  // random bits of the stochastic rounding of half storage: a hash of the
+  // cell and of this step's value of f[0] (so they change every step without
+  // a seed), spread over the directions by a second multiply
+  uint32_t h = 0;
+  if constexpr (Storage<SO>::kShifted) h = fmix32(uint32_t(cell) * 0x9E3779B9u ^ __float_as_uint(float(f[0])));
 #pragma unroll
-  for (int q = 0; q < Q; ++q) fout[(long long)q * N + cell] = Storage<SO>::store(f[q], weight<L, T>(q));
+  for (int q = 0; q < Q; ++q)
+    fout[(long long)q * N + cell] = Storage<SO>::store(f[q], weight<L, T>(q), (h ^ (uint32_t(q) * 0x9E3779B9u)) * 0x85EBCA6Bu);
 }
 
 template <class L, typename SI, typename SO, int COLL, bool PULL, bool FORCED = false>

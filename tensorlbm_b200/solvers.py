@@ -117,7 +117,8 @@ class LBMSolver:
         tau: shear relaxation time.
         collision: "bgk", "mrt", "smagorinsky", "cumulant" (D3Q27 legacy),
             "cumulant_geier" (D3Q27), "cumulant_d3q19".
-        storage: "f32", "f64", "f16" or "bf16" (half formats hold f - w).
+        storage: "f32", "f64", "f16" or "bf16" (half formats hold the deviation f - w,
+            scaled by 2^14 for f16, stochastically rounded).
         wall_mask, obstacle_mask: bool fields; both bounce back, only the
             obstacle enters the momentum-exchange force.
         u_lid, u_in, rho_out: enable the lid / Zou-He inlet / outlet planes.
@@ -275,7 +276,7 @@ class LBMSolver:
 
     @property
     def state(self) -> torch.Tensor:
-        """Stored post-collision populations P_n (storage format, f - w for half formats)."""
+        """Stored post-collision populations P_n (storage format: (f - w) 2^14 for f16, f - w for bf16)."""
         return self._buf[self._cur]
 
     @property
