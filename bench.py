@@ -385,6 +385,17 @@ def run_ours(args) -> None:
                                                      2 * 19 * 2, peak)
     if want("d3q19_bgk_f32"):
         variants["d3q19_bgk_f32"] = _variant(torch, dev, "D3Q19", "bgk", "f32", args.steps, args.warmup, bpc, peak)
+    for name, lat, coll, st, bpc_v, steps_v in (
+            ("d3q19_bgk_f16_shifted", "D3Q19", "bgk", "f16", 2 * 19 * 2, args.steps),
+            ("d3q19_bgk_bf16_shifted", "D3Q19", "bgk", "bf16", 2 * 19 * 2, args.steps),
+            ("d3q27_cumulant_f16_shifted", "D3Q27", "cumulant", "f16", 2 * 27 * 2, max(args.steps // 2, 3))):
+        if want(name):
+            variants[name] = _variant(torch, dev, lat, coll, st, steps_v, args.warmup, bpc_v, peak)
+    # half storage against float32 for the same collision (MLUPS ratio)
+    for half, full in (("d3q19_bgk_f16_shifted", "d3q19_bgk_f32"), ("d3q19_bgk_bf16_shifted", "d3q19_bgk_f32"),
+                       ("d3q19_mrt_f16_shifted", None), ("d3q27_cumulant_f16_shifted", "d3q27_cumulant_f32")):
+        if half in variants and full in variants:
+            variants[half]["speedup_vs_f32"] = round(variants[half]["mlups"] / variants[full]["mlups"], 3)
     if want("les_mlp_128_vs_smagorinsky_256"):
         variants["les_mlp_128_vs_smagorinsky_256"] = _les_variant(torch, dev, args.steps, args.warmup, peak)
     if want("d2q9_batched_512_cylinders"):
@@ -546,8 +557,9 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--variants", default="all",
-                    help="comma list of variants to run (d3q27_cumulant_f32, d3q19_mrt_f16_shifted, "
-                         "d3q19_bgk_f32, les_mlp_128_vs_smagorinsky_256, d2q9_batched_512_cylinders) or 'all'")
+                    help="comma list of variants to run (d3q27_cumulant_f32, d3q27_cumulant_f16_shifted, "
+                         "d3q19_mrt_f16_shifted, d3q19_bgk_f32, d3q19_bgk_f16_shifted, d3q19_bgk_bf16_shifted, "
+                         "les_mlp_128_vs_smagorinsky_256, d2q9_batched_512_cylinders) or 'all'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-slab", type=int, default=8, help="z-planes per CPU sample slab")
     ap.add_argument("--cpu-steps", type=int, default=2)
