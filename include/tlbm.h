@@ -301,10 +301,16 @@ typedef struct tlbm_batch_desc {
 
 /* One step of every domain, one launch (grid = tiles).  domains and tiles are
  * device arrays.  forces (may be NULL): ndomains x 3 doubles, accumulated
- * (zero before the step).  status bit 0: non-finite density. */
+ * (zero before the step).  force_slot (device int, may be NULL): when given,
+ * the forces go to forces + 3 * ndomains * (*force_slot), so that a captured
+ * CUDA graph can record into a history whose slot tlbm_batch_advance_slot
+ * moves on.  status bit 0: non-finite density. */
 TLBM_API int tlbm_batch_step(const tlbm_batch_desc* b, const tlbm_batch_domain* domains, const int32_t* tiles,
                              int64_t ntiles, const void* f_in, void* f_out, const uint8_t* flags, double* forces,
-                             unsigned int* status, void* stream);
+                             const int32_t* force_slot, unsigned int* status, void* stream);
+
+/* *slot += 1 on the stream (one thread).  No reference counterpart. */
+TLBM_API int tlbm_batch_advance_slot(int32_t* slot, void* stream);
 
 /* nsteps steps in one persistent cooperative launch; the state ping-pongs
  * f_a -> f_b -> f_a ..., so it ends in f_a when nsteps is even.  Step s with

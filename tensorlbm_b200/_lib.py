@@ -102,7 +102,8 @@ SIGNATURES: dict[str, list] = {
     "tlbm_link_blocks": [_I64],
     "tlbm_link_count": [_P, _I64, _P, _P, _P],
     "tlbm_link_list": [_P, _I64, _P, _P, _P],
-    "tlbm_batch_step": [ctypes.POINTER(BatchDesc), _P, _P, _I64, _P, _P, _P, _P, _P, _P],
+    "tlbm_batch_step": [ctypes.POINTER(BatchDesc), _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P],
+    "tlbm_batch_advance_slot": [_P, _P],
     "tlbm_batch_run": [ctypes.POINTER(BatchDesc), _P, _P, _I64, _P, _P, _P, _I32, _P, _I32, _P, _P, _I64, _P],
     "tlbm_link_list_noalloc": [_P, _I64, _P, _I64, _P, _P],
     "tlbm_link_list_static_capacity": [],

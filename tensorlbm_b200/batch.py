@@ -179,11 +179,42 @@ class BatchedSolver:
     def _bufs(self):
         return (self.fa, self.fb) if self._cur == 0 else (self.fb, self.fa)
 
-    def _launch(self, src, dst, forces) -> None:
+    def _launch(self, src, dst, forces, slot=None) -> None:
         st = _fn("tlbm_batch_step")(ctypes.byref(self._desc()), self.domains_dev.data_ptr(), self.tiles_dev.data_ptr(),
                                    self.ntiles, src.data_ptr(), dst.data_ptr(), self.flags.data_ptr(),
-                                   _lib.ptr(forces), self.status.data_ptr(), _lib.stream_of(self.device))
+                                   _lib.ptr(forces), _lib.ptr(slot), self.status.data_ptr(),
+                                   _lib.stream_of(self.device))
         _lib.check(st, "tlbm_batch_step")
+
+    def _run_recorded_graph(self, n: int, record_every: int, hist: torch.Tensor) -> int:
+        """Graph-replayed steps that record forces: the recording launch finds
+        its history slot through a device counter that the graph advances.
+        Returns the number of steps done (a multiple of the captured chunk)."""
+        k = record_every if record_every % 2 == 0 else 2 * record_every  # even: the parity returns
+        reps = n // k
+        if reps == 0:
+            return 0
+        slot = torch.zeros(1, dtype=torch.int32, device=self.device)
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s), torch.cuda.graph(g, stream=s):
+            c = self._cur
+            for j in range(k):
+                src, dst = (self.fa, self.fb) if c == 0 else (self.fb, self.fa)
+                if j % record_every == 0:
+                    self._launch(src, dst, hist, slot)
+                    _lib.check(_fn("tlbm_batch_advance_slot")(slot.data_ptr(), _lib.stream_of(self.device)),
+                               "tlbm_batch_advance_slot")
+                else:
+                    self._launch(src, dst, None)
+                c ^= 1
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        for _ in range(reps):
+            g.replay()
+        self.steps_done += reps * k
+        del g
+        return reps * k
 
     def step(self, n: int = 1, *, record_forces: bool = False) -> "BatchedSolver":
         for _ in range(n):
@@ -213,6 +244,14 @@ class BatchedSolver:
             _lib.check(st, "tlbm_batch_run")
             self._cur ^= n & 1
             self.steps_done += n
+            return hist
+        if record_every > 0 and self.mode == "graph":
+            done = self._run_recorded_graph(n, record_every, hist)
+            for k in range(done, n):
+                src, dst = self._bufs()
+                self._launch(src, dst, hist[k // record_every] if k % record_every == 0 else None)
+                self._cur ^= 1
+                self.steps_done += 1
             return hist
         if record_every > 0 or self.mode == "launch" or n < chunk:
             for k in range(n):

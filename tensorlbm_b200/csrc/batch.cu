@@ -61,7 +61,9 @@ __device__ __forceinline__ void process_tile(const tlbm_batch_domain* __restrict
 template <class L, typename S, int COLL>
 __global__ void __launch_bounds__(256) k_batch_step(const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
                                                     const S* fin, S* fout, const uint8_t* flags, double* forces,
-                                                    unsigned int* status) {
+                                                    const int* force_slot, int ndomains, unsigned int* status) {
+  // with a slot counter, the forces of this step go to record *force_slot
+  if (forces && force_slot) forces += 3LL * ndomains * (*force_slot);
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x)
     process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status);
 }
@@ -121,12 +123,12 @@ __global__ void __launch_bounds__(256) k_batch_run(const tlbm_batch_domain* doms
 
 template <class L, typename S, int COLL>
 int launch_batch(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
-                 const void* fin, void* fout, const uint8_t* flags, double* forces, unsigned int* status,
-                 cudaStream_t s) {
+                 const void* fin, void* fout, const uint8_t* flags, double* forces, const int* force_slot,
+                 unsigned int* status, cudaStream_t s) {
   const dim3 block(b.tile_x, b.tile_y);
   const long long grid = ntiles < 0x7fffffffLL ? ntiles : 0x7fffffffLL;
   k_batch_step<L, S, COLL><<<(unsigned)grid, block, 0, s>>>(doms, tiles, ntiles, (const S*)fin, (S*)fout, flags,
-                                                           forces, status);
+                                                           forces, force_slot, b.ndomains, status);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }
 
@@ -167,6 +169,8 @@ int launch_batch_run(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, co
   return TLBM_OK;
 }
 
+__global__ void k_advance_slot(int* slot) { slot[0] += 1; }
+
 int check_batch(const tlbm_batch_desc* b, const tlbm_batch_domain* doms, const int* tiles, long long ntiles) {
   if (!b || !doms || !tiles) return TLBM_ERR_ARG;
   if (b->lattice != TLBM_D2Q9) return TLBM_ERR_UNSUPPORTED;
@@ -186,7 +190,7 @@ extern "C" {
 
 TLBM_API int tlbm_batch_step(const tlbm_batch_desc* b, const tlbm_batch_domain* domains, const int32_t* tiles,
                              int64_t ntiles, const void* f_in, void* f_out, const uint8_t* flags, double* forces,
-                             unsigned int* status, void* stream) {
+                             const int32_t* force_slot, unsigned int* status, void* stream) {
   int st = check_batch(b, domains, tiles, ntiles);
   if (st != TLBM_OK) return st;
   if (!f_in || !f_out) return TLBM_ERR_ARG;
@@ -194,8 +198,16 @@ TLBM_API int tlbm_batch_step(const tlbm_batch_desc* b, const tlbm_batch_domain* 
   if (ntiles == 0) return TLBM_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (b->collision == TLBM_COLL_BGK)
-    return launch_batch<D2Q9, float, TLBM_COLL_BGK>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces, status, s);
-  return launch_batch<D2Q9, float, TLBM_COLL_MRT>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces, status, s);
+    return launch_batch<D2Q9, float, TLBM_COLL_BGK>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces,
+                                                    force_slot, status, s);
+  return launch_batch<D2Q9, float, TLBM_COLL_MRT>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces,
+                                                  force_slot, status, s);
+}
+
+TLBM_API int tlbm_batch_advance_slot(int32_t* slot, void* stream) {
+  if (!slot) return TLBM_ERR_ARG;
+  k_advance_slot<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(slot);
+  return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }
 
 TLBM_API int tlbm_batch_run(const tlbm_batch_desc* b, const tlbm_batch_domain* domains, const int32_t* tiles,
