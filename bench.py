@@ -282,6 +282,23 @@ def _batched_variant(torch, dev, steps, peak):
             "nonfinite_domains_tau_max": unstable_tau[-1] if unstable_tau else None}
 
 
+def max_over_ranks(t: float, device) -> float:
+    """The slowest rank's time (every rank takes part; a no-op on one process)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return t
+    tt = torch.tensor([t], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt)
+
+
+def whole_job_mlups(world: int, cells_per_rank: int, steps: int, t_max: float) -> float:
+    """Cell updates of all ranks (one replica each) per second of the slowest rank, in millions."""
+    return world * cells_per_rank * steps / t_max / 1e6
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -322,15 +339,11 @@ def run_ours(args) -> None:
         torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
-    t = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        tt = torch.tensor([t], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t = float(tt)
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3, dev)
     s.steps_done += args.steps + args.warmup
     drag = float(force[0])
     finite = not s.nonfinite_seen()
-    value = world * cells * args.steps / t / 1e6
+    value = whole_job_mlups(world, cells, args.steps, t)
     per_launch = t / args.steps
     achieved = bpc * cells / per_launch / 1e9
     del s
@@ -360,12 +373,8 @@ def run_ours(args) -> None:
     host_out.copy_(s2.f, non_blocking=True)
     e3.record(cur)
     torch.cuda.synchronize(dev)
-    t_e2e = e2.elapsed_time(e3) / 1e3
-    if world > 1:
-        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_e2e = float(tt)
-    e2e_value = world * cells * args.steps / t_e2e / 1e6
+    t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3, dev)
+    e2e_value = whole_job_mlups(world, cells, args.steps, t_e2e)
     state_bytes = host_f0.numel() * 4
     del s2, f_dev
     torch.cuda.empty_cache()
