@@ -79,6 +79,71 @@ template <> struct Storage<__nv_bfloat16> {
   }
 };
 
+// Two consecutive values of one direction (cells x and x + 1, x even) moved
+// as one aligned vector.  split() converts to the compute type; join()
+// converts back with the stochastic rounding of the half formats, whose
+// random bits come from one 32-bit hash per cell (ha, hb; zero for a
+// non-finite cell, so that NaN / Inf pass unchanged) multiplied by an odd
+// constant per direction q (a multiplicative hash; the top bits are used).
+__device__ __forceinline__ uint32_t direction_mix(int q) { return 0x9E3779B9u * uint32_t(2 * q + 1); }
+
+// cvt.rz.{f16,bf16}x2.f32 d, a, b puts the conversion of a in the upper half
+// of d and of b in the lower half (the lower half is the lower address).
+__device__ __forceinline__ uint32_t cvt_rz_f16x2(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+__device__ __forceinline__ uint32_t cvt_rz_bf16x2(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rz.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+
+template <typename S> struct PairIO;
+template <> struct PairIO<float> {
+  using V = float2;
+  __device__ __forceinline__ static void split(V v, float, float& a, float& b) { a = v.x; b = v.y; }
+  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, uint32_t, int) { return make_float2(a, b); }
+};
+template <> struct PairIO<double> {
+  using V = double2;
+  __device__ __forceinline__ static void split(V v, double, double& a, double& b) { a = v.x; b = v.y; }
+  __device__ __forceinline__ static V join(double a, double b, double, uint32_t, uint32_t, int) {
+    return make_double2(a, b);
+  }
+};
+template <> struct PairIO<__half> {
+  using V = uint32_t;
+  static constexpr float kScale = Storage<__half>::kScale;
+  __device__ __forceinline__ static void split(V v, float w, float& a, float& b) {
+    const float2 t = __half22float2(*reinterpret_cast<const __half2*>(&v));
+    a = fmaf(t.x, 1.0f / kScale, w);
+    b = fmaf(t.y, 1.0f / kScale, w);
+  }
+  // (v - w) * 2^14 rounded once (the scaling is exact), plus 13 random bits
+  // below the kept mantissa, truncated: the same format as Storage::store
+  __device__ __forceinline__ static V join(float a, float b, float w, uint32_t ha, uint32_t hb, int q) {
+    const uint32_t m = direction_mix(q);
+    const uint32_t ba = __float_as_uint(fmaf(a, kScale, -w * kScale)) + ((ha * m) >> 19);
+    const uint32_t bb = __float_as_uint(fmaf(b, kScale, -w * kScale)) + ((hb * m) >> 19);
+    return cvt_rz_f16x2(__uint_as_float(ba), __uint_as_float(bb));
+  }
+};
+template <> struct PairIO<__nv_bfloat16> {
+  using V = uint32_t;
+  __device__ __forceinline__ static void split(V v, float w, float& a, float& b) {
+    a = __uint_as_float(v << 16) + w;
+    b = __uint_as_float(v & 0xFFFF0000u) + w;
+  }
+  __device__ __forceinline__ static V join(float a, float b, float w, uint32_t ha, uint32_t hb, int q) {
+    const uint32_t m = direction_mix(q);
+    const uint32_t ba = __float_as_uint(a - w) + ((ha * m) >> 16);
+    const uint32_t bb = __float_as_uint(b - w) + ((hb * m) >> 16);
+    return cvt_rz_bf16x2(__uint_as_float(ba), __uint_as_float(bb));
+  }
+};
+
 // Lattice weight in compute type T.  TensorLBM's D2Q9 module keeps its weights
 // as float32 even for float64 fields (tensorlbm/d2q9.py:22-25, 35-36), so a
 // float64 D2Q9 computation uses the float32-rounded weights; D3Q19/D3Q27 cast

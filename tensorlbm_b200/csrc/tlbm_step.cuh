@@ -10,6 +10,8 @@
 // 128-byte row access (shifted by one element for c_x = +-1).
 #pragma once
 
+#include <type_traits>
+
 #include "tlbm_bc.cuh"
 
 namespace tlbm {
@@ -40,6 +42,76 @@ template <typename SI, typename SO> struct Domain {
   long long plane, n;
   uint32_t bc;
 };
+
+// Boundary conditions of one cell after the pull, in TensorLBM's order:
+// Zou/He inlet / outlet planes, full-way (or moving-wall) bounce-back, lid.
+template <class L, typename T, typename SI, typename SO>
+__device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x, int y, long long cell, uint8_t fl,
+                                                 T (&f)[L::Q], const BcParams<T>& bp) {
+  constexpr int Q = L::Q;
+  const long long N = d.n;
+  // Zou/He inlet / outlet planes
+  if ((d.bc & TLBM_BC_ZH_INLET) && x == 0) {
+    if constexpr (Q == 9) zou_he_inlet_d2q9(f, bp.u_in, bp.uy_in);
+    else zou_he_inlet_3d<L>(f, bp.u_in, bp.uy_in, bp.uz_in, bp.one_minus_u);
+  }
+  if ((d.bc & TLBM_BC_ZH_OUTLET) && x == d.nx - 1) {
+    if constexpr (Q == 9) zou_he_outlet_d2q9(f, bp.rho_out, bp.two_thirds_rho_out, bp.sixth_rho_out);
+    else zou_he_outlet_3d<L>(f, bp.rho_out);
+  }
+  // full-way bounce-back; Ladd moving wall where flagged.  A moving obstacle
+  // cell that is also a wall cell has SOLID cleared (wall XOR obstacle): it
+  // takes the wall swap first, then the moving-wall pass, as
+  // bounce_back(wall) followed by moving_wall_bounce_back(obstacle).
+  if ((fl & TLBM_FLAG_MOVING) && d.wall_u) {
+    const T* uw = static_cast<const T*>(d.wall_u);
+    if (!(fl & TLBM_FLAG_SOLID)) bounce_back<L>(f);
+    moving_wall_bounce_back<L>(f, uw[cell], uw[N + cell], L::DIM == 3 ? uw[2 * N + cell] : T(0));
+  } else if (fl & TLBM_FLAG_SOLID) {
+    bounce_back<L>(f);
+  }
+  // moving lid
+  if ((d.bc & TLBM_BC_LID) && y == d.ny - 1) {
+    if constexpr (Q == 9) moving_lid_d2q9(f, bp.u_lid);
+    else if constexpr (Q == 19) moving_lid_d3q19(f, bp.u_lid);
+  }
+}
+
+// Collision of one cell (or the reversal of a half-way wall cell), the
+// optional exact-difference linear force, and the non-finite status bit.
+template <class L, typename SI, typename SO, int COLL, bool FORCED, typename T>
+__device__ __forceinline__ void relax(const Domain<SI, SO>& d, long long cell, uint8_t fl, T (&f)[L::Q],
+                                      const CollideParams<T>& cp) {
+  constexpr int Q = L::Q;
+  if constexpr (COLL != TLBM_COLL_NONE) {
+    if (fl & TLBM_FLAG_HALFWAY) {
+      // pre-stream half-way wall: keep the populations, reversed, uncollided
+      bounce_back<L>(f);
+    } else {
+      const bool has_tau = d.tau_field != nullptr;
+      const T tau_cell = has_tau ? T(d.tau_field[cell]) : T(0);
+      if constexpr (FORCED) {
+        // exact-difference forcing of F = A rho u: collide, then add
+        // feq(rho, (1 + A) u) - feq(rho, u) with the pre-collision moments
+        T rho, ux, uy, uz;
+        macroscopic_fused<L>(f, rho, ux, uy, uz);
+        collide<L, COLL, T, Storage<SI>::kShifted>(f, cp, tau_cell, has_tau);
+        const T k = T(1) + cp.force_a;
+        const T usq = ux * ux + uy * uy + uz * uz;
+        const T usq_k = usq * k * k;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+          f[q] += feq_fused<L>(q, rho, ux * k, uy * k, uz * k, usq_k) - feq_fused<L>(q, rho, ux, uy, uz, usq);
+      } else {
+        collide<L, COLL, T, Storage<SI>::kShifted>(f, cp, tau_cell, has_tau);
+      }
+      if (d.status) {
+        const T r = f[0];
+        if (!(r == r) || r - r != T(0)) atomicOr(d.status, 1u);
+      }
+    }
+  }
+}
 
 // The update of cell (x, y, z) of one domain.  Every thread of a warp must
 // call it (inactive ones with active = false) because the force reduction is
@@ -86,71 +158,18 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
   }
 
   if constexpr (PULL) {
-    // 1. momentum-exchange force sample (post-stream, pre-bounce-back)
+    // momentum-exchange force sample (post-stream, pre-bounce-back)
     if (d.force) {
       const bool ob = active && (fl & TLBM_FLAG_OBSTACLE);
       T mx = T(0), my = T(0), mz = T(0);
       if (ob) cell_momentum<L>(f, mx, my, mz);
       accumulate_force(d.force, __any_sync(0xffffffffu, ob), mx, my, mz);
     }
-    if (active) {
-      // 2. Zou/He inlet / outlet planes
-      if ((d.bc & TLBM_BC_ZH_INLET) && x == 0) {
-        if constexpr (Q == 9) zou_he_inlet_d2q9(f, bp.u_in, bp.uy_in);
-        else zou_he_inlet_3d<L>(f, bp.u_in, bp.uy_in, bp.uz_in, bp.one_minus_u);
-      }
-      if ((d.bc & TLBM_BC_ZH_OUTLET) && x == d.nx - 1) {
-        if constexpr (Q == 9) zou_he_outlet_d2q9(f, bp.rho_out, bp.two_thirds_rho_out, bp.sixth_rho_out);
-        else zou_he_outlet_3d<L>(f, bp.rho_out);
-      }
-      // 3. full-way bounce-back; Ladd moving wall where flagged.  A moving
-      //    obstacle cell that is also a wall cell has SOLID cleared (wall XOR
-      //    obstacle): it takes the wall swap first, then the moving-wall pass,
-      //    as bounce_back(wall) followed by moving_wall_bounce_back(obstacle).
-      if ((fl & TLBM_FLAG_MOVING) && d.wall_u) {
-        const T* uw = static_cast<const T*>(d.wall_u);
-        if (!(fl & TLBM_FLAG_SOLID)) bounce_back<L>(f);
-        moving_wall_bounce_back<L>(f, uw[cell], uw[N + cell], L::DIM == 3 ? uw[2 * N + cell] : T(0));
-      } else if (fl & TLBM_FLAG_SOLID) {
-        bounce_back<L>(f);
-      }
-      // 4. moving lid
-      if ((d.bc & TLBM_BC_LID) && y == d.ny - 1) {
-        if constexpr (Q == 9) moving_lid_d2q9(f, bp.u_lid);
-        else if constexpr (Q == 19) moving_lid_d3q19(f, bp.u_lid);
-      }
-    }
+    if (active) apply_boundaries<L>(d, x, y, cell, fl, f, bp);
   }
 
   if (!active) return;
-  if constexpr (COLL != TLBM_COLL_NONE) {
-    if (fl & TLBM_FLAG_HALFWAY) {
-      // pre-stream half-way wall: keep the populations, reversed, uncollided
-      bounce_back<L>(f);
-    } else {
-      const bool has_tau = d.tau_field != nullptr;
-      const T tau_cell = has_tau ? T(d.tau_field[cell]) : T(0);
-      if constexpr (FORCED) {
-        // exact-difference forcing of F = A rho u: collide, then add
-        // feq(rho, (1 + A) u) - feq(rho, u) with the pre-collision moments
-        T rho, ux, uy, uz;
-        macroscopic_fused<L>(f, rho, ux, uy, uz);
-        collide<L, COLL, T, Storage<SI>::kShifted>(f, cp, tau_cell, has_tau);
-        const T k = T(1) + cp.force_a;
-        const T usq = ux * ux + uy * uy + uz * uz;
-        const T usq_k = usq * k * k;
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-          f[q] += feq_fused<L>(q, rho, ux * k, uy * k, uz * k, usq_k) - feq_fused<L>(q, rho, ux, uy, uz, usq);
-      } else {
-        collide<L, COLL, T, Storage<SI>::kShifted>(f, cp, tau_cell, has_tau);
-      }
-      if (d.status) {
-        const T r = f[0];
-        if (!(r == r) || r - r != T(0)) atomicOr(d.status, 1u);
-      }
-    }
-  }
+  relax<L, SI, SO, COLL, FORCED>(d, cell, fl, f, cp);
   // random bits of the stochastic rounding of half storage: a hash of the
   // cell and of this step's value of f[0] (so they change every step without
   // a seed), spread over the directions by a second multiply
@@ -184,6 +203,120 @@ __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typena
   cell_update<L, SI, SO, COLL, PULL, FORCED>(d, x, y, z, (x < p.nx) && (y < p.ny), cp, bp);
 }
 
+// Two cells per thread: (x, y, z) and (x + 1, y, z) with x even.  The pull
+// of a direction with c_x = 0 is one aligned vector load of both cells'
+// values, every store is one vector store, and the index arithmetic (32-bit
+// offsets from the cell; the wrap is folded into six per-thread deltas) is
+// shared by the two cells.  Each cell then takes exactly the per-cell path
+// of k_step (boundaries, collision, forcing, status), so the float32 and
+// float64 results are those of k_step bit for bit.
+// Requires nx even, n < 2^31, and f_in / f_out aligned to two values.
+template <class L, typename S, int COLL, bool FORCED = false>
+__global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typename Storage<S>::T> cp,
+                                                 BcParams<typename Storage<S>::T> bp) {
+  using T = typename Storage<S>::T;
+  using IO = PairIO<S>;
+  using V = typename IO::V;
+  constexpr int Q = L::Q;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool active = (x < nx) && (y < ny);
+  const int plane = nx * ny;
+  const int N = int(p.n);
+  const int c = z * plane + y * nx + x;
+  Domain<S, S> d;
+  d.fin = static_cast<const S*>(p.f_in);
+  d.fout = static_cast<S*>(p.f_out);
+  d.flags = p.flags;
+  d.tau_field = p.tau_field;
+  d.force = p.force;
+  d.status = p.status;
+  d.wall_u = p.wall_velocity;
+  d.nx = nx;
+  d.ny = ny;
+  d.nz = nz;
+  d.plane = p.plane;
+  d.n = p.n;
+  d.bc = p.bc;
+
+  T fa[Q], fb[Q];
+  uint32_t fl2 = 0;
+  if (active) {
+    // offsets from cell c to the source rows (periodic wrap on every axis)
+    const int dym = (y == 0) ? (ny - 1) * nx : -nx;
+    const int dyp = (y == ny - 1) ? -(ny - 1) * nx : nx;
+    const int dzm = (L::DIM == 3) ? ((z == 0) ? (nz - 1) * plane : -plane) : 0;
+    const int dzp = (L::DIM == 3) ? ((z == nz - 1) ? -(nz - 1) * plane : plane) : 0;
+    const int dxm = (x == 0) ? nx - 1 : -1;      // cell x pulls c_x = +1 from x - 1
+    const int dxp = (x + 2 == nx) ? 2 - nx : 2;  // cell x + 1 pulls c_x = -1 from x + 2
+    const S* __restrict__ fin = d.fin;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int row = c + (L::cy(q) > 0 ? dym : (L::cy(q) < 0 ? dyp : 0)) +
+                      (L::cz(q) > 0 ? dzm : (L::cz(q) < 0 ? dzp : 0));
+      const S* fq = fin + (long long)q * N;
+      const T w = weight<L, T>(q);
+      if (L::cx(q) == 0) {
+        IO::split(__ldg(reinterpret_cast<const V*>(fq + row)), w, fa[q], fb[q]);
+      } else if (L::cx(q) > 0) {
+        fa[q] = Storage<S>::load(__ldg(fq + row + dxm), w);
+        fb[q] = Storage<S>::load(__ldg(fq + row), w);
+      } else {
+        fa[q] = Storage<S>::load(__ldg(fq + row + 1), w);
+        fb[q] = Storage<S>::load(__ldg(fq + row + dxp), w);
+      }
+    }
+    if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(d.flags + c));
+  }
+  const uint8_t fla = uint8_t(fl2), flb = uint8_t(fl2 >> 8);
+
+  // momentum-exchange force sample (post-stream, pre-bounce-back)
+  if (d.force) {
+    const bool oa = active && (fla & TLBM_FLAG_OBSTACLE), ob = active && (flb & TLBM_FLAG_OBSTACLE);
+    double mx = 0.0, my = 0.0, mz = 0.0;
+    if (oa) {
+      T ax, ay, az;
+      cell_momentum<L>(fa, ax, ay, az);
+      mx = double(ax), my = double(ay), mz = double(az);
+    }
+    if (ob) {
+      T bx, by, bz;
+      cell_momentum<L>(fb, bx, by, bz);
+      mx += double(bx), my += double(by), mz += double(bz);
+    }
+    accumulate_force(d.force, __any_sync(0xffffffffu, oa || ob), mx, my, mz);
+  }
+  if (!active) return;
+  apply_boundaries<L>(d, x, y, (long long)c, fla, fa, bp);
+  relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
+  apply_boundaries<L>(d, x + 1, y, (long long)c + 1, flb, fb, bp);
+  relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
+
+  uint32_t ha = 0, hb = 0;
+  if constexpr (Storage<S>::kShifted) {
+    // one hash per cell of its index and of this step's f_0 (so the bits
+    // change every step without a seed); zero for a non-finite cell
+    ha = (fa[0] - fa[0] == T(0)) ? fmix32(uint32_t(c) * 0x9E3779B9u ^ __float_as_uint(float(fa[0]))) : 0u;
+    hb = (fb[0] - fb[0] == T(0)) ? fmix32(uint32_t(c + 1) * 0x9E3779B9u ^ __float_as_uint(float(fb[0]))) : 0u;
+  }
+  S* __restrict__ fout = d.fout;
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+    *reinterpret_cast<V*>(fout + (long long)q * N + c) = IO::join(fa[q], fb[q], weight<L, T>(q), ha, hb, q);
+}
+
+// Whether the pair kernel can run this step: nx even (pairs never straddle a
+// row), 32-bit cell offsets, and both population buffers (and the flags)
+// aligned to two values.
+template <typename S>
+inline bool pair_layout_ok(const StepParams& p) {
+  const auto al = [](const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; };
+  return (p.nx % 2 == 0) && p.n < (1LL << 31) && al(p.f_in, 2 * sizeof(S)) && al(p.f_out, 2 * sizeof(S)) &&
+         (p.flags == nullptr || al(p.flags, 2));
+}
+
 inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block) {
   int bx = 32;
   while (bx < nx && bx < 256) bx <<= 1;
@@ -201,6 +334,13 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
                                                d.omega_even, d.c_smag);
   cp.force_a = T(d.force_lin);
   const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
+  if constexpr (PULL && std::is_same<SI, SO>::value) {
+    if (pair_layout_ok<SI>(p)) {
+      step_launch_shape(p.nx / 2, p.ny, p.nz, grid, block);
+      k_step_x2<L, SI, COLL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
+      return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
+    }
+  }
   k_step<L, SI, SO, COLL, PULL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }
