@@ -634,8 +634,27 @@ __device__ __forceinline__ void collide_bgk_fast(T (&f)[L::Q], T inv_tau) {
   T rho, ux, uy, uz;
   macroscopic_fused<L>(f, rho, ux, uy, uz);
   const T usq = usq_fused<L>(ux, uy, uz);
+  // f' = (1 - om) f + om feq with feq_q = w rho (1 - 1.5 u.u + 4.5 cu^2 + 3 cu):
+  // a direction and its opposite share cu up to sign, so om feq of the pair
+  // is s +- d with s = om w rho (1 - 1.5 u.u + 4.5 cu^2), d = 3 om w rho cu
+  const T om = inv_tau, keep = T(1) - inv_tau;
+  const T orho = om * rho;
+  const T obase = orho * (T(1) - T(1.5) * usq);
+  f[0] = fma(f[0], keep, weight<L, T>(0) * obase);
 #pragma unroll
-  for (int q = 0; q < L::Q; ++q) f[q] = fma(feq_fused<L>(q, rho, ux, uy, uz, usq) - f[q], inv_tau, f[q]);
+  for (int q = 1; q < L::Q; ++q) {
+    if (L::opp(q) < q) continue;
+    const int qb = L::opp(q);
+    T cu = T(0);
+    if (L::cx(q) != 0) cu = (L::cx(q) > 0) ? cu + ux : cu - ux;
+    if (L::cy(q) != 0) cu = (L::cy(q) > 0) ? cu + uy : cu - uy;
+    if (L::cz(q) != 0) cu = (L::cz(q) > 0) ? cu + uz : cu - uz;
+    const T w = weight<L, T>(q);
+    const T sq = fma((T(4.5) * w * orho) * cu, cu, w * obase);
+    const T k3 = T(3) * w * orho;
+    f[q] = fma(f[q], keep, fma(k3, cu, sq));
+    f[qb] = fma(f[qb], keep, fma(-k3, cu, sq));
+  }
 }
 
 template <class L, typename T>

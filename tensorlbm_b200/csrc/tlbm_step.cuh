@@ -203,6 +203,15 @@ __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typena
   cell_update<L, SI, SO, COLL, PULL, FORCED>(d, x, y, z, (x < p.nx) && (y < p.ny), cp, bp);
 }
 
+// base + i elements as one wide multiply-add (mad.wide.s32), instead of a
+// sign extension and a two-word add per address
+template <typename E>
+__device__ __forceinline__ E* at_offset(E* base, int i) {
+  E* r;
+  asm("mad.wide.s32 %0, %1, %2, %3;" : "=l"(r) : "r"(i), "n"(int(sizeof(E))), "l"(base));
+  return r;
+}
+
 // Two cells per thread: (x, y, z) and (x + 1, y, z) with x even.  The pull
 // of a direction with c_x = 0 is one aligned vector load of both cells'
 // values, every store is one vector store, and the index arithmetic (32-bit
@@ -210,7 +219,8 @@ __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typena
 // shared by the two cells.  Each cell then takes exactly the per-cell path
 // of k_step (boundaries, collision, forcing, status), so the float32 and
 // float64 results are those of k_step bit for bit.
-// Requires nx even, n < 2^31, and f_in / f_out aligned to two values.
+// Requires nx even, (Q/2 + 2) n < 2^31 (32-bit offsets), and f_in / f_out
+// aligned to two values.
 template <class L, typename S, int COLL, bool FORCED = false>
 __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typename Storage<S>::T> cp,
                                                  BcParams<typename Storage<S>::T> bp) {
@@ -218,6 +228,7 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
   using IO = PairIO<S>;
   using V = typename IO::V;
   constexpr int Q = L::Q;
+  constexpr int MID = Q / 2;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -251,24 +262,28 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
     const int dzp = (L::DIM == 3) ? ((z == nz - 1) ? -(nz - 1) * plane : plane) : 0;
     const int dxm = (x == 0) ? nx - 1 : -1;      // cell x pulls c_x = +1 from x - 1
     const int dxp = (x + 2 == nx) ? 2 - nx : 2;  // cell x + 1 pulls c_x = -1 from x + 2
-    const S* __restrict__ fin = d.fin;
+    // every source is a 32-bit element offset from this cell's value in
+    // direction MID: (q - MID) N (the same for all threads) plus the row and
+    // x deltas, so that each address is one wide multiply-add
+    const S* __restrict__ pin = at_offset(d.fin + (long long)MID * N, c);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const int row = c + (L::cy(q) > 0 ? dym : (L::cy(q) < 0 ? dyp : 0)) +
-                      (L::cz(q) > 0 ? dzm : (L::cz(q) < 0 ? dzp : 0));
-      const S* fq = fin + (long long)q * N;
+      const int o = (q - MID) * N + (L::cy(q) > 0 ? dym : (L::cy(q) < 0 ? dyp : 0)) +
+                    (L::cz(q) > 0 ? dzm : (L::cz(q) < 0 ? dzp : 0));
       const T w = weight<L, T>(q);
       if (L::cx(q) == 0) {
-        IO::split(__ldg(reinterpret_cast<const V*>(fq + row)), w, fa[q], fb[q]);
+        IO::split(__ldg(reinterpret_cast<const V*>(at_offset(pin, o))), w, fa[q], fb[q]);
       } else if (L::cx(q) > 0) {
-        fa[q] = Storage<S>::load(__ldg(fq + row + dxm), w);
-        fb[q] = Storage<S>::load(__ldg(fq + row), w);
+        const int ia = o + dxm;
+        fa[q] = Storage<S>::load(__ldg(at_offset(pin, ia)), w);
+        fb[q] = Storage<S>::load(__ldg(at_offset(pin, o)), w);
       } else {
-        fa[q] = Storage<S>::load(__ldg(fq + row + 1), w);
-        fb[q] = Storage<S>::load(__ldg(fq + row + dxp), w);
+        const int ia = o + 1, ib = o + dxp;
+        fa[q] = Storage<S>::load(__ldg(at_offset(pin, ia)), w);
+        fb[q] = Storage<S>::load(__ldg(at_offset(pin, ib)), w);
       }
     }
-    if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(d.flags + c));
+    if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));
   }
   const uint8_t fla = uint8_t(fl2), flb = uint8_t(fl2 >> 8);
 
@@ -301,19 +316,19 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
     ha = (fa[0] - fa[0] == T(0)) ? fmix32(uint32_t(c) * 0x9E3779B9u ^ __float_as_uint(float(fa[0]))) : 0u;
     hb = (fb[0] - fb[0] == T(0)) ? fmix32(uint32_t(c + 1) * 0x9E3779B9u ^ __float_as_uint(float(fb[0]))) : 0u;
   }
-  S* __restrict__ fout = d.fout;
+  S* __restrict__ pout = at_offset(d.fout + (long long)MID * N, c);
 #pragma unroll
   for (int q = 0; q < Q; ++q)
-    *reinterpret_cast<V*>(fout + (long long)q * N + c) = IO::join(fa[q], fb[q], weight<L, T>(q), ha, hb, q);
+    __stwb(reinterpret_cast<V*>(at_offset(pout, (q - MID) * N)), IO::join(fa[q], fb[q], weight<L, T>(q), ha, hb, q));
 }
 
 // Whether the pair kernel can run this step: nx even (pairs never straddle a
-// row), 32-bit cell offsets, and both population buffers (and the flags)
-// aligned to two values.
-template <typename S>
+// row), offsets of +-(Q/2 + 1) n within 32 bits, and both population buffers
+// (and the flags) aligned to two values.
+template <class L, typename S>
 inline bool pair_layout_ok(const StepParams& p) {
   const auto al = [](const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; };
-  return (p.nx % 2 == 0) && p.n < (1LL << 31) && al(p.f_in, 2 * sizeof(S)) && al(p.f_out, 2 * sizeof(S)) &&
+  return (p.nx % 2 == 0) && (long long)(L::Q / 2 + 2) * p.n < (1LL << 31) && al(p.f_in, 2 * sizeof(S)) && al(p.f_out, 2 * sizeof(S)) &&
          (p.flags == nullptr || al(p.flags, 2));
 }
 
@@ -335,7 +350,7 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   cp.force_a = T(d.force_lin);
   const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
   if constexpr (PULL && std::is_same<SI, SO>::value) {
-    if (pair_layout_ok<SI>(p)) {
+    if (pair_layout_ok<L, SI>(p)) {
       step_launch_shape(p.nx / 2, p.ny, p.nz, grid, block);
       k_step_x2<L, SI, COLL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
       return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
