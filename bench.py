@@ -282,6 +282,135 @@ def _batched_variant(torch, dev, steps, peak):
             "nonfinite_domains_tau_max": unstable_tau[-1] if unstable_tau else None}
 
 
+REF_TRITON = "reference_triton_256"   # opt-in variant: --variants reference_triton_256
+
+
+def _import_reference_package():
+    """TensorLBM itself, pip-installed unmodified into baseline/_ref.  Its
+    package __init__ imports plotting / HDF5 modules that no compute path
+    calls and that the image lacks, so those names resolve to inert stubs."""
+    import types
+
+    class _Stub(types.ModuleType):
+        def __getattr__(self, name):
+            if name.startswith("__"):
+                raise AttributeError(name)
+            sub = _Stub(f"{self.__name__}.{name}")
+            sys.modules[sub.__name__] = sub
+            return sub
+
+        def __call__(self, *a, **k):
+            return self
+
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "tensorlbm").is_dir():
+        raise FileNotFoundError(f"{ref} holds no tensorlbm install")
+    for name in ("matplotlib", "matplotlib.pyplot", "h5py"):
+        sys.modules.setdefault(name, _Stub(name))
+    if str(ref) not in sys.path:
+        sys.path.insert(0, str(ref))
+    from tensorlbm import triton_fused, triton_fused_obstacle
+
+    return triton_fused, triton_fused_obstacle
+
+
+def _reference_triton_variant(torch, dev, steps, warmup, peak, n=256):
+    """TensorLBM's own GPU kernels (Triton, JIT-compiled here for the B200)
+    against this library on the same n^3 field and step count:
+
+    * `triton_fused` (periodic pull + BGK, D3Q19) in float32 / float16 /
+      bfloat16 storage against the periodic fused step in f32 / f16 / bf16
+      shifted storage, with one float32 parity check of the stored state after
+      `warmup` steps (both sides start from collide(f0));
+    * `triton_fused_obstacle_xfar_les` (BGK + Smagorinsky C_s = 0.17 + full-way
+      bounce-back + fused drag, its default tiling) against the fused
+      Smagorinsky step with bounce-back and FP64 drag, on a sphere of 8 % of
+      the cells.
+    Both sides launch eagerly, one kernel per step (this library's graph path
+    is not used here)."""
+    from tensorlbm_b200 import LBMSolver
+    from tensorlbm_b200.ai.pipeline import equilibrium_field, random_solenoidal_field
+
+    tf, tfo = _import_reference_package()
+
+    def timed(fn):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / 1e3
+
+    cells = n ** 3
+    tau = 0.53
+    f0 = equilibrium_field(random_solenoidal_field(n, 4.0, 0.05, 11, dev))
+    out = {"grid": n, "tau": tau, "steps": steps}
+    for storage, dt, bpc in (("f32", torch.float32, 152), ("f16", torch.float16, 76), ("bf16", torch.bfloat16, 76)):
+        a = tf.triton_collide(f0, tau).to(dt)
+        b = torch.empty_like(a)
+
+        def ref_steps(k):
+            nonlocal a, b
+            for _ in range(k):
+                tf.triton_fused(a, tau, out=b)
+                a, b = b, a
+
+        ref_steps(warmup)
+        s = LBMSolver("D3Q19", (n, n, n), tau, "bgk", device=dev, storage=storage).load(f0)
+        s.step(warmup)
+        if storage == "f32":
+            torch.cuda.synchronize(dev)
+            out["f32_state_max_rel_diff_after_warmup"] = float((s.state - a).abs().max() / a.abs().max())
+        t_ref = timed(lambda: ref_steps(steps))
+        t_us = timed(lambda: s.step(steps))
+        out[storage] = {"reference_mlups": round(cells * steps / t_ref / 1e6, 1),
+                        "ours_mlups": round(cells * steps / t_us / 1e6, 1),
+                        "speedup": round(t_ref / t_us, 2),
+                        "reference_roofline_frac": round(bpc * cells * steps / t_ref / 1e9 / peak, 4),
+                        "ours_roofline_frac": round(bpc * cells * steps / t_us / 1e9 / peak, 4)}
+        del a, b, s
+        torch.cuda.empty_cache()
+
+    # obstacle + Smagorinsky + drag; sphere radius for an 8 % solid fraction
+    r = n * (0.08 * 3.0 / (4.0 * math.pi)) ** (1.0 / 3.0)
+    i = torch.arange(n, device=dev, dtype=torch.float32)
+    zz, yy, xx = torch.meshgrid(i, i, i, indexing="ij")
+    c = (n - 1) / 2.0
+    solid = ((xx - c) ** 2 + (yy - c) ** 2 + (zz - c) ** 2) <= r * r
+    del zz, yy, xx
+    nu = (tau - 0.5) / 3.0
+    a = f0.clone()
+    b = torch.empty_like(a)
+    mask8 = solid.to(torch.int8)
+    fbuf = [torch.zeros((), dtype=torch.float32, device=dev) for _ in range(3)]
+
+    def ref_obst(k):
+        nonlocal a, b
+        for _ in range(k):
+            for t in fbuf:
+                t.zero_()
+            tfo.triton_fused_obstacle_xfar_les(a, nu, mask8, 0.17, 1.0, collision="BGK", out=b,
+                                               fx_buf=fbuf[0], fy_buf=fbuf[1], fz_buf=fbuf[2])
+            a, b = b, a
+
+    ref_obst(warmup)
+    t_ref = timed(lambda: ref_obst(steps))
+    del a, b
+    s = LBMSolver("D3Q19", (n, n, n), tau, "smagorinsky", device=dev, c_smag=0.17, obstacle_mask=solid,
+                  track_force=True).load(f0)
+    s.step(warmup)
+    t_us = timed(lambda: s.step(steps))
+    out["obstacle_smagorinsky_f32"] = {"solid_fraction": round(float(solid.float().mean()), 4),
+                                       "reference_mlups": round(cells * steps / t_ref / 1e6, 1),
+                                       "ours_mlups": round(cells * steps / t_us / 1e6, 1),
+                                       "speedup": round(t_ref / t_us, 2),
+                                       "ours_roofline_frac": round(152 * cells * steps / t_us / 1e9 / peak, 4)}
+    del s, f0, solid, mask8
+    torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(t: float, device) -> float:
     """The slowest rank's time (every rank takes part; a no-op on one process)."""
     import torch
@@ -409,6 +538,8 @@ def run_ours(args) -> None:
         variants["les_mlp_128_vs_smagorinsky_256"] = _les_variant(torch, dev, args.steps, args.warmup, peak)
     if want("d2q9_batched_512_cylinders"):
         variants["d2q9_batched_512_cylinders"] = _batched_variant(torch, dev, args.steps, peak)
+    if wanted is not None and REF_TRITON in wanted and not args.no_variants:
+        variants[REF_TRITON] = _reference_triton_variant(torch, dev, args.steps, args.warmup, peak)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
