@@ -24,6 +24,7 @@ template <typename T> struct CollideParams {
   T tau_sq;                 // tau^2
   T tau_eff_max;            // max(1, tau + 0.5), turbulence.py:88-99
   T force_a;                // linear body force F = A rho u (exact-difference forcing); 0 = none
+  bool cum_unit_rates;      // omega_b = omega_odd = omega_even = 1 (D3Q27 legacy cumulant fast path)
 };
 
 // ---------------------------------------------------------------------------
@@ -485,10 +486,126 @@ __device__ __forceinline__ void legacy_inverse(T (&c)[27]) {
           T(2) * c101 * c101 * c020 - T(2) * c011 * c011 * c200;
 }
 
+// D3Q27 legacy cumulant collision with omega_b = omega_odd = omega_even = 1
+// (cumulant.py:935 defaults).  Those rates set every post-collision
+// cumulant above second order to zero and leave no bulk part, so only the
+// central moments of f_neq up to second order enter (restricted 1-D passes:
+// an entry of total degree <= 2 only needs entries of total degree <= 2),
+// and the back transform (cumulant.py:580-651) reduces to the products of
+// the relaxed second-order cumulants at orders 4 and 6.  Same operator as
+// the general path below; only which zero terms are formed differs.
+template <typename T>
+__device__ __forceinline__ void collide_cumulant_legacy_unit(T (&f)[27], T om) {
+  using L = D3Q27;
+  T rho, ux, uy, uz;
+  macroscopic_fused<L>(f, rho, ux, uy, uz);
+  const T usq = usq_fused<L>(ux, uy, uz);
+  T fe[27];
+  Cube<T> g;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    fe[q] = feq_fused<L>(q, rho, ux, uy, uz, usq);
+    g[L::cx(q) + 1][L::cy(q) + 1][L::cz(q) + 1] = f[q] - fe[q];
+  }
+  // raw moments along x on all 9 lines
+  raw_1d<0>(g);
+  // along y: all degrees where x-degree 0, degrees 0-1 where 1, degree 0 where 2
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    T vm = g[0][0][k], v0 = g[0][1][k], vp = g[0][2][k];
+    g[0][0][k] = vm + v0 + vp;
+    g[0][1][k] = vp - vm;
+    g[0][2][k] = vp + vm;
+    vm = g[1][0][k], v0 = g[1][1][k], vp = g[1][2][k];
+    g[1][0][k] = vm + v0 + vp;
+    g[1][1][k] = vp - vm;
+    g[2][0][k] = g[2][0][k] + g[2][1][k] + g[2][2][k];
+  }
+  // along z: the entries of total degree <= 2
+  T m[3][3][3];
+  {
+    const T vm = g[0][0][0], v0 = g[0][0][1], vp = g[0][0][2];
+    m[0][0][0] = vm + v0 + vp;
+    m[0][0][1] = vp - vm;
+    m[0][0][2] = vp + vm;
+  }
+  m[1][0][0] = g[1][0][0] + g[1][0][1] + g[1][0][2];
+  m[1][0][1] = g[1][0][2] - g[1][0][0];
+  m[0][1][0] = g[0][1][0] + g[0][1][1] + g[0][1][2];
+  m[0][1][1] = g[0][1][2] - g[0][1][0];
+  m[2][0][0] = g[2][0][0] + g[2][0][1] + g[2][0][2];
+  m[1][1][0] = g[1][1][0] + g[1][1][1] + g[1][1][2];
+  m[0][2][0] = g[0][2][0] + g[0][2][1] + g[0][2][2];
+  // binomial shifts x, y, z (cumulant.py:390-412) on the same entries
+  {
+    const T tu = T(2) * ux, uu = ux * ux;
+    const T a0 = m[0][0][0], a1 = m[1][0][0];
+    m[1][0][0] = a1 - ux * a0;
+    m[2][0][0] = m[2][0][0] - tu * a1 + uu * a0;
+    m[1][1][0] = m[1][1][0] - ux * m[0][1][0];
+    m[1][0][1] = m[1][0][1] - ux * m[0][0][1];
+  }
+  {
+    const T tu = T(2) * uy, uu = uy * uy;
+    const T a0 = m[0][0][0], a1 = m[0][1][0];
+    m[0][1][0] = a1 - uy * a0;
+    m[0][2][0] = m[0][2][0] - tu * a1 + uu * a0;
+    m[1][1][0] = m[1][1][0] - uy * m[1][0][0];
+    m[0][1][1] = m[0][1][1] - uy * m[0][0][1];
+  }
+  {
+    const T tu = T(2) * uz, uu = uz * uz;
+    const T a0 = m[0][0][0], a1 = m[0][0][1];
+    m[0][0][1] = a1 - uz * a0;
+    m[0][0][2] = m[0][0][2] - tu * a1 + uu * a0;
+    m[1][0][1] = m[1][0][1] - uz * m[1][0][0];
+    m[0][1][1] = m[0][1][1] - uz * m[0][1][0];
+  }
+  // relaxation: deviatoric second order by 1 - omega, bulk and orders >= 3 to zero
+  const T ks = T(1) - om;
+  const T tr = m[2][0][0] + m[0][2][0] + m[0][0][2];
+  const T c200 = ks * (m[2][0][0] - tr / T(3)), c020 = ks * (m[0][2][0] - tr / T(3)),
+          c002 = ks * (m[0][0][2] - tr / T(3));
+  const T c110 = ks * m[1][1][0], c101 = ks * m[1][0][1], c011 = ks * m[0][1][1];
+  // central moments of the relaxed cumulants (cumulant.py:580-651 with zeros)
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g[a][b][c] = T(0);
+  g[0][0][0] = m[0][0][0];
+  g[1][0][0] = m[1][0][0];
+  g[0][1][0] = m[0][1][0];
+  g[0][0][1] = m[0][0][1];
+  g[2][0][0] = c200;
+  g[0][2][0] = c020;
+  g[0][0][2] = c002;
+  g[1][1][0] = c110;
+  g[1][0][1] = c101;
+  g[0][1][1] = c011;
+  g[2][2][0] = c200 * c020 + T(2) * c110 * c110;
+  g[2][0][2] = c200 * c002 + T(2) * c101 * c101;
+  g[0][2][2] = c020 * c002 + T(2) * c011 * c011;
+  g[2][1][1] = c200 * c011 + T(2) * c101 * c110;
+  g[1][2][1] = c020 * c101 + T(2) * c110 * c011;
+  g[1][1][2] = c002 * c110 + T(2) * c101 * c011;
+  g[2][2][2] = -T(2) * c200 * c020 * c002 - T(4) * c110 * c101 * c011 - T(2) * c110 * c110 * c002 -
+               T(2) * c101 * c101 * c020 - T(2) * c011 * c011 * c200;
+  T fns[27];
+  populations(g, ux, uy, uz, fns);
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = fe[q] + fns[q];
+}
+
 // D3Q27 legacy cumulant collision (cumulant.py:935-1047)
 template <typename T>
 __device__ __forceinline__ void collide_cumulant_legacy(T (&f)[27], const CollideParams<T>& cp) {
   using L = D3Q27;
+  if (cp.cum_unit_rates) {
+    collide_cumulant_legacy_unit(f, cp.inv_tau);
+    return;
+  }
   T rho, ux, uy, uz;
   macroscopic_fused<L>(f, rho, ux, uy, uz);
   const T usq = usq_fused<L>(ux, uy, uz);
@@ -737,6 +854,7 @@ __host__ __device__ CollideParams<T> make_collide_params(double tau, double s_e,
   cp.smag_coef_cum = T(18.0 * c_smag * c_smag);
   cp.omega_b_minus_omega = T(omega_b - 1.0 / tau);
   cp.keep_even = T(1.0 - omega_even);
+  cp.cum_unit_rates = (omega_b == 1.0) && (omega_odd == 1.0) && (omega_even == 1.0);
   cp.tau_sq = T(tau * tau);
   cp.tau_eff_max = T(tau + 0.5 > 1.0 ? tau + 0.5 : 1.0);
   cp.force_a = T(0);
