@@ -349,7 +349,11 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
                                                d.omega_even, d.c_smag);
   cp.force_a = T(d.force_lin);
   const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
-  if constexpr (PULL && std::is_same<SI, SO>::value) {
+  // the forced instantiations stay on one cell per thread: two cells with
+  // the pre-collision moments held for the force need 121 registers (2 blocks
+  // per SM) and ran slower than k_step (26.8 against 28.0 GLUPS, forced
+  // Smagorinsky at 256^3)
+  if constexpr (PULL && !FORCED && std::is_same<SI, SO>::value) {
     if (pair_layout_ok<L, SI>(p)) {
       step_launch_shape(p.nx / 2, p.ny, p.nz, grid, block);
       k_step_x2<L, SI, COLL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
