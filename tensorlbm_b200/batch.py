@@ -106,6 +106,7 @@ class BatchedSolver:
         self.ctas_per_sm = ctas_per_sm
         self.set_tile(*tile)
         self.steps_done = 0
+        self.step_offsets = [0] * n   # steps each domain had completed before the last load()/resume()
         self._cur = 0
         self._graph = None
         self.forces: list[torch.Tensor] = []
@@ -171,10 +172,27 @@ class BatchedSolver:
                                         self._flags_view(i).data_ptr(), None, s), "collide")
         self._cur = 0
         self.steps_done = 0
+        self.step_offsets = [0] * len(self.domains)
         self.forces = []
         self._graph = None
         self._f0 = [f.to(self.device, torch.float32).clone() for f in fields]
         return self
+
+    def resume(self, fields: list[torch.Tensor], steps: list[int]) -> "BatchedSolver":
+        """Continue from checkpointed TensorLBM-phase fields; ``steps[i]`` is the
+        step count domain i had completed.  The state is rebuilt as
+        collide(S_n), which is exactly the stored state (float32), so the
+        continuation is bit-exact."""
+        if len(steps) != len(self.domains):
+            raise ValueError(f"{len(steps)} step counts for {len(self.domains)} domains")
+        self.load(fields)
+        self.step_offsets = [int(k) for k in steps]
+        return self
+
+    @property
+    def step_counts(self) -> list[int]:
+        """Completed steps of each domain (all advance together)."""
+        return [k + self.steps_done for k in self.step_offsets]
 
     def _bufs(self):
         return (self.fa, self.fb) if self._cur == 0 else (self.fb, self.fa)

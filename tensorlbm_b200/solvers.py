@@ -169,6 +169,7 @@ class LBMSolver:
         self._buf = [torch.empty(full, dtype=self.buf_dtype, device=self.device) for _ in range(2)]
         self._cur = 0
         self.steps_done = 0
+        self.step_offset = 0          # steps completed before the last load()/resume()
         self._f0: torch.Tensor | None = None
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.forces: list[torch.Tensor] = []
@@ -211,9 +212,36 @@ class LBMSolver:
                                         None, self._stream()), "convert")
         self._cur = 0
         self.steps_done = 0
+        self.step_offset = 0
         self.forces = []
         self._graph = None
         return self
+
+    def resume(self, populations: torch.Tensor, *, step: int = 0,
+               stored_state: torch.Tensor | None = None) -> "LBMSolver":
+        """Continue a run from a checkpoint.
+
+        populations: the TensorLBM-phase field S_n (what ``f`` returned when it
+        was saved); step: the completed step count n.  With ``stored_state``
+        (this solver's own stored P_n in the same storage format, from
+        ``state``) the continuation is bit-exact for every storage format;
+        without it the state is rebuilt as collide(S_n), which is exactly P_n
+        for float32 / float64 storage and a fresh stochastic rounding of it for
+        FP16 / BF16."""
+        self.load(populations)
+        if stored_state is not None:
+            buf = self._buf[0]
+            if tuple(stored_state.shape) != tuple(buf.shape) or stored_state.dtype != buf.dtype:
+                raise ValueError(f"stored_state {tuple(stored_state.shape)} {stored_state.dtype} does not match "
+                                 f"this solver's {tuple(buf.shape)} {buf.dtype} ({self.storage} storage)")
+            buf.copy_(stored_state.to(self.device))
+        self.step_offset = int(step)
+        return self
+
+    @property
+    def step_index(self) -> int:
+        """Completed steps, including those before the last load()/resume()."""
+        return self.step_offset + self.steps_done
 
     def _launch(self, src: torch.Tensor, dst: torch.Tensor, force: torch.Tensor | None) -> None:
         st = _lib.load().tlbm_step(ctypes.byref(self._desc), src.data_ptr(), dst.data_ptr(), _lib.ptr(self.flags),

@@ -102,6 +102,31 @@ def moving_wall(torch) -> None:
     print("wrote moving_wall.npz")
 
 
+def checkpoints(torch) -> None:
+    """Checkpoint files written by TensorLBM itself (checkpoint.py): a
+    format-1 pair directory and a format-2 solver-state file, to pin the
+    readers of tensorlbm_b200.checkpoint to the reference's own output."""
+    import shutil
+    import types
+
+    from tensorlbm.checkpoint import eager_state_dict, save_checkpoint, save_solver_checkpoint
+
+    out = HERE / "checkpoint_ref"
+    if out.exists():
+        shutil.rmtree(out)
+    g = torch.Generator().manual_seed(20261203)
+    f = torch.rand((19, 2, 3, 4), generator=g, dtype=torch.float32)
+    save_checkpoint(f, 123, out / "pair", extra={"case": "golden", "tau": 0.6})
+    solver = types.SimpleNamespace(tau=0.55, nz=2, ny=3, nx=4, Q=19, lattice="D3Q19",
+                                   mask=torch.rand((2, 3, 4), generator=g) > 0.7)
+    torch.manual_seed(7)
+    state = eager_state_dict(solver, f * 2.0, step=77, extra={"note": "golden"})
+    save_solver_checkpoint(out / "solver_v2.pt", state, metadata={"run": "golden"})
+    np.savez_compressed(out / "expected.npz", f=f.numpy(), f2=(f * 2.0).numpy(), mask=solver.mask.numpy(),
+                        rng_after_seed7=torch.rand(4, generator=torch.Generator().manual_seed(7)).numpy())
+    print(f"wrote {out}")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -114,6 +139,9 @@ def main() -> None:
     torch.set_num_threads(8)
     if args.only == "moving_wall":
         moving_wall(torch)
+        return
+    if args.only == "checkpoints":
+        checkpoints(torch)
         return
     from tensorlbm import boundaries as b2
     from tensorlbm import boundaries3d as b3
