@@ -59,7 +59,8 @@ typedef enum tlbm_collision {
   TLBM_COLL_CUMULANT = 3,         /* D3Q27 legacy, cumulant.py:935 */
   TLBM_COLL_CUMULANT_GEIER = 4,   /* D3Q27 Geier 2015, cumulant.py:1050 */
   TLBM_COLL_CUMULANT_D3Q19 = 5,   /* cumulant.py:1159 (Smagorinsky via c_smag) */
-  TLBM_COLL_SMAGORINSKY = 6       /* turbulence.py:245 (D3Q19), :216 (D2Q9), :472 (D3Q27) */
+  TLBM_COLL_SMAGORINSKY = 6,      /* turbulence.py:245 (D3Q19), :216 (D2Q9), :472 (D3Q27) */
+  TLBM_COLL_TRT = 7               /* solver.py:440, solver3d.py:303, d3q27.py:438 (tau = tau_plus > 1/2) */
 } tlbm_collision;
 
 /* Boundary conditions applied by tlbm_step after the pull, in this order:
@@ -106,6 +107,8 @@ typedef struct tlbm_desc {
                           f += feq(rho, (1 + A) u) - feq(rho, u); 0 = none.  BGK, MRT and
                           Smagorinsky collisions (else TLBM_ERR_UNSUPPORTED) on float32
                           populations (else TLBM_ERR_DTYPE); |A| < 1.  New in this library. */
+  double lambda_trt;   /* TRT magic parameter: tau_minus = 1/2 + lambda_trt / (tau - 1/2)
+                          (TLBM_COLL_TRT; TensorLBM's default is 3/16) */
 } tlbm_desc;
 
 /* ---- fused time step ------------------------------------------------------

@@ -137,6 +137,23 @@ def collide_bgk(f: np.ndarray, tau: float) -> np.ndarray:
     return f - (f - feq) / f.dtype.type(tau)
 
 
+def collide_trt(f: np.ndarray, tau_plus: float, lambda_trt: float = 3.0 / 16.0) -> np.ndarray:
+    """solver.py:440-486, solver3d.py:303-336, d3q27.py:438-480: the symmetric
+    part relaxes with tau_plus, the antisymmetric part with
+    tau_minus = 1/2 + Lambda / (tau_plus - 1/2) (formed in float64, used as a
+    scalar of the field's dtype)."""
+    q = f.shape[0]
+    t = f.dtype.type
+    rho, ux, uy, uz = macroscopic(f)
+    feq = equilibrium(q, rho, ux, uy, uz)
+    tau_minus = 0.5 + lambda_trt / (tau_plus - 0.5)
+    opp = opposite(q)
+    half = t(0.5)
+    f_plus, f_minus = half * (f + f[opp]), half * (f - f[opp])
+    e_plus, e_minus = half * (feq + feq[opp]), half * (feq - feq[opp])
+    return f - (f_plus - e_plus) / t(tau_plus) - (f_minus - e_minus) / t(tau_minus)
+
+
 def mrt_matrix(q: int) -> np.ndarray:
     """Moment bases: solver.py:24-34 (D2Q9), solver3d.py:24-55 (D3Q19),
     d3q27.py:545-635 (D3Q27 Gram-Schmidt)."""
@@ -471,6 +488,7 @@ def collide_cumulant_geier_d3q27(f: np.ndarray, tau: float, omega_b=1.0, omega_o
 COLLIDERS = {
     "bgk": collide_bgk,
     "mrt": collide_mrt,
+    "trt": collide_trt,
     "smagorinsky": collide_smagorinsky,
     "cumulant_d3q19": collide_cumulant_d3q19,
     "cumulant": collide_cumulant_d3q27,

@@ -23,7 +23,7 @@ ERR_TOO_LARGE = 9
 # tlbm_dtype
 F32, F64, F16_SHIFTED, BF16_SHIFTED = 0, 1, 2, 3
 # tlbm_collision
-COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY = range(7)
+COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY, COLL_TRT = range(8)
 # tlbm_bc_bits / tlbm_flag_bits
 BC_LID, BC_ZH_INLET, BC_ZH_OUTLET = 1, 2, 4
 FLAG_SOLID, FLAG_OBSTACLE, FLAG_HALFWAY, FLAG_MOVING = 1, 2, 4, 8
@@ -56,6 +56,7 @@ class Desc(ctypes.Structure):
         ("rho_out", ctypes.c_double),
         ("wall_velocity", ctypes.c_void_p),
         ("force_lin", ctypes.c_double),
+        ("lambda_trt", ctypes.c_double),
     ]
 
 

@@ -25,6 +25,8 @@ template <typename T> struct CollideParams {
   T tau_eff_max;            // max(1, tau + 0.5), turbulence.py:88-99
   T force_a;                // linear body force F = A rho u (exact-difference forcing); 0 = none
   bool cum_unit_rates;      // omega_b = omega_odd = omega_even = 1 (D3Q27 legacy cumulant fast path)
+  T tau_minus;              // TRT antisymmetric relaxation time
+  double inv_tau_minus64;   // RN64(1 / float(tau_minus)) for the exact TRT quotient
 };
 
 // ---------------------------------------------------------------------------
@@ -176,6 +178,31 @@ __device__ __forceinline__ void collide_bgk(T (&f)[L::Q], T tau, double inv_tau6
     const T fe = feq_q<L>(q, rho, ux, uy, uz, usq);
     f[q] = xsub(f[q], div_by(xsub(f[q], fe), tau, inv_tau64));
   }
+}
+
+// ---------------------------------------------------------------------------
+// TRT (solver.py:440-486, solver3d.py:303-336, d3q27.py:438-480), bit-exact:
+// f - (f+ - feq+)/tau_plus - (f- - feq-)/tau_minus with f+- = (f +- f_opp)/2
+// formed one rounded operation at a time, like the torch expression.
+// ---------------------------------------------------------------------------
+template <class L, typename T>
+__device__ __forceinline__ void collide_trt(T (&f)[L::Q], T tau_p, double inv_p64, T tau_m, double inv_m64) {
+  T rho, ux, uy, uz;
+  macroscopic<L>(f, rho, ux, uy, uz);
+  const T usq = usq_of<L>(ux, uy, uz);
+  T fe[L::Q], out[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    constexpr T half = T(0.5);
+    const int o = L::opp(q);
+    const T fp = xmul(half, xadd(f[q], f[o])), fm = xmul(half, xsub(f[q], f[o]));
+    const T ep = xmul(half, xadd(fe[q], fe[o])), em = xmul(half, xsub(fe[q], fe[o]));
+    out[q] = xsub(xsub(f[q], div_by(xsub(fp, ep), tau_p, inv_p64)), div_by(xsub(fm, em), tau_m, inv_m64));
+  }
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) f[q] = out[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -822,6 +849,8 @@ __device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp
     collide_mrt<L>(f, r);
   } else if constexpr (COLL == TLBM_COLL_SMAGORINSKY) {
     collide_smagorinsky<L>(f, cp);
+  } else if constexpr (COLL == TLBM_COLL_TRT) {
+    collide_trt<L>(f, cp.tau, cp.inv_tau64, cp.tau_minus, cp.inv_tau_minus64);
   } else if constexpr (COLL == TLBM_COLL_CUMULANT_D3Q19) {
     static_assert(L::Q == 19, "D3Q19 only");
     collide_cumulant_d3q19(f, cp);
@@ -855,10 +884,21 @@ __host__ __device__ CollideParams<T> make_collide_params(double tau, double s_e,
   cp.omega_b_minus_omega = T(omega_b - 1.0 / tau);
   cp.keep_even = T(1.0 - omega_even);
   cp.cum_unit_rates = (omega_b == 1.0) && (omega_odd == 1.0) && (omega_even == 1.0);
+  cp.tau_minus = cp.tau;
+  cp.inv_tau_minus64 = cp.inv_tau64;
   cp.tau_sq = T(tau * tau);
   cp.tau_eff_max = T(tau + 0.5 > 1.0 ? tau + 0.5 : 1.0);
   cp.force_a = T(0);
   return cp;
+}
+
+// TRT: tau_minus = 1/2 + Lambda / (tau_plus - 1/2) in float64 (a Python
+// scalar in the reference), used as a scalar of the field's type
+template <typename T>
+__host__ __device__ void set_trt_rates(CollideParams<T>& cp, double tau_plus, double lambda_trt) {
+  const double tm = 0.5 + lambda_trt / (tau_plus - 0.5);
+  cp.tau_minus = T(tm);
+  cp.inv_tau_minus64 = 1.0 / double(T(tm));
 }
 
 }  // namespace tlbm

@@ -27,6 +27,11 @@ def collide_bgk27(f: torch.Tensor, tau: float) -> torch.Tensor:
     return _ops.collide(27, f, _lib.COLL_BGK, tau)
 
 
+def collide_trt27(f: torch.Tensor, tau_plus: float, lambda_trt: float = 3.0 / 16.0) -> torch.Tensor:
+    """Two-relaxation-time collision, bit-exact.  tensorlbm/d3q27.py:438."""
+    return _ops.collide(27, f, _lib.COLL_TRT, tau_plus, lambda_trt=lambda_trt)
+
+
 def collide_mrt27(f: torch.Tensor, tau: float, s_e: float = 1.19, s_eps: float = 1.4, s_q: float = 1.2,
                   s_pi: float | None = None) -> torch.Tensor:
     """Gram-Schmidt 27x27 MRT, tensorlbm/d3q27.py:643."""

@@ -24,6 +24,11 @@ def collide_mrt(f: torch.Tensor, tau: float, s_e: float = 1.64, s_eps: float = 1
     return _ops.collide(9, f, _lib.COLL_MRT, tau, s_e=s_e, s_eps=s_eps, s_q=s_q, tau_field=tau_field)
 
 
+def collide_trt(f: torch.Tensor, tau_plus: float, lambda_trt: float = 3.0 / 16.0) -> torch.Tensor:
+    """Two-relaxation-time collision, bit-exact.  tensorlbm/solver.py:440."""
+    return _ops.collide(9, f, _lib.COLL_TRT, tau_plus, lambda_trt=lambda_trt)
+
+
 def stream(f: torch.Tensor) -> torch.Tensor:
     """Periodic pull streaming.  tensorlbm/solver.py:396."""
     return _ops.stream(9, f)

@@ -21,6 +21,11 @@ def collide_mrt3d(f: torch.Tensor, tau: float, s_e: float = 1.19, s_eps: float =
 collide_mrt3d_low_memory = collide_mrt3d
 
 
+def collide_trt3d(f: torch.Tensor, tau_plus: float, lambda_trt: float = 3.0 / 16.0) -> torch.Tensor:
+    """Two-relaxation-time collision, bit-exact.  tensorlbm/solver3d.py:303."""
+    return _ops.collide(19, f, _lib.COLL_TRT, tau_plus, lambda_trt=lambda_trt)
+
+
 def stream3d(f: torch.Tensor) -> torch.Tensor:
     """Periodic pull streaming.  tensorlbm/solver3d.py:210."""
     return _ops.stream(19, f)

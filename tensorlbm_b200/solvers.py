@@ -34,6 +34,7 @@ COLLISIONS = {
     "cumulant_geier": _lib.COLL_CUMULANT_GEIER,
     "cumulant_d3q19": _lib.COLL_CUMULANT_D3Q19,
     "smagorinsky": _lib.COLL_SMAGORINSKY,
+    "trt": _lib.COLL_TRT,
 }
 _LATTICES = {"D2Q9": 9, "D3Q19": 19, "D3Q27": 27, 9: 9, 19: 19, 27: 27}
 # storage dtype -> (C code, torch dtype of the buffer)
@@ -69,6 +70,7 @@ class StepConfig:
     u_in: tuple[float, float, float] | float | None = None  # Zou/He inlet at x = 0
     rho_out: float | None = None     # Zou/He outlet at x = nx-1
     force_lin: float = 0.0           # linear body force F = A rho u (BGK / MRT / Smagorinsky, float32)
+    lambda_trt: float = 3.0 / 16.0   # TRT magic parameter (solver.py:440)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -99,7 +101,7 @@ class StepConfig:
             s_q=d_sq if self.s_q is None else self.s_q,
             s_pi=self.s_pi, omega_b=self.omega_b, omega_odd=self.omega_odd, omega_even=self.omega_even,
             c_smag=self.c_smag, bc=bc, u_lid=self.u_lid or 0.0, u_in=u_in,
-            rho_out=1.0 if self.rho_out is None else self.rho_out,
+            rho_out=1.0 if self.rho_out is None else self.rho_out, lambda_trt=self.lambda_trt,
         )
         if coll in (_lib.COLL_BGK, _lib.COLL_MRT, _lib.COLL_SMAGORINSKY):
             d.force_lin = float(self.force_lin)
@@ -115,7 +117,8 @@ class LBMSolver:
         lattice: "D2Q9", "D3Q19" or "D3Q27" (or 9 / 19 / 27).
         shape: (ny, nx) or (nz, ny, nx).
         tau: shear relaxation time.
-        collision: "bgk", "mrt", "smagorinsky", "cumulant" (D3Q27 legacy),
+        collision: "bgk", "mrt", "trt" (tau = tau_plus, ``lambda_trt=`` the magic
+            parameter), "smagorinsky", "cumulant" (D3Q27 legacy),
             "cumulant_geier" (D3Q27), "cumulant_d3q19".
         storage: "f32", "f64", "f16" or "bf16" (half formats hold the deviation f - w,
             scaled by 2^14 for f16, stochastically rounded).

@@ -127,6 +127,28 @@ def checkpoints(torch) -> None:
     print(f"wrote {out}")
 
 
+def trt(torch) -> None:
+    """TRT collisions (solver.py:440, solver3d.py:303, d3q27.py:438) on the
+    seeded near-equilibrium fields of the other collision fixtures."""
+    from tensorlbm.d3q27 import collide_trt27
+    from tensorlbm.solver import collide_trt
+    from tensorlbm.solver3d import collide_trt3d
+
+    out = {}
+    _, _, f9 = near_eq_field(torch, 9, (8, 8), torch.float32, 11)
+    out.update(f9=f9, trt9=collide_trt(f9, 0.6), trt9_lam=collide_trt(f9, 0.57, lambda_trt=0.25))
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        _, _, f19 = near_eq_field(torch, 19, (4, 4, 8), dt, 21)
+        _, _, f27 = near_eq_field(torch, 27, (4, 4, 8), dt, 31)
+        out.update({f"f19_{tag}": f19, f"trt19_{tag}": collide_trt3d(f19, 0.6),
+                    f"trt19_lam_{tag}": collide_trt3d(f19, 0.57, lambda_trt=0.25),
+                    f"f27_{tag}": f27, f"trt27_{tag}": collide_trt27(f27, 0.6),
+                    f"trt27_lam_{tag}": collide_trt27(f27, 0.57, lambda_trt=0.25)})
+    arrays = {k: v.detach().cpu().numpy() for k, v in out.items()}
+    np.savez_compressed(HERE / "collide_trt.npz", **arrays)
+    print("wrote collide_trt.npz")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -142,6 +164,9 @@ def main() -> None:
         return
     if args.only == "checkpoints":
         checkpoints(torch)
+        return
+    if args.only == "trt":
+        trt(torch)
         return
     from tensorlbm import boundaries as b2
     from tensorlbm import boundaries3d as b3

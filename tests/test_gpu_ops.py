@@ -248,3 +248,41 @@ def test_moving_wall_bounce_back(cuda, tag):
     assert same(out19[:, ~g["rotor"]], g[f"f19_{tag}"][:, ~g["rotor"]])
     with pytest.raises(ValueError):
         rotating_cylinder.moving_wall_bounce_back(f9, disc, ux2, uy2[:-1])
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_collide_trt(cuda, tag):
+    """The TRT kernels against the reference's outputs, bit for bit."""
+    from tensorlbm_b200 import d3q27, solver, solver3d
+
+    g = golden("collide_trt")
+    if tag == "f32":
+        assert same(N(solver.collide_trt(T(g["f9"], cuda), 0.6)), g["trt9"])
+        assert same(N(solver.collide_trt(T(g["f9"], cuda), 0.57, lambda_trt=0.25)), g["trt9_lam"])
+    for q, fn in ((19, solver3d.collide_trt3d), (27, d3q27.collide_trt27)):
+        f = T(g[f"f{q}_{tag}"], cuda)
+        assert same(N(fn(f, 0.6)), g[f"trt{q}_{tag}"])
+        assert same(N(fn(f, 0.57, lambda_trt=0.25)), g[f"trt{q}_lam_{tag}"])
+
+
+def test_trt_sphere_channel_vs_oracle(cuda):
+    """The fused step with TRT (pull, Zou/He, bounce-back, drag) against the
+    oracle's collide -> stream -> boundaries chain: bit-exact."""
+    from tensorlbm_b200 import LBMSolver, boundaries3d
+
+    nz, ny, nx = 8, 10, 20
+    obst = boundaries3d.sphere_mask(nx, ny, nz, 7.0, 5.0, 4.0, 2.2, cuda)
+    o = obst.cpu().numpy()
+    ux = np.full((nz, ny, nx), 0.04, np.float32)
+    ux[o] = 0.0
+    z = np.zeros_like(ux)
+    f0 = O.equilibrium(19, np.ones_like(ux), ux, z, z)
+    s = LBMSolver("D3Q19", (nz, ny, nx), 0.56, "trt", device=cuda, obstacle_mask=obst, u_in=0.04, rho_out=1.0,
+                  track_force=True, lambda_trt=0.2)
+    s.load(T(f0, cuda)).step(6)
+    ref, forces = f0, []
+    for _ in range(6):
+        ref, fo = O.channel_step(ref, 0.56, 0.04, 1.0, None, o, "trt", lambda_trt=0.2)
+        forces.append(fo)
+    assert same(N(s.f), ref)
+    assert np.max(np.abs(N(s.force_history()) - np.array(forces))) < 1e-6 * np.max(np.abs(np.array(forces)))

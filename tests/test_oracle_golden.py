@@ -168,3 +168,15 @@ def test_chain_sphere(name, coll):
     assert same(f, g["f"])
     ref = g["forces"].astype(np.float64)
     assert np.max(np.abs(np.array(forces)[:, :3] - ref)) < 1e-5 * np.max(np.abs(ref[:, 0]))
+
+
+def test_collide_trt():
+    """TRT (solver.py:440, solver3d.py:303, d3q27.py:438): the oracle against
+    the reference's own outputs, bit for bit, default and custom Lambda."""
+    g = golden("collide_trt")
+    assert same(O.collide_trt(g["f9"], 0.6), g["trt9"])
+    assert same(O.collide_trt(g["f9"], 0.57, 0.25), g["trt9_lam"])
+    for tag in ("f32", "f64"):
+        for q in (19, 27):
+            assert same(O.collide_trt(g[f"f{q}_{tag}"], 0.6), g[f"trt{q}_{tag}"])
+            assert same(O.collide_trt(g[f"f{q}_{tag}"], 0.57, 0.25), g[f"trt{q}_lam_{tag}"])
