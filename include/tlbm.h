@@ -83,8 +83,14 @@ typedef enum tlbm_flag_bits {
                                populations are stored reversed (where(wall, f_pre[opp], f)
                                before stream: cases/base.py:270-289 pre-boundaries,
                                lbm_step_correct.py:62 "bb" mode) */
-  TLBM_FLAG_MOVING = 8u     /* Ladd moving wall (with SOLID): swap plus 2 w rho (c.u_w)/c_s^2,
+  TLBM_FLAG_MOVING = 8u,    /* Ladd moving wall (with SOLID): swap plus 2 w rho (c.u_w)/c_s^2,
                                u_w from tlbm_desc.wall_velocity (propeller_benchmark.py:221) */
+  TLBM_FLAG_CURVED = 16u    /* fluid cell with Bouzidi (BFL) interpolated links to a curved wall
+                               (bfl_common.py:106): after the pull, in place of the bounce-back,
+                               f[opp_d] = 2q P_d + (1-2q) P_d(x-c_d) (q < 1/2) or
+                               P_d/(2q) + (2q-1)/(2q) P_opp (q >= 1/2) on every link d of the cell;
+                               tables tlbm_desc.link_row / link_q.  With a force buffer the step
+                               adds the BFL ledger sum_links c_d (P_d + f_bc) (bfl_d3q19.py:339) */
 } tlbm_flag_bits;
 
 typedef struct tlbm_desc {
@@ -109,6 +115,8 @@ typedef struct tlbm_desc {
                           populations (else TLBM_ERR_DTYPE); |A| < 1.  New in this library. */
   double lambda_trt;   /* TRT magic parameter: tau_minus = 1/2 + lambda_trt / (tau - 1/2)
                           (TLBM_COLL_TRT; TensorLBM's default is 3/16) */
+  const int32_t* link_row; /* TLBM_FLAG_CURVED cells: row of the cell in link_q (may be NULL: no links) */
+  const float* link_q;     /* (rows, Q) wall fraction of each link of the row, in (0, 1]; 0 = no link */
 } tlbm_desc;
 
 /* ---- fused time step ------------------------------------------------------
@@ -403,6 +411,26 @@ TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, doub
 
 TLBM_API const char* tlbm_status_string(int status);
 TLBM_API int tlbm_abi_version(void);
+
+/* ---- curved walls (Bouzidi / BFL interpolated bounce-back) -------------------
+ * tlbm_sphere_links: the boundary links of a sphere and their wall fractions,
+ * the outputs of compute_q_sphere_common (bfl_common.py:384) / compute_q_sphere_27
+ * (interpolated_bc_common.py:136): link_mask (Q, nz, ny, nx) bytes (1 = link
+ * (x, d): x outside, x + c_d inside, float64 squared distances against r^2) and
+ * q_field (Q, nz, ny, nx) float32 (ray-sphere fraction along c_d in float64,
+ * clamped to [1e-6, 1]; 0.5 off the links).  solid (nz, ny, nx, may be NULL)
+ * receives the cells inside the sphere by the same test.  D3Q19 / D3Q27. */
+TLBM_API int tlbm_sphere_links(int32_t lattice, int32_t nx, int32_t ny, int32_t nz, double cx, double cy, double cz,
+                               double radius, uint8_t* link_mask, float* q_field, uint8_t* solid, void* stream);
+
+/* tlbm_bfl_bounce_back: the link update of bfl_bounce_back_common (bfl_common.py:106)
+ * on whole fields: f_out = f except f_out[opp_d](x) = BFL value of link (x, d),
+ * from the post-stream f and the pre-stream f_prev (d->lattice D3Q19 / D3Q27,
+ * d->dtype F32 / F64, d->nx/ny/nz).  force (may be NULL) receives, added in
+ * float64, sum over links of c_d (f_prev_d + value) (bfl_d3q19.py:339-377).
+ * Replaces: bfl_bounce_back_common, bouzidi_bounce_back_d3q19 (stationary wall). */
+TLBM_API int tlbm_bfl_bounce_back(const tlbm_desc* d, const void* f, const void* f_prev, const uint8_t* link_mask,
+                                  const float* q_field, void* f_out, double* force, void* stream);
 
 #ifdef __cplusplus
 }

@@ -519,6 +519,95 @@ def bounce_back(f: np.ndarray, mask: np.ndarray) -> np.ndarray:
     return np.where(mask[None], f[opposite(f.shape[0])], f)
 
 
+# ---------------------------------------------------------------------------
+# Bouzidi (BFL) interpolated bounce-back on curved walls
+# ---------------------------------------------------------------------------
+
+
+def sphere_links(q: int, nx: int, ny: int, nz: int, cx: float, cy: float, cz: float, radius: float):
+    """Boundary links of a sphere and their wall fractions: bfl_common.py:384-477
+    (D3Q19, D3Q27) and interpolated_bc_common.py:136-233 (D3Q27).  Link (x, d):
+    x outside the sphere and x + c_d inside (float64 squared distances against
+    radius^2); its fraction is the ray-sphere intersection along c_d in float64,
+    clamped to [1e-6, 1] and stored as float32 (0.5 off the links)."""
+    zz, yy, xx = np.meshgrid(np.arange(nz, dtype=np.float64), np.arange(ny, dtype=np.float64),
+                             np.arange(nx, dtype=np.float64), indexing="ij")
+    r2 = radius ** 2
+    mask = np.zeros((q, nz, ny, nx), dtype=bool)
+    qf = np.full((q, nz, ny, nx), 0.5, dtype=np.float32)
+    for d in range(q):
+        dcx, dcy, dcz = (float(v) for v in C[q][d])
+        if dcx == 0.0 and dcy == 0.0 and dcz == 0.0:
+            continue
+        near = ((xx + dcx - cx) ** 2 + (yy + dcy - cy) ** 2 + (zz + dcz - cz) ** 2) <= r2
+        fluid = ((xx - cx) ** 2 + (yy - cy) ** 2 + (zz - cz) ** 2) > r2
+        link = fluid & near
+        if not link.any():
+            continue
+        dx, dy, dz = xx - cx, yy - cy, zz - cz
+        a = dcx ** 2 + dcy ** 2 + dcz ** 2
+        b = 2.0 * (dcx * dx + dcy * dy + dcz * dz)
+        c = dx ** 2 + dy ** 2 + dz ** 2 - r2
+        disc = b ** 2 - 4.0 * a * c
+        root = np.sqrt(np.where(link & (disc >= 0.0), disc, 0.0))
+        t1 = (-b - root) / (2.0 * a)
+        t2 = (-b + root) / (2.0 * a)
+        v1 = (t1 > 1e-10) & (t1 <= 1.0 + 1e-10)
+        v2 = (t2 > 1e-10) & (t2 <= 1.0 + 1e-10)
+        frac = np.where(v1 & v2, np.minimum(t1, t2), np.where(v1, t1, np.where(v2, t2, 0.5)))
+        mask[d] = link
+        qf[d] = np.where(link, np.clip(frac, 1e-6, 1.0).astype(np.float32), qf[d])
+    return mask, qf
+
+
+def _bfl_values(f_prev: np.ndarray, mask: np.ndarray, qf: np.ndarray):
+    """Per link (x, d) the value sent back into x along -c_d (bfl_common.py:169-180):
+    q < 1/2: 2q P_d(x) + (1 - 2q) P_d(x - c_d);  q >= 1/2: P_d(x)/(2q) + ((2q - 1)/(2q)) P_opp(x),
+    each product and sum rounded in the populations' dtype (q promoted to it)."""
+    q = f_prev.shape[0]
+    t = f_prev.dtype.type
+    qv = qf.astype(f_prev.dtype)
+    up = stream(f_prev)                                # P_d(x - c_d)
+    lin = (qv < t(0.5)) & mask
+    quad = (~lin) & mask
+    bc_lin = t(2.0) * qv * f_prev + (t(1.0) - t(2.0) * qv) * up
+    sq = np.where(quad, qv, t(1.0))
+    inv = t(1.0) / (t(2.0) * sq)
+    bc_quad = f_prev * inv + (t(2.0) * sq - t(1.0)) * inv * f_prev[opposite(q)]
+    return np.where(lin, bc_lin, bc_quad)
+
+
+def bfl_bounce_back(f: np.ndarray, f_prev: np.ndarray, mask: np.ndarray, qf: np.ndarray) -> np.ndarray:
+    """bfl_common.py:106-190: f_out[opp_d](x) = value of link (x, d); f elsewhere.
+    f is post-stream, f_prev the pre-stream populations."""
+    opp = opposite(f.shape[0])
+    bc = _bfl_values(f_prev, mask, qf)
+    return np.where(mask[opp], bc[opp], f)
+
+
+def bfl_force(f_prev: np.ndarray, mask: np.ndarray, qf: np.ndarray) -> np.ndarray:
+    """Force ledger of bfl_d3q19.py:339-377 (stationary wall, laboratory frame):
+    sum over links of c_d (P_d(x) + value), the pair sum rounded in the
+    populations' dtype, accumulated here in float64."""
+    q = f_prev.shape[0]
+    bc = _bfl_values(f_prev, mask, qf)
+    link_sum = (f_prev + bc).astype(np.float64)
+    out = np.zeros(3)
+    for d in range(1, q):
+        out += C[q][d].astype(np.float64) * link_sum[d][mask[d]].sum()
+    return out
+
+
+def bfl_chain_step(f: np.ndarray, tau: float, solid: np.ndarray, mask: np.ndarray, qf: np.ndarray,
+                   collision: str = "bgk", **kw):
+    """One step in bfl_step's order (bfl_common.py:882-955) after the collision:
+    solid cells keep their pre-collision populations, bounce_back_cells_3d on
+    the solid, stream, then the link update.  Returns (f, force)."""
+    g = np.where(solid[None], f, COLLIDERS[collision](f, tau, **kw))
+    g = bounce_back(g, solid)
+    return bfl_bounce_back(stream(g), g, mask, qf), bfl_force(g, mask, qf)
+
+
 def moving_wall_bounce_back(f: np.ndarray, mask: np.ndarray, *wall_u: np.ndarray) -> np.ndarray:
     """Ladd moving wall: where(mask, bounce_back(f) + ((2 w_q) rho) (c_q . u_w) 3, f),
     rho = sum0(f), the float32 W tensor cast to f's dtype for both lattices and

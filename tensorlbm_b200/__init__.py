@@ -38,6 +38,9 @@ _PATCHES = {
     "boundary_registry": ["derive_missing_mask"],
     "rotating_cylinder": ["moving_wall_bounce_back"],
     "propeller_benchmark": ["moving_wall_bounce_back_3d"],
+    "bfl_common": ["compute_q_sphere_common", "bfl_bounce_back_common"],
+    "interpolated_bc_common": ["compute_q_sphere_27"],
+    "bfl_d3q19": ["bouzidi_bounce_back_d3q19"],
 }
 
 

@@ -26,7 +26,7 @@ F32, F64, F16_SHIFTED, BF16_SHIFTED = 0, 1, 2, 3
 COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY, COLL_TRT = range(8)
 # tlbm_bc_bits / tlbm_flag_bits
 BC_LID, BC_ZH_INLET, BC_ZH_OUTLET = 1, 2, 4
-FLAG_SOLID, FLAG_OBSTACLE, FLAG_HALFWAY, FLAG_MOVING = 1, 2, 4, 8
+FLAG_SOLID, FLAG_OBSTACLE, FLAG_HALFWAY, FLAG_MOVING, FLAG_CURVED = 1, 2, 4, 8, 16
 
 TORCH_TO_DTYPE = {torch.float32: F32, torch.float64: F64}
 
@@ -57,6 +57,8 @@ class Desc(ctypes.Structure):
         ("wall_velocity", ctypes.c_void_p),
         ("force_lin", ctypes.c_double),
         ("lambda_trt", ctypes.c_double),
+        ("link_row", ctypes.c_void_p),
+        ("link_q", ctypes.c_void_p),
     ]
 
 
@@ -107,6 +109,8 @@ SIGNATURES: dict[str, list] = {
     "tlbm_batch_advance_slot": [_P, _P],
     "tlbm_batch_run": [ctypes.POINTER(BatchDesc), _P, _P, _I64, _P, _P, _P, _I32, _P, _I32, _P, _P, _I64, _P],
     "tlbm_link_list_noalloc": [_P, _I64, _P, _I64, _P, _P],
+    "tlbm_sphere_links": [_I32, _I32, _I32, _I32, _D, _D, _D, _D, _P, _P, _P, _P],
+    "tlbm_bfl_bounce_back": [ctypes.POINTER(Desc), _P, _P, _P, _P, _P, _P, _P],
     "tlbm_link_list_static_capacity": [],
     "tlbm_les_filter_moments": [_P, _I32, _I32, _I32, _I32, _D, _P, _P],
     "tlbm_les_samples": [_P, _I32, _I32, _I32, _D, _D, _P, _P, _P, _P, _P],

@@ -49,6 +49,8 @@ __device__ __forceinline__ void process_tile(const tlbm_batch_domain* __restrict
   d.force = forces ? forces + 3 * (long long)di : nullptr;
   d.status = status;
   d.wall_u = nullptr;
+  d.link_row = nullptr;
+  d.link_q = nullptr;
   d.nx = dm.nx;
   d.ny = dm.ny;
   d.nz = 1;

@@ -73,6 +73,8 @@ StepParams make_params(const tlbm_desc& d, const void* fin, void* fout, const ui
   p.force = force;
   p.status = status;
   p.wall_velocity = d.wall_velocity;
+  p.link_row = d.link_row;
+  p.link_q = d.link_q;
   p.nx = d.nx;
   p.ny = d.ny;
   p.nz = d.nz;

@@ -164,6 +164,8 @@ struct StepParams {
   double* force;            // [3] accumulated momentum-exchange force, may be null
   unsigned int* status;     // bit0: non-finite density seen, may be null
   const void* wall_velocity;  // (DIM, n) moving-wall velocity, compute type, may be null
+  const int32_t* link_row;  // CURVED cells: row in link_q, may be null
+  const float* link_q;      // (rows, Q) BFL wall fractions, 0 = no link, may be null
   int nx, ny, nz;
   long long plane;          // nx*ny
   long long n;              // nx*ny*nz

@@ -16,16 +16,20 @@
 
 namespace tlbm {
 
-// Warp-reduce one cell's momentum in float64 and add 2x it to force[0..2].
-// Blocks are at least 32 wide in x, so a warp is 32 consecutive x of one row.
+// Warp-reduce one cell's momentum in float64 and add scale x it to
+// force[0..2]: 2 for the full-way momentum exchange (each population of an
+// obstacle cell is reflected), 1 for a ledger that already holds both halves
+// of every link (Bouzidi).  Blocks are at least 32 wide in x, so a warp is 32
+// consecutive x of one row.
 template <typename T>
-__device__ __forceinline__ void accumulate_force(double* force, bool any_in_warp, T mx, T my, T mz) {
+__device__ __forceinline__ void accumulate_force(double* force, bool any_in_warp, T mx, T my, T mz,
+                                                 double scale = 2.0) {
   if (!any_in_warp) return;
   const double sx = warp_sum(double(mx)), sy = warp_sum(double(my)), sz = warp_sum(double(mz));
   if ((threadIdx.x & 31) == 0) {
-    atomicAdd(force + 0, 2.0 * sx);
-    atomicAdd(force + 1, 2.0 * sy);
-    atomicAdd(force + 2, 2.0 * sz);
+    atomicAdd(force + 0, scale * sx);
+    atomicAdd(force + 1, scale * sy);
+    atomicAdd(force + 2, scale * sz);
   }
 }
 
@@ -38,16 +42,77 @@ template <typename SI, typename SO> struct Domain {
   double* force;            // may be null
   unsigned int* status;     // may be null
   const void* wall_u;       // (DIM, n) wall velocity of TLBM_FLAG_MOVING cells, compute type; may be null
+  const int32_t* link_row;  // TLBM_FLAG_CURVED cells: row in link_q; may be null
+  const float* link_q;      // (rows, Q) BFL wall fractions (0 = no link); may be null
   int nx, ny, nz;
   long long plane, n;
   uint32_t bc;
 };
 
-// Boundary conditions of one cell after the pull, in TensorLBM's order:
-// Zou/He inlet / outlet planes, full-way (or moving-wall) bounce-back, lid.
+// The value a Bouzidi link (x, d) sends back into x along -c_d
+// (bfl_common.py:169-180): Pd = P_d(x), up = P_d(x - c_d) (the pulled value),
+// Po = P_opp(x); every product and sum rounded on its own like the torch
+// expression, q promoted to the populations' type.
+template <typename T>
+__device__ __forceinline__ T bfl_value(T q, T Pd, T up, T Po) {
+  const T q2 = xmul(T(2), q);
+  if (q < T(0.5)) return xadd(xmul(q2, Pd), xmul(xsub(T(1), q2), up));
+  const T inv = xdiv(T(1), q2);
+  return xadd(xmul(Pd, inv), xmul(xmul(xsub(q2, T(1)), inv), Po));
+}
+
+// Bouzidi links of a TLBM_FLAG_CURVED cell: after the pull, f[opp_d] of every
+// link (x, d) becomes the link value; a direction and its opposite are done
+// together, so every read (pulled values, the cell's own stored P) precedes
+// the writes.  With a force buffer the ledger sum_links c_d (P_d + value) is
+// added to (mx, my, mz) in float64 (bfl_d3q19.py:339-377).
 template <class L, typename T, typename SI, typename SO>
+__device__ __forceinline__ void curved_links(const Domain<SI, SO>& d, long long cell, T (&f)[L::Q], double& mx,
+                                             double& my, double& mz) {
+  const float* __restrict__ lq = d.link_q + (long long)__ldg(d.link_row + cell) * L::Q;
+  const long long N = d.n;
+  const bool ledger = d.force != nullptr;
+#pragma unroll
+  for (int a = 1; a < L::Q; ++a) {
+    const int b = L::opp(a);
+    if (b < a) continue;
+    const float qa = __ldg(lq + a), qb = __ldg(lq + b);
+    if (!(qa > 0.0f) && !(qb > 0.0f)) continue;
+    const T pa = Storage<SI>::load(__ldg(d.fin + (long long)a * N + cell), weight<L, T>(a));
+    const T pb = Storage<SI>::load(__ldg(d.fin + (long long)b * N + cell), weight<L, T>(b));
+    const T ua = f[a], ub = f[b];
+    if (qa > 0.0f) {
+      const T v = bfl_value(T(qa), pa, ua, pb);
+      f[b] = v;
+      if (ledger) {
+        const double s = double(xadd(pa, v));
+        mx += L::cx(a) * s;
+        my += L::cy(a) * s;
+        mz += L::cz(a) * s;
+      }
+    }
+    if (qb > 0.0f) {
+      const T v = bfl_value(T(qb), pb, ub, pa);
+      f[a] = v;
+      if (ledger) {
+        const double s = double(xadd(pb, v));
+        mx += L::cx(b) * s;
+        my += L::cy(b) * s;
+        mz += L::cz(b) * s;
+      }
+    }
+  }
+}
+
+// Boundary conditions of one cell after the pull, in TensorLBM's order:
+// Zou/He inlet / outlet planes, full-way (or moving-wall) bounce-back or the
+// Bouzidi links of a curved wall, lid.  (mx, my, mz) collect the BFL force.
+// kCurved = false compiles the Bouzidi links out (the two-cells-per-thread
+// kernel, which never runs with link tables).
+template <class L, typename T, typename SI, typename SO, bool kCurved = true>
 __device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x, int y, long long cell, uint8_t fl,
-                                                 T (&f)[L::Q], const BcParams<T>& bp) {
+                                                 T (&f)[L::Q], const BcParams<T>& bp, double& mx, double& my,
+                                                 double& mz) {
   constexpr int Q = L::Q;
   const long long N = d.n;
   // Zou/He inlet / outlet planes
@@ -69,6 +134,9 @@ __device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x,
     moving_wall_bounce_back<L>(f, uw[cell], uw[N + cell], L::DIM == 3 ? uw[2 * N + cell] : T(0));
   } else if (fl & TLBM_FLAG_SOLID) {
     bounce_back<L>(f);
+  }
+  if constexpr (L::DIM == 3 && kCurved) {
+    if ((fl & TLBM_FLAG_CURVED) && d.link_q) curved_links<L>(d, cell, f, mx, my, mz);
   }
   // moving lid
   if ((d.bc & TLBM_BC_LID) && y == d.ny - 1) {
@@ -165,7 +233,11 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
       if (ob) cell_momentum<L>(f, mx, my, mz);
       accumulate_force(d.force, __any_sync(0xffffffffu, ob), mx, my, mz);
     }
-    if (active) apply_boundaries<L>(d, x, y, cell, fl, f, bp);
+    // boundaries; the ledger of Bouzidi links is reduced on its own
+    double bx = 0.0, by = 0.0, bz = 0.0;
+    if (active) apply_boundaries<L>(d, x, y, cell, fl, f, bp, bx, by, bz);
+    if (d.force && d.link_q)
+      accumulate_force(d.force, __any_sync(0xffffffffu, active && (fl & TLBM_FLAG_CURVED)), bx, by, bz, 1.0);
   }
 
   if (!active) return;
@@ -194,6 +266,8 @@ __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typena
   d.force = p.force;
   d.status = p.status;
   d.wall_u = p.wall_velocity;
+  d.link_row = p.link_row;
+  d.link_q = p.link_q;
   d.nx = p.nx;
   d.ny = p.ny;
   d.nz = p.nz;
@@ -245,6 +319,8 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
   d.force = p.force;
   d.status = p.status;
   d.wall_u = p.wall_velocity;
+  d.link_row = p.link_row;
+  d.link_q = p.link_q;
   d.nx = nx;
   d.ny = ny;
   d.nz = nz;
@@ -304,9 +380,10 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
     accumulate_force(d.force, __any_sync(0xffffffffu, oa || ob), mx, my, mz);
   }
   if (!active) return;
-  apply_boundaries<L>(d, x, y, (long long)c, fla, fa, bp);
+  double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;  // no Bouzidi links here
+  apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+  apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
   relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
-  apply_boundaries<L>(d, x + 1, y, (long long)c + 1, flb, fb, bp);
   relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
 
   uint32_t ha = 0, hb = 0;
@@ -322,13 +399,13 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
     __stwb(reinterpret_cast<V*>(at_offset(pout, (q - MID) * N)), IO::join(fa[q], fb[q], weight<L, T>(q), ha, hb, q));
 }
 
-// Whether the pair kernel can run this step: nx even (pairs never straddle a
-// row), offsets of +-(Q/2 + 1) n within 32 bits, and both population buffers
-// (and the flags) aligned to two values.
+// Whether the pair kernel can run this step: no Bouzidi link tables, nx even
+// (pairs never straddle a row), offsets of +-(Q/2 + 1) n within 32 bits, and
+// both population buffers (and the flags) aligned to two values.
 template <class L, typename S>
 inline bool pair_layout_ok(const StepParams& p) {
   const auto al = [](const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; };
-  return (p.nx % 2 == 0) && (long long)(L::Q / 2 + 2) * p.n < (1LL << 31) && al(p.f_in, 2 * sizeof(S)) && al(p.f_out, 2 * sizeof(S)) &&
+  return (p.nx % 2 == 0) && p.link_q == nullptr && (long long)(L::Q / 2 + 2) * p.n < (1LL << 31) && al(p.f_in, 2 * sizeof(S)) && al(p.f_out, 2 * sizeof(S)) &&
          (p.flags == nullptr || al(p.flags, 2));
 }
 

@@ -127,11 +127,13 @@ class LBMSolver:
         u_lid, u_in, rho_out: enable the lid / Zou-He inlet / outlet planes.
         tau_field: optional per-cell tau (BGK and MRT shear rate).
         track_force: record the float64 force of every step.
+        curved_wall: a :class:`tensorlbm_b200.bfl.CurvedWall` (Bouzidi links of a
+            curved obstacle, D3Q19 / D3Q27); its force is the BFL ledger.
     """
 
     def __init__(self, lattice, shape, tau: float, collision: str = "bgk", *, device=None, storage="f32",
                  wall_mask=None, obstacle_mask=None, wall_mode: str = "fullway", tau_field=None,
-                 track_force: bool = False, wall_velocity=None, **cfg):
+                 track_force: bool = False, wall_velocity=None, curved_wall=None, **cfg):
         q = _LATTICES[lattice]
         if isinstance(storage, torch.dtype):
             storage = _TORCH_STORAGE[storage]
@@ -162,6 +164,22 @@ class LBMSolver:
             self.flags.bitwise_or_(moving * _lib.FLAG_MOVING)
             self.wall_u = torch.stack([u.to(device=self.device, dtype=self.compute_dtype)
                                        for u in wall_velocity]).contiguous()
+        self.curved = None
+        if curved_wall is not None:
+            # Bouzidi links: solid cells bounce back full-way (not in the drag),
+            # the cells with links take the interpolated update; the drag of
+            # the wall is the BFL ledger
+            if q == 9:
+                raise NotImplementedError("curved walls are built for D3Q19 and D3Q27")
+            if curved_wall.q != q or tuple(curved_wall.solid.shape) != shape:
+                raise ValueError(f"curved_wall is for Q={curved_wall.q} {tuple(curved_wall.solid.shape)}, "
+                                 f"the solver is Q={q} {shape}")
+            if self.flags is None:
+                self.flags = torch.zeros(shape, dtype=torch.uint8, device=self.device)
+            solid = curved_wall.solid.to(self.device)
+            self.flags.bitwise_or_(solid.to(torch.uint8) * _lib.FLAG_SOLID)
+            self.flags.bitwise_or_(curved_wall.cells.to(self.device).to(torch.uint8) * _lib.FLAG_CURVED)
+            self.curved = curved_wall
         self.tau_field = None
         if tau_field is not None:
             if tuple(tau_field.shape) != shape:
@@ -176,12 +194,17 @@ class LBMSolver:
         self._f0: torch.Tensor | None = None
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.forces: list[torch.Tensor] = []
-        self._desc = self.cfg.desc(self.code)
-        self._desc_none = self.cfg.desc(self.code, "none")
-        if self.wall_u is not None:
-            self._desc.wall_velocity = self.wall_u.data_ptr()
-            self._desc_none.wall_velocity = self.wall_u.data_ptr()
+        self._desc = self._attach(self.cfg.desc(self.code))
+        self._desc_none = self._attach(self.cfg.desc(self.code, "none"))
         self._graph = None
+
+    def _attach(self, d: _lib.Desc) -> _lib.Desc:
+        """Per-cell tables of the solver on a descriptor (moving-wall velocity, Bouzidi links)."""
+        if self.wall_u is not None:
+            d.wall_velocity = self.wall_u.data_ptr()
+        if self.curved is not None:
+            self.curved.attach(d)
+        return d
 
     # -- state -----------------------------------------------------------------
 
@@ -269,9 +292,7 @@ class LBMSolver:
     def set_force_lin(self, a: float) -> "LBMSolver":
         """Change the linear body force A of F = A rho u (drops the captured graph)."""
         self.cfg.force_lin = float(a)
-        wall = self._desc.wall_velocity
-        self._desc = self.cfg.desc(self.code)
-        self._desc.wall_velocity = wall
+        self._desc = self._attach(self.cfg.desc(self.code))
         self._graph = None
         return self
 

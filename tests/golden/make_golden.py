@@ -149,6 +149,60 @@ def trt(torch) -> None:
     print("wrote collide_trt.npz")
 
 
+def bfl(torch) -> None:
+    """Bouzidi (BFL) interpolated bounce-back: the sphere link fields
+    (bfl_common.py:384, interpolated_bc_common.py:136), the link update
+    (bfl_common.py:106) with its force ledger (bfl_d3q19.py:195), and a short
+    chain composed in bfl_step's order (bfl_common.py:882): BGK collide ->
+    solid cells back to pre-collision -> bounce_back_cells_3d -> stream3d ->
+    BFL on the links (with force)."""
+    from tensorlbm.bfl_common import bfl_bounce_back_common, compute_q_sphere_common
+    from tensorlbm.bfl_d3q19 import bouzidi_bounce_back_d3q19
+    from tensorlbm.boundaries3d import bounce_back_cells_3d
+    from tensorlbm.d3q19 import equilibrium3d
+    from tensorlbm.interpolated_bc_common import compute_q_sphere_27
+    from tensorlbm.solver3d import collide_bgk3d, stream3d
+
+    out = {}
+    cpu = torch.device("cpu")
+    m19, q19 = compute_q_sphere_common(16, 14, 12, 7.3, 6.6, 5.8, 3.7, cpu, lattice="D3Q19")
+    m27, q27 = compute_q_sphere_27(12, 11, 10, 5.4, 5.1, 4.7, 2.9, cpu)
+    m27c, q27c = compute_q_sphere_common(12, 11, 10, 5.4, 5.1, 4.7, 2.9, cpu, lattice="D3Q27")
+    assert torch.equal(m27, m27c) and torch.equal(q27, q27c)
+    out.update(m19=m19, q19=q19, m27=m27, q27=q27)
+    for q, m, qf, sp, seed in ((19, m19, q19, (12, 14, 16), 61), (27, m27, q27, (10, 11, 12), 62)):
+        _, _, fa = near_eq_field(torch, q, sp, torch.float32, seed)
+        _, _, fb = near_eq_field(torch, q, sp, torch.float32, seed + 100)
+        out[f"f{q}"], out[f"fprev{q}"] = fa, fb
+        out[f"bfl{q}"] = bfl_bounce_back_common(fa, fb, m, qf, lattice=f"D3Q{q}")
+    f19_force, force = bouzidi_bounce_back_d3q19(out["f19"], out["fprev19"], m19, q19, return_force=True)
+    assert torch.equal(f19_force, out["bfl19"])
+    out["force19"] = torch.stack(list(force))
+
+    # chain: periodic 24 x 16 x 16 box, sphere r = 3.6 at (9.3, 7.6, 8.2), BGK tau 0.56
+    nz, ny, nx = 16, 16, 24
+    mask, qfield = compute_q_sphere_common(nx, ny, nz, 9.3, 7.6, 8.2, 3.6, cpu, lattice="D3Q19")
+    zz, yy, xx = torch.meshgrid(*(torch.arange(n, dtype=torch.float64) for n in (nz, ny, nx)), indexing="ij")
+    solid = ((xx - 9.3) ** 2 + (yy - 7.6) ** 2 + (zz - 8.2) ** 2) <= 3.6 ** 2
+    ux = torch.full((nz, ny, nx), 0.03, dtype=torch.float32)
+    ux[solid] = 0.0
+    zero = torch.zeros_like(ux)
+    f = equilibrium3d(torch.ones_like(ux), ux, zero, zero)
+    out.update(chain_f0=f.clone(), chain_mask=mask, chain_q=qfield, chain_solid=solid)
+    tau, forces = 0.56, []
+    for _ in range(8):
+        f_post = collide_bgk3d(f, tau)
+        g = torch.where(solid.unsqueeze(0), f, f_post)            # no dynamics in the solid
+        g = bounce_back_cells_3d(g, solid)
+        f, fo = bouzidi_bounce_back_d3q19(stream3d(g), g, mask, qfield, return_force=True)
+        forces.append(torch.stack(list(fo)))
+    out.update(chain_f=f, chain_forces=torch.stack(forces), chain_tau=torch.tensor(tau))
+    arrays = {k: v.detach().cpu().numpy() for k, v in out.items()}
+    np.savez_compressed(HERE / "bfl.npz", **arrays)
+    print(f"wrote bfl.npz ({(HERE / 'bfl.npz').stat().st_size / 1024:.0f} KB); links per grid "
+          f"{int(m19.sum())}, {int(m27.sum())}, chain {int(mask.sum())}")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -167,6 +221,9 @@ def main() -> None:
         return
     if args.only == "trt":
         trt(torch)
+        return
+    if args.only == "bfl":
+        bfl(torch)
         return
     from tensorlbm import boundaries as b2
     from tensorlbm import boundaries3d as b3

@@ -180,3 +180,24 @@ def test_collide_trt():
         for q in (19, 27):
             assert same(O.collide_trt(g[f"f{q}_{tag}"], 0.6), g[f"trt{q}_{tag}"])
             assert same(O.collide_trt(g[f"f{q}_{tag}"], 0.57, 0.25), g[f"trt{q}_lam_{tag}"])
+
+
+def test_bfl_links_update_and_chain():
+    """Bouzidi links of a sphere (bfl_common.py:384, interpolated_bc_common.py:136),
+    the link update (bfl_common.py:106) and the 8-step chain in bfl_step's
+    order: bit for bit against the reference; the force ledger (float64 here,
+    float32 sums there) to float32 rounding."""
+    g = golden("bfl")
+    m19, q19 = O.sphere_links(19, 16, 14, 12, 7.3, 6.6, 5.8, 3.7)
+    m27, q27 = O.sphere_links(27, 12, 11, 10, 5.4, 5.1, 4.7, 2.9)
+    assert same(m19, g["m19"]) and same(q19, g["q19"]) and same(m27, g["m27"]) and same(q27, g["q27"])
+    assert same(O.bfl_bounce_back(g["f19"], g["fprev19"], g["m19"], g["q19"]), g["bfl19"])
+    assert same(O.bfl_bounce_back(g["f27"], g["fprev27"], g["m27"], g["q27"]), g["bfl27"])
+    fo = O.bfl_force(g["fprev19"], g["m19"], g["q19"])
+    assert np.max(np.abs(fo - g["force19"])) < 1e-5 * np.max(np.abs(g["force19"]))
+    f, forces = g["chain_f0"], []
+    for _ in range(8):
+        f, fo = O.bfl_chain_step(f, float(g["chain_tau"]), g["chain_solid"], g["chain_mask"], g["chain_q"])
+        forces.append(fo)
+    assert same(f, g["chain_f"])
+    assert np.max(np.abs(np.array(forces) - g["chain_forces"])) < 1e-5 * np.max(np.abs(g["chain_forces"]))
