@@ -49,7 +49,10 @@ typedef enum tlbm_dtype {
   TLBM_F32 = 0,
   TLBM_F64 = 1,
   TLBM_F16_SHIFTED = 2,
-  TLBM_BF16_SHIFTED = 3
+  TLBM_BF16_SHIFTED = 3,
+  TLBM_F16 = 4,        /* plain float16 f, round-to-nearest on store: the storage of
+                          triton_fused.py:440-522 (D3Q19 stream and BGK only) */
+  TLBM_BF16 = 5        /* plain bfloat16 f, round-to-nearest (D3Q19 stream and BGK only) */
 } tlbm_dtype;
 
 typedef enum tlbm_collision {

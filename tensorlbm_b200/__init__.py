@@ -41,6 +41,7 @@ _PATCHES = {
     "bfl_common": ["compute_q_sphere_common", "bfl_bounce_back_common"],
     "interpolated_bc_common": ["compute_q_sphere_27"],
     "bfl_d3q19": ["bouzidi_bounce_back_d3q19"],
+    "triton_fused": ["triton_fused", "triton_collide", "triton_stream", "TritonFusedSolver3D", "is_available"],
 }
 
 

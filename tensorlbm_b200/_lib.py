@@ -21,7 +21,7 @@ LIB_PATH = pathlib.Path(os.environ.get("TLBM_LIB", _HERE / "libtlbm.so"))
 OK, ERR_SHAPE, ERR_DTYPE, ERR_ALIAS, ERR_LAUNCH, ERR_TIMEOUT, ERR_NONFINITE, ERR_ARG, ERR_UNSUPPORTED = range(9)
 ERR_TOO_LARGE = 9
 # tlbm_dtype
-F32, F64, F16_SHIFTED, BF16_SHIFTED = 0, 1, 2, 3
+F32, F64, F16_SHIFTED, BF16_SHIFTED, F16, BF16 = 0, 1, 2, 3, 4, 5
 # tlbm_collision
 COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY, COLL_TRT = range(8)
 # tlbm_bc_bits / tlbm_flag_bits

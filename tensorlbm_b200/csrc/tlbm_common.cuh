@@ -79,6 +79,39 @@ template <> struct Storage<__nv_bfloat16> {
   }
 };
 
+// Plain half formats: f itself in float16 / bfloat16, rounded to nearest on
+// store (the storage tiers of TensorLBM's Triton kernel).  Distinct types so
+// that they do not collide with the shifted formats above.
+struct f16_plain { __half h; };
+struct bf16_plain { __nv_bfloat16 h; };
+template <> struct Storage<f16_plain> {
+  using T = float;
+  static constexpr bool kShifted = false;
+  __device__ __forceinline__ static float load(f16_plain v, float) { return __half2float(v.h); }
+  __device__ __forceinline__ static f16_plain store(float v, float, uint32_t) { return {__float2half_rn(v)}; }
+};
+template <> struct Storage<bf16_plain> {
+  using T = float;
+  static constexpr bool kShifted = false;
+  __device__ __forceinline__ static float load(bf16_plain v, float) { return __bfloat162float(v.h); }
+  __device__ __forceinline__ static bf16_plain store(float v, float, uint32_t) { return {__float2bfloat16_rn(v)}; }
+};
+
+// read-only cached load of a storage element (the plain half structs go
+// through their 16-bit pattern)
+template <typename S>
+__device__ __forceinline__ S ldg(const S* p) { return __ldg(p); }
+template <>
+__device__ __forceinline__ f16_plain ldg(const f16_plain* p) {
+  const unsigned short b = __ldg(reinterpret_cast<const unsigned short*>(p));
+  return {__ushort_as_half(b)};
+}
+template <>
+__device__ __forceinline__ bf16_plain ldg(const bf16_plain* p) {
+  const unsigned short b = __ldg(reinterpret_cast<const unsigned short*>(p));
+  return {__ushort_as_bfloat16(b)};
+}
+
 // Two consecutive values of one direction (cells x and x + 1, x even) moved
 // as one aligned vector.  split() converts to the compute type; join()
 // converts back with the stochastic rounding of the half formats, whose
@@ -141,6 +174,30 @@ template <> struct PairIO<__nv_bfloat16> {
     const uint32_t ba = __float_as_uint(a - w) + ((ha * m) >> 16);
     const uint32_t bb = __float_as_uint(b - w) + ((hb * m) >> 16);
     return cvt_rz_bf16x2(__uint_as_float(ba), __uint_as_float(bb));
+  }
+};
+
+template <> struct PairIO<f16_plain> {
+  using V = uint32_t;
+  __device__ __forceinline__ static void split(V v, float, float& a, float& b) {
+    const float2 t = __half22float2(*reinterpret_cast<const __half2*>(&v));
+    a = t.x;
+    b = t.y;
+  }
+  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, uint32_t, int) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const V*>(&h);
+  }
+};
+template <> struct PairIO<bf16_plain> {
+  using V = uint32_t;
+  __device__ __forceinline__ static void split(V v, float, float& a, float& b) {
+    a = __uint_as_float(v << 16);
+    b = __uint_as_float(v & 0xFFFF0000u);
+  }
+  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, uint32_t, int) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const V*>(&h);
   }
 };
 

@@ -46,9 +46,27 @@ int dispatch_collision(const tlbm_desc& d, const StepParams& p, cudaStream_t s) 
   }
 }
 
+// plain half storage (the drop-in for TensorLBM's Triton kernel): D3Q19
+// stream and BGK only
+template <class L, typename S, bool PULL>
+int dispatch_plain(const tlbm_desc& d, const StepParams& p, cudaStream_t s) {
+  if constexpr (L::Q == 19) {
+    if (d.force_lin != 0.0) return TLBM_ERR_UNSUPPORTED;
+    switch (d.collision) {
+      case TLBM_COLL_NONE: return launch_step<L, S, S, TLBM_COLL_NONE, PULL>(p, d, s);
+      case TLBM_COLL_BGK: return launch_step<L, S, S, TLBM_COLL_BGK, PULL>(p, d, s);
+      default: return TLBM_ERR_UNSUPPORTED;
+    }
+  } else {
+    return TLBM_ERR_UNSUPPORTED;
+  }
+}
+
 template <class L, bool PULL>
 int dispatch_same_dtype(const tlbm_desc& d, const StepParams& p, cudaStream_t s) {
   switch (d.dtype) {
+    case TLBM_F16: return dispatch_plain<L, f16_plain, PULL>(d, p, s);
+    case TLBM_BF16: return dispatch_plain<L, bf16_plain, PULL>(d, p, s);
     case TLBM_F32: return dispatch_collision<L, float, PULL>(d, p, s);
     case TLBM_F64: return dispatch_collision<L, double, PULL>(d, p, s);
     case TLBM_F16_SHIFTED: return dispatch_collision<L, __half, PULL>(d, p, s);

@@ -78,8 +78,8 @@ __device__ __forceinline__ void curved_links(const Domain<SI, SO>& d, long long 
     if (b < a) continue;
     const float qa = __ldg(lq + a), qb = __ldg(lq + b);
     if (!(qa > 0.0f) && !(qb > 0.0f)) continue;
-    const T pa = Storage<SI>::load(__ldg(d.fin + (long long)a * N + cell), weight<L, T>(a));
-    const T pb = Storage<SI>::load(__ldg(d.fin + (long long)b * N + cell), weight<L, T>(b));
+    const T pa = Storage<SI>::load(ldg(d.fin + (long long)a * N + cell), weight<L, T>(a));
+    const T pb = Storage<SI>::load(ldg(d.fin + (long long)b * N + cell), weight<L, T>(b));
     const T ua = f[a], ub = f[b];
     if (qa > 0.0f) {
       const T v = bfl_value(T(qa), pa, ua, pb);
@@ -216,7 +216,7 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
         const int sy = L::cy(q) > 0 ? ym : (L::cy(q) < 0 ? yp : y);
         const int sz = L::cz(q) > 0 ? zm : (L::cz(q) < 0 ? zp : z);
         const long long src = (long long)sz * d.plane + (long long)sy * d.nx + sx;
-        f[q] = Storage<SI>::load(__ldg(fin + (long long)q * N + src), weight<L, T>(q));
+        f[q] = Storage<SI>::load(ldg(fin + (long long)q * N + src), weight<L, T>(q));
       }
     } else {
 #pragma unroll
@@ -351,12 +351,12 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
         IO::split(__ldg(reinterpret_cast<const V*>(at_offset(pin, o))), w, fa[q], fb[q]);
       } else if (L::cx(q) > 0) {
         const int ia = o + dxm;
-        fa[q] = Storage<S>::load(__ldg(at_offset(pin, ia)), w);
-        fb[q] = Storage<S>::load(__ldg(at_offset(pin, o)), w);
+        fa[q] = Storage<S>::load(ldg(at_offset(pin, ia)), w);
+        fb[q] = Storage<S>::load(ldg(at_offset(pin, o)), w);
       } else {
         const int ia = o + 1, ib = o + dxp;
-        fa[q] = Storage<S>::load(__ldg(at_offset(pin, ia)), w);
-        fb[q] = Storage<S>::load(__ldg(at_offset(pin, ib)), w);
+        fa[q] = Storage<S>::load(ldg(at_offset(pin, ia)), w);
+        fb[q] = Storage<S>::load(ldg(at_offset(pin, ib)), w);
       }
     }
     if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));

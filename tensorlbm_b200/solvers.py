@@ -410,38 +410,6 @@ def make_step(lattice, shape, tau: float, collision: str = "bgk", *, device=None
     return step
 
 
-class FusedSolver3D:
-    """Periodic D3Q19 BGK step with the surface of ``TritonFusedSolver3D``
-    (``triton_fused.py:676-865``): ``step(f)`` returns ``collide(stream(f))``.
-
-    fp32 is the drop-in format.  For float16 / bfloat16 storage use
-    :class:`LBMSolver` with ``storage="f16"`` / ``"bf16"``, which keeps the
-    shifted deviations f - w instead of plain half values."""
-
-    def __init__(self, nz: int, ny: int, nx: int, tau: float, device="cuda:0", dtype=None, **_unused):
-        dtype = torch.float32 if dtype is None else dtype
-        if dtype != torch.float32:
-            raise NotImplementedError("FusedSolver3D is the float32 drop-in; use LBMSolver(storage='f16'|'bf16')")
-        self.nz, self.ny, self.nx = int(nz), int(ny), int(nx)
-        self.tau = float(tau)
-        self.device = _ops.cuda_device(device)
-        self.dtype = dtype
-        self._desc = _ops.make_desc(19, (self.nx, self.ny, self.nz), _lib.F32, _lib.COLL_BGK, self.tau)
-        self._buf_a: torch.Tensor | None = None
-        self._buf_b: torch.Tensor | None = None
-
-    def step(self, f: torch.Tensor) -> torch.Tensor:
-        if f.dtype != self.dtype:
-            raise ValueError(f"step() input dtype {f.dtype} does not match the solver's storage dtype {self.dtype}")
-        if tuple(f.shape) != (19, self.nz, self.ny, self.nx):
-            raise ValueError(f"f shape {tuple(f.shape)} != {(19, self.nz, self.ny, self.nx)}")
-        _lib.require_cuda(f)
-        f = f.contiguous()
-        if self._buf_a is None or self._buf_a.shape != f.shape:
-            self._buf_a = torch.empty_like(f)
-            self._buf_b = torch.empty_like(f)
-        out = self._buf_b if f.data_ptr() == self._buf_a.data_ptr() else self._buf_a
-        st = _lib.load().tlbm_step(ctypes.byref(self._desc), f.data_ptr(), out.data_ptr(), None, None, None, None,
-                                   _lib.stream_of(self.device))
-        _lib.check(st, "FusedSolver3D.step")
-        return out
+# The TritonFusedSolver3D surface (triton_fused.py:676-960): float32, float16
+# and bfloat16 storage, precision-policy names; see tensorlbm_b200.triton_fused.
+from .triton_fused import TritonFusedSolver3D as FusedSolver3D  # noqa: E402
