@@ -369,6 +369,23 @@ def _reference_triton_variant(torch, dev, steps, warmup, peak, n=256):
                         "speedup": round(t_ref / t_us, 2),
                         "reference_roofline_frac": round(bpc * cells * steps / t_ref / 1e9 / peak, 4),
                         "ours_roofline_frac": round(bpc * cells * steps / t_us / 1e9 / peak, 4)}
+        if storage != "f32":
+            # like for like: this library's triton_fused drop-in on the same plain half storage
+            from tensorlbm_b200 import triton_fused as ours_tf
+
+            pa, pb = a.clone(), torch.empty_like(a)
+
+            def plain_steps(k):
+                nonlocal pa, pb
+                for _ in range(k):
+                    ours_tf.triton_fused(pa, tau, out=pb)
+                    pa, pb = pb, pa
+
+            plain_steps(warmup)
+            t_plain = timed(lambda: plain_steps(steps))
+            out[storage]["ours_plain_storage_mlups"] = round(cells * steps / t_plain / 1e6, 1)
+            out[storage]["speedup_plain_storage"] = round(t_ref / t_plain, 2)
+            del pa, pb
         del a, b, s
         torch.cuda.empty_cache()
 

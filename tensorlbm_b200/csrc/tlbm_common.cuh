@@ -47,12 +47,14 @@ __device__ __forceinline__ float stochastic_truncate_bits(float d, uint32_t r) {
 template <> struct Storage<float> {
   using T = float;
   static constexpr bool kShifted = false;
+  static constexpr bool kFast = false;   // exact (reference-rounded) collisions
   __device__ __forceinline__ static float load(float v, float) { return v; }
   __device__ __forceinline__ static float store(float v, float, uint32_t) { return v; }
 };
 template <> struct Storage<double> {
   using T = double;
   static constexpr bool kShifted = false;
+  static constexpr bool kFast = false;
   __device__ __forceinline__ static double load(double v, double) { return v; }
   __device__ __forceinline__ static double store(double v, double, uint32_t) { return v; }
 };
@@ -61,6 +63,7 @@ template <> struct Storage<double> {
 template <> struct Storage<__half> {
   using T = float;
   static constexpr bool kShifted = true;
+  static constexpr bool kFast = true;    // fused-arithmetic collisions (no bit-exact target)
   static constexpr float kScale = 16384.0f;
   __device__ __forceinline__ static float load(__half v, float w) {
     return fmaf(__half2float(v), 1.0f / kScale, w);
@@ -73,6 +76,7 @@ template <> struct Storage<__half> {
 template <> struct Storage<__nv_bfloat16> {
   using T = float;
   static constexpr bool kShifted = true;
+  static constexpr bool kFast = true;
   __device__ __forceinline__ static float load(__nv_bfloat16 v, float w) { return __bfloat162float(v) + w; }
   __device__ __forceinline__ static __nv_bfloat16 store(float v, float w, uint32_t r) {
     return __float2bfloat16_rz(stochastic_truncate_bits<16>(v - w, r));
@@ -87,12 +91,14 @@ struct bf16_plain { __nv_bfloat16 h; };
 template <> struct Storage<f16_plain> {
   using T = float;
   static constexpr bool kShifted = false;
+  static constexpr bool kFast = true;
   __device__ __forceinline__ static float load(f16_plain v, float) { return __half2float(v.h); }
   __device__ __forceinline__ static f16_plain store(float v, float, uint32_t) { return {__float2half_rn(v)}; }
 };
 template <> struct Storage<bf16_plain> {
   using T = float;
   static constexpr bool kShifted = false;
+  static constexpr bool kFast = true;
   __device__ __forceinline__ static float load(bf16_plain v, float) { return __bfloat162float(v.h); }
   __device__ __forceinline__ static bf16_plain store(float v, float, uint32_t) { return {__float2bfloat16_rn(v)}; }
 };

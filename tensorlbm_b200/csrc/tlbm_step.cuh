@@ -163,7 +163,7 @@ __device__ __forceinline__ void relax(const Domain<SI, SO>& d, long long cell, u
         // feq(rho, (1 + A) u) - feq(rho, u) with the pre-collision moments
         T rho, ux, uy, uz;
         macroscopic_fused<L>(f, rho, ux, uy, uz);
-        collide<L, COLL, T, Storage<SI>::kShifted>(f, cp, tau_cell, has_tau);
+        collide<L, COLL, T, Storage<SI>::kFast>(f, cp, tau_cell, has_tau);
         const T k = T(1) + cp.force_a;
         const T usq = ux * ux + uy * uy + uz * uz;
         const T usq_k = usq * k * k;
@@ -171,7 +171,7 @@ __device__ __forceinline__ void relax(const Domain<SI, SO>& d, long long cell, u
         for (int q = 0; q < Q; ++q)
           f[q] += feq_fused<L>(q, rho, ux * k, uy * k, uz * k, usq_k) - feq_fused<L>(q, rho, ux, uy, uz, usq);
       } else {
-        collide<L, COLL, T, Storage<SI>::kShifted>(f, cp, tau_cell, has_tau);
+        collide<L, COLL, T, Storage<SI>::kFast>(f, cp, tau_cell, has_tau);
       }
       if (d.status) {
         const T r = f[0];
