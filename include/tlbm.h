@@ -63,7 +63,9 @@ typedef enum tlbm_collision {
   TLBM_COLL_CUMULANT_GEIER = 4,   /* D3Q27 Geier 2015, cumulant.py:1050 */
   TLBM_COLL_CUMULANT_D3Q19 = 5,   /* cumulant.py:1159 (Smagorinsky via c_smag) */
   TLBM_COLL_SMAGORINSKY = 6,      /* turbulence.py:245 (D3Q19), :216 (D2Q9), :472 (D3Q27) */
-  TLBM_COLL_TRT = 7               /* solver.py:440, solver3d.py:303, d3q27.py:438 (tau = tau_plus > 1/2) */
+  TLBM_COLL_TRT = 7,              /* solver.py:440, solver3d.py:303, d3q27.py:438 (tau = tau_plus > 1/2) */
+  TLBM_COLL_CASCADED = 8          /* cascaded_collision.py:445 (D3Q19), :512 (D3Q27); rates: omega_b = s_bulk,
+                                     omega_odd = s_3, omega_even = s_4, cm_s5 / cm_s6 (D3Q27) */
 } tlbm_collision;
 
 /* Boundary conditions applied by tlbm_step after the pull, in this order:
@@ -120,6 +122,8 @@ typedef struct tlbm_desc {
                           (TLBM_COLL_TRT; TensorLBM's default is 3/16) */
   const int32_t* link_row; /* TLBM_FLAG_CURVED cells: row of the cell in link_q (may be NULL: no links) */
   const float* link_q;     /* (rows, Q) wall fraction of each link of the row, in (0, 1]; 0 = no link */
+  double cm_s5, cm_s6;     /* cascaded D3Q27 5th / 6th-order rates; negative = omega_even (TensorLBM's
+                              defaults) */
 } tlbm_desc;
 
 /* ---- fused time step ------------------------------------------------------

@@ -154,6 +154,71 @@ def collide_trt(f: np.ndarray, tau_plus: float, lambda_trt: float = 3.0 / 16.0) 
     return f - (f_plus - e_plus) / t(tau_plus) - (f_minus - e_minus) / t(tau_minus)
 
 
+_CASCADED_DEGREES = {
+    19: [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (0, 2, 0), (0, 0, 2), (1, 1, 0), (1, 0, 1), (0, 1, 1),
+         (2, 1, 0), (2, 0, 1), (1, 2, 0), (0, 2, 1), (1, 0, 2), (0, 1, 2), (2, 2, 0), (2, 0, 2), (0, 2, 2)],
+    27: [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (0, 2, 0), (0, 0, 2), (1, 1, 0), (1, 0, 1), (0, 1, 1),
+         (2, 1, 0), (2, 0, 1), (1, 2, 0), (0, 2, 1), (1, 0, 2), (0, 1, 2), (1, 1, 1), (2, 2, 0), (2, 0, 2), (0, 2, 2),
+         (2, 1, 1), (1, 2, 1), (1, 1, 2), (2, 2, 1), (2, 1, 2), (1, 2, 2), (2, 2, 2)],
+}
+
+
+def collide_cascaded(f: np.ndarray, tau: float, s_bulk: float = 1.0, s_3: float = 1.0, s_4: float = 1.0,
+                     s_5=None, s_6=None) -> np.ndarray:
+    """cascaded_collision.py:445-576: raw moments of f_neq by the float64 monomial
+    matrix cast to the field's dtype, binomial shift x, y, z over the complete
+    (degree 0, 1, 2) triples, per-order relaxation with the trace / deviator
+    split at second order (:330-442), unshift z, y, x, inverse matrix."""
+    q = f.shape[0]
+    dt = f.dtype
+    deg = _CASCADED_DEGREES[q]
+    c = C[q].astype(np.float64)
+    m64 = np.array([c[:, 0] ** a * c[:, 1] ** b * c[:, 2] ** d for a, b, d in deg])
+    M, Minv = m64.astype(dt), np.linalg.inv(m64).astype(dt)
+    rho, ux, uy, uz = macroscopic(f)
+    feq = equilibrium(q, rho, ux, uy, uz)
+    sp = f.shape[1:]
+    m = (M @ (f - feq).reshape(q, -1)).reshape((q,) + sp)
+    groups = []
+    for dim in range(3):
+        other = [d for d in range(3) if d != dim]
+        bucket = {}
+        for idx, dg in enumerate(deg):
+            bucket.setdefault((dg[other[0]], dg[other[1]]), {})[dg[dim]] = idx
+        groups.append([(v[0], v[1], v[2]) for _, v in sorted(bucket.items()) if all(k in v for k in (0, 1, 2))])
+
+    def shift(k, g, u, sign):
+        out = k.copy()
+        for i0, i1, i2 in g:
+            if sign < 0:
+                out[i1] = k[i1] - u * k[i0]
+                out[i2] = k[i2] - 2.0 * u * k[i1] + u * u * k[i0]
+            else:
+                out[i1] = k[i1] + u * k[i0]
+                out[i2] = k[i2] + 2.0 * u * k[i1] + u * u * k[i0]
+        return out
+
+    for g, u in zip(groups, (ux, uy, uz)):
+        m = shift(m, g, u, -1)
+    k = m.copy()
+    tr = m[4] + m[5] + m[6]
+    trs = (1.0 - s_bulk) * tr
+    om = 1.0 / tau
+    for i in (4, 5, 6):
+        k[i] = (1.0 - om) * (m[i] - tr / 3.0) + trs / 3.0
+    for i in (7, 8, 9):
+        k[i] = (1.0 - om) * m[i]
+    s5 = s_4 if s_5 is None else s_5
+    s6 = s_4 if s_6 is None else s_6
+    for i, dg in enumerate(deg):
+        order = sum(dg)
+        if order >= 3:
+            k[i] = (1.0 - {3: s_3, 4: s_4, 5: s5, 6: s6}[order]) * m[i]
+    for g, u in zip(groups[::-1], (uz, uy, ux)):
+        k = shift(k, g, u, 1)
+    return feq + (Minv @ k.reshape(q, -1)).reshape((q,) + sp)
+
+
 def mrt_matrix(q: int) -> np.ndarray:
     """Moment bases: solver.py:24-34 (D2Q9), solver3d.py:24-55 (D3Q19),
     d3q27.py:545-635 (D3Q27 Gram-Schmidt)."""
@@ -489,6 +554,7 @@ COLLIDERS = {
     "bgk": collide_bgk,
     "mrt": collide_mrt,
     "trt": collide_trt,
+    "cascaded": collide_cascaded,
     "smagorinsky": collide_smagorinsky,
     "cumulant_d3q19": collide_cumulant_d3q19,
     "cumulant": collide_cumulant_d3q27,

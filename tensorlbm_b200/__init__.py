@@ -42,6 +42,7 @@ _PATCHES = {
     "interpolated_bc_common": ["compute_q_sphere_27"],
     "bfl_d3q19": ["bouzidi_bounce_back_d3q19"],
     "triton_fused": ["triton_fused", "triton_collide", "triton_stream", "TritonFusedSolver3D", "is_available"],
+    "cascaded_collision": ["collide_cascaded_d3q19", "collide_cascaded_d3q27"],
 }
 
 

@@ -23,7 +23,8 @@ ERR_TOO_LARGE = 9
 # tlbm_dtype
 F32, F64, F16_SHIFTED, BF16_SHIFTED, F16, BF16 = 0, 1, 2, 3, 4, 5
 # tlbm_collision
-COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY, COLL_TRT = range(8)
+(COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY, COLL_TRT,
+ COLL_CASCADED) = range(9)
 # tlbm_bc_bits / tlbm_flag_bits
 BC_LID, BC_ZH_INLET, BC_ZH_OUTLET = 1, 2, 4
 FLAG_SOLID, FLAG_OBSTACLE, FLAG_HALFWAY, FLAG_MOVING, FLAG_CURVED = 1, 2, 4, 8, 16
@@ -59,6 +60,8 @@ class Desc(ctypes.Structure):
         ("lambda_trt", ctypes.c_double),
         ("link_row", ctypes.c_void_p),
         ("link_q", ctypes.c_void_p),
+        ("cm_s5", ctypes.c_double),
+        ("cm_s6", ctypes.c_double),
     ]
 
 

@@ -99,7 +99,7 @@ def make_desc(q: int, grid: tuple[int, int, int], dtype_code: int, collision: in
               s_e: float = 0.0, s_eps: float = 0.0, s_q: float = 0.0, s_pi: float | None = None,
               omega_b: float = 1.0, omega_odd: float = 1.0, omega_even: float = 1.0, c_smag: float = 0.0,
               bc: int = 0, u_lid: float = 0.0, u_in=(0.0, 0.0, 0.0), rho_out: float = 1.0,
-              lambda_trt: float = 3.0 / 16.0) -> _lib.Desc:
+              lambda_trt: float = 3.0 / 16.0, cm_s5: float | None = None, cm_s6: float | None = None) -> _lib.Desc:
     d = _lib.Desc()
     d.lattice = q
     d.dtype = dtype_code
@@ -115,6 +115,8 @@ def make_desc(q: int, grid: tuple[int, int, int], dtype_code: int, collision: in
     d.u_in[0], d.u_in[1], d.u_in[2] = (float(v) for v in u_in)
     d.rho_out = float(rho_out)
     d.lambda_trt = float(lambda_trt)
+    d.cm_s5 = -1.0 if cm_s5 is None else float(cm_s5)
+    d.cm_s6 = -1.0 if cm_s6 is None else float(cm_s6)
     return d
 
 

@@ -323,7 +323,7 @@ def load_case_checkpoint(directory: str | Path, *, identity: Mapping[str, Any]) 
 
 _LATTICE_NAME = {9: "D2Q9", 19: "D3Q19", 27: "D3Q27"}
 _PARAMS = ("collision", "s_e", "s_eps", "s_q", "s_pi", "omega_b", "omega_odd", "omega_even", "c_smag", "u_lid",
-           "u_in", "rho_out", "force_lin", "lambda_trt")
+           "u_in", "rho_out", "force_lin", "lambda_trt", "cm_s5", "cm_s6")
 
 
 def solver_state_dict(solver, *, step: int | None = None, extra: Mapping[str, Any] | None = None) -> dict[str, Any]:

@@ -105,6 +105,7 @@ int check_desc(const tlbm_desc* d) {
   if (!shape_ok(d->lattice, d->nx, d->ny, d->nz)) return TLBM_ERR_SHAPE;
   if (d->collision != TLBM_COLL_NONE && !(d->tau > 0.0)) return TLBM_ERR_ARG;
   if (d->collision == TLBM_COLL_TRT && !(d->tau > 0.5 && d->lambda_trt == d->lambda_trt)) return TLBM_ERR_ARG;
+  if (d->collision == TLBM_COLL_CASCADED && !(d->tau > 0.5)) return TLBM_ERR_ARG;
   if ((d->bc & TLBM_BC_LID) && d->lattice == TLBM_D3Q27) return TLBM_ERR_UNSUPPORTED;
   if (d->bc & ~(uint32_t)(TLBM_BC_LID | TLBM_BC_ZH_INLET | TLBM_BC_ZH_OUTLET)) return TLBM_ERR_ARG;
   if (d->force_lin != 0.0) {

@@ -185,9 +185,59 @@ def gen_mrt_header() -> str:
     return "\n".join(parts)
 
 
+# cascaded central-moment collision (cascaded_collision.py:59-187): the D3Q19
+# monomial basis, its raw-moment matrix and inverse (float64, as the reference
+# builds them with numpy) and the 1-D shift groups
+CASCADED_D3Q19_DEGREES = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (0, 2, 0), (0, 0, 2), (1, 1, 0),
+                          (1, 0, 1), (0, 1, 1), (2, 1, 0), (2, 0, 1), (1, 2, 0), (0, 2, 1), (1, 0, 2), (0, 1, 2),
+                          (2, 2, 0), (2, 0, 2), (0, 2, 2)]
+
+
+def _shift_groups(degrees):
+    """Per axis, the (degree 0, 1, 2) index triples of moments that agree in
+    the other two degrees; incomplete triples are not shifted."""
+    out = []
+    for dim in range(3):
+        other = [d for d in range(3) if d != dim]
+        bucket = {}
+        for idx, deg in enumerate(degrees):
+            bucket.setdefault((deg[other[0]], deg[other[1]]), {})[deg[dim]] = idx
+        out.append([(m[0], m[1], m[2]) for key, m in sorted(bucket.items()) if all(k in m for k in (0, 1, 2))])
+    return out
+
+
+def gen_cascaded_header() -> str:
+    import numpy as np
+
+    c = np.array(lat.LATTICES[19].c, dtype=np.float64)
+    deg = CASCADED_D3Q19_DEGREES
+    m = np.array([c[:, 0] ** a * c[:, 1] ** b * c[:, 2] ** d for a, b, d in deg])
+    minv = np.linalg.inv(m)
+    groups = _shift_groups(deg)
+    lines = ["// Generated by tensorlbm_b200/csrc/gen_tables.py - do not edit.",
+             "#pragma once",
+             "",
+             "// D3Q19 cascaded central-moment basis (TensorLBM cascaded_collision.py:59-79 order)",
+             "struct CascadedD3Q19 {"]
+    rows = ", ".join("{" + ", ".join(str(int(v)) for v in r) + "}" for r in m)
+    lines.append(f"  __host__ __device__ static constexpr int M(int i, int q) {{ constexpr int t[19][19] = {{{rows}}}; "
+                 "return t[i][q]; }")
+    rows = ", ".join("{" + ", ".join(_lit(v) for v in r) + "}" for r in minv)
+    lines.append(f"  __host__ __device__ static constexpr double Minv(int q, int i) {{ constexpr double t[19][19] = "
+                 f"{{{rows}}}; return t[q][i]; }}")
+    for axis, g in zip("xyz", groups):
+        body = ", ".join("{" + ", ".join(str(v) for v in t) + "}" for t in g)
+        lines.append(f"  static constexpr int kGroups{axis.upper()} = {len(g)};")
+        lines.append(f"  __host__ __device__ static constexpr int group_{axis}(int k, int j) {{ constexpr int t[{len(g)}][3] "
+                     f"= {{{body}}}; return t[k][j]; }}")
+    lines += ["};", ""]
+    return "\n".join(lines)
+
+
 def main() -> None:
     OUT.mkdir(parents=True, exist_ok=True)
-    for name, text in (("lattice_tables.cuh", gen_lattice_tables()), ("mrt_tables.cuh", gen_mrt_header())):
+    for name, text in (("lattice_tables.cuh", gen_lattice_tables()), ("mrt_tables.cuh", gen_mrt_header()),
+                       ("cascaded_tables.cuh", gen_cascaded_header())):
         path = OUT / name
         if not path.exists() or path.read_text() != text:
             path.write_text(text)

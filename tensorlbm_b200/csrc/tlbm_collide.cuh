@@ -25,6 +25,7 @@ template <typename T> struct CollideParams {
   T tau_eff_max;            // max(1, tau + 0.5), turbulence.py:88-99
   T force_a;                // linear body force F = A rho u (exact-difference forcing); 0 = none
   bool cum_unit_rates;      // omega_b = omega_odd = omega_even = 1 (D3Q27 legacy cumulant fast path)
+  T cm_s5, cm_s6;           // cascaded D3Q27 5th / 6th-order rates (omega_odd, omega_even are s_3, s_4)
   T tau_minus;              // TRT antisymmetric relaxation time
   double inv_tau_minus64;   // RN64(1 / float(tau_minus)) for the exact TRT quotient
 };
@@ -513,6 +514,123 @@ __device__ __forceinline__ void legacy_inverse(T (&c)[27]) {
           T(2) * c101 * c101 * c020 - T(2) * c011 * c011 * c200;
 }
 
+// ---------------------------------------------------------------------------
+// Cascaded central-moment collision (cascaded_collision.py:445-576): central
+// moments of f_neq, the second order split into trace (rate s_bulk) and
+// deviator (1/tau), every higher order relaxed at its own rate, back to
+// populations.  D3Q19 uses TensorLBM's 19-monomial basis (no corner
+// monomials, so only the complete shift triples are shifted); D3Q27 the full
+// 3x3x3 cube with the factorised transforms.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void cascaded_relax_second(T& kxx, T& kyy, T& kzz, T& kxy, T& kxz, T& kyz, T om, T sb) {
+  const T tr = kxx + kyy + kzz;
+  const T trs = (T(1) - sb) * tr, ks = T(1) - om;
+  kxx = ks * (kxx - tr / T(3)) + trs / T(3);
+  kyy = ks * (kyy - tr / T(3)) + trs / T(3);
+  kzz = ks * (kzz - tr / T(3)) + trs / T(3);
+  kxy = ks * kxy;
+  kxz = ks * kxz;
+  kyz = ks * kyz;
+}
+
+template <int AX, typename T>
+__device__ __forceinline__ void cascaded19_shift(T (&m)[19], T u, bool inverse) {
+  using B = CascadedD3Q19;
+  constexpr int G = AX == 0 ? B::kGroupsX : (AX == 1 ? B::kGroupsY : B::kGroupsZ);
+  const T tu = T(2) * u, uu = u * u;
+#pragma unroll
+  for (int k = 0; k < G; ++k) {
+    const int i0 = AX == 0 ? B::group_x(k, 0) : (AX == 1 ? B::group_y(k, 0) : B::group_z(k, 0));
+    const int i1 = AX == 0 ? B::group_x(k, 1) : (AX == 1 ? B::group_y(k, 1) : B::group_z(k, 1));
+    const int i2 = AX == 0 ? B::group_x(k, 2) : (AX == 1 ? B::group_y(k, 2) : B::group_z(k, 2));
+    const T m0 = m[i0], m1 = m[i1], m2 = m[i2];
+    if (inverse) {
+      m[i1] = m1 + u * m0;
+      m[i2] = m2 + tu * m1 + uu * m0;
+    } else {
+      m[i1] = m1 - u * m0;
+      m[i2] = m2 - tu * m1 + uu * m0;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void collide_cascaded_d3q19(T (&f)[19], const CollideParams<T>& cp) {
+  using L = D3Q19;
+  using B = CascadedD3Q19;
+  T rho, ux, uy, uz;
+  macroscopic_fused<L>(f, rho, ux, uy, uz);
+  const T usq = usq_fused<L>(ux, uy, uz);
+  T fe[19], fn[19], m[19];
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    fe[q] = feq_fused<L>(q, rho, ux, uy, uz, usq);
+    fn[q] = f[q] - fe[q];
+  }
+#pragma unroll
+  for (int i = 0; i < 19; ++i) {
+    T acc = T(0);
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      if (B::M(i, q) == 1) acc += fn[q];
+      else if (B::M(i, q) == -1) acc -= fn[q];
+    }
+    m[i] = acc;
+  }
+  cascaded19_shift<0>(m, ux, false);
+  cascaded19_shift<1>(m, uy, false);
+  cascaded19_shift<2>(m, uz, false);
+  cascaded_relax_second(m[4], m[5], m[6], m[7], m[8], m[9], cp.inv_tau, cp.omega_b);
+  const T k3 = T(1) - cp.omega_odd, k4 = T(1) - cp.omega_even;
+#pragma unroll
+  for (int i = 10; i < 16; ++i) m[i] = k3 * m[i];
+#pragma unroll
+  for (int i = 16; i < 19; ++i) m[i] = k4 * m[i];
+  cascaded19_shift<2>(m, uz, true);
+  cascaded19_shift<1>(m, uy, true);
+  cascaded19_shift<0>(m, ux, true);
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    T acc = T(0);
+#pragma unroll
+    for (int i = 0; i < 19; ++i)
+      if (B::Minv(q, i) != 0.0) acc += T(B::Minv(q, i)) * m[i];
+    f[q] = fe[q] + acc;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void collide_cascaded_d3q27(T (&f)[27], const CollideParams<T>& cp) {
+  using L = D3Q27;
+  T rho, ux, uy, uz;
+  macroscopic_fused<L>(f, rho, ux, uy, uz);
+  const T usq = usq_fused<L>(ux, uy, uz);
+  T fe[27], fn[27];
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    fe[q] = feq_fused<L>(q, rho, ux, uy, uz, usq);
+    fn[q] = f[q] - fe[q];
+  }
+  Cube<T> g;
+  central_moments(fn, ux, uy, uz, g);
+  cascaded_relax_second(g[2][0][0], g[0][2][0], g[0][0][2], g[1][1][0], g[1][0][1], g[0][1][1], cp.inv_tau,
+                        cp.omega_b);
+  const T keep[7] = {T(1), T(1), T(1), T(1) - cp.omega_odd, T(1) - cp.omega_even, T(1) - cp.cm_s5,
+                     T(1) - cp.cm_s6};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if (a + b + c >= 3) g[a][b][c] = keep[a + b + c] * g[a][b][c];
+  T fns[27];
+  populations(g, ux, uy, uz, fns);
+#pragma unroll
+  for (int q = 0; q < 27; ++q) f[q] = fe[q] + fns[q];
+}
+
 // D3Q27 legacy cumulant collision with omega_b = omega_odd = omega_even = 1
 // (cumulant.py:935 defaults).  Those rates set every post-collision
 // cumulant above second order to zero and leave no bulk part, so only the
@@ -849,6 +967,9 @@ __device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp
     collide_mrt<L>(f, r);
   } else if constexpr (COLL == TLBM_COLL_SMAGORINSKY) {
     collide_smagorinsky<L>(f, cp);
+  } else if constexpr (COLL == TLBM_COLL_CASCADED) {
+    if constexpr (L::Q == 19) collide_cascaded_d3q19(f, cp);
+    else if constexpr (L::Q == 27) collide_cascaded_d3q27(f, cp);
   } else if constexpr (COLL == TLBM_COLL_TRT) {
     collide_trt<L>(f, cp.tau, cp.inv_tau64, cp.tau_minus, cp.inv_tau_minus64);
   } else if constexpr (COLL == TLBM_COLL_CUMULANT_D3Q19) {
@@ -884,6 +1005,8 @@ __host__ __device__ CollideParams<T> make_collide_params(double tau, double s_e,
   cp.omega_b_minus_omega = T(omega_b - 1.0 / tau);
   cp.keep_even = T(1.0 - omega_even);
   cp.cum_unit_rates = (omega_b == 1.0) && (omega_odd == 1.0) && (omega_even == 1.0);
+  cp.cm_s5 = cp.omega_even;
+  cp.cm_s6 = cp.omega_even;
   cp.tau_minus = cp.tau;
   cp.inv_tau_minus64 = cp.inv_tau64;
   cp.tau_sq = T(tau * tau);

@@ -8,6 +8,7 @@
 
 #include "../../include/tlbm.h"
 #include "generated/lattice_tables.cuh"
+#include "generated/cascaded_tables.cuh"
 #include "generated/mrt_tables.cuh"
 
 namespace tlbm {

@@ -426,6 +426,8 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
                                                d.omega_even, d.c_smag);
   cp.force_a = T(d.force_lin);
   if (d.collision == TLBM_COLL_TRT) set_trt_rates(cp, d.tau, d.lambda_trt);
+  if (d.cm_s5 >= 0.0) cp.cm_s5 = T(d.cm_s5);
+  if (d.cm_s6 >= 0.0) cp.cm_s6 = T(d.cm_s6);
   const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
   // the forced instantiations stay on one cell per thread: two cells with
   // the pre-collision moments held for the force need 121 registers (2 blocks

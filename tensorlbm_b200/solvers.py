@@ -35,6 +35,7 @@ COLLISIONS = {
     "cumulant_d3q19": _lib.COLL_CUMULANT_D3Q19,
     "smagorinsky": _lib.COLL_SMAGORINSKY,
     "trt": _lib.COLL_TRT,
+    "cascaded": _lib.COLL_CASCADED,
 }
 _LATTICES = {"D2Q9": 9, "D3Q19": 19, "D3Q27": 27, 9: 9, 19: 19, 27: 27}
 # storage dtype -> (C code, torch dtype of the buffer)
@@ -71,6 +72,8 @@ class StepConfig:
     rho_out: float | None = None     # Zou/He outlet at x = nx-1
     force_lin: float = 0.0           # linear body force F = A rho u (BGK / MRT / Smagorinsky, float32)
     lambda_trt: float = 3.0 / 16.0   # TRT magic parameter (solver.py:440)
+    cm_s5: float | None = None       # cascaded D3Q27 5th / 6th-order rates (None: omega_even)
+    cm_s6: float | None = None
     extra: dict = field(default_factory=dict)
 
     @property
@@ -102,6 +105,7 @@ class StepConfig:
             s_pi=self.s_pi, omega_b=self.omega_b, omega_odd=self.omega_odd, omega_even=self.omega_even,
             c_smag=self.c_smag, bc=bc, u_lid=self.u_lid or 0.0, u_in=u_in,
             rho_out=1.0 if self.rho_out is None else self.rho_out, lambda_trt=self.lambda_trt,
+            cm_s5=self.cm_s5, cm_s6=self.cm_s6,
         )
         if coll in (_lib.COLL_BGK, _lib.COLL_MRT, _lib.COLL_SMAGORINSKY):
             d.force_lin = float(self.force_lin)
@@ -119,7 +123,9 @@ class LBMSolver:
         tau: shear relaxation time.
         collision: "bgk", "mrt", "trt" (tau = tau_plus, ``lambda_trt=`` the magic
             parameter), "smagorinsky", "cumulant" (D3Q27 legacy),
-            "cumulant_geier" (D3Q27), "cumulant_d3q19".
+            "cumulant_geier" (D3Q27), "cumulant_d3q19", "cascaded" (D3Q19 / D3Q27;
+            ``omega_b``, ``omega_odd``, ``omega_even``, ``cm_s5``, ``cm_s6`` are
+            s_bulk, s_3, s_4, s_5, s_6).
         storage: "f32", "f64", "f16" or "bf16" (half formats hold the deviation f - w,
             scaled by 2^14 for f16, stochastically rounded).
         wall_mask, obstacle_mask: bool fields; both bounce back, only the

@@ -203,6 +203,22 @@ def bfl(torch) -> None:
           f"{int(m19.sum())}, {int(m27.sum())}, chain {int(mask.sum())}")
 
 
+def cascaded(torch) -> None:
+    """Cascaded central-moment collisions (cascaded_collision.py:445, :512)."""
+    from tensorlbm.cascaded_collision import collide_cascaded_d3q19, collide_cascaded_d3q27
+
+    out = {}
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        _, _, f19 = near_eq_field(torch, 19, (4, 4, 8), dt, 71)
+        _, _, f27 = near_eq_field(torch, 27, (4, 4, 8), dt, 72)
+        out.update({f"f19_{tag}": f19, f"c19_{tag}": collide_cascaded_d3q19(f19, 0.6),
+                    f"c19r_{tag}": collide_cascaded_d3q19(f19, 0.57, s_bulk=1.2, s_3=0.9, s_4=1.3),
+                    f"f27_{tag}": f27, f"c27_{tag}": collide_cascaded_d3q27(f27, 0.6),
+                    f"c27r_{tag}": collide_cascaded_d3q27(f27, 0.57, s_bulk=1.2, s_3=0.9, s_4=1.3, s_5=1.1, s_6=0.8)})
+    np.savez_compressed(HERE / "collide_cascaded.npz", **{k: v.numpy() for k, v in out.items()})
+    print("wrote collide_cascaded.npz")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -224,6 +240,9 @@ def main() -> None:
         return
     if args.only == "bfl":
         bfl(torch)
+        return
+    if args.only == "cascaded":
+        cascaded(torch)
         return
     from tensorlbm import boundaries as b2
     from tensorlbm import boundaries3d as b3

@@ -286,3 +286,40 @@ def test_trt_sphere_channel_vs_oracle(cuda):
         forces.append(fo)
     assert same(N(s.f), ref)
     assert np.max(np.abs(N(s.force_history()) - np.array(forces))) < 1e-6 * np.max(np.abs(np.array(forces)))
+
+
+@pytest.mark.parametrize("tag,tol", [("f32", 5 * F32_TOL), ("f64", 1e-12)])
+def test_collide_cascaded(cuda, tag, tol):
+    """The cascaded kernels against the reference's outputs (fused moment
+    transforms: float32 rounding, not bit for bit)."""
+    from tensorlbm_b200 import cascaded_collision as cc
+
+    g = golden("collide_cascaded")
+    for q, fn, kw in ((19, cc.collide_cascaded_d3q19, dict(s_bulk=1.2, s_3=0.9, s_4=1.3)),
+                      (27, cc.collide_cascaded_d3q27, dict(s_bulk=1.2, s_3=0.9, s_4=1.3, s_5=1.1, s_6=0.8))):
+        f = T(g[f"f{q}_{tag}"], cuda)
+        assert rel_err(N(fn(f, 0.6)), g[f"c{q}_{tag}"]) < tol
+        assert rel_err(N(fn(f, 0.57, **kw)), g[f"c{q}r_{tag}"]) < tol
+    with pytest.raises(ValueError):
+        cc.collide_cascaded_d3q19(T(g["f19_f32"], cuda), 0.5)
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_cascaded_sphere_channel_vs_oracle(cuda, q):
+    """The fused step with the cascaded collision against the oracle's chain."""
+    from tensorlbm_b200 import LBMSolver, boundaries3d
+
+    nz, ny, nx = 8, 10, 20
+    obst = boundaries3d.sphere_mask(nx, ny, nz, 7.0, 5.0, 4.0, 2.2, cuda)
+    o = obst.cpu().numpy()
+    ux = np.full((nz, ny, nx), 0.04, np.float32)
+    ux[o] = 0.0
+    z = np.zeros_like(ux)
+    f0 = O.equilibrium(q, np.ones_like(ux), ux, z, z)
+    s = LBMSolver(q, (nz, ny, nx), 0.56, "cascaded", device=cuda, obstacle_mask=obst, u_in=0.04, rho_out=1.0,
+                  omega_b=1.1, omega_odd=0.95)
+    s.load(T(f0, cuda)).step(6)
+    ref = f0
+    for _ in range(6):
+        ref, _ = O.channel_step(ref, 0.56, 0.04, 1.0, None, o, "cascaded", s_bulk=1.1, s_3=0.95)
+    assert rel_err(N(s.f), ref) < 1e-5

@@ -201,3 +201,16 @@ def test_bfl_links_update_and_chain():
         forces.append(fo)
     assert same(f, g["chain_f"])
     assert np.max(np.abs(np.array(forces) - g["chain_forces"])) < 1e-5 * np.max(np.abs(g["chain_forces"]))
+
+
+def test_collide_cascaded():
+    """Cascaded central-moment collisions (cascaded_collision.py:445, :512): the
+    oracle against the reference's outputs (its float32 matrix products are
+    restated with numpy's, equal here to rounding)."""
+    g = golden("collide_cascaded")
+    for tag, tol in (("f32", 1e-6), ("f64", 1e-13)):
+        for q in (19, 27):
+            f = g[f"f{q}_{tag}"]
+            assert np.max(np.abs(O.collide_cascaded(f, 0.6) - g[f"c{q}_{tag}"])) < tol * np.max(np.abs(f))
+            kw = dict(s_bulk=1.2, s_3=0.9, s_4=1.3) if q == 19 else dict(s_bulk=1.2, s_3=0.9, s_4=1.3, s_5=1.1, s_6=0.8)
+            assert np.max(np.abs(O.collide_cascaded(f, 0.57, **kw) - g[f"c{q}r_{tag}"])) < tol * np.max(np.abs(f))
