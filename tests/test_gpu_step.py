@@ -350,3 +350,50 @@ def test_rotating_obstacle_fused_chain(cuda, q):
     want = np.array(forces)
     tol = 1e-6 if coll == "bgk" else 1e-4  # per-cell momenta are float32, as in TensorLBM
     assert np.max(np.abs(got[:, :want.shape[1]] - want)) <= tol * max(np.max(np.abs(want)), 1e-30)
+
+
+@pytest.mark.parametrize("nx", [23, 24])
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+def test_one_and_two_cells_per_thread_match_oracle(cuda, nx, coll):
+    """Odd nx runs the one-cell-per-thread kernel, even nx the pair kernel:
+    both against the oracle's sphere-channel chain (BGK bit for bit)."""
+    from tensorlbm_b200 import LBMSolver, boundaries3d
+
+    nz, ny = 9, 10
+    obst = boundaries3d.sphere_mask(nx, ny, nz, 8.0, 5.0, 4.0, 2.3, cuda)
+    o = obst.cpu().numpy()
+    ux = np.full((nz, ny, nx), 0.04, np.float32)
+    ux[o] = 0.0
+    z = np.zeros_like(ux)
+    f0 = O.equilibrium(19, np.ones_like(ux), ux, z, z)
+    s = LBMSolver("D3Q19", (nz, ny, nx), 0.55, coll, device=cuda, obstacle_mask=obst, u_in=0.04, rho_out=1.0,
+                  track_force=True)
+    s.load(T(f0, cuda)).step(7)
+    ref, forces = f0, []
+    for _ in range(7):
+        ref, fo = O.channel_step(ref, 0.55, 0.04, 1.0, None, o, coll)
+        forces.append(fo)
+    if coll == "bgk":
+        assert same(N(s.f), ref)
+    else:
+        assert rel_err(N(s.f), ref) < CHAIN_TOL
+    assert np.max(np.abs(N(s.force_history()) - np.array(forces))) < 1e-5 * np.max(np.abs(np.array(forces)))
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_half_storage_odd_and_even_nx_agree(cuda, storage):
+    """The half formats through both kernels: the same flow to storage precision."""
+    from tensorlbm_b200 import LBMSolver
+
+    rng = np.random.default_rng(5)
+    out = {}
+    for nx in (31, 32):
+        sp = (6, 8, nx)
+        u = [(0.03 * np.sin(2 * np.pi * np.arange(nx) / nx) * np.ones(sp)).astype(np.float32),
+             (0.02 * rng.standard_normal(sp)).astype(np.float32), np.zeros(sp, np.float32)]
+        f0 = O.equilibrium(19, np.ones(sp, np.float32), *u)
+        a = LBMSolver("D3Q19", sp, 0.6, "bgk", device=cuda, storage=storage).load(T(f0, cuda)).step(20)
+        b = LBMSolver("D3Q19", sp, 0.6, "bgk", device=cuda, storage="f32").load(T(f0, cuda)).step(20)
+        out[nx] = float((a.f - b.f).abs().max() / b.f.abs().max())
+    tol = 2e-4 if storage == "f16" else 1e-3
+    assert out[31] < tol and out[32] < tol, out
