@@ -419,6 +419,39 @@ TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, doub
 TLBM_API const char* tlbm_status_string(int status);
 TLBM_API int tlbm_abi_version(void);
 
+/* ---- AA pattern: the step in place, one population buffer -------------------
+ * Between steps the buffer holds one of three layouts: TLBM_AA_LOADED (slot q
+ * of x holds S_0 as loaded), TLBM_AA_SWAPPED (slot opp(q) of x holds x's
+ * post-collision population q) or TLBM_AA_NATURAL (slot q of x holds what
+ * streamed into x, not yet bounded).  tlbm_step_aa advances one step in place
+ * (loaded -> swapped -> natural -> swapped ...) with the boundaries,
+ * collision, forcing and status of tlbm_step.  The pipeline runs one collision
+ * behind the two-buffer step (one buffer cannot keep P_{n-1}): the first
+ * launch collides S_0 without boundaries (the two-buffer load pass), launch n
+ * >= 2 is the regular step, and tlbm_aa_populations after n launches returns
+ * S_n, equal to the two-buffer field bit for bit (float32).  Launch n samples
+ * the obstacle force of step n - 1; the readout samples step n.
+ * Not supported here: Bouzidi links, moving walls (TLBM_ERR_UNSUPPORTED).
+ * dtype F32, F16_SHIFTED, BF16_SHIFTED; collisions BGK, MRT, TRT, Smagorinsky,
+ * cumulant (D3Q27), cascaded.
+ * Replaces the second buffer of the two-buffer step (half the memory: D3Q19
+ * float32 fits about 2.3 G cells in 180 GB instead of 1.2 G). */
+typedef enum tlbm_aa_layout { TLBM_AA_SWAPPED = 0, TLBM_AA_NATURAL = 1, TLBM_AA_LOADED = 2 } tlbm_aa_layout;
+
+/* f0: the TensorLBM-phase populations in the compute type (float32); f: the
+ * AA buffer in d->dtype (f0 == f allowed for float32).  Writes the loaded
+ * layout. */
+TLBM_API int tlbm_aa_load(const tlbm_desc* d, const void* f0, void* f, const uint8_t* flags, const float* tau_field,
+                          void* stream);
+/* One step in place from the given layout; the buffer then holds the other. */
+TLBM_API int tlbm_step_aa(const tlbm_desc* d, void* f, int32_t layout, const uint8_t* flags, const float* tau_field,
+                          double* force, unsigned int* status, void* stream);
+/* The TensorLBM-phase populations (boundaries applied, float32) of an AA
+ * buffer in the given layout, into out (out != f); force (may be NULL) gets
+ * the obstacle force sample of that state added. */
+TLBM_API int tlbm_aa_populations(const tlbm_desc* d, const void* f, int32_t layout, const uint8_t* flags,
+                                 void* out, double* force, void* stream);
+
 /* ---- curved walls (Bouzidi / BFL interpolated bounce-back) -------------------
  * tlbm_sphere_links: the boundary links of a sphere and their wall fractions,
  * the outputs of compute_q_sphere_common (bfl_common.py:384) / compute_q_sphere_27

@@ -113,6 +113,9 @@ SIGNATURES: dict[str, list] = {
     "tlbm_batch_run": [ctypes.POINTER(BatchDesc), _P, _P, _I64, _P, _P, _P, _I32, _P, _I32, _P, _P, _I64, _P],
     "tlbm_link_list_noalloc": [_P, _I64, _P, _I64, _P, _P],
     "tlbm_sphere_links": [_I32, _I32, _I32, _I32, _D, _D, _D, _D, _P, _P, _P, _P],
+    "tlbm_aa_load": [ctypes.POINTER(Desc), _P, _P, _P, _P, _P],
+    "tlbm_step_aa": [ctypes.POINTER(Desc), _P, _I32, _P, _P, _P, _P, _P],
+    "tlbm_aa_populations": [ctypes.POINTER(Desc), _P, _I32, _P, _P, _P, _P],
     "tlbm_bfl_bounce_back": [ctypes.POINTER(Desc), _P, _P, _P, _P, _P, _P, _P],
     "tlbm_link_list_static_capacity": [],
     "tlbm_les_filter_moments": [_P, _I32, _I32, _I32, _I32, _D, _P, _P],

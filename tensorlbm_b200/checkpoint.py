@@ -353,6 +353,7 @@ def solver_state_dict(solver, *, step: int | None = None, extra: Mapping[str, An
         "storage": solver.storage,
         "storage_dtype": str(solver.buf_dtype),
         "stored_state": solver.state,
+        "aa_layout": solver.aa_layout,
         "cell_flags": solver.flags.detach().cpu() if solver.flags is not None else None,
         "solver_params": {k: getattr(cfg, k) for k in _PARAMS},
     }
@@ -383,9 +384,12 @@ def solver_load_state_dict(solver, state: Mapping[str, Any], *, exact: bool = Tr
     if tuple(pop.shape) != (solver.q,) + tuple(solver.cfg.shape):
         raise CheckpointError(f"populations {tuple(pop.shape)} do not fit the solver")
     raw = st.get("stored_state")
-    use_raw = exact and isinstance(raw, torch.Tensor) and st.get("storage") == solver.storage
+    # the raw state fits when the storage format and the memory pattern (two
+    # buffers, or one AA buffer with its layout) are the solver's
+    same_pattern = (st.get("aa_layout") is None) == (solver.aa_layout is None)
+    use_raw = exact and isinstance(raw, torch.Tensor) and st.get("storage") == solver.storage and same_pattern
     return solver.resume(pop.to(device=solver.device, dtype=solver.compute_dtype), step=int(st["step"]),
-                         stored_state=raw if use_raw else None)
+                         stored_state=raw if use_raw else None, aa_layout=st.get("aa_layout"))
 
 
 def save_solver(solver, path: str | Path, *, metadata: Mapping[str, Any] | None = None) -> Path:

@@ -1,6 +1,7 @@
 // extern "C" entry points (include/tlbm.h): argument checks, then dispatch to
 // the typed kernels.  No entry point allocates or synchronises.
 #include "ops.cuh"
+#include "tlbm_aa.cuh"
 #include "tlbm_dispatch.cuh"
 
 using namespace tlbm;
@@ -124,6 +125,23 @@ int dispatch(const tlbm_desc& d, int dtype_out, bool pull, const StepParams& p, 
     case TLBM_D3Q27: return dispatch_step_d3q27(d, dtype_out, pull, p, s);
     default: return TLBM_ERR_UNSUPPORTED;
   }
+}
+
+int dispatch_aa_any(const tlbm_desc& d, int mode, const StepParams& p, cudaStream_t s) {
+  switch (d.lattice) {
+    case TLBM_D2Q9: return dispatch_aa_d2q9(mode, p, d, s);
+    case TLBM_D3Q19: return dispatch_aa_d3q19(mode, p, d, s);
+    case TLBM_D3Q27: return dispatch_aa_d3q27(mode, p, d, s);
+    default: return TLBM_ERR_UNSUPPORTED;
+  }
+}
+
+int check_aa(const tlbm_desc* d) {
+  const int st = check_desc(d);
+  if (st != TLBM_OK) return st;
+  if (d->link_q || d->link_row || d->wall_velocity) return TLBM_ERR_UNSUPPORTED;
+  if (d->dtype != TLBM_F32 && d->dtype != TLBM_F16_SHIFTED && d->dtype != TLBM_BF16_SHIFTED) return TLBM_ERR_DTYPE;
+  return TLBM_OK;
 }
 
 }  // namespace
@@ -341,5 +359,40 @@ TLBM_API const char* tlbm_status_string(int status) {
 }
 
 TLBM_API int tlbm_abi_version(void) { return TLBM_ABI_VERSION; }
+
+TLBM_API int tlbm_aa_load(const tlbm_desc* d, const void* f0, void* f, const uint8_t* flags, const float* tau_field,
+                          void* stream) {
+  const int st = check_aa(d);
+  if (st != TLBM_OK) return st;
+  if (!f0 || !f) return TLBM_ERR_ARG;
+  if (f0 == f && d->dtype != TLBM_F32) return TLBM_ERR_ALIAS;
+  tlbm_desc dd = *d;
+  dd.bc = 0;
+  const StepParams p = make_params(dd, f0, f, flags, tau_field, nullptr, nullptr);
+  return dispatch_aa_any(dd, 2, p, as_stream(stream));
+}
+
+TLBM_API int tlbm_step_aa(const tlbm_desc* d, void* f, int32_t layout, const uint8_t* flags, const float* tau_field,
+                          double* force, unsigned int* status, void* stream) {
+  const int st = check_aa(d);
+  if (st != TLBM_OK) return st;
+  if (!f || layout < TLBM_AA_SWAPPED || layout > TLBM_AA_LOADED) return TLBM_ERR_ARG;
+  const StepParams p = make_params(*d, f, f, flags, tau_field, force, status);
+  const int mode = layout == TLBM_AA_SWAPPED ? 1 : (layout == TLBM_AA_NATURAL ? 0 : 5);
+  return dispatch_aa_any(*d, mode, p, as_stream(stream));
+}
+
+TLBM_API int tlbm_aa_populations(const tlbm_desc* d, const void* f, int32_t layout, const uint8_t* flags,
+                                 void* out, double* force, void* stream) {
+  const int st = check_aa(d);
+  if (st != TLBM_OK) return st;
+  if (!f || !out || layout < TLBM_AA_SWAPPED || layout > TLBM_AA_LOADED) return TLBM_ERR_ARG;
+  if (f == out) return TLBM_ERR_ALIAS;
+  tlbm_desc dd = *d;
+  dd.force_lin = 0.0;
+  const StepParams p = make_params(dd, f, out, flags, nullptr, force, nullptr);
+  const int mode = layout == TLBM_AA_SWAPPED ? 4 : (layout == TLBM_AA_NATURAL ? 3 : 6);
+  return dispatch_aa_any(dd, mode, p, as_stream(stream));
+}
 
 }  // extern "C"

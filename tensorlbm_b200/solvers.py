@@ -139,7 +139,7 @@ class LBMSolver:
 
     def __init__(self, lattice, shape, tau: float, collision: str = "bgk", *, device=None, storage="f32",
                  wall_mask=None, obstacle_mask=None, wall_mode: str = "fullway", tau_field=None,
-                 track_force: bool = False, wall_velocity=None, curved_wall=None, **cfg):
+                 track_force: bool = False, wall_velocity=None, curved_wall=None, pattern: str = "ab", **cfg):
         q = _LATTICES[lattice]
         if isinstance(storage, torch.dtype):
             storage = _TORCH_STORAGE[storage]
@@ -193,7 +193,16 @@ class LBMSolver:
             self.tau_field = tau_field.to(device=self.device, dtype=torch.float32).contiguous()
         self.track_force = track_force
         full = (q,) + shape
-        self._buf = [torch.empty(full, dtype=self.buf_dtype, device=self.device) for _ in range(2)]
+        if pattern not in ("ab", "aa"):
+            raise ValueError(f"pattern must be 'ab' (two buffers) or 'aa' (one buffer, in place), got {pattern!r}")
+        if pattern == "aa" and (self.curved is not None or storage == "f64" or self.wall_u is not None):
+            raise NotImplementedError("the AA pattern supports f32 / f16 / bf16 storage without curved or "
+                                      "moving walls")
+        self.pattern = pattern
+        # two buffers (index of the current one in _cur), or one AA buffer
+        # (its layout in _cur: 0 swapped, 1 natural)
+        self._buf = [torch.empty(full, dtype=self.buf_dtype, device=self.device)
+                     for _ in range(1 if pattern == "aa" else 2)]
         self._cur = 0
         self.steps_done = 0
         self.step_offset = 0          # steps completed before the last load()/resume()
@@ -232,7 +241,11 @@ class LBMSolver:
         self._f0 = f.clone()
         lib = _lib.load()
         dc = self.cfg.desc(_lib.F64 if self.storage == "f64" else _lib.F32)
-        if self.storage in ("f32", "f64"):
+        if self.pattern == "aa":
+            da = self._attach(self.cfg.desc(self.code))
+            _lib.check(lib.tlbm_aa_load(ctypes.byref(da), f.data_ptr(), self._buf[0].data_ptr(), _lib.ptr(self.flags),
+                                        _lib.ptr(self.tau_field), self._stream()), "aa_load")
+        elif self.storage in ("f32", "f64"):
             _lib.check(lib.tlbm_collide(ctypes.byref(dc), dc.dtype, f.data_ptr(), self._buf[0].data_ptr(), _lib.ptr(self.flags),
                                         _lib.ptr(self.tau_field), self._stream()), "collide")
         else:
@@ -242,15 +255,15 @@ class LBMSolver:
             conv = self.cfg.desc(_lib.F32, "none")
             _lib.check(lib.tlbm_collide(ctypes.byref(conv), self.code, tmp.data_ptr(), self._buf[0].data_ptr(), None,
                                         None, self._stream()), "convert")
-        self._cur = 0
+        self._cur = 2 if self.pattern == "aa" else 0   # AA: the loaded layout
         self.steps_done = 0
         self.step_offset = 0
         self.forces = []
         self._graph = None
         return self
 
-    def resume(self, populations: torch.Tensor, *, step: int = 0,
-               stored_state: torch.Tensor | None = None) -> "LBMSolver":
+    def resume(self, populations: torch.Tensor, *, step: int = 0, stored_state: torch.Tensor | None = None,
+               aa_layout: int | None = None) -> "LBMSolver":
         """Continue a run from a checkpoint.
 
         populations: the TensorLBM-phase field S_n (what ``f`` returned when it
@@ -267,6 +280,10 @@ class LBMSolver:
                 raise ValueError(f"stored_state {tuple(stored_state.shape)} {stored_state.dtype} does not match "
                                  f"this solver's {tuple(buf.shape)} {buf.dtype} ({self.storage} storage)")
             buf.copy_(stored_state.to(self.device))
+            if self.pattern == "aa":
+                if aa_layout not in (0, 1, 2):
+                    raise ValueError("an AA stored state needs its layout (0 swapped, 1 natural, 2 loaded)")
+                self._cur = int(aa_layout)
         self.step_offset = int(step)
         return self
 
@@ -281,6 +298,16 @@ class LBMSolver:
                                    self._stream())
         _lib.check(st, "tlbm_step")
 
+    def _launch_parity(self, c: int, force: torch.Tensor | None) -> None:
+        """One step from parity c: the current buffer (two buffers) or the layout (AA)."""
+        if self.pattern == "aa":
+            st = _lib.load().tlbm_step_aa(ctypes.byref(self._desc), self._buf[0].data_ptr(), c, _lib.ptr(self.flags),
+                                          _lib.ptr(self.tau_field), _lib.ptr(force), self.status.data_ptr(),
+                                          self._stream())
+            _lib.check(st, "tlbm_step_aa")
+        else:
+            self._launch(self._buf[c], self._buf[1 - c], force)
+
     def step(self, n: int = 1) -> "LBMSolver":
         """Advance n time steps (n fused kernel launches)."""
         if self._f0 is None:
@@ -290,10 +317,15 @@ class LBMSolver:
             if self.track_force:
                 force = torch.zeros(3, dtype=torch.float64, device=self.device)
                 self.forces.append(force)
-            self._launch(self._buf[self._cur], self._buf[1 - self._cur], force)
-            self._cur ^= 1
+            self._launch_parity(self._cur, force)
+            self._cur = self._next_parity(self._cur)
             self.steps_done += 1
         return self
+
+    def _next_parity(self, c: int) -> int:
+        if self.pattern == "aa":
+            return 1 if c == 0 else 0   # loaded / natural -> swapped, swapped -> natural
+        return c ^ 1
 
     def set_force_lin(self, a: float) -> "LBMSolver":
         """Change the linear body force A of F = A rho u (drops the captured graph)."""
@@ -308,6 +340,10 @@ class LBMSolver:
         Force tracking records one force per step, so it runs eagerly."""
         if not graph or self.track_force or n < chunk:
             return self.step(n)
+        if self.pattern == "aa" and self._cur == 2:
+            # leave the loaded layout eagerly: the graph then cycles swapped <-> natural
+            self.step(1)
+            n -= 1
         if self._graph is None or self._graph[1] != chunk or self._graph[2] != self._cur:
             # capture `chunk` (even) steps starting from the current buffer parity
             chunk = chunk + (chunk & 1)
@@ -319,8 +355,8 @@ class LBMSolver:
                 with torch.cuda.graph(g, stream=s):
                     c = cur0
                     for _ in range(chunk):
-                        self._launch(self._buf[c], self._buf[1 - c], None)
-                        c ^= 1
+                        self._launch_parity(c, None)
+                        c = self._next_parity(c)
             torch.cuda.current_stream(self.device).wait_stream(s)
             self._graph = (g, chunk, cur0)
         g, chunk, _ = self._graph
@@ -334,8 +370,15 @@ class LBMSolver:
 
     @property
     def state(self) -> torch.Tensor:
-        """Stored post-collision populations P_n (storage format: (f - w) 2^14 for f16, f - w for bf16)."""
-        return self._buf[self._cur]
+        """Stored post-collision populations P_n (storage format: (f - w) 2^14 for f16, f - w for bf16);
+        for the AA pattern the raw buffer, in the layout ``aa_layout``."""
+        return self._buf[0] if self.pattern == "aa" else self._buf[self._cur]
+
+    @property
+    def aa_layout(self) -> int | None:
+        """AA pattern: 0 swapped (post-collision), 1 natural (streamed, not yet bounded),
+        2 loaded (S_0 as loaded); None for two buffers."""
+        return self._cur if self.pattern == "aa" else None
 
     @property
     def f(self) -> torch.Tensor:
@@ -345,6 +388,11 @@ class LBMSolver:
         if self.steps_done == 0:
             return self._f0.clone()
         out = torch.empty((self.q,) + self.cfg.shape, dtype=self.compute_dtype, device=self.device)
+        if self.pattern == "aa":
+            st = _lib.load().tlbm_aa_populations(ctypes.byref(self._desc), self._buf[0].data_ptr(), self._cur,
+                                                 _lib.ptr(self.flags), out.data_ptr(), None, self._stream())
+            _lib.check(st, "aa_populations")
+            return out
         prev = self._buf[1 - self._cur]
         if self.storage in ("f32", "f64"):
             st = _lib.load().tlbm_step(ctypes.byref(self._desc_none), prev.data_ptr(), out.data_ptr(),
@@ -363,15 +411,29 @@ class LBMSolver:
 
     def moment_sums(self) -> torch.Tensor:
         """float64 (mass, jx, jy, jz) of the stored post-collision state."""
-        return _ops.moment_sums(self.q, self.state, self.code)
+        sums = _ops.moment_sums(self.q, self.state, self.code)
+        if self.pattern == "aa" and self._cur == 0:
+            sums[1:] = -sums[1:]   # swapped layout: slot opp(q) holds population q
+        return sums   # AA: of the latest collided state, one collision behind the two-buffer step
 
     def nonfinite_seen(self) -> bool:
         """True if any step produced a non-finite density (reads one int)."""
         return bool(self.status.item() != 0)
 
     def force_history(self) -> torch.Tensor:
+        """float64 force of every recorded step (row k: step k + 1 since the last load)."""
         if not self.forces:
             return torch.zeros((0, 3), dtype=torch.float64, device=self.device)
+        if self.pattern == "aa":
+            # AA launch k samples step k - 1: drop the sample of the loaded
+            # state and take the latest step's from a readout of the buffer
+            last = torch.zeros(3, dtype=torch.float64, device=self.device)
+            tmp = torch.empty((self.q,) + self.cfg.shape, dtype=self.compute_dtype, device=self.device)
+            st = _lib.load().tlbm_aa_populations(ctypes.byref(self._desc), self._buf[0].data_ptr(), self._cur,
+                                                 _lib.ptr(self.flags), tmp.data_ptr(), last.data_ptr(),
+                                                 self._stream())
+            _lib.check(st, "aa_populations")
+            return torch.stack(self.forces[1:] + [last])
         return torch.stack(self.forces)
 
 
