@@ -132,12 +132,12 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 
 
-def _make_solver(torch, dev, lattice, collision, storage, track_force):
+def _make_solver(torch, dev, lattice, collision, storage, track_force, pattern="ab"):
     from tensorlbm_b200 import LBMSolver, boundaries3d
 
     obst = boundaries3d.sphere_mask(NX, NY, NZ, CX, CY, CZ, D / 2, dev)
     s = LBMSolver(lattice, (NZ, NY, NX), TAU, collision, device=dev, storage=storage, obstacle_mask=obst,
-                  u_in=U_IN, rho_out=1.0, track_force=track_force)
+                  u_in=U_IN, rho_out=1.0, track_force=track_force, pattern=pattern)
     return s, obst
 
 
@@ -158,15 +158,15 @@ def _time_steps(torch, s, steps, warmup, force_buf):
 
     cur = torch.cuda.current_stream(s.device)
     for _ in range(warmup):
-        s._launch(s._buf[s._cur], s._buf[1 - s._cur], force_buf)
-        s._cur ^= 1
+        s._launch_parity(s._cur, force_buf)
+        s._cur = s._next_parity(s._cur)
     torch.cuda.synchronize(s.device)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(cur)
     for _ in range(steps):
-        s._launch(s._buf[s._cur], s._buf[1 - s._cur], force_buf)
-        s._cur ^= 1
+        s._launch_parity(s._cur, force_buf)
+        s._cur = s._next_parity(s._cur)
     e1.record(cur)
     torch.cuda.synchronize(s.device)
     s.steps_done += steps + warmup
@@ -174,8 +174,8 @@ def _time_steps(torch, s, steps, warmup, force_buf):
     return e0.elapsed_time(e1) / 1e3
 
 
-def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_cell, peak):
-    s, obst = _make_solver(torch, dev, lattice, collision, storage, False)
+def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_cell, peak, pattern="ab"):
+    s, obst = _make_solver(torch, dev, lattice, collision, storage, False, pattern)
     s.load(_initial_state(torch, dev, lattice, obst))
     force = torch.zeros(3, dtype=torch.float64, device=dev)
     t = _time_steps(torch, s, steps, warmup, force)
@@ -185,8 +185,11 @@ def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_c
     finite = not s.nonfinite_seen()
     del s
     torch.cuda.empty_cache()
-    return {"mlups": round(mlups, 1), "ms_per_step": round(1e3 * t / steps, 4), "achieved_gbs": round(gbs, 1),
-            "roofline_frac": round(gbs / peak, 4), "bytes_per_cell": bytes_per_cell, "finite": finite}
+    out = {"mlups": round(mlups, 1), "ms_per_step": round(1e3 * t / steps, 4), "achieved_gbs": round(gbs, 1),
+           "roofline_frac": round(gbs / peak, 4), "bytes_per_cell": bytes_per_cell, "finite": finite}
+    if pattern == "aa":
+        out["pattern"] = "aa (one population buffer, in place)"
+    return out
 
 
 def _les_variant(torch, dev, steps, warmup, peak, n_mlp=128, n_smag=256):
@@ -551,6 +554,10 @@ def run_ours(args) -> None:
                        ("d3q19_mrt_f16_shifted", None), ("d3q27_cumulant_f16_shifted", "d3q27_cumulant_f32")):
         if half in variants and full in variants:
             variants[half]["speedup_vs_f32"] = round(variants[half]["mlups"] / variants[full]["mlups"], 3)
+    for name, lat, coll, st, bpc_v in (("d3q19_mrt_f32_aa", "D3Q19", "mrt", "f32", bpc),
+                                       ("d3q19_bgk_f16_shifted_aa", "D3Q19", "bgk", "f16", 2 * 19 * 2)):
+        if want(name):
+            variants[name] = _variant(torch, dev, lat, coll, st, args.steps, args.warmup, bpc_v, peak, "aa")
     if want("les_mlp_128_vs_smagorinsky_256"):
         variants["les_mlp_128_vs_smagorinsky_256"] = _les_variant(torch, dev, args.steps, args.warmup, peak)
     if want("d2q9_batched_512_cylinders"):

@@ -107,6 +107,134 @@ __global__ void __launch_bounds__(256) k_step_aa(StepParams p, CollideParams<typ
   }
 }
 
+// The two AA steps with two cells per thread ((x, x + 1), x even), as the
+// two-buffer pair kernel does it: 32-bit offsets from a base at direction
+// Q/2, vector accesses where both cells' slots are adjacent (every access of
+// an even step; the c_x = 0 directions of an odd step), two scalar accesses
+// otherwise.  Same per-cell path and the same packed stochastic rounding as
+// k_step_x2.  Requires what pair_layout_ok checks.
+template <class L, typename S, int COLL, int READ, int WRITE, bool FORCED = false>
+__global__ void __launch_bounds__(256) k_step_aa_x2(StepParams p, CollideParams<typename Storage<S>::T> cp,
+                                                    BcParams<typename Storage<S>::T> bp) {
+  using T = typename Storage<S>::T;
+  using IO = PairIO<S>;
+  using V = typename IO::V;
+  constexpr int Q = L::Q;
+  constexpr int MID = Q / 2;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool active = (x < nx) && (y < ny);
+  const int plane = nx * ny;
+  const int N = int(p.n);
+  const int c = z * plane + y * nx + x;
+  Domain<S, S> d;
+  d.fin = static_cast<const S*>(p.f_in);
+  d.fout = static_cast<S*>(p.f_out);
+  d.flags = p.flags;
+  d.tau_field = p.tau_field;
+  d.force = p.force;
+  d.status = p.status;
+  d.wall_u = p.wall_velocity;
+  d.link_row = nullptr;
+  d.link_q = nullptr;
+  d.nx = nx;
+  d.ny = ny;
+  d.nz = nz;
+  d.plane = p.plane;
+  d.n = p.n;
+  d.bc = p.bc;
+  // row deltas to y -+ 1 and z -+ 1 (periodic) and the x deltas of the pair
+  const int dym = (y == 0) ? (ny - 1) * nx : -nx;
+  const int dyp = (y == ny - 1) ? -(ny - 1) * nx : nx;
+  const int dzm = (L::DIM == 3) ? ((z == 0) ? (nz - 1) * plane : -plane) : 0;
+  const int dzp = (L::DIM == 3) ? ((z == nz - 1) ? -(nz - 1) * plane : plane) : 0;
+  const int dxm = (x == 0) ? nx - 1 : -1;      // x - 1
+  const int dxp = (x + 2 == nx) ? 2 - nx : 2;  // x + 2
+  // offset of the row of (x, y, z) + sign * c_q
+  const auto row = [&](int q, int sign) -> int {
+    const int cy = sign * L::cy(q), cz = sign * L::cz(q);
+    return (cy > 0 ? dyp : (cy < 0 ? dym : 0)) + (cz > 0 ? dzp : (cz < 0 ? dzm : 0));
+  };
+  S* __restrict__ base = at_offset(d.fout + (long long)MID * N, c);  // f_in == f_out
+  const S* __restrict__ rbase = base;
+
+  T fa[Q], fb[Q];
+  uint32_t fl2 = 0;
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const T w = weight<L, T>(q);
+      if (READ == kAaReadOwn) {
+        IO::split(__ldg(reinterpret_cast<const V*>(at_offset(rbase, (q - MID) * N))), w, fa[q], fb[q]);
+      } else {
+        // population q of cell x comes from slot opp(q) of x - c_q
+        const int o = (L::opp(q) - MID) * N + row(q, -1);
+        if (L::cx(q) == 0) {
+          IO::split(__ldg(reinterpret_cast<const V*>(at_offset(rbase, o))), w, fa[q], fb[q]);
+        } else if (L::cx(q) > 0) {
+          fa[q] = Storage<S>::load(ldg(at_offset(rbase, o + dxm)), w);
+          fb[q] = Storage<S>::load(ldg(at_offset(rbase, o)), w);
+        } else {
+          fa[q] = Storage<S>::load(ldg(at_offset(rbase, o + 1)), w);
+          fb[q] = Storage<S>::load(ldg(at_offset(rbase, o + dxp)), w);
+        }
+      }
+    }
+    if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));
+  }
+  const uint8_t fla = uint8_t(fl2), flb = uint8_t(fl2 >> 8);
+  if (d.force) {
+    const bool oa = active && (fla & TLBM_FLAG_OBSTACLE), ob = active && (flb & TLBM_FLAG_OBSTACLE);
+    double mx = 0.0, my = 0.0, mz = 0.0;
+    if (oa) {
+      T ax, ay, az;
+      cell_momentum<L>(fa, ax, ay, az);
+      mx = double(ax), my = double(ay), mz = double(az);
+    }
+    if (ob) {
+      T bx, by, bz;
+      cell_momentum<L>(fb, bx, by, bz);
+      mx += double(bx), my += double(by), mz += double(bz);
+    }
+    accumulate_force(d.force, __any_sync(0xffffffffu, oa || ob), mx, my, mz);
+  }
+  if (!active) return;
+  double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
+  apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+  apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+  relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
+  relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
+  uint32_t ha = 0, hb = 0;
+  if constexpr (Storage<S>::kShifted) {
+    ha = (fa[0] - fa[0] == T(0)) ? fmix32(uint32_t(c) * 0x9E3779B9u ^ __float_as_uint(float(fa[0]))) : 0u;
+    hb = (fb[0] - fb[0] == T(0)) ? fmix32(uint32_t(c + 1) * 0x9E3779B9u ^ __float_as_uint(float(fb[0]))) : 0u;
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const V v = IO::join(fa[q], fb[q], weight<L, T>(q), ha, hb, q);
+    if (WRITE == kAaWriteSwapped) {
+      __stwb(reinterpret_cast<V*>(at_offset(base, (L::opp(q) - MID) * N)), v);
+    } else {
+      // population q of cell x goes to slot q of x + c_q
+      const int o = (q - MID) * N + row(q, 1);
+      if (L::cx(q) == 0) {
+        __stwb(reinterpret_cast<V*>(at_offset(base, o)), v);
+      } else {
+        const S* parts = reinterpret_cast<const S*>(&v);
+        if (L::cx(q) > 0) {
+          *at_offset(base, o + 1) = parts[0];
+          *at_offset(base, o + dxp) = parts[1];
+        } else {
+          *at_offset(base, o + dxm) = parts[0];
+          *at_offset(base, o) = parts[1];
+        }
+      }
+    }
+  }
+}
+
 template <class L, typename SI, typename SO, int COLL, int READ, int WRITE, int BC, bool FORCED = false>
 int launch_aa(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   using T = typename Storage<SI>::T;
@@ -119,6 +247,19 @@ int launch_aa(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   if (d.cm_s5 >= 0.0) cp.cm_s5 = T(d.cm_s5);
   if (d.cm_s6 >= 0.0) cp.cm_s6 = T(d.cm_s6);
   const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
+  // the two unforced steps (boundaries, same storage, own-swapped or
+  // gather-scatter) run two cells per thread when the layout allows it;
+  // forced steps keep one cell per thread, as the two-buffer step does
+  constexpr bool kStep = BC == kAaBc && !FORCED && std::is_same<SI, SO>::value && COLL != TLBM_COLL_NONE &&
+                         ((READ == kAaReadOwn && WRITE == kAaWriteSwapped) ||
+                          (READ == kAaReadGather && WRITE == kAaWriteScatter));
+  if constexpr (kStep) {
+    if (pair_layout_ok<L, SI>(p)) {
+      step_launch_shape(p.nx / 2, p.ny, p.nz, grid, block);
+      k_step_aa_x2<L, SI, COLL, READ, WRITE, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
+      return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
+    }
+  }
   k_step_aa<L, SI, SO, COLL, READ, WRITE, BC, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }

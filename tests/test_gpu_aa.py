@@ -54,6 +54,21 @@ def test_aa_forced_and_odd_nx(cuda):
     assert torch.equal(aa.f, ab.f)
 
 
+@pytest.mark.parametrize("q,coll,steps", [(19, "mrt", 7), (27, "cumulant", 8)])
+def test_aa_one_cell_per_thread(cuda, q, coll, steps):
+    """Odd nx: the AA steps take one cell per thread, the even-nx runs above
+    two; both match the two-buffer step bit for bit."""
+    ab, aa = _sphere_channel(cuda, q, coll, steps, nx=23)
+    assert torch.equal(aa.f, ab.f)
+
+
+def test_aa_pair_forced_rows(cuda):
+    """Forced steps on an even nx keep one cell per thread; the unforced pair
+    steps around them must agree with it."""
+    ab, aa = _sphere_channel(cuda, 19, "mrt", 10, force_lin=2e-5)
+    assert torch.equal(aa.f, ab.f)
+
+
 def test_aa_d2q9_walls(cuda):
     from tensorlbm_b200 import LBMSolver
 
