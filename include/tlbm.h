@@ -472,6 +472,21 @@ TLBM_API int tlbm_sphere_links(int32_t lattice, int32_t nx, int32_t ny, int32_t 
 TLBM_API int tlbm_bfl_bounce_back(const tlbm_desc* d, const void* f, const void* f_prev, const uint8_t* link_mask,
                                   const float* q_field, void* f_out, double* force, void* stream);
 
+/* ---- link-wise momentum exchange (MEM drag variants) -----------------------
+ * tlbm_link_momentum_sums: for every cell x with near[x] != 0 and every
+ * direction q >= 1 whose periodic neighbour x + c_q has solid != 0,
+ *   sums[q]     += (f_q(x) + f_opp(q)(x + c_q)) * w   (in d->dtype, summed in float64)
+ *   sums[Q + q] += 1
+ * with w = 1 when q_wall is NULL, else w = 1 / max(q_wall, 1e-6) in float32,
+ * q_wall (nz, ny, nx) or, with q_wall_per_direction != 0, (Q, nz, ny, nx).
+ * sums (2Q float64) is zeroed first.  f is (Q, nz, ny, nx), post-streaming;
+ * d->lattice, d->dtype (F32 / F64) and d->nx/ny/nz are read.  The forces of
+ * momentum_exchange_standard (momentum_exchange.py:75), _galilean (:138),
+ * _background_subtracted (:206) and _bfl (:285) are sum_q c_q times sums[q]
+ * (times 1 + 1/(2 tau); minus the background per link times sums[Q + q]). */
+TLBM_API int tlbm_link_momentum_sums(const tlbm_desc* d, const void* f, const uint8_t* solid, const uint8_t* near,
+                                     const float* q_wall, int32_t q_wall_per_direction, double* sums, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

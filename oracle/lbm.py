@@ -674,6 +674,65 @@ def bfl_chain_step(f: np.ndarray, tau: float, solid: np.ndarray, mask: np.ndarra
     return bfl_bounce_back(stream(g), g, mask, qf), bfl_force(g, mask, qf)
 
 
+# ---------------------------------------------------------------------------
+# Link-wise momentum exchange (MEM drag variants)
+# ---------------------------------------------------------------------------
+
+def _roll_to_neighbour(a: np.ndarray, c) -> np.ndarray:
+    """a[x + c] with periodic wrap (torch.roll(a, -c) in momentum_exchange.py:53-70)."""
+    if a.ndim == 2:
+        return np.roll(a, shift=(-int(c[1]), -int(c[0])), axis=(0, 1))
+    return np.roll(a, shift=(-int(c[2]), -int(c[1]), -int(c[0])), axis=(0, 1, 2))
+
+
+def link_momentum_sums(f: np.ndarray, solid: np.ndarray, near: np.ndarray, q_wall=None) -> np.ndarray:
+    """Per direction q >= 1 over the fluid->solid links (near[x] and
+    solid[x + c_q]): the sum of (f_q(x) + f_opp(x + c_q)), weighted by
+    1 / max(q_wall, 1e-6) (float32) when q_wall is given, and the link count.
+    Per-link values in f's dtype, the sums in float64 (momentum_exchange.py:75-360
+    sums each direction in f's dtype).  Returns 2Q float64."""
+    q = f.shape[0]
+    opp = opposite(q)
+    out = np.zeros(2 * q)
+    inv = None
+    if q_wall is not None:
+        inv = (np.float32(1.0) / np.maximum(q_wall.astype(np.float32), np.float32(1e-6))).astype(np.float32)
+    for i in range(1, q):
+        link = near & _roll_to_neighbour(solid, C[q][i])
+        val = f[i] + _roll_to_neighbour(f[opp[i]], C[q][i])
+        if inv is not None:
+            w = inv[i] if inv.ndim == f.ndim else inv
+            val = val * w.astype(f.dtype)
+        out[i] = val[link].astype(np.float64).sum()
+        out[q + i] = float(link.sum())
+    return out
+
+
+def mem_force(sums: np.ndarray, variant: str = "standard", tau: float = 1.0, rho0: float = 1.0,
+              u0=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Force on the wall from the link sums: standard Ladd sum (momentum_exchange.py:75),
+    Galilean factor 1 + 1/(2 tau) (:138), the uniform-stream background
+    2 rho0 w_q (1 + 4.5 (c_q.u0)^2 - 1.5 |u0|^2) per link removed (:206, with
+    the float32 weights of the reference);
+    "bfl" is the standard form of the 1/q-weighted sums (:285)."""
+    q = sums.size // 2
+    c = C[q].astype(np.float64)
+    s = sums[:q].copy()
+    if variant == "galilean":
+        s = s * (1.0 + 1.0 / (2.0 * tau))
+    elif variant == "background":
+        u = np.zeros(3)
+        u[:len(u0)] = u0
+        cu = c @ u[:c.shape[1]]
+        w32 = W64[q].astype(np.float32).astype(np.float64)       # W.float() in the reference
+        bg = 2.0 * rho0 * w32 * (1.0 + 4.5 * cu * cu - 1.5 * float(u @ u))
+        s = s - bg * sums[q:]
+    elif variant not in ("standard", "bfl"):
+        raise ValueError(f"unknown MEM variant {variant!r}")
+    s[0] = 0.0
+    return (c * s[:, None]).sum(axis=0)
+
+
 def moving_wall_bounce_back(f: np.ndarray, mask: np.ndarray, *wall_u: np.ndarray) -> np.ndarray:
     """Ladd moving wall: where(mask, bounce_back(f) + ((2 w_q) rho) (c_q . u_w) 3, f),
     rho = sum0(f), the float32 W tensor cast to f's dtype for both lattices and

@@ -117,6 +117,7 @@ SIGNATURES: dict[str, list] = {
     "tlbm_step_aa": [ctypes.POINTER(Desc), _P, _I32, _P, _P, _P, _P, _P],
     "tlbm_aa_populations": [ctypes.POINTER(Desc), _P, _I32, _P, _P, _P, _P],
     "tlbm_bfl_bounce_back": [ctypes.POINTER(Desc), _P, _P, _P, _P, _P, _P, _P],
+    "tlbm_link_momentum_sums": [ctypes.POINTER(Desc), _P, _P, _P, _P, _I32, _P, _P],
     "tlbm_link_list_static_capacity": [],
     "tlbm_les_filter_moments": [_P, _I32, _I32, _I32, _I32, _D, _P, _P],
     "tlbm_les_samples": [_P, _I32, _I32, _I32, _D, _D, _P, _P, _P, _P, _P],

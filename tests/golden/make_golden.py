@@ -219,6 +219,45 @@ def cascaded(torch) -> None:
     print("wrote collide_cascaded.npz")
 
 
+def mem(torch) -> None:
+    """Link-wise momentum-exchange drag variants (momentum_exchange.py:75, :138,
+    :206, :285) on a seeded field: a sphere plus a wall plane at x = nx - 1
+    (links that cross the periodic x face), the near-wall mask restricted to
+    z < nz - 3 so that the uniform-stream background does not cancel, scalar and
+    per-direction wall fractions with zeros (the 1e-6 clamp)."""
+    from tensorlbm import momentum_exchange as me
+
+    nz, ny, nx = 12, 14, 16
+    zz, yy, xx = torch.meshgrid(*(torch.arange(n, dtype=torch.float64) for n in (nz, ny, nx)), indexing="ij")
+    solid = ((xx - 6.3) ** 2 + (yy - 7.1) ** 2 + (zz - 5.6) ** 2) <= 3.4 ** 2
+    solid[:, :, nx - 1] = True
+    any_solid = torch.zeros_like(solid)
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                any_solid |= torch.roll(solid, (dz, dy, dx), dims=(0, 1, 2))
+    near = any_solid & ~solid
+    near[nz - 3:] = False
+    g = torch.Generator().manual_seed(81)
+    q_scalar = torch.rand((nz, ny, nx), generator=g)
+    q_scalar[q_scalar < 0.05] = 0.0
+    q_dir = torch.rand((19, nz, ny, nx), generator=g)
+    q_dir[q_dir < 0.05] = 0.0
+    out = dict(solid=solid, near=near, q_scalar=q_scalar, q_dir=q_dir)
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        _, _, f = near_eq_field(torch, 19, (nz, ny, nx), dt, 82)
+        out[f"f_{tag}"] = f
+        out[f"standard_{tag}"] = torch.tensor(me.momentum_exchange_standard(f, solid, near), dtype=torch.float64)
+        out[f"galilean_{tag}"] = torch.tensor(me.momentum_exchange_galilean(f, solid, near, 0.6), dtype=torch.float64)
+        out[f"background_{tag}"] = torch.tensor(
+            me.momentum_exchange_background_subtracted(f, solid, near, rho0=1.02, u0=(0.05, 0.01, -0.02)),
+            dtype=torch.float64)
+        out[f"bfl_scalar_{tag}"] = torch.tensor(me.momentum_exchange_bfl(f, solid, near, q_scalar), dtype=torch.float64)
+        out[f"bfl_dir_{tag}"] = torch.tensor(me.momentum_exchange_bfl(f, solid, near, q_dir), dtype=torch.float64)
+    np.savez_compressed(HERE / "mem.npz", **{k: v.numpy() for k, v in out.items()})
+    print(f"wrote mem.npz; links {int(near.sum())} near cells")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -243,6 +282,9 @@ def main() -> None:
         return
     if args.only == "cascaded":
         cascaded(torch)
+        return
+    if args.only == "mem":
+        mem(torch)
         return
     from tensorlbm import boundaries as b2
     from tensorlbm import boundaries3d as b3

@@ -214,3 +214,23 @@ def test_collide_cascaded():
             assert np.max(np.abs(O.collide_cascaded(f, 0.6) - g[f"c{q}_{tag}"])) < tol * np.max(np.abs(f))
             kw = dict(s_bulk=1.2, s_3=0.9, s_4=1.3) if q == 19 else dict(s_bulk=1.2, s_3=0.9, s_4=1.3, s_5=1.1, s_6=0.8)
             assert np.max(np.abs(O.collide_cascaded(f, 0.57, **kw) - g[f"c{q}r_{tag}"])) < tol * np.max(np.abs(f))
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_mem_variants_against_reference(tag):
+    """Standard, Galilean, background-subtracted and BFL-weighted link-wise
+    momentum exchange (momentum_exchange.py:75-360).  The reference sums each
+    direction in the populations' dtype, the oracle in float64: the bound is a
+    few units in the last place of the per-direction sums."""
+    g = golden("mem")
+    f, solid, near = g[f"f_{tag}"], g["solid"], g["near"]
+    eps = 2e-7 if tag == "f32" else 1e-13
+    cases = {"standard": (None, dict()), "galilean": (None, dict(variant="galilean", tau=0.6)),
+             "background": (None, dict(variant="background", rho0=1.02, u0=(0.05, 0.01, -0.02))),
+             "bfl_scalar": (g["q_scalar"], dict(variant="bfl")), "bfl_dir": (g["q_dir"], dict(variant="bfl"))}
+    for name, (qw, kw) in cases.items():
+        sums = O.link_momentum_sums(f, solid, near, qw)
+        got = O.mem_force(sums, **kw)
+        tol = eps * 2.0 * np.abs(sums[:19]).sum()
+        assert np.abs(got - g[f"{name}_{tag}"]).max() <= tol, name
+    assert O.link_momentum_sums(f, solid, near)[19:].sum() > 100          # links on the sphere and the x wall
