@@ -143,6 +143,17 @@ typedef struct tlbm_desc {
 TLBM_API int tlbm_step(const tlbm_desc* d, const void* f_in, void* f_out, const uint8_t* flags,
                        const float* tau_field, double* force, unsigned int* status, void* stream);
 
+/* tlbm_step on the planes z_begin .. z_begin + z_count - 1 only (the others of
+ * f_out are not written); neighbours still wrap periodically over d->nz.  With
+ * one ghost plane on each side of a slab (planes 0 and nz - 1 hold the
+ * neighbouring slabs' boundary planes) and z_begin = 1, z_count = nz - 2, the
+ * owned planes get exactly the values of the undivided domain: the slab step
+ * of the z-decomposed solver (triton_fused_distributed.py:564 runs its kernel
+ * over the ghost planes as well).  force and status cover the updated planes. */
+TLBM_API int tlbm_step_planes(const tlbm_desc* d, const void* f_in, void* f_out, const uint8_t* flags,
+                              const float* tau_field, double* force, unsigned int* status, int32_t z_begin,
+                              int32_t z_count, void* stream);
+
 /* Local collision only (no streaming, no boundaries); f_in may equal f_out.
  * dtype_out may differ from d->dtype only for TLBM_COLL_NONE (format
  * conversion).  flags (may be NULL): TLBM_FLAG_HALFWAY cells are stored

@@ -43,6 +43,8 @@ _PATCHES = {
     "bfl_d3q19": ["bouzidi_bounce_back_d3q19"],
     "triton_fused": ["triton_fused", "triton_collide", "triton_stream", "TritonFusedSolver3D", "is_available"],
     "cascaded_collision": ["collide_cascaded_d3q19", "collide_cascaded_d3q27"],
+    "triton_fused_distributed": ["DistributedTritonFusedSolver3D", "crossing_face_indices", "init_distributed",
+                                 "rank", "world_size", "distributed_is_available"],
     "momentum_exchange": ["momentum_exchange_standard", "momentum_exchange_galilean",
                           "momentum_exchange_background_subtracted", "momentum_exchange_bfl"],
 }

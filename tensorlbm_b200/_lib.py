@@ -89,6 +89,7 @@ _D = ctypes.c_double
 # name -> argtypes (restype int unless listed in _RESTYPES)
 SIGNATURES: dict[str, list] = {
     "tlbm_step": [ctypes.POINTER(Desc), _P, _P, _P, _P, _P, _P, _P],
+    "tlbm_step_planes": [ctypes.POINTER(Desc), _P, _P, _P, _P, _P, _P, _I32, _I32, _P],
     "tlbm_collide": [ctypes.POINTER(Desc), _I32, _P, _P, _P, _P, _P],
     "tlbm_stream": [_I32, _I32, _I32, _I32, _I32, _P, _P, _P],
     "tlbm_equilibrium": [_I32, _I32, _I64, _P, _P, _P, _P, _P, _P],

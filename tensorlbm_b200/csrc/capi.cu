@@ -79,6 +79,8 @@ StepParams make_params(const tlbm_desc& d, const void* fin, void* fout, const ui
   p.nx = d.nx;
   p.ny = d.ny;
   p.nz = d.nz;
+  p.z0 = 0;
+  p.z_count = d.nz;
   p.plane = (long long)d.nx * d.ny;
   p.n = p.plane * d.nz;
   p.bc = d.bc;
@@ -155,6 +157,20 @@ TLBM_API int tlbm_step(const tlbm_desc* d, const void* f_in, void* f_out, const 
   if (!f_in || !f_out) return TLBM_ERR_ARG;
   if (f_in == f_out) return TLBM_ERR_ALIAS;
   const StepParams p = make_params(*d, f_in, f_out, flags, tau_field, force, status);
+  return dispatch(*d, d->dtype, true, p, as_stream(stream));
+}
+
+TLBM_API int tlbm_step_planes(const tlbm_desc* d, const void* f_in, void* f_out, const uint8_t* flags,
+                              const float* tau_field, double* force, unsigned int* status, int32_t z_begin,
+                              int32_t z_count, void* stream) {
+  int st = check_desc(d);
+  if (st != TLBM_OK) return st;
+  if (!f_in || !f_out) return TLBM_ERR_ARG;
+  if (f_in == f_out) return TLBM_ERR_ALIAS;
+  if (z_begin < 0 || z_count < 1 || (long long)z_begin + z_count > d->nz) return TLBM_ERR_SHAPE;
+  StepParams p = make_params(*d, f_in, f_out, flags, tau_field, force, status);
+  p.z0 = z_begin;
+  p.z_count = z_count;
   return dispatch(*d, d->dtype, true, p, as_stream(stream));
 }
 

@@ -231,6 +231,7 @@ struct StepParams {
   const int32_t* link_row;  // CURVED cells: row in link_q, may be null
   const float* link_q;      // (rows, Q) BFL wall fractions, 0 = no link, may be null
   int nx, ny, nz;
+  int z0, z_count;          // the step updates planes [z0, z0 + z_count) (periodic wrap over nz)
   long long plane;          // nx*ny
   long long n;              // nx*ny*nz
   uint32_t bc;              // TLBM_BC_* bits

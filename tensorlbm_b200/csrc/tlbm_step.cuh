@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(256) k_step(StepParams p, CollideParams<typena
                                               BcParams<typename Storage<SI>::T> bp) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
+  const int z = p.z0 + int(blockIdx.z);
   Domain<SI, SO> d;
   d.fin = static_cast<const SI*>(p.f_in);
   d.fout = static_cast<SO*>(p.f_out);
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
+  const int z = p.z0 + int(blockIdx.z);
   const bool active = (x < nx) && (y < ny);
   const int plane = nx * ny;
   const int N = int(p.n);
@@ -421,7 +421,7 @@ template <class L, typename SI, typename SO, int COLL, bool PULL, bool FORCED = 
 int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   using T = typename Storage<SI>::T;
   dim3 grid, block;
-  step_launch_shape(p.nx, p.ny, p.nz, grid, block);
+  step_launch_shape(p.nx, p.ny, p.z_count, grid, block);
   CollideParams<T> cp = make_collide_params<T>(d.tau, d.s_e, d.s_eps, d.s_q, d.s_pi, d.omega_b, d.omega_odd,
                                                d.omega_even, d.c_smag);
   cp.force_a = T(d.force_lin);
@@ -435,7 +435,7 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   // Smagorinsky at 256^3)
   if constexpr (PULL && !FORCED && std::is_same<SI, SO>::value) {
     if (pair_layout_ok<L, SI>(p)) {
-      step_launch_shape(p.nx / 2, p.ny, p.nz, grid, block);
+      step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block);
       k_step_x2<L, SI, COLL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
       return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
     }
