@@ -11,9 +11,14 @@ with D3Q19 MRT on float16 shifted storage ("variants").
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torchrun: each rank advances its own replica (the step does
-not shard; nothing is exchanged), the time is the max over ranks and the value
-is the total cell updates of all ranks per second.  Rank 0 prints one JSON line.
+N > 1 runs under torchrun as a z-slab decomposition of one periodic-in-z
+domain of 512 x 256 x (256 N) cells with one sphere per slab (weak scaling:
+every rank steps a 512 x 256 x 256 slab): each step computes the slab's two
+boundary planes, exchanges their crossing populations (5 lanes per face) with
+the neighbouring ranks over NCCL while the interior planes are computed, and
+the next step waits for that exchange on the stream.  The time is the max over
+ranks and the value is the total cell updates of all ranks per second.  Rank 0
+prints one JSON line.
 
 --impl reference times the CPU implementation of the same step (the numpy
 restatement of TensorLBM's torch operators in oracle/) on the host cores.
@@ -138,6 +143,21 @@ def _make_solver(torch, dev, lattice, collision, storage, track_force, pattern="
     obst = boundaries3d.sphere_mask(NX, NY, NZ, CX, CY, CZ, D / 2, dev)
     s = LBMSolver(lattice, (NZ, NY, NX), TAU, collision, device=dev, storage=storage, obstacle_mask=obst,
                   u_in=U_IN, rho_out=1.0, track_force=track_force, pattern=pattern)
+    return s, obst
+
+
+def _make_headline(torch, dev, world: int, rank: int, track_force: bool = False):
+    """The headline solver: one GPU's domain, or this rank's slab of the
+    z-decomposed domain (the same sphere in every slab) with the halo exchange
+    over the default process group."""
+    if world == 1:
+        return _make_solver(torch, dev, "D3Q19", "mrt", "f32", track_force)
+    from tensorlbm_b200 import boundaries3d
+    from tensorlbm_b200.slabs import SlabSolver
+
+    obst = boundaries3d.sphere_mask(NX, NY, NZ, CX, CY, CZ, D / 2, dev)
+    s = SlabSolver("D3Q19", (NZ * world, NY, NX), TAU, "mrt", device=dev, world=world, rank=rank,
+                   obstacle_mask=obst.repeat(world, 1, 1), u_in=U_IN, rho_out=1.0, track_force=track_force)
     return s, obst
 
 
@@ -444,7 +464,7 @@ def max_over_ranks(t: float, device) -> float:
 
 
 def whole_job_mlups(world: int, cells_per_rank: int, steps: int, t_max: float) -> float:
-    """Cell updates of all ranks (one replica each) per second of the slowest rank, in millions."""
+    """Cell updates of all ranks (one slab each) per second of the slowest rank, in millions."""
     return world * cells_per_rank * steps / t_max / 1e6
 
 
@@ -467,9 +487,9 @@ def run_ours(args) -> None:
     bpc = 2 * 19 * 4
 
     # ---- headline: D3Q19 MRT float32, one fused kernel per step, FP64 drag ----
-    s, obst = _make_solver(torch, dev, "D3Q19", "mrt", "f32", False)
+    s, obst = _make_headline(torch, dev, world, rank)
     f0 = _initial_state(torch, dev, "D3Q19", obst)
-    s.load(f0)
+    s.load(f0)                          # N > 1: this rank's owned planes, ghosts exchanged
     force = torch.zeros(3, dtype=torch.float64, device=dev)
     for _ in range(args.warmup):
         s._launch(s._buf[s._cur], s._buf[1 - s._cur], force)
@@ -484,6 +504,8 @@ def run_ours(args) -> None:
         for _ in range(args.steps):
             s._launch(s._buf[s._cur], s._buf[1 - s._cur], force)
             s._cur ^= 1
+        if world > 1:
+            s.synchronize()             # the last step's halo has landed
         e1.record(cur)
         torch.cuda.synchronize(dev)
     if world > 1:
@@ -505,7 +527,10 @@ def run_ours(args) -> None:
     del f0
     host_out = torch.empty(host_f0.shape, dtype=torch.float32).pin_memory()
     host_drag = torch.empty((args.steps, 3), dtype=torch.float64).pin_memory()
-    s2 = LBMSolver("D3Q19", (NZ, NY, NX), TAU, "mrt", device=dev, obstacle_mask=obst, u_in=U_IN, rho_out=1.0)
+    if world == 1:
+        s2 = LBMSolver("D3Q19", (NZ, NY, NX), TAU, "mrt", device=dev, obstacle_mask=obst, u_in=U_IN, rho_out=1.0)
+    else:
+        s2, _ = _make_headline(torch, dev, world, rank)
     torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
@@ -597,7 +622,10 @@ def run_ours(args) -> None:
             "boundaries": "zou_he velocity inlet x=0, zou_he pressure outlet x=nx-1, periodic y/z, "
                           "full-way bounce-back + FP64 momentum-exchange drag on the sphere",
             "l2": "no flush: the two population buffers are 5.1 GB, 40x the 126 MB L2",
-            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "parallelism": (f"z-slabs x{world}: global grid {NX}x{NY}x{NZ * world}, one sphere per slab, "
+                            f"NCCL halo exchange of the 5 crossing lanes per face every step "
+                            f"({2 * 5 * NX * NY * 4} B sent per rank per step), overlapped with the interior "
+                            f"planes") if world > 1 else "single GPU",
             "drag_fx_last_step": drag,
             "finite": finite,
         },
@@ -620,7 +648,7 @@ def run_ours(args) -> None:
             "what": "pinned host f0 -> device, load (collision pass), K fused steps through LBMSolver with the "
                     "float64 drag copied to pinned host memory every step, final TensorLBM-phase f -> host",
         },
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (3 if world > 1 else 1),
         "clocks": clocks.summary(),
         "variants": variants,
         "cpu_baseline": cpu,
