@@ -185,6 +185,8 @@ __global__ void __launch_bounds__(256) k_step_aa_x2(StepParams p, CollideParams<
     if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));
   }
   const uint8_t fla = uint8_t(fl2), flb = uint8_t(fl2 >> 8);
+  // warp-uniform: does any lane need boundary code (a flag or a condition plane)
+  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || x == 0 || x + 2 == nx || y == ny - 1));
   if (d.force) {
     const bool oa = active && (fla & TLBM_FLAG_OBSTACLE), ob = active && (flb & TLBM_FLAG_OBSTACLE);
     double mx = 0.0, my = 0.0, mz = 0.0;
@@ -201,19 +203,37 @@ __global__ void __launch_bounds__(256) k_step_aa_x2(StepParams p, CollideParams<
     accumulate_force(d.force, __any_sync(0xffffffffu, oa || ob), mx, my, mz);
   }
   if (!active) return;
-  double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-  apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-  apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
-  relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
-  relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
-  uint32_t ha = 0, hb = 0;
-  if constexpr (Storage<S>::kShifted) {
-    ha = (fa[0] - fa[0] == T(0)) ? fmix32(uint32_t(c) * 0x9E3779B9u ^ __float_as_uint(float(fa[0]))) : 0u;
-    hb = (fb[0] - fb[0] == T(0)) ? fmix32(uint32_t(c + 1) * 0x9E3779B9u ^ __float_as_uint(float(fb[0]))) : 0u;
+  if constexpr (!uniform_edge_branch<L, COLL>()) {
+    double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
+    apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+    relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
+    relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
+  } else {
+    bool keep_a = false, keep_b = false;   // half-way wall cells: reversed, not collided
+    if (edge) {
+      double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
+      apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+      apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+      if (fla & TLBM_FLAG_HALFWAY) {
+        bounce_back<L>(fa);
+        keep_a = true;
+      }
+      if (flb & TLBM_FLAG_HALFWAY) {
+        bounce_back<L>(fb);
+        keep_b = true;
+      }
+    }
+    if (!keep_a) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c, fa, cp);
+    if (!keep_b) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c + 1, fb, cp);
   }
+  uint32_t h = 0;
+  if constexpr (Storage<S>::kShifted)
+    h = fmix32(uint32_t(c) * 0x9E3779B9u ^ __float_as_uint(float(fa[0])) ^
+               (__float_as_uint(float(fb[0])) * 0x85EBCA6Bu));
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
-    const V v = IO::join(fa[q], fb[q], weight<L, T>(q), ha, hb, q);
+    const V v = IO::join(fa[q], fb[q], weight<L, T>(q), h, q);
     if (WRITE == kAaWriteSwapped) {
       __stwb(reinterpret_cast<V*>(at_offset(base, (L::opp(q) - MID) * N)), v);
     } else {

@@ -121,22 +121,33 @@ __device__ __forceinline__ bf16_plain ldg(const bf16_plain* p) {
 
 // Two consecutive values of one direction (cells x and x + 1, x even) moved
 // as one aligned vector.  split() converts to the compute type; join()
-// converts back with the stochastic rounding of the half formats, whose
-// random bits come from one 32-bit hash per cell (ha, hb; zero for a
-// non-finite cell, so that NaN / Inf pass unchanged) multiplied by an odd
-// constant per direction q (a multiplicative hash; the top bits are used).
+// converts back with the stochastic rounding of the half formats.  Their
+// random bits come from one 32-bit hash h of the pair and an odd constant per
+// direction q: p = h * M_q mod 2^32 is a bijection of h, so every bit field of
+// p is uniform; p ^ (p >> 13) keeps the fields uniform and mixes the upper
+// bits of p into the low field (the low k bits of p depend only on the low k
+// bits of h).  The high word of h * M_q would not do: it is uniform on
+// [0, M_q) only, which leaves its top bits biased for a small M_q.
 __device__ __forceinline__ uint32_t direction_mix(int q) { return 0x9E3779B9u * uint32_t(2 * q + 1); }
+__device__ __forceinline__ uint32_t pair_bits(uint32_t h, int q) {
+  const uint32_t p = h * direction_mix(q);
+  return p ^ (p >> 13);
+}
 
-// cvt.rz.{f16,bf16}x2.f32 d, a, b puts the conversion of a in the upper half
-// of d and of b in the lower half (the lower half is the lower address).
-__device__ __forceinline__ uint32_t cvt_rz_f16x2(float lo, float hi) {
+// Stochastic rounding in hardware (sm_100a, PTX ISA 8.7):
+// cvt.rs.{f16,bf16}x2.f32 d, a, b, rbits puts a in the upper half and b in the
+// lower half of d; the f32 bits below the kept mantissa plus a field of rbits
+// (f16: rbits[28:16] for a, rbits[12:0] for b; bf16: rbits[31:16] and
+// rbits[15:0]) carry into the kept mantissa, then the rest is truncated: the
+// magnitude rounds up with probability equal to the dropped fraction.
+__device__ __forceinline__ uint32_t cvt_rs_f16x2(float lo, float hi, uint32_t rbits) {
   uint32_t r;
-  asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi), "f"(lo), "r"(rbits));
   return r;
 }
-__device__ __forceinline__ uint32_t cvt_rz_bf16x2(float lo, float hi) {
+__device__ __forceinline__ uint32_t cvt_rs_bf16x2(float lo, float hi, uint32_t rbits) {
   uint32_t r;
-  asm("cvt.rz.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi), "f"(lo), "r"(rbits));
   return r;
 }
 
@@ -144,12 +155,12 @@ template <typename S> struct PairIO;
 template <> struct PairIO<float> {
   using V = float2;
   __device__ __forceinline__ static void split(V v, float, float& a, float& b) { a = v.x; b = v.y; }
-  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, uint32_t, int) { return make_float2(a, b); }
+  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, int) { return make_float2(a, b); }
 };
 template <> struct PairIO<double> {
   using V = double2;
   __device__ __forceinline__ static void split(V v, double, double& a, double& b) { a = v.x; b = v.y; }
-  __device__ __forceinline__ static V join(double a, double b, double, uint32_t, uint32_t, int) {
+  __device__ __forceinline__ static V join(double a, double b, double, uint32_t, int) {
     return make_double2(a, b);
   }
 };
@@ -161,13 +172,10 @@ template <> struct PairIO<__half> {
     a = fmaf(t.x, 1.0f / kScale, w);
     b = fmaf(t.y, 1.0f / kScale, w);
   }
-  // (v - w) * 2^14 rounded once (the scaling is exact), plus 13 random bits
-  // below the kept mantissa, truncated: the same format as Storage::store
-  __device__ __forceinline__ static V join(float a, float b, float w, uint32_t ha, uint32_t hb, int q) {
-    const uint32_t m = direction_mix(q);
-    const uint32_t ba = __float_as_uint(fmaf(a, kScale, -w * kScale)) + ((ha * m) >> 19);
-    const uint32_t bb = __float_as_uint(fmaf(b, kScale, -w * kScale)) + ((hb * m) >> 19);
-    return cvt_rz_f16x2(__uint_as_float(ba), __uint_as_float(bb));
+  // (v - w) * 2^14 rounded once (the scaling is exact), then stochastically
+  // rounded to f16: the format of Storage::store
+  __device__ __forceinline__ static V join(float a, float b, float w, uint32_t h, int q) {
+    return cvt_rs_f16x2(fmaf(a, kScale, -w * kScale), fmaf(b, kScale, -w * kScale), pair_bits(h, q));
   }
 };
 template <> struct PairIO<__nv_bfloat16> {
@@ -176,11 +184,8 @@ template <> struct PairIO<__nv_bfloat16> {
     a = __uint_as_float(v << 16) + w;
     b = __uint_as_float(v & 0xFFFF0000u) + w;
   }
-  __device__ __forceinline__ static V join(float a, float b, float w, uint32_t ha, uint32_t hb, int q) {
-    const uint32_t m = direction_mix(q);
-    const uint32_t ba = __float_as_uint(a - w) + ((ha * m) >> 16);
-    const uint32_t bb = __float_as_uint(b - w) + ((hb * m) >> 16);
-    return cvt_rz_bf16x2(__uint_as_float(ba), __uint_as_float(bb));
+  __device__ __forceinline__ static V join(float a, float b, float w, uint32_t h, int q) {
+    return cvt_rs_bf16x2(a - w, b - w, pair_bits(h, q));
   }
 };
 
@@ -191,7 +196,7 @@ template <> struct PairIO<f16_plain> {
     a = t.x;
     b = t.y;
   }
-  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, uint32_t, int) {
+  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, int) {
     const __half2 h = __floats2half2_rn(a, b);
     return *reinterpret_cast<const V*>(&h);
   }
@@ -202,7 +207,7 @@ template <> struct PairIO<bf16_plain> {
     a = __uint_as_float(v << 16);
     b = __uint_as_float(v & 0xFFFF0000u);
   }
-  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, uint32_t, int) {
+  __device__ __forceinline__ static V join(float a, float b, float, uint32_t, int) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<const V*>(&h);
   }

@@ -145,17 +145,32 @@ __device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x,
   }
 }
 
+template <class L, typename SI, typename SO, int COLL, bool FORCED, typename T>
+__device__ __forceinline__ void relax_fluid(const Domain<SI, SO>& d, long long cell, T (&f)[L::Q],
+                                            const CollideParams<T>& cp);
+
 // Collision of one cell (or the reversal of a half-way wall cell), the
 // optional exact-difference linear force, and the non-finite status bit.
 template <class L, typename SI, typename SO, int COLL, bool FORCED, typename T>
 __device__ __forceinline__ void relax(const Domain<SI, SO>& d, long long cell, uint8_t fl, T (&f)[L::Q],
                                       const CollideParams<T>& cp) {
-  constexpr int Q = L::Q;
   if constexpr (COLL != TLBM_COLL_NONE) {
     if (fl & TLBM_FLAG_HALFWAY) {
       // pre-stream half-way wall: keep the populations, reversed, uncollided
       bounce_back<L>(f);
     } else {
+      relax_fluid<L, SI, SO, COLL, FORCED>(d, cell, f, cp);
+    }
+  }
+}
+
+// The collision of a fluid cell, the optional force and the status bit.
+template <class L, typename SI, typename SO, int COLL, bool FORCED, typename T>
+__device__ __forceinline__ void relax_fluid(const Domain<SI, SO>& d, long long cell, T (&f)[L::Q],
+                                            const CollideParams<T>& cp) {
+  constexpr int Q = L::Q;
+  if constexpr (COLL != TLBM_COLL_NONE) {
+    {
       const bool has_tau = d.tau_field != nullptr;
       const T tau_cell = has_tau ? T(d.tau_field[cell]) : T(0);
       if constexpr (FORCED) {
@@ -286,6 +301,17 @@ __device__ __forceinline__ E* at_offset(E* base, int i) {
   return r;
 }
 
+// Pair kernels: interior warps skip the boundary code on a warp-uniform branch
+// (2-9 % faster for the D3Q19 collisions and the half formats on the sphere
+// channel).  The D3Q27 legacy cumulant ran 4 % slower that way; it and the
+// other collisions that run at the 128-register cap (Geier cumulant,
+// cascaded) keep the per-cell path.
+template <class L, int COLL>
+__host__ __device__ constexpr bool uniform_edge_branch() {
+  return !(L::Q == 27 && (COLL == TLBM_COLL_CUMULANT || COLL == TLBM_COLL_CUMULANT_GEIER ||
+                          COLL == TLBM_COLL_CASCADED));
+}
+
 // Two cells per thread: (x, y, z) and (x + 1, y, z) with x even.  The pull
 // of a direction with c_x = 0 is one aligned vector load of both cells'
 // values, every store is one vector store, and the index arithmetic (32-bit
@@ -362,6 +388,10 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
     if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));
   }
   const uint8_t fla = uint8_t(fl2), flb = uint8_t(fl2 >> 8);
+  // whether any lane of the warp has a flagged cell or sits on a plane with a
+  // condition: warps of the interior then skip all boundary code on a
+  // warp-uniform branch
+  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || x == 0 || x + 2 == nx || y == ny - 1));
 
   // momentum-exchange force sample (post-stream, pre-bounce-back)
   if (d.force) {
@@ -380,23 +410,41 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
     accumulate_force(d.force, __any_sync(0xffffffffu, oa || ob), mx, my, mz);
   }
   if (!active) return;
-  double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;  // no Bouzidi links here
-  apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-  apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
-  relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
-  relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
-
-  uint32_t ha = 0, hb = 0;
-  if constexpr (Storage<S>::kShifted) {
-    // one hash per cell of its index and of this step's f_0 (so the bits
-    // change every step without a seed); zero for a non-finite cell
-    ha = (fa[0] - fa[0] == T(0)) ? fmix32(uint32_t(c) * 0x9E3779B9u ^ __float_as_uint(float(fa[0]))) : 0u;
-    hb = (fb[0] - fb[0] == T(0)) ? fmix32(uint32_t(c + 1) * 0x9E3779B9u ^ __float_as_uint(float(fb[0]))) : 0u;
+  if constexpr (!uniform_edge_branch<L, COLL>()) {
+    double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
+    apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+    relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
+    relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
+  } else {
+    bool keep_a = false, keep_b = false;   // half-way wall cells: reversed, not collided
+    if (edge) {
+      double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
+      apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+      apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+      if (COLL != TLBM_COLL_NONE && (fla & TLBM_FLAG_HALFWAY)) {
+        bounce_back<L>(fa);
+        keep_a = true;
+      }
+      if (COLL != TLBM_COLL_NONE && (flb & TLBM_FLAG_HALFWAY)) {
+        bounce_back<L>(fb);
+        keep_b = true;
+      }
+    }
+    if (!keep_a) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c, fa, cp);
+    if (!keep_b) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c + 1, fb, cp);
   }
+
+  // one hash per pair of its index and of this step's f_0 values (so the bits
+  // change every step without a seed); NaN / Inf convert exactly whatever the bits
+  uint32_t h = 0;
+  if constexpr (Storage<S>::kShifted)
+    h = fmix32(uint32_t(c) * 0x9E3779B9u ^ __float_as_uint(float(fa[0])) ^
+               (__float_as_uint(float(fb[0])) * 0x85EBCA6Bu));
   S* __restrict__ pout = at_offset(d.fout + (long long)MID * N, c);
 #pragma unroll
   for (int q = 0; q < Q; ++q)
-    __stwb(reinterpret_cast<V*>(at_offset(pout, (q - MID) * N)), IO::join(fa[q], fb[q], weight<L, T>(q), ha, hb, q));
+    __stwb(reinterpret_cast<V*>(at_offset(pout, (q - MID) * N)), IO::join(fa[q], fb[q], weight<L, T>(q), h, q));
 }
 
 // Whether the pair kernel can run this step: no Bouzidi link tables, nx even
