@@ -919,6 +919,48 @@ __device__ __forceinline__ void collide_bgk_fast(T (&f)[L::Q], T inv_tau) {
   }
 }
 
+// BGK on the stored deviations of the shifted half formats, G_q = s (f_q - w_q):
+// with R = sum G (so rho = 1 + R / s) and B = om s rho,
+//   s om (feq_q - w_q) = w_q (om R + B (3 cu + 4.5 cu^2 - 1.5 u.u)),
+// so G'_q = (1 - om) G_q + that, without forming f.  Same operation count as
+// collide_bgk_fast, and no shift or scale on the loads and stores around it.
+template <class L, typename T>
+__device__ __forceinline__ void collide_bgk_deviation(T (&g)[L::Q], T om, T s) {
+  T R = g[0];
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) R += g[q];
+  T jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) {
+    if (L::cx(q) != 0) jx = (L::cx(q) > 0) ? jx + g[q] : jx - g[q];
+    if (L::cy(q) != 0) jy = (L::cy(q) > 0) ? jy + g[q] : jy - g[q];
+    if (L::cz(q) != 0) jz = (L::cz(q) > 0) ? jz + g[q] : jz - g[q];
+  }
+  const T rho = fma(R, T(1) / s, T(1));
+  const T srho = s * (rho > T(1e-12) ? rho : T(1e-12));
+  const T irs = T(1) / srho;
+  const T ux = jx * irs, uy = jy * irs, uz = (L::DIM == 3) ? jz * irs : T(0);
+  const T usq = usq_fused<L>(ux, uy, uz);
+  const T keep = T(1) - om;
+  const T B = om * srho;
+  const T base = fma(B, T(-1.5) * usq, om * R);
+  g[0] = fma(g[0], keep, weight<L, T>(0) * base);
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) {
+    if (L::opp(q) < q) continue;
+    const int qb = L::opp(q);
+    T cu = T(0);
+    if (L::cx(q) != 0) cu = (L::cx(q) > 0) ? cu + ux : cu - ux;
+    if (L::cy(q) != 0) cu = (L::cy(q) > 0) ? cu + uy : cu - uy;
+    if (L::cz(q) != 0) cu = (L::cz(q) > 0) ? cu + uz : cu - uz;
+    const T w = weight<L, T>(q);
+    const T sq = fma((T(4.5) * w * B) * cu, cu, w * base);
+    const T k3 = T(3) * w * B;
+    g[q] = fma(g[q], keep, fma(k3, cu, sq));
+    g[qb] = fma(g[qb], keep, fma(-k3, cu, sq));
+  }
+}
+
 template <class L, typename T>
 __device__ __forceinline__ void collide_smagorinsky_fast(T (&f)[L::Q], const CollideParams<T>& cp) {
   T rho, ux, uy, uz;

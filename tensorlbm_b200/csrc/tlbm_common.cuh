@@ -66,9 +66,11 @@ template <> struct Storage<__half> {
   static constexpr bool kShifted = true;
   static constexpr bool kFast = true;    // fused-arithmetic collisions (no bit-exact target)
   static constexpr float kScale = 16384.0f;
+  static constexpr float kRaw = kScale;   // stored value = kRaw (f - w)
   __device__ __forceinline__ static float load(__half v, float w) {
     return fmaf(__half2float(v), 1.0f / kScale, w);
   }
+  __device__ __forceinline__ static float load_raw(__half v) { return __half2float(v); }
   __device__ __forceinline__ static __half store(float v, float w, uint32_t r) {
     return __float2half_rz(stochastic_truncate_bits<13>((v - w) * kScale, r));
   }
@@ -78,7 +80,9 @@ template <> struct Storage<__nv_bfloat16> {
   using T = float;
   static constexpr bool kShifted = true;
   static constexpr bool kFast = true;
+  static constexpr float kRaw = 1.0f;      // stored value = f - w
   __device__ __forceinline__ static float load(__nv_bfloat16 v, float w) { return __bfloat162float(v) + w; }
+  __device__ __forceinline__ static float load_raw(__nv_bfloat16 v) { return __bfloat162float(v); }
   __device__ __forceinline__ static __nv_bfloat16 store(float v, float w, uint32_t r) {
     return __float2bfloat16_rz(stochastic_truncate_bits<16>(v - w, r));
   }
@@ -177,6 +181,15 @@ template <> struct PairIO<__half> {
   __device__ __forceinline__ static V join(float a, float b, float w, uint32_t h, int q) {
     return cvt_rs_f16x2(fmaf(a, kScale, -w * kScale), fmaf(b, kScale, -w * kScale), pair_bits(h, q));
   }
+  // the stored values themselves, (f - w) 2^14, without the shift
+  __device__ __forceinline__ static void split_raw(V v, float& a, float& b) {
+    const float2 t = __half22float2(*reinterpret_cast<const __half2*>(&v));
+    a = t.x;
+    b = t.y;
+  }
+  __device__ __forceinline__ static V join_raw(float a, float b, uint32_t h, int q) {
+    return cvt_rs_f16x2(a, b, pair_bits(h, q));
+  }
 };
 template <> struct PairIO<__nv_bfloat16> {
   using V = uint32_t;
@@ -186,6 +199,13 @@ template <> struct PairIO<__nv_bfloat16> {
   }
   __device__ __forceinline__ static V join(float a, float b, float w, uint32_t h, int q) {
     return cvt_rs_bf16x2(a - w, b - w, pair_bits(h, q));
+  }
+  __device__ __forceinline__ static void split_raw(V v, float& a, float& b) {
+    a = __uint_as_float(v << 16);
+    b = __uint_as_float(v & 0xFFFF0000u);
+  }
+  __device__ __forceinline__ static V join_raw(float a, float b, uint32_t h, int q) {
+    return cvt_rs_bf16x2(a, b, pair_bits(h, q));
   }
 };
 

@@ -301,6 +301,32 @@ __device__ __forceinline__ E* at_offset(E* base, int i) {
   return r;
 }
 
+// Pulls of the pair kernel: the compute value, or for the deviation-form BGK
+// (RAW) the stored deviation itself.
+template <bool RAW, typename S>
+__device__ __forceinline__ typename Storage<S>::T pull_value(S v, typename Storage<S>::T w) {
+  if constexpr (RAW) return Storage<S>::load_raw(v);
+  else return Storage<S>::load(v, w);
+}
+template <bool RAW, typename S, typename T>
+__device__ __forceinline__ void pull_pair(typename PairIO<S>::V v, T w, T& a, T& b) {
+  if constexpr (RAW) PairIO<S>::split_raw(v, a, b);
+  else PairIO<S>::split(v, w, a, b);
+}
+
+// Interior cells of a shifted half format with BGK: the collision on the
+// stored deviations, the per-cell tau, the status bit.
+template <class L, typename SI, typename SO, typename T>
+__device__ __forceinline__ void relax_deviation(const Domain<SI, SO>& d, long long cell, T (&g)[L::Q],
+                                                const CollideParams<T>& cp) {
+  const T om = d.tau_field ? T(1) / T(d.tau_field[cell]) : cp.inv_tau;
+  collide_bgk_deviation<L>(g, om, T(Storage<SI>::kRaw));
+  if (d.status) {
+    const T r = g[0];
+    if (!(r == r) || r - r != T(0)) atomicOr(d.status, 1u);
+  }
+}
+
 // Pair kernels: interior warps skip the boundary code on a warp-uniform branch
 // (2-9 % faster for the D3Q19 collisions and the half formats on the sphere
 // channel).  The D3Q27 legacy cumulant ran 4 % slower that way; it and the
@@ -329,6 +355,12 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
   using V = typename IO::V;
   constexpr int Q = L::Q;
   constexpr int MID = Q / 2;
+  // shifted float16 storage with BGK: interior warps collide on the stored
+  // deviations (no shift or scale around the loads and stores).  Not bf16: it
+  // saves only an add per value there and took the kernel past 64 registers
+  // (3 instead of 4 blocks per SM, 7 % slower).
+  constexpr bool kDev = std::is_same<S, __half>::value && COLL == TLBM_COLL_BGK && !FORCED &&
+                        uniform_edge_branch<L, COLL>();
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -374,15 +406,15 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
                     (L::cz(q) > 0 ? dzm : (L::cz(q) < 0 ? dzp : 0));
       const T w = weight<L, T>(q);
       if (L::cx(q) == 0) {
-        IO::split(__ldg(reinterpret_cast<const V*>(at_offset(pin, o))), w, fa[q], fb[q]);
+        pull_pair<kDev, S>(__ldg(reinterpret_cast<const V*>(at_offset(pin, o))), w, fa[q], fb[q]);
       } else if (L::cx(q) > 0) {
         const int ia = o + dxm;
-        fa[q] = Storage<S>::load(ldg(at_offset(pin, ia)), w);
-        fb[q] = Storage<S>::load(ldg(at_offset(pin, o)), w);
+        fa[q] = pull_value<kDev>(ldg(at_offset(pin, ia)), w);
+        fb[q] = pull_value<kDev>(ldg(at_offset(pin, o)), w);
       } else {
         const int ia = o + 1, ib = o + dxp;
-        fa[q] = Storage<S>::load(ldg(at_offset(pin, ia)), w);
-        fb[q] = Storage<S>::load(ldg(at_offset(pin, ib)), w);
+        fa[q] = pull_value<kDev>(ldg(at_offset(pin, ia)), w);
+        fb[q] = pull_value<kDev>(ldg(at_offset(pin, ib)), w);
       }
     }
     if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));
@@ -392,6 +424,16 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
   // condition: warps of the interior then skip all boundary code on a
   // warp-uniform branch
   const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || x == 0 || x + 2 == nx || y == ny - 1));
+  if constexpr (kDev) {
+    if (edge) {
+      // the boundary code and the drag work on the populations themselves
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        fa[q] = fma(fa[q], T(1) / T(Storage<S>::kRaw), weight<L, T>(q));
+        fb[q] = fma(fb[q], T(1) / T(Storage<S>::kRaw), weight<L, T>(q));
+      }
+    }
+  }
 
   // momentum-exchange force sample (post-stream, pre-bounce-back)
   if (d.force) {
@@ -431,8 +473,23 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
         keep_b = true;
       }
     }
-    if (!keep_a) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c, fa, cp);
-    if (!keep_b) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c + 1, fb, cp);
+    if constexpr (kDev) {
+      if (edge) {
+        if (!keep_a) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c, fa, cp);
+        if (!keep_b) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c + 1, fb, cp);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {   // back to the stored deviations
+          fa[q] = (fa[q] - weight<L, T>(q)) * T(Storage<S>::kRaw);
+          fb[q] = (fb[q] - weight<L, T>(q)) * T(Storage<S>::kRaw);
+        }
+      } else {
+        relax_deviation<L>(d, (long long)c, fa, cp);
+        relax_deviation<L>(d, (long long)c + 1, fb, cp);
+      }
+    } else {
+      if (!keep_a) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c, fa, cp);
+      if (!keep_b) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c + 1, fb, cp);
+    }
   }
 
   // one hash per pair of its index and of this step's f_0 values (so the bits
@@ -443,8 +500,12 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
                (__float_as_uint(float(fb[0])) * 0x85EBCA6Bu));
   S* __restrict__ pout = at_offset(d.fout + (long long)MID * N, c);
 #pragma unroll
-  for (int q = 0; q < Q; ++q)
-    __stwb(reinterpret_cast<V*>(at_offset(pout, (q - MID) * N)), IO::join(fa[q], fb[q], weight<L, T>(q), h, q));
+  for (int q = 0; q < Q; ++q) {
+    if constexpr (kDev)
+      __stwb(reinterpret_cast<V*>(at_offset(pout, (q - MID) * N)), IO::join_raw(fa[q], fb[q], h, q));
+    else
+      __stwb(reinterpret_cast<V*>(at_offset(pout, (q - MID) * N)), IO::join(fa[q], fb[q], weight<L, T>(q), h, q));
+  }
 }
 
 // Whether the pair kernel can run this step: no Bouzidi link tables, nx even
