@@ -186,7 +186,9 @@ __global__ void __launch_bounds__(256) k_step_aa_x2(StepParams p, CollideParams<
   }
   const uint8_t fla = uint8_t(fl2), flb = uint8_t(fl2 >> 8);
   // warp-uniform: does any lane need boundary code (a flag or a condition plane)
-  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || x == 0 || x + 2 == nx || y == ny - 1));
+  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || ((p.bc & TLBM_BC_ZH_INLET) && x == 0) ||
+                                                       ((p.bc & TLBM_BC_ZH_OUTLET) && x + 2 == nx) ||
+                                                       ((p.bc & TLBM_BC_LID) && y == ny - 1)));
   if (d.force) {
     const bool oa = active && (fla & TLBM_FLAG_OBSTACLE), ob = active && (flb & TLBM_FLAG_OBSTACLE);
     double mx = 0.0, my = 0.0, mz = 0.0;

@@ -423,7 +423,9 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
   // whether any lane of the warp has a flagged cell or sits on a plane with a
   // condition: warps of the interior then skip all boundary code on a
   // warp-uniform branch
-  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || x == 0 || x + 2 == nx || y == ny - 1));
+  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || ((p.bc & TLBM_BC_ZH_INLET) && x == 0) ||
+                                                       ((p.bc & TLBM_BC_ZH_OUTLET) && x + 2 == nx) ||
+                                                       ((p.bc & TLBM_BC_LID) && y == ny - 1)));
   if constexpr (kDev) {
     if (edge) {
       // the boundary code and the drag work on the populations themselves
