@@ -37,7 +37,7 @@ def test_backward_matches_autograd_f64():
     th = torch.tensor(theta, requires_grad=True)
     lt = _torch_loss(th, torch.tensor(z), torch.tensor(t), torch.tensor(w))
     lt.backward()
-    assert abs(loss - float(lt)) <= 1e-12 * abs(loss)
+    assert abs(loss - float(lt.detach())) <= 1e-12 * abs(loss)
     assert np.max(np.abs(g - th.grad.numpy())) <= 1e-10 * np.max(np.abs(g))
 
 
