@@ -754,7 +754,8 @@ def main() -> None:
                          "les_mlp_128_vs_smagorinsky_256, d2q9_batched_512_cylinders) or 'all'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-slab", type=int, default=8, help="z-planes per CPU sample slab")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    # 16 steps of one 512x256x8 slab: about 10 s of single-core oracle work
+    ap.add_argument("--cpu-steps", type=int, default=16)
     ap.add_argument("--grid", default=None,
                     help="nx,ny,nz of a smaller channel (profiling only; the sphere keeps its size, centred)")
     args = ap.parse_args()

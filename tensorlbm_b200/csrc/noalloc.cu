@@ -18,7 +18,7 @@ namespace {
 // kLinkStaticMaxBlocks * 1024 bytes (128 Mi entries; 1 MiB of device memory,
 // held by every device that loads the library until the process exits).
 constexpr long long kLinkStaticMaxBlocks = 131072;
-__device__ __align__(256) long long g_link_scratch[kLinkStaticMaxBlocks + 1];
+static __device__ __align__(256) long long g_link_scratch[kLinkStaticMaxBlocks + 1];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
