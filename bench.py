@@ -20,8 +20,10 @@ the next step waits for that exchange on the stream.  The time is the max over
 ranks and the value is the total cell updates of all ranks per second.  Rank 0
 prints one JSON line.
 
---impl reference times the CPU implementation of the same step (the numpy
-restatement of TensorLBM's torch operators in oracle/) on the host cores.
+--impl reference times TensorLBM's own CPU implementation of the same chain
+(its torch operators, unmodified, from baseline/_ref) on every host core, on a
+bounded z-slab sample of the workload; the same sample is the cpu_baseline of
+our arm.
 """
 
 from __future__ import annotations
@@ -49,6 +51,26 @@ METRIC = "MLUPS (D3Q19 MRT sphere channel 512x256x256, fused step)"
 WORKLOAD = "d3q19_mrt_sphere_channel_512x256x256"
 HBM_FALLBACK_GBS = 6650.0
 SPEC_HBM_GBS = 8000.0
+DATA = "synthetic: equilibrium initial state of the inlet velocity (zero in the sphere)"
+
+
+def workload_config(world: int) -> dict:
+    """The workload both arms report (identical dicts)."""
+    return {
+        "workload": WORKLOAD,
+        "grid": [NX, NY, NZ],
+        "lattice": "D3Q19",
+        "collision": "mrt",
+        "sphere": {"diameter": D, "center": [CX, CY, CZ]},
+        "u_in": U_IN, "re": RE, "tau": TAU,
+        "boundaries": "zou_he velocity inlet x=0, zou_he pressure outlet x=nx-1, periodic y/z, "
+                      "full-way bounce-back + FP64 momentum-exchange drag on the sphere",
+        "l2": "no flush: the two population buffers are 5.1 GB, 40x the 126 MB L2",
+        "parallelism": (f"z-slabs x{world}: global grid {NX}x{NY}x{NZ * world}, one sphere per slab, "
+                        f"NCCL halo exchange of the 5 crossing lanes per face every step "
+                        f"({2 * 5 * NX * NY * 4} B sent per rank per step), overlapped with the interior "
+                        f"planes") if world > 1 else "single GPU",
+    }
 
 
 def _peaks() -> tuple[float, str]:
@@ -73,40 +95,100 @@ def _traffic(workload: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks, power and clock-event (throttle) reasons during the timed
+    region, polled through NVML every 2 ms in a background thread (a
+    20-step region of the headline lasts about 16 ms), plus one sample as the
+    region opens and one as it closes.  Falls back to ``nvidia-smi -lms 100``
+    when NVML cannot be loaded."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_s: float = 0.002):
         self.index = index
-        self.rows: list[list[str]] = []
+        self.period = period_s
+        self.rows: list[tuple[float, float, float, int]] = []   # sm MHz, max MHz, watts, reason bits
+        self.smi_rows: list[list[str]] = []
         self.proc = None
         self.thread = None
+        self.nvml = None
+        self.handle = None
+        self.stop = threading.Event()
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        self.nvml = pynvml
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _sample(self):
+        n, h = self.nvml, self.handle
+        try:
+            reasons = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            reasons = n.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.rows.append((float(n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)),
+                          float(n.nvmlDeviceGetMaxClockInfo(h, n.NVML_CLOCK_SM)),
+                          n.nvmlDeviceGetPowerUsage(h) / 1000.0, int(reasons)))
+
+    def _poll(self):
+        while not self.stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                return
+            time.sleep(self.period)
 
     def __enter__(self):
+        try:
+            self.handle = self._nvml_handle()
+            self._sample()
+            self.source = "nvml"
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread = threading.Thread(target=self._read_smi, daemon=True)
             self.thread.start()
-            # wait for the sampler to be running, then keep only samples taken
-            # from here on (the timed region starts when this returns)
             t0 = time.time()
-            while not self.rows and time.time() - t0 < 3.0:
+            while not self.smi_rows and time.time() - t0 < 3.0:
                 time.sleep(0.01)
-            self.rows.clear()
+            self.smi_rows.clear()
+            self.source = "nvidia-smi"
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
 
-    def _read(self):
+    def _read_smi(self):
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+            self.smi_rows.append([c.strip() for c in line.split(",")])
 
     def __exit__(self, *exc):
+        self.stop.set()
+        if self.nvml is not None:
+            if self.thread is not None:
+                self.thread.join(timeout=2)
+            try:
+                self._sample()
+            except Exception:
+                pass
+            return
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -117,19 +199,25 @@ class ClockSampler:
             self.thread.join(timeout=2)
 
     def summary(self) -> dict:
-        sm, smax, reasons = [], None, set()
+        sm, smax, watts, reasons = [], None, [], set()
+        for mhz, mx, w, bits in self.rows:
+            sm.append(mhz)
+            smax = mx
+            watts.append(w)
+            reasons.update(name for name, bit in self.REASONS if bits & bit)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
+        for r in self.smi_rows:
             try:
                 sm.append(float(r[1]))
                 smax = float(r[2])
+                watts.append(float(r[3]))
                 for name, v in zip(names, r[5:9]):
                     if v.strip().lower() == "active":
                         reasons.add(name)
             except (ValueError, IndexError):
                 continue
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "power_w_max": max(watts) if watts else None, "source": self.source}
 
 
 # ---------------------------------------------------------------------------
@@ -309,29 +397,10 @@ REF_TRITON = "reference_triton_256"   # opt-in variant: --variants reference_tri
 
 
 def _import_reference_package():
-    """TensorLBM itself, pip-installed unmodified into baseline/_ref.  Its
-    package __init__ imports plotting / HDF5 modules that no compute path
-    calls and that the image lacks, so those names resolve to inert stubs."""
-    import types
+    """TensorLBM's own Triton kernels, from its unmodified install in baseline/_ref."""
+    from baseline import reference
 
-    class _Stub(types.ModuleType):
-        def __getattr__(self, name):
-            if name.startswith("__"):
-                raise AttributeError(name)
-            sub = _Stub(f"{self.__name__}.{name}")
-            sys.modules[sub.__name__] = sub
-            return sub
-
-        def __call__(self, *a, **k):
-            return self
-
-    ref = ROOT / "baseline" / "_ref"
-    if not (ref / "tensorlbm").is_dir():
-        raise FileNotFoundError(f"{ref} holds no tensorlbm install")
-    for name in ("matplotlib", "matplotlib.pyplot", "h5py"):
-        sys.modules.setdefault(name, _Stub(name))
-    if str(ref) not in sys.path:
-        sys.path.insert(0, str(ref))
+    reference.import_reference()
     from tensorlbm import triton_fused, triton_fused_obstacle
 
     return triton_fused, triton_fused_obstacle
@@ -592,7 +661,7 @@ def run_ours(args) -> None:
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample(args, processes=1)
+        cpu = cpu_sample(args)
 
     if world > 1:
         torch.distributed.barrier()
@@ -611,24 +680,9 @@ def run_ours(args) -> None:
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic: equilibrium initial state of the inlet velocity (zero in the sphere)",
-        "config": {
-            "workload": WORKLOAD,
-            "grid": [NX, NY, NZ],
-            "lattice": "D3Q19",
-            "collision": "mrt",
-            "sphere": {"diameter": D, "center": [CX, CY, CZ]},
-            "u_in": U_IN, "re": RE, "tau": TAU,
-            "boundaries": "zou_he velocity inlet x=0, zou_he pressure outlet x=nx-1, periodic y/z, "
-                          "full-way bounce-back + FP64 momentum-exchange drag on the sphere",
-            "l2": "no flush: the two population buffers are 5.1 GB, 40x the 126 MB L2",
-            "parallelism": (f"z-slabs x{world}: global grid {NX}x{NY}x{NZ * world}, one sphere per slab, "
-                            f"NCCL halo exchange of the 5 crossing lanes per face every step "
-                            f"({2 * 5 * NX * NY * 4} B sent per rank per step), overlapped with the interior "
-                            f"planes") if world > 1 else "single GPU",
-            "drag_fx_last_step": drag,
-            "finite": finite,
-        },
+        "data": DATA,
+        "config": workload_config(world),
+        "result": {"drag_fx_last_step": drag, "finite": finite},
         "roofline": {
             "bound": "hbm",
             "achieved": round(achieved, 1),
@@ -657,12 +711,52 @@ def run_ours(args) -> None:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline / reference arm: the numpy restatement of TensorLBM's chain
+# CPU baseline / reference arm: TensorLBM's own torch chain on the host cores
 # ---------------------------------------------------------------------------
 
+CPU_SAMPLE_STEPS_MAX = 30      # timed steps of the CPU sample (both arms), fewer if --steps is smaller
+CPU_SAMPLE_BUDGET_S = 90.0     # and no more timed seconds than this
 
-def _cpu_slab_worker(args_tuple):
-    nzs, steps = args_tuple
+
+def _reference_chain(nzs: int):
+    """The config-2 chain of TensorLBM itself (unmodified, baseline/_ref) on a
+    512 x 256 x nzs z-slab of the channel (sphere centred in the slab):
+    collide_mrt3d -> stream3d -> compute_obstacle_forces_3d ->
+    zou_he_inlet_velocity_3d -> zou_he_outlet_pressure_3d ->
+    bounce_back_cells_3d(sphere), the order of d3q27_sphere_flow.py:246-256
+    with the D3Q19 MRT operators.  Returns (step, f0)."""
+    import torch
+
+    from baseline import reference
+
+    reference.import_reference()
+    from tensorlbm.boundaries3d import (bounce_back_cells_3d, sphere_mask, zou_he_inlet_velocity_3d,
+                                        zou_he_outlet_pressure_3d)
+    from tensorlbm.d3q19 import equilibrium3d
+    from tensorlbm.obstacles import compute_obstacle_forces_3d
+    from tensorlbm.solver3d import collide_mrt3d, stream3d
+
+    cpu = torch.device("cpu")
+    obst = sphere_mask(NX, NY, nzs, CX, CY, nzs / 2, D / 2, cpu)
+    ux = torch.full((nzs, NY, NX), U_IN)
+    ux[obst] = 0.0
+    z = torch.zeros_like(ux)
+    f0 = equilibrium3d(torch.ones_like(ux), ux, z, z)
+
+    def step(f):
+        f = collide_mrt3d(f, TAU)
+        f = stream3d(f)
+        fx, _, _ = compute_obstacle_forces_3d(f, obst)
+        f = zou_he_inlet_velocity_3d(f, U_IN)
+        f = zou_he_outlet_pressure_3d(f, 1.0)
+        f = bounce_back_cells_3d(f, obst)
+        return f, fx
+
+    return step, f0
+
+
+def _oracle_chain(nzs: int):
+    """The oracle's restatement of the same chain (used when TensorLBM is not installed)."""
     import numpy as np
 
     from oracle import lbm as O
@@ -671,44 +765,52 @@ def _cpu_slab_worker(args_tuple):
     ux = np.full((nzs, NY, NX), U_IN, np.float32)
     ux[obst] = 0.0
     z = np.zeros_like(ux)
-    f = O.equilibrium(19, np.ones_like(ux), ux, z, z)
-    O.channel_step(f, TAU, U_IN, 1.0, None, obst, "mrt")  # warm-up
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        f, _ = O.channel_step(f, TAU, U_IN, 1.0, None, obst, "mrt")
-    return time.perf_counter() - t0
+    f0 = O.equilibrium(19, np.ones_like(ux), ux, z, z)
+    return (lambda f: O.channel_step(f, TAU, U_IN, 1.0, None, obst, "mrt")), f0
 
 
-def cpu_sample(args, processes: int) -> dict:
-    """Time the oracle's D3Q19 MRT channel step on z-slabs of the bench grid."""
-    import multiprocessing as mp
+def cpu_sample(args) -> dict:
+    """Time the CPU chain of the headline workload on a z-slab sample: TensorLBM's
+    torch operators with every host core (kind "reference"), or the oracle port
+    on one core when TensorLBM is not installed (kind "port").  The same slab
+    and step count serve the cpu_baseline of our arm and the reference arm."""
+    from baseline import reference
 
     nzs = args.cpu_slab
-    steps = max(1, args.cpu_steps)
-    if processes == 1:
-        from threadpoolctl import threadpool_limits
+    want = max(1, min(args.steps, CPU_SAMPLE_STEPS_MAX))
+    import contextlib
 
-        with threadpool_limits(1):
-            t = _cpu_slab_worker((nzs, steps))
-        cells = NX * NY * nzs
-    else:
-        ctx = mp.get_context("spawn")
-        with ctx.Pool(processes, initializer=_limit_blas) as pool:
+    with contextlib.ExitStack() as stack:
+        if reference.available():
+            import torch
+
+            threads_before = torch.get_num_threads()
+            torch.set_num_threads(os.cpu_count() or 1)
+            stack.callback(torch.set_num_threads, threads_before)
+            step, f = _reference_chain(nzs)
+            used, kind = torch.get_num_threads(), "reference"
+            what = ("TensorLBM's own torch CPU operators (unmodified, baseline/_ref): collide_mrt3d -> stream3d -> "
+                    "compute_obstacle_forces_3d -> zou_he_inlet_velocity_3d -> zou_he_outlet_pressure_3d -> "
+                    "bounce_back_cells_3d")
+        else:
+            from threadpoolctl import threadpool_limits
+
+            stack.enter_context(threadpool_limits(1))
+            step, f = _oracle_chain(nzs)
+            used, kind = 1, "port"
+            what = "numpy restatement of the same chain (oracle/), one core"
+        f, _ = step(f)                              # warm-up (index caches, allocator)
+        done, t = 0, 0.0
+        while done < want and t < CPU_SAMPLE_BUDGET_S:
             t0 = time.perf_counter()
-            times = pool.map(_cpu_slab_worker, [(nzs, steps)] * processes)
-            t = max(times)
-            del t0
-        cells = NX * NY * nzs * processes
-    mlups = cells * steps / t / 1e6
-    return {"value": round(mlups, 3), "unit": "MLUPS", "cores": processes, "kind": "port",
-            "sample": f"{processes} x {NX}x{NY}x{nzs} z-slab(s) of the channel with the sphere, {steps} step(s) "
-                      f"each (numpy restatement of collide_mrt3d -> stream3d -> forces -> zou_he -> bounce_back)"}
-
-
-def _limit_blas():
-    from threadpoolctl import threadpool_limits
-
-    threadpool_limits(1)
+            f, _ = step(f)
+            t += time.perf_counter() - t0
+            done += 1
+    cells = NX * NY * nzs
+    return {"value": round(cells * done / t / 1e6, 3), "unit": "MLUPS", "cores": used, "kind": kind,
+            "host_cpus": os.cpu_count(),
+            "sample": f"one {NX}x{NY}x{nzs} z-slab of the sphere channel (sphere centred in the slab, periodic "
+                      f"y/z), 1 warm-up step, {done} timed step(s) ({t:.1f} s): {what}"}
 
 
 def run_reference(args) -> None:
@@ -716,11 +818,7 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    procs = os.cpu_count() or 1
-    # bounded: each step is `procs` slabs in parallel; steps/warmup follow the CLI
-    cpu_steps = max(1, min(args.steps, 3))
-    args.cpu_steps = cpu_steps
-    sample = cpu_sample(args, processes=procs)
+    sample = cpu_sample(args)
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -730,13 +828,15 @@ def run_reference(args) -> None:
         "steps": args.steps,
         "warmup": args.warmup,
         "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "lattice": "D3Q19", "collision": "mrt"},
+        "data": DATA,
+        "config": workload_config(world),
         "cpu_baseline": sample,
         "e2e": {"value": sample["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "TensorLBM is a Python package whose CPU path is torch; its restatement in oracle/ is timed here "
-                "because the reference source is not present on the GPU machine",
+        "note": "TensorLBM is a pure-Python torch package; its CPU path runs here on a bounded z-slab sample of "
+                "the workload (see cpu_baseline.sample), on every host core",
     }
     print(json.dumps(line))
 
@@ -753,9 +853,7 @@ def main() -> None:
                          "d3q19_mrt_f16_shifted, d3q19_bgk_f32, d3q19_bgk_f16_shifted, d3q19_bgk_bf16_shifted, "
                          "les_mlp_128_vs_smagorinsky_256, d2q9_batched_512_cylinders) or 'all'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-slab", type=int, default=8, help="z-planes per CPU sample slab")
-    # 16 steps of one 512x256x8 slab: about 10 s of single-core oracle work
-    ap.add_argument("--cpu-steps", type=int, default=16)
+    ap.add_argument("--cpu-slab", type=int, default=16, help="z-planes of the CPU sample slab")
     ap.add_argument("--grid", default=None,
                     help="nx,ny,nz of a smaller channel (profiling only; the sphere keeps its size, centred)")
     args = ap.parse_args()

@@ -286,7 +286,8 @@ TLBM_API int tlbm_link_list(const uint8_t* mask, int64_t count, const int64_t* b
  * most tlbm_link_list_static_capacity() bytes (128 Mi); larger masks return
  * TLBM_ERR_TOO_LARGE before any work.  *count_out (device int64) receives the
  * number of non-zero entries; the first min(count, out_capacity) indices are
- * written to out.  The first call on each device looks the array up with
+ * written to out (out may be NULL when out_capacity is 0: a count-only
+ * query).  The first call on each device looks the array up with
  * cudaGetSymbolAddress (make it before any stream capture).  All calls share
  * the array: calls whose kernels overlap on the GPU (different streams or
  * devices sharing nothing but the array - it is per device) race and must be

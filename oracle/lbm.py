@@ -890,6 +890,25 @@ def missing_mask(q: int, shape, solid=None, periodic=(False, False, False)) -> n
     return out
 
 
+def link_index(missing: np.ndarray) -> np.ndarray:
+    """Row-major flat indices of the True entries, the order of torch.nonzero
+    that boundary_registry.py:488's callers apply to the missing mask."""
+    return np.flatnonzero(missing.reshape(-1)).astype(np.int64)
+
+
+def correct_mass(f: np.ndarray, target_mass: float) -> np.ndarray:
+    """f * (target / sum(f)) in the field dtype, unchanged when |sum| < 1e-30:
+    solver.py:420-437, solver3d.py:287-300, d3q27.py:729-745.  The sum is taken
+    in float64 and then rounded to the field dtype; torch sums float32 in its own
+    blocked order, so for float64 fields the scale can differ from the
+    reference's by the rounding of the sum (the golden test allows 1e-14)."""
+    t = f.dtype.type
+    cur = t(f.sum(dtype=np.float64))
+    if abs(cur) < 1e-30:
+        return f
+    return f * (t(target_mass) / cur)
+
+
 def cavity_walls_3d(n_z, n_y, n_x) -> np.ndarray:
     """Five no-slip walls of benchmarks/verified/cavity_3d_full/run.py:85-89."""
     wall = np.zeros((n_z, n_y, n_x), dtype=bool)

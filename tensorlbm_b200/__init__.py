@@ -50,26 +50,65 @@ _PATCHES = {
 }
 
 
+# (module name, attribute) -> the object install() replaced there
+_ORIGINALS: dict = {}
+
+
 def install(package=None) -> list[str]:
     """Replace TensorLBM's hot-path functions with these kernels in a live import.
 
-    ``package`` defaults to ``import tensorlbm``.  Returns the patched names.
-    Every replaced function requires CUDA tensors afterwards."""
+    ``package`` defaults to ``import tensorlbm``.  Each name of ``_PATCHES`` is
+    replaced in its defining module.  Then every loaded module of the package
+    is searched for globals that *are* one of the replaced objects (an identity
+    check) and those are rebound too: runners that bound a name at import time
+    (``from .d3q27 import collide_bgk27`` in ``d3q27_sphere_flow.py``, or
+    ``from .solver3d import collide_bgk3d`` in ``sphere_flow.py``) then call the
+    kernels as well.  Modules imported later pick the new names up from the
+    patched defining modules.  Returns the patched ``module.name`` entries.
+    Every replaced function requires CUDA tensors afterwards; :func:`uninstall`
+    puts the originals back."""
     import importlib
+    import sys
 
     if package is None:
         package = importlib.import_module("tensorlbm")
+    prefix = package.__name__
+    swap = {}        # id(original) -> (original, replacement)
     patched = []
     for mod_name, names in _PATCHES.items():
         ours = importlib.import_module(f"{__name__}.{mod_name}")
         try:
-            theirs = importlib.import_module(f"{package.__name__}.{mod_name}")
+            theirs = importlib.import_module(f"{prefix}.{mod_name}")
         except ImportError:
             continue
         for name in names:
-            if hasattr(theirs, name):
-                setattr(theirs, name, getattr(ours, name))
-                if hasattr(package, name):
-                    setattr(package, name, getattr(ours, name))
-                patched.append(f"{mod_name}.{name}")
+            if not hasattr(theirs, name):
+                continue
+            orig, repl = getattr(theirs, name), getattr(ours, name)
+            if orig is not repl:
+                swap[id(orig)] = (orig, repl)
+            patched.append(f"{mod_name}.{name}")
+    for mname, mod in list(sys.modules.items()):
+        if mod is None or not (mname == prefix or mname.startswith(prefix + ".")):
+            continue
+        for attr, val in list(vars(mod).items()):
+            hit = swap.get(id(val))
+            if hit is not None and hit[0] is val:
+                _ORIGINALS.setdefault((mname, attr), val)
+                setattr(mod, attr, hit[1])
     return patched
+
+
+def uninstall() -> int:
+    """Undo :func:`install`: every rebound global gets its original object
+    back.  Returns the number of bindings restored."""
+    import sys
+
+    n = 0
+    for (mname, attr), val in list(_ORIGINALS.items()):
+        mod = sys.modules.get(mname)
+        if mod is not None:
+            setattr(mod, attr, val)
+            n += 1
+    _ORIGINALS.clear()
+    return n

@@ -13,12 +13,13 @@
 
 namespace {
 
-// Block counts of the compaction: one int64 per 1024 mask bytes, plus one slot
-// for the total.  kLinkStaticMaxBlocks blocks cover masks of up to
-// kLinkStaticMaxBlocks * 1024 bytes (128 Mi entries; 1 MiB of device memory,
-// held by every device that loads the library until the process exits).
+// Block counts of the compaction: one int64 per 1024 mask bytes (the total
+// goes to the caller's count_out, not here).  kLinkStaticMaxBlocks blocks cover
+// masks of up to kLinkStaticMaxBlocks * 1024 bytes (128 Mi entries; 1 MiB of
+// device memory, held by every device that loads the library until the process
+// exits).
 constexpr long long kLinkStaticMaxBlocks = 131072;
-static __device__ __align__(256) long long g_link_scratch[kLinkStaticMaxBlocks + 1];
+static __device__ __align__(256) long long g_link_scratch[kLinkStaticMaxBlocks];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
@@ -86,7 +87,8 @@ TLBM_API int64_t tlbm_link_list_static_capacity(void) { return kLinkStaticMaxBlo
 TLBM_API int tlbm_link_list_noalloc(const uint8_t* mask, int64_t count, int64_t* out, int64_t out_capacity,
                                     int64_t* count_out, void* stream) {
   if (count < 0 || out_capacity < 0) return TLBM_ERR_SHAPE;
-  if (!count_out || (count > 0 && (!mask || !out))) return TLBM_ERR_ARG;
+  // out may be null for a count-only query (out_capacity == 0): nothing is written to it
+  if (!count_out || (count > 0 && (!mask || (out_capacity > 0 && !out)))) return TLBM_ERR_ARG;
   const long long nb = tlbm::op_link_blocks(count);
   if (nb > kLinkStaticMaxBlocks) return TLBM_ERR_TOO_LARGE;
   if (tlbm::op_link_blocks(kChunk) != 1 || tlbm::op_link_blocks(kChunk + 1) != 2) return TLBM_ERR_UNSUPPORTED;
@@ -97,7 +99,7 @@ TLBM_API int tlbm_link_list_noalloc(const uint8_t* mask, int64_t count, int64_t*
   // every block count the scan reads is written by this call's count kernel,
   // so nothing of the previous call's contents needs clearing
   st = tlbm::op_link_count(mask, count, scratch, (long long*)count_out, s);
-  if (st != TLBM_OK || nb == 0) return st;
+  if (st != TLBM_OK || nb == 0 || out_capacity == 0) return st;
   k_link_list_capped<<<(int)nb, kThreads, 0, s>>>(mask, count, scratch, (long long*)out, out_capacity);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }

@@ -153,14 +153,22 @@ class StagedTransport(ProcessGroupTransport):
         super().__init__(group)
         self.wire_dtype = wire_dtype
         self._stage = None
+        self._lanes = None
+        self._index = None
 
     def start(self, geom: SlabGeometry, f: torch.Tensor):
         shape = (geom.n_cross, geom.ny, geom.nx)
-        if self._stage is None or self._stage[0].shape != shape or self._stage[0].device != f.device:
+        lanes = (tuple(geom.cross_up), tuple(geom.cross_dn))
+        if (self._stage is None or self._stage[0].shape != shape or self._stage[0].device != f.device
+                or self._lanes != lanes):
+            # staging planes and lane indices are built once per geometry and
+            # device, so an exchange allocates nothing and copies nothing from the host
             self._stage = [torch.empty(shape, dtype=self.wire_dtype, device=f.device) for _ in range(4)]
+            self._lanes = lanes
+            self._index = (torch.tensor(lanes[0], dtype=torch.int64, device=f.device),
+                           torch.tensor(lanes[1], dtype=torch.int64, device=f.device))
         send_up, send_dn, recv_up, recv_dn = self._stage
-        up = torch.tensor(geom.cross_up, device=f.device)
-        dn = torch.tensor(geom.cross_dn, device=f.device)
+        up, dn = self._index
         send_up.copy_(f[:, geom.nz_local].index_select(0, up))
         send_dn.copy_(f[:, 1].index_select(0, dn))
         ops = [dist.P2POp(dist.isend, send_up, geom.right_neighbor, self.group, tag=1),

@@ -258,6 +258,70 @@ def mem(torch) -> None:
     print(f"wrote mem.npz; links {int(near.sum())} near cells")
 
 
+def links_c2(torch) -> None:
+    """The solid mask and link list of the 512x256x256 sphere channel at full
+    size: sphere_mask(512, 256, 256, 128, 128, 128, 16) (boundaries3d.py:29),
+    derive_missing_mask with periodic y/z and a closed x (boundary_registry.py:488),
+    then torch.nonzero, for D3Q19 and D3Q27.  The (n, 4) (q, z, y, x) list is
+    stored as flat row-major indices, delta-encoded (the first entry, then the
+    differences, all positive because nonzero is ordered), next to the SHA-256
+    of the int64 nonzero output, so a test can check every entry and the exact
+    bytes torch returned."""
+    import hashlib
+
+    from tensorlbm import boundaries3d as b3
+    from tensorlbm.boundary_registry import derive_missing_mask
+
+    cpu = torch.device("cpu")
+    nz, ny, nx = 256, 256, 512
+    solid = b3.sphere_mask(nx, ny, nz, 128, 128, 128, 16, cpu)
+    out = {"shape": np.array([nz, ny, nx])}
+    for lat in ("D3Q19", "D3Q27"):
+        miss = derive_missing_mask((nz, ny, nx), solid_mask=solid, periodic={"y": True, "z": True, "x": False},
+                                   lattice=lat)
+        links = torch.nonzero(miss)
+        q = miss.shape[0]
+        del miss
+        dims = torch.tensor([nz * ny * nx, ny * nx, nx, 1], dtype=torch.int64)
+        flat = (links * dims).sum(dim=1).numpy()
+        assert np.all(np.diff(flat) > 0)
+        delta = np.diff(flat, prepend=np.int64(0))
+        assert delta.max() < 2**32
+        tag = lat[2:].lower()
+        out[f"count_{tag}"] = np.int64(links.shape[0])
+        out[f"q_{tag}"] = np.int64(q)
+        out[f"delta_{tag}"] = delta.astype(np.uint32)
+        out[f"sha256_{tag}"] = np.frombuffer(hashlib.sha256(links.contiguous().numpy().tobytes()).digest(),
+                                             dtype=np.uint8)
+        print(f"  {lat}: {links.shape[0]} links")
+    np.savez_compressed(HERE / "links_c2.npz", **out)
+    print(f"wrote links_c2.npz ({(HERE / 'links_c2.npz').stat().st_size / 1024:.0f} KB)")
+
+
+def mass(torch) -> None:
+    """Global mass correction f * (target / f.sum()) (solver.py:420,
+    solver3d.py:287, d3q27.py:729) on seeded near-equilibrium fields, float32
+    and float64, plus the all-zero field that the 1e-30 guard returns as is."""
+    from tensorlbm.d3q27 import correct_mass27
+    from tensorlbm.solver import correct_mass
+    from tensorlbm.solver3d import correct_mass3d
+
+    out = {}
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        _, _, f9 = near_eq_field(torch, 9, (16, 32), dt, 91)
+        _, _, f19 = near_eq_field(torch, 19, (4, 6, 16), dt, 92)
+        _, _, f27 = near_eq_field(torch, 27, (4, 6, 16), dt, 93)
+        t9, t19, t27 = 0.97 * float(f9.double().sum()), 1.013 * float(f19.double().sum()), 1001.5
+        out.update({f"f9_{tag}": f9, f"t9_{tag}": t9, f"m9_{tag}": correct_mass(f9, t9),
+                    f"f19_{tag}": f19, f"t19_{tag}": t19, f"m19_{tag}": correct_mass3d(f19, t19),
+                    f"f27_{tag}": f27, f"t27_{tag}": t27, f"m27_{tag}": correct_mass27(f27, t27)})
+    zero = torch.zeros((19, 2, 3, 4))
+    out["zero_out"] = correct_mass3d(zero, 5.0)
+    arrays = {k: (v.numpy() if isinstance(v, torch.Tensor) else np.asarray(v)) for k, v in out.items()}
+    np.savez_compressed(HERE / "mass.npz", **arrays)
+    print("wrote mass.npz")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -285,6 +349,12 @@ def main() -> None:
         return
     if args.only == "mem":
         mem(torch)
+        return
+    if args.only == "links_c2":
+        links_c2(torch)
+        return
+    if args.only == "mass":
+        mass(torch)
         return
     from tensorlbm import boundaries as b2
     from tensorlbm import boundaries3d as b3

@@ -218,6 +218,32 @@ def test_link_list_large_and_empty(cuda):
     assert _ops.link_list(torch.zeros(1000, dtype=torch.bool, device=cuda)).numel() == 0
 
 
+@pytest.mark.parametrize("lat", ["D3Q19", "D3Q27"])
+def test_links_c2_full_size(cuda, lat):
+    """The 512x256x256 sphere channel's solid mask, missing mask and link list,
+    built on the GPU, against the list torch.nonzero returned for the
+    reference's derive_missing_mask (periodic y/z, closed x): every index, and
+    the SHA-256 of the (n, 4) int64 rows."""
+    import hashlib
+
+    from tensorlbm_b200 import _ops, boundaries3d
+    from tensorlbm_b200 import boundary_registry as br
+
+    g = golden("links_c2")
+    tag = lat[2:].lower()
+    nz, ny, nx = (int(v) for v in g["shape"])
+    solid = boundaries3d.sphere_mask(nx, ny, nz, 128, 128, 128, 16, cuda)
+    miss = br.derive_missing_mask((nz, ny, nx), solid_mask=solid, periodic={"y": True, "z": True, "x": False},
+                                  lattice=lat)
+    assert tuple(miss.shape) == (int(g[f"q_{tag}"]), nz, ny, nx)
+    flat = N(_ops.link_list(miss))
+    assert flat.size == int(g[f"count_{tag}"])
+    assert np.array_equal(flat, np.cumsum(g[f"delta_{tag}"].astype(np.int64)))
+    rows = N(br.link_list(miss))
+    assert rows.dtype == np.int64 and rows.shape == (flat.size, 4)
+    assert hashlib.sha256(np.ascontiguousarray(rows).tobytes()).digest() == g[f"sha256_{tag}"].tobytes()
+
+
 def test_correct_mass(cuda):
     from tensorlbm_b200 import solver3d
 
@@ -225,6 +251,24 @@ def test_correct_mass(cuda):
     out = solver3d.correct_mass3d(f, 123.0)
     assert abs(float(out.sum()) - 123.0) < 1e-9
     assert torch.equal(solver3d.correct_mass3d(torch.zeros_like(f), 5.0), torch.zeros_like(f))
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_correct_mass_golden(cuda, tag):
+    """correct_mass / correct_mass3d / correct_mass27 against the reference's
+    outputs (solver.py:420, solver3d.py:287, d3q27.py:729).  The reference
+    sums in the field dtype, the kernel in float64 and rounds once: the bound
+    is the rounding of the sum (1e-6 relative in float32, 1e-14 in float64)."""
+    from tensorlbm_b200 import d3q27, solver, solver3d
+
+    g = golden("mass")
+    tol = 1e-6 if tag == "f32" else 1e-14
+    for q, fn in ((9, solver.correct_mass), (19, solver3d.correct_mass3d), (27, d3q27.correct_mass27)):
+        ref = g[f"m{q}_{tag}"]
+        got = N(fn(T(g[f"f{q}_{tag}"], cuda), float(g[f"t{q}_{tag}"])))
+        assert got.dtype == ref.dtype and rel_err(got, ref) <= tol, (q, rel_err(got, ref))
+        assert rel_err(got, O.correct_mass(g[f"f{q}_{tag}"], float(g[f"t{q}_{tag}"]))) <= tol
+    assert same(N(solver3d.correct_mass3d(torch.zeros((19, 2, 3, 4), device=cuda), 5.0)), g["zero_out"])
 
 
 @pytest.mark.parametrize("tag", ["f32", "f64"])

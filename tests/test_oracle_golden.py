@@ -234,3 +234,53 @@ def test_mem_variants_against_reference(tag):
         tol = eps * 2.0 * np.abs(sums[:19]).sum()
         assert np.abs(got - g[f"{name}_{tag}"]).max() <= tol, name
     assert O.link_momentum_sums(f, solid, near)[19:].sum() > 100          # links on the sphere and the x wall
+
+
+def c2_links_decoded(g, tag):
+    """Flat row-major (q, z, y, x) indices of the 512x256x256 link list."""
+    return np.cumsum(g[f"delta_{tag}"].astype(np.int64))
+
+
+@pytest.mark.parametrize("tag", ["q19", "q27"])
+def test_links_c2_full_size(tag):
+    """The full-size sphere-channel link list (512x256x256, sphere D = 32 at
+    (128, 128, 128), periodic y/z, closed x) that torch.nonzero returned for
+    the reference's missing mask: the stored digest of its int64 rows, and the
+    oracle's missing mask over the whole grid.  The oracle runs on the band of
+    48 planes around the sphere (a periodic-z subdomain holds the same links
+    there, since no solid lies near the band's edges); every other plane is an
+    empty periodic slice, checked against the oracle's own empty-slab mask."""
+    import hashlib
+
+    g = golden("links_c2")
+    nz, ny, nx = (int(v) for v in g["shape"])
+    q = int(g[f"q_{tag}"])
+    flat = c2_links_decoded(g, tag)
+    assert flat.size == int(g[f"count_{tag}"])
+    rows = np.stack(np.unravel_index(flat, (q, nz, ny, nx)), axis=1).astype(np.int64)
+    assert hashlib.sha256(np.ascontiguousarray(rows).tobytes()).digest() == g[f"sha256_{tag}"].tobytes()
+
+    z0, z1 = 104, 152
+    band = O.missing_mask(q, (z1 - z0, ny, nx), O.sphere_mask(nx, ny, z1 - z0, 128, 128, 128 - z0, 16),
+                          periodic=(True, True, False))
+    empty = O.missing_mask(q, (2, ny, nx), None, periodic=(True, True, False))[:, 0]
+    expect = []
+    for i in range(q):
+        full = np.broadcast_to(empty[i], (nz, ny, nx)).copy()
+        full[z0:z1] = band[i]
+        expect.append(np.flatnonzero(full) + i * nz * ny * nx)
+    assert np.array_equal(np.concatenate(expect), flat)
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+@pytest.mark.parametrize("q", [9, 19, 27])
+def test_correct_mass(q, tag):
+    """Global mass correction (solver.py:420, solver3d.py:287, d3q27.py:729).
+    The reference sums in the field dtype in torch's order, the oracle in
+    float64: the bound is the rounding of the sum."""
+    g = golden("mass")
+    ref = g[f"m{q}_{tag}"]
+    got = O.correct_mass(g[f"f{q}_{tag}"], float(g[f"t{q}_{tag}"]))
+    tol = 1e-6 if tag == "f32" else 1e-14
+    assert got.dtype == ref.dtype and np.max(np.abs(got - ref)) <= tol * np.max(np.abs(ref))
+    assert same(O.correct_mass(np.zeros((19, 2, 3, 4), np.float32), 5.0), g["zero_out"])

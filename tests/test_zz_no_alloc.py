@@ -74,6 +74,11 @@ def test_noalloc_capacity_and_limit(cuda):
     got, total = _noalloc(lib, stream, m, 100)
     assert total == ref.numel() and total > 100
     assert torch.equal(got, ref[:100])
+    # count-only query: no output buffer at all (null pointer, capacity 0)
+    n0 = torch.full((1,), -1, dtype=torch.int64, device=cuda)
+    _lib.check(lib.tlbm_link_list_noalloc(m.data_ptr(), m.numel(), None, 0, n0.data_ptr(), stream), "count only")
+    torch.cuda.synchronize(cuda)
+    assert int(n0.item()) == ref.numel()
     cap = lib.tlbm_link_list_static_capacity()
     assert cap == 128 * 1024 * 1024
     out = torch.empty(1, dtype=torch.int64, device=cuda)
