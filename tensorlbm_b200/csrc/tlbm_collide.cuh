@@ -8,6 +8,7 @@
 #pragma once
 
 #include "tlbm_common.cuh"
+#include "tlbm_pair.cuh"
 
 namespace tlbm {
 
@@ -45,6 +46,12 @@ __device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// a > lo ? a : lo and a < hi ? a : hi (F2 has per-component forms in tlbm_pair.cuh)
+__device__ __forceinline__ float clamp_lo(float a, float lo) { return a > lo ? a : lo; }
+__device__ __forceinline__ double clamp_lo(double a, double lo) { return a > lo ? a : lo; }
+__device__ __forceinline__ float clamp_hi(float a, float hi) { return a < hi ? a : hi; }
+__device__ __forceinline__ double clamp_hi(double a, double hi) { return a < hi ? a : hi; }
 
 // sum of +-x, +-y, +-z terms for compile-time components a, b, c in {-1, 0, 1}
 // (c_x u_x + c_y u_y + c_z u_z with exact integer products; only additions round)
@@ -145,7 +152,7 @@ __device__ __forceinline__ void macroscopic_fused(const T (&f)[L::Q], T& rho, T&
     if (L::cy(q) != 0) jy = (L::cy(q) > 0) ? jy + f[q] : jy - f[q];
     if (L::cz(q) != 0) jz = (L::cz(q) > 0) ? jz + f[q] : jz - f[q];
   }
-  const T ir = T(1) / (rho > T(1e-12) ? rho : T(1e-12));
+  const T ir = T(1) / clamp_lo(rho, T(1e-12));
   ux = jx * ir;
   uy = jy * ir;
   uz = (L::DIM == 3) ? jz * ir : T(0);
@@ -937,7 +944,7 @@ __device__ __forceinline__ void collide_bgk_deviation(T (&g)[L::Q], T om, T s) {
     if (L::cz(q) != 0) jz = (L::cz(q) > 0) ? jz + g[q] : jz - g[q];
   }
   const T rho = fma(R, T(1) / s, T(1));
-  const T srho = s * (rho > T(1e-12) ? rho : T(1e-12));
+  const T srho = s * clamp_lo(rho, T(1e-12));
   const T irs = T(1) / srho;
   const T ux = jx * irs, uy = jy * irs, uz = (L::DIM == 3) ? jz * irs : T(0);
   const T usq = usq_fused<L>(ux, uy, uz);
@@ -953,11 +960,11 @@ __device__ __forceinline__ void collide_bgk_deviation(T (&g)[L::Q], T om, T s) {
     if (L::cx(q) != 0) cu = (L::cx(q) > 0) ? cu + ux : cu - ux;
     if (L::cy(q) != 0) cu = (L::cy(q) > 0) ? cu + uy : cu - uy;
     if (L::cz(q) != 0) cu = (L::cz(q) > 0) ? cu + uz : cu - uz;
-    const T w = weight<L, T>(q);
-    const T sq = fma((T(4.5) * w * B) * cu, cu, w * base);
-    const T k3 = T(3) * w * B;
+    const double w = L::w(q);
+    const T sq = fma(T(T(4.5 * w) * B) * cu, cu, T(T(w) * base));
+    const T k3 = T(T(3.0 * w) * B), k3n = T(T(-3.0 * w) * B);
     g[q] = fma(g[q], keep, fma(k3, cu, sq));
-    g[qb] = fma(g[qb], keep, fma(-k3, cu, sq));
+    g[qb] = fma(g[qb], keep, fma(k3n, cu, sq));
   }
 }
 
@@ -980,15 +987,15 @@ __device__ __forceinline__ void collide_smagorinsky_fast(T (&f)[L::Q], const Col
   }
   T rad = pxx * pxx + pyy * pyy + T(2) * pxy * pxy;
   if constexpr (L::DIM == 3) rad += pzz * pzz + T(2) * (pxz * pxz + pyz * pyz);
-  rad = rad > T(1e-30) ? rad : T(1e-30);
-  const T rs = rho > T(1e-12) ? rho : T(1e-12);
+  rad = clamp_lo(rad, T(1e-30));
+  const T rs = clamp_lo(rho, T(1e-12));
   T disc = cp.tau_sq + cp.smag_coef * sqrt(rad) / rs;
-  disc = disc > T(0) ? disc : T(0);
+  disc = clamp_lo(disc, T(0));
   T te = T(0.5) * (cp.tau + sqrt(disc));
-  te = te < T(0.5001) ? T(0.5001) : (te > cp.tau_eff_max ? cp.tau_eff_max : te);
-  const T inv = T(1) / te;
+  te = clamp_hi(clamp_lo(te, T(0.5001)), cp.tau_eff_max);
+  const T ninv = T(-1) / te;
 #pragma unroll
-  for (int q = 0; q < L::Q; ++q) f[q] = fma(-fn[q], inv, f[q]);
+  for (int q = 0; q < L::Q; ++q) f[q] = fma(fn[q], ninv, f[q]);
 }
 
 // ---------------------------------------------------------------------------
