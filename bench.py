@@ -349,31 +349,53 @@ def _les_variant(torch, dev, steps, warmup, peak, n_mlp=128, n_smag=256):
 def _batched_variant(torch, dev, steps, peak):
     """512 D2Q9 BGK cylinder channels (nx ~ U{128..1024}, ny = nx/4, D = ny/8,
     Re ~ U(40, 300), seed 20261203) advanced together, against the same domains
-    run one after the other (TensorLBM's scan runner does points sequentially)."""
+    run one after the other (TensorLBM's scan runner does points sequentially).
+    At least 500 steps.  Domains whose BGK run turns non-finite (tau - 1/2
+    down to 0.0027; TensorLBM's own chain diverges on them at the same step)
+    are retired, as a scan marks a failed point, so the batch's time is spent
+    on the live domains; the throughput counts live cell updates only.  The
+    sequential sample is 16 domains that stay finite."""
     from tensorlbm_b200 import LBMSolver, batch
 
+    steps = max(steps, 500)
+    chunk = 100
     doms = batch.uniform_scan(512, seed=20261203, device=dev)
     f0 = batch.equilibrium_start(doms, dev)
-    b = batch.BatchedSolver(doms, "bgk", device=dev)
+    b = batch.BatchedSolver(doms, "bgk", device=dev, retire=True)
     b.load(f0)
     tune = batch.autotune(b, steps=5)
-    b.load(f0)
-    t = b.timed_steps(steps)
-    cells = b.n_cells
-    mlups = cells * steps / t / 1e6
-    fin = b.finite_domains().cpu()
-    finite_domains = int(fin.sum())
-    # BGK at tau - 1/2 = 3 u D / Re (down to 0.002 on the coarsest, fastest
-    # domains) is unstable; those domains overflow exactly as a plain run would
-    unstable_tau = sorted(round(doms[i].tau, 4) for i in range(len(doms)) if not bool(fin[i]))
-    del b
-    # sequential plain runs on a sample of 32 domains (graph-replayed fused steps)
-    sample = doms[:32]
-    seq_cells, seq_t = 0, 0.0
+    cells = torch.tensor([d.nx * d.ny for d in doms], dtype=torch.float64)
     cur = torch.cuda.current_stream(dev)
-    for d, f in zip(sample, f0[:32]):
+
+    def timed_run(record_every):
+        b.load(f0)
+        b.run(chunk, record_every=record_every)       # warm-up: graphs captured
+        b.load(f0)
+        t, live_updates = 0.0, 0.0
+        for _ in range(0, steps, chunk):
+            live = (~b.retired_domains()).cpu()
+            live_updates += float(cells[live].sum()) * chunk
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(cur)
+            b.run(chunk, record_every=record_every)
+            e1.record(cur)
+            torch.cuda.synchronize(dev)
+            t += e0.elapsed_time(e1) / 1e3
+        return t, live_updates
+
+    t, live_updates = timed_run(0)
+    finite = (~b.retired_domains()).cpu()
+    t_rec, live_rec = timed_run(10)
+    total = b.n_cells
+    # sequential plain runs of 16 domains that stayed finite (graph-replayed fused steps)
+    idx = [i for i in range(len(doms)) if bool(finite[i])]
+    pick = [idx[int(k * (len(idx) - 1) / 15)] for k in range(16)] if len(idx) >= 16 else idx
+    seq_cells, seq_t = 0, 0.0
+    for i in pick:
+        d = doms[i]
         s = LBMSolver("D2Q9", (d.ny, d.nx), d.tau, "bgk", device=dev, wall_mask=d.wall_mask,
-                      obstacle_mask=d.obstacle_mask, u_in=d.u_in, rho_out=d.rho_out).load(f)
+                      obstacle_mask=d.obstacle_mask, u_in=d.u_in, rho_out=d.rho_out).load(f0[i])
         s.run(64)
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -384,13 +406,88 @@ def _batched_variant(torch, dev, steps, peak):
         seq_t += e0.elapsed_time(e1) / 1e3
         seq_cells += d.nx * d.ny
     seq_mlups = seq_cells * steps / seq_t / 1e6
+    live_mlups = live_updates / t / 1e6
+    del b
     torch.cuda.empty_cache()
-    return {"mlups": round(mlups, 1), "ms_per_step": round(1e3 * t / steps, 4), "domains": 512, "cells": cells,
-            "roofline_frac": round(72 * cells / (t / steps) / 1e9 / peak, 4), "bytes_per_cell": 72,
-            "mode": tune["best"]["mode"], "tile": list(tune["best"]["tile"]),
-            "sequential_mlups_32_domain_sample": round(seq_mlups, 1),
-            "speedup_vs_sequential": round(mlups / seq_mlups, 2), "finite_domains": finite_domains,
-            "nonfinite_domains_tau_max": unstable_tau[-1] if unstable_tau else None}
+    return {"steps": steps, "domains": 512, "cells": total,
+            "mlups_live": round(live_mlups, 1), "ms_per_step": round(1e3 * t / steps, 4),
+            "mlups_all_cells": round(total * steps / t / 1e6, 1),
+            "mlups_live_recording_forces_every_10": round(live_rec / t_rec / 1e6, 1),
+            "roofline_frac_live": round(72 * live_updates / t / 1e9 / peak, 4), "bytes_per_cell": 72,
+            "mode": tune["best"]["mode"], "tile": list(tune["best"]["tile"]), "order": tune["best"]["order"],
+            "ctas_per_sm": tune["best"]["ctas_per_sm"],
+            "finite_domains": int(finite.sum()), "retired_domains": 512 - int(finite.sum()),
+            "sequential_mlups_16_finite_domains": round(seq_mlups, 1),
+            "speedup_vs_sequential": round(live_mlups / seq_mlups, 2)}
+
+
+C2_LONG = "c2_20k_vs_fp64"     # opt-in variant: --variants c2_20k_vs_fp64 [--long-steps N]
+
+
+def _c2_long_variant(torch, dev, steps, every):
+    """Config 2 at its stated length: the 512 x 256 x 256 sphere channel
+    (D3Q19 MRT and D3Q27 legacy cumulant) run for `steps` steps with float32
+    storage beside the same run with float64 storage (the FP64 oracle run on
+    the GPU), the FP64 drag of both recorded every step.  Every `every` steps:
+    velocity L2 error ||u32 - u64|| / ||u64|| over the fluid, the largest
+    population error relative to max |f64|, the density error, and the drag
+    difference."""
+    from tensorlbm_b200.d3q19 import macroscopic3d
+    from tensorlbm_b200.d3q27 import macroscopic27
+
+    out = {}
+    for lattice, coll in (("D3Q19", "mrt"), ("D3Q27", "cumulant")):
+        runs = {}
+        for st in ("f32", "f64"):
+            s, obst = _make_solver(torch, dev, lattice, coll, st, False)
+            f0 = _initial_state(torch, dev, lattice, obst)
+            s.load(f0.double() if st == "f64" else f0)
+            runs[st] = (s, torch.zeros((steps, 3), dtype=torch.float64, device=dev))
+            del f0
+        fluid = ~obst
+        mac = macroscopic3d if lattice == "D3Q19" else macroscopic27
+        hist = []
+        t = {"f32": 0.0, "f64": 0.0}
+        for k0 in range(0, steps, every):
+            k1 = min(steps, k0 + every)
+            for st, (s, drag) in runs.items():
+                torch.cuda.synchronize(dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for k in range(k0, k1):
+                    s._launch_parity(s._cur, drag[k])
+                    s._cur = s._next_parity(s._cur)
+                e1.record()
+                torch.cuda.synchronize(dev)
+                t[st] += e0.elapsed_time(e1) / 1e3
+                s.steps_done += k1 - k0
+            fa, fb = runs["f32"][0].f, runs["f64"][0].f
+            ra, *ua = mac(fa)
+            rb, *ub = mac(fb)
+            num = sum(float(((a.double() - b)[fluid] ** 2).sum()) for a, b in zip(ua, ub))
+            den = sum(float((b[fluid] ** 2).sum()) for b in ub)
+            da, db = runs["f32"][1][k1 - 1], runs["f64"][1][k1 - 1]
+            hist.append({"step": k1, "velocity_l2": math.sqrt(num / den),
+                         "f_max_rel": float((fa.double() - fb).abs().max() / fb.abs().max()),
+                         "rho_max_abs": float((ra.double() - rb).abs().max()),
+                         "drag_fx_f32": float(da[0]), "drag_fx_f64": float(db[0]),
+                         "drag_fx_rel": float(abs(da[0] - db[0]) / abs(db[0])),
+                         "finite": bool(torch.isfinite(fa).all())})
+            del fa, fb, ra, rb, ua, ub
+        d32, d64 = runs["f32"][1], runs["f64"][1]
+        tail = slice(steps - steps // 10, steps)
+        cells = NX * NY * NZ
+        out[f"{lattice.lower()}_{coll}"] = {
+            "steps": steps, "tau": TAU, "history": hist,
+            "drag_fx_mean_last10pct_f32": float(d32[tail, 0].mean()),
+            "drag_fx_mean_last10pct_f64": float(d64[tail, 0].mean()),
+            "drag_fx_max_rel_after_1000": float(((d32[1000:, 0] - d64[1000:, 0]).abs()
+                                                 / d64[1000:, 0].abs()).max()) if steps > 1000 else None,
+            "mlups_f32": round(cells * steps / t["f32"] / 1e6, 1),
+            "mlups_f64": round(cells * steps / t["f64"] / 1e6, 1)}
+        del runs, d32, d64
+        torch.cuda.empty_cache()
+    return out
 
 
 REF_TRITON = "reference_triton_256"   # opt-in variant: --variants reference_triton_256
@@ -658,6 +755,8 @@ def run_ours(args) -> None:
         variants["d2q9_batched_512_cylinders"] = _batched_variant(torch, dev, args.steps, peak)
     if wanted is not None and REF_TRITON in wanted and not args.no_variants:
         variants[REF_TRITON] = _reference_triton_variant(torch, dev, args.steps, args.warmup, peak)
+    if wanted is not None and C2_LONG in wanted and not args.no_variants:
+        variants[C2_LONG] = _c2_long_variant(torch, dev, args.long_steps, args.long_every)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -854,6 +953,8 @@ def main() -> None:
                          "les_mlp_128_vs_smagorinsky_256, d2q9_batched_512_cylinders) or 'all'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-slab", type=int, default=16, help="z-planes of the CPU sample slab")
+    ap.add_argument("--long-steps", type=int, default=20000, help="steps of the c2_20k_vs_fp64 variant")
+    ap.add_argument("--long-every", type=int, default=2000, help="comparison interval of c2_20k_vs_fp64")
     ap.add_argument("--grid", default=None,
                     help="nx,ny,nz of a smaller channel (profiling only; the sphere keeps its size, centred)")
     args = ap.parse_args()

@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 #define TLBM_API __attribute__((visibility("default")))
-#define TLBM_ABI_VERSION 1
+#define TLBM_ABI_VERSION 2
 
 typedef enum tlbm_status {
   TLBM_OK = 0,
@@ -297,16 +297,19 @@ TLBM_API int tlbm_link_list_noalloc(const uint8_t* mask, int64_t count, int64_t*
                                     int64_t* count_out, void* stream);
 TLBM_API int64_t tlbm_link_list_static_capacity(void);
 
-/* ---- batched runner: many independent small D2Q9 domains ----------------------
+/* ---- batched runner: many independent small domains --------------------------
  * Replaces the sequential per-point loop of the scan runner
- * (scan_runner.py:697 run_scan_point, :979 ScanExecutor) for the cylinder-flow
- * chain of cylinder_flow.py:854-899 (collide -> stream -> force -> Zou/He inlet
- * -> outlet -> bounce-back).  Each domain is a (9, ny, nx) block at f_offset
- * (elements) in one packed population buffer, with its ny*nx flag bytes at
- * cell_offset in one packed flag buffer.  tiles holds ntiles triplets
- * (domain, x0, y0) of tile_x x tile_y cells; every cell of every domain must be
- * in exactly one tile.  Every domain evolves bit for bit as tlbm_step would
- * advance it alone. */
+ * (scan_runner.py:697 run_scan_point, :979 ScanExecutor): D2Q9 for the
+ * cylinder-flow chain of cylinder_flow.py:854-899 (collide -> stream -> force
+ * -> Zou/He inlet -> outlet -> bounce-back), D3Q19 for the case chain of
+ * cases/base.py:270-289 (collide -> pre-streaming half-way walls -> stream ->
+ * lid), the lid-driven cavity of cases/cavity.py:25-110.  Each domain is a
+ * (Q, nz, ny, nx) block at f_offset (elements) in one packed population
+ * buffer, with its nz*ny*nx flag bytes at cell_offset in one packed flag
+ * buffer.  tiles holds ntiles triplets (domain, x0, r0) of tile_x x tile_y
+ * cells, where r0 counts the domain's nz*ny rows (row r is y = r % ny,
+ * z = r / ny); every cell of every domain must be in exactly one tile.  Every
+ * domain evolves bit for bit as tlbm_step would advance it alone. */
 typedef struct tlbm_batch_domain {
   int64_t f_offset;
   int64_t cell_offset;
@@ -315,11 +318,12 @@ typedef struct tlbm_batch_domain {
   double u_in;      /* Zou/He inlet x-velocity (TLBM_BC_ZH_INLET) */
   double rho_out;   /* Zou/He outlet density (TLBM_BC_ZH_OUTLET) */
   uint32_t bc;
-  uint32_t reserved;
+  int32_t nz;       /* planes (D3Q19); 0 or 1 for D2Q9 */
+  double u_lid;     /* lid x-velocity at y = ny - 1 (TLBM_BC_LID) */
 } tlbm_batch_domain;
 
 typedef struct tlbm_batch_desc {
-  int32_t lattice;      /* TLBM_D2Q9 */
+  int32_t lattice;      /* TLBM_D2Q9 or TLBM_D3Q19 */
   int32_t dtype;        /* TLBM_F32 */
   int32_t collision;    /* TLBM_COLL_BGK or TLBM_COLL_MRT */
   int32_t ndomains;
@@ -327,6 +331,11 @@ typedef struct tlbm_batch_desc {
   int32_t tile_y;
   int32_t ctas_per_sm;  /* persistent mode: CTAs per SM (0 = occupancy limit) */
   int32_t reserved;
+  uint32_t* domain_status; /* device, ndomains words, or NULL.  When given, a
+                            * domain's non-finite density sets its own word
+                            * (bit 0) instead of the status word, and a domain
+                            * whose word is non-zero is retired: later tiles
+                            * and steps skip it, its state stays as it was. */
 } tlbm_batch_desc;
 
 /* One step of every domain, one launch (grid = tiles).  domains and tiles are
@@ -430,6 +439,10 @@ TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, doub
 
 TLBM_API const char* tlbm_status_string(int status);
 TLBM_API int tlbm_abi_version(void);
+/* sizeof of the structs a binding mirrors: 0 tlbm_desc, 1 tlbm_batch_domain,
+ * 2 tlbm_batch_desc (-1 otherwise), so that a binding can check its layout.
+ * No reference counterpart. */
+TLBM_API int64_t tlbm_struct_size(int32_t which);
 
 /* ---- AA pattern: the step in place, one population buffer -------------------
  * Between steps the buffer holds one of three layouts: TLBM_AA_LOADED (slot q

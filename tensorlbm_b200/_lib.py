@@ -70,7 +70,8 @@ class BatchDomain(ctypes.Structure):
 
     _fields_ = [("f_offset", ctypes.c_int64), ("cell_offset", ctypes.c_int64), ("nx", ctypes.c_int32),
                 ("ny", ctypes.c_int32), ("tau", ctypes.c_double), ("u_in", ctypes.c_double),
-                ("rho_out", ctypes.c_double), ("bc", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("rho_out", ctypes.c_double), ("bc", ctypes.c_uint32), ("nz", ctypes.c_int32),
+                ("u_lid", ctypes.c_double)]
 
 
 class BatchDesc(ctypes.Structure):
@@ -78,7 +79,7 @@ class BatchDesc(ctypes.Structure):
 
     _fields_ = [("lattice", ctypes.c_int32), ("dtype", ctypes.c_int32), ("collision", ctypes.c_int32),
                 ("ndomains", ctypes.c_int32), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("ctas_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32), ("domain_status", ctypes.c_void_p)]
 
 
 _P = ctypes.c_void_p
@@ -133,9 +134,11 @@ SIGNATURES: dict[str, list] = {
     "tlbm_les_step": [_I32, _I32, _I32, _D, _D, _D, _P, _P, _P, _P, _P, _P, _P],
     "tlbm_status_string": [ctypes.c_int],
     "tlbm_abi_version": [],
+    "tlbm_struct_size": [_I32],
 }
 _RESTYPES = {"tlbm_link_blocks": _I64, "tlbm_link_list_static_capacity": _I64, "tlbm_status_string": ctypes.c_char_p,
-             "tlbm_mlp_param_count": _I32, "tlbm_mlp_blob_bytes": _I32, "tlbm_mlp_grad_blocks": _I64}
+             "tlbm_mlp_param_count": _I32, "tlbm_mlp_blob_bytes": _I32, "tlbm_mlp_grad_blocks": _I64,
+             "tlbm_struct_size": _I64}
 
 _lib: ctypes.CDLL | None = None
 

@@ -9,8 +9,15 @@ A = epsilon / (2 K) from the current kinetic energy K, so that the injection
 rate is the target dissipation whatever the integral scale does (Carroll &
 Blanquart 2013).  A grid filtered by a factor r uses dx_r = dt_r = r (acoustic
 scaling): nu_r = nu / r, epsilon_r = epsilon r, and one filtered step covers r
-DNS steps.  ``HITConfig.les`` lists the LES
-grids; the first one runs the learned closure.
+DNS steps.  ``HITConfig.les`` lists the LES grids: every grid but the last
+runs the learned closure (its nu_t scale calibrated on that grid), Smagorinsky
+and no model; the last runs Smagorinsky, the fine-grid judge (a single grid
+runs all three).
+
+The a-posteriori error of an LES is mean |ln(E_LES(k) / E_fDNS(k))| over the
+shells 1 <= k <= min(m/2, 21), where E_fDNS is the spectrum of the DNS
+block-filtered (mean over r^3 cells) to the LES grid m = n / r, both averaged
+over the comparison window's spectra.
 
 Run as a module for the full experiment:
 
@@ -134,7 +141,7 @@ class HITConfig:
     max_samples_per_grid: int = 3_000_000
     chunk: int = 50                 # steps per CUDA graph replay
     dns_collision: str = "mrt"      # BGK diverges at the DNS's tau ~ 0.515
-    calibration: tuple = (1.0, 0.7, 0.5, 0.35, 0.25, 0.15)  # candidate nu_t scale factors
+    calibration: tuple = (1.0, 0.7, 0.5, 0.35, 0.25, 0.15, 0.1, 0.05)  # candidate nu_t scale factors
 
     force_every: int = 100          # steps between updates of the constant-power force
 
@@ -386,32 +393,41 @@ def run(cfg: HITConfig, out_dir: pathlib.Path, device="cuda:0", log=print) -> di
         torch.cuda.empty_cache()
         return specs, secs, finite, fb
 
-    # in-the-loop calibration of the network's scale on the TRAINING window:
-    # the LES starts from the first training snapshot and is compared with the
-    # filtered spectra of the later training snapshots (not the comparison window)
-    m0 = cfg.les[0]
-    r0 = n // m0
-    train_ref = np.mean([energy_spectrum(mm[1:4]).cpu().numpy() for mm in moms[m0][1:]], axis=0)
+    # in-the-loop calibration of the network's scale on the TRAINING window, on
+    # every grid that runs the closure: the LES starts from the first training
+    # snapshot and is compared with the filtered spectra of the later training
+    # snapshots (not the comparison window)
+    closure_grids = list(cfg.les[:-1]) if len(cfg.les) > 1 else list(cfg.les)
     base_scale = model.nu_scale
-    calib = {}
-    if cfg.snapshots > 1:
-        for alpha in cfg.calibration:
-            model.nu_scale = base_scale * alpha
-            model.invalidate()
-            specs, _, fin, _ = les_run("mlp", m0, moms[m0][0], cfg.snapshots - 1, max(1, gap // r0))
-            err = _spec_error(np.mean(specs, axis=0), train_ref, min(m0 // 2, 21)) if fin else float("inf")
-            calib[str(alpha)] = err
-            log(f"calibration alpha {alpha}: error {err:.4f}")
-    alpha_best = float(min(calib, key=calib.get)) if calib else 1.0
-    res["calibration"] = {"errors": calib, "alpha": alpha_best}
+    calib, alpha_of = {}, {}
+    for m in closure_grids:
+        r = n // m
+        train_ref = np.mean([energy_spectrum(mm[1:4]).cpu().numpy() for mm in moms[m][1:]], axis=0)
+        errs = {}
+        if cfg.snapshots > 1:
+            for alpha in cfg.calibration:
+                model.nu_scale = base_scale * alpha
+                model.invalidate()
+                specs, _, fin, _ = les_run("mlp", m, moms[m][0], cfg.snapshots - 1, max(1, gap // r))
+                err = _spec_error(np.mean(specs, axis=0), train_ref, min(m // 2, 21)) if fin else float("inf")
+                errs[str(alpha)] = err
+                log(f"calibration {m}^3 alpha {alpha}: error {err:.4f}")
+        calib[str(m)] = errs
+        alpha_of[m] = float(min(errs, key=errs.get)) if errs else 1.0
+    alpha_best = alpha_of[closure_grids[0]]
+    res["calibration"] = {"errors": calib[str(closure_grids[0])], "alpha": alpha_best,
+                          "per_grid": {str(m): {"errors": calib[str(m)], "alpha": alpha_of[m]} for m in closure_grids}}
     model.nu_scale = base_scale * alpha_best
     model.invalidate()
     model.save(out_dir / "closure.npz")
 
+    plan = []
+    for m in closure_grids:
+        plan += [("mlp", m, "mlp", alpha_of[m]), ("mlp_uncalibrated", m, "mlp", 1.0), ("smagorinsky", m, "smag", None),
+                 ("no_model", m, "bgk", None)]
+    plan.append(("smagorinsky", cfg.les[-1], "smag", None))
     runs: dict = {}
-    for name, m, kind, alpha in (("mlp", cfg.les[0], "mlp", alpha_best), ("mlp_uncalibrated", cfg.les[0], "mlp", 1.0),
-                                 ("smagorinsky", cfg.les[0], "smag", None),
-                                 ("smagorinsky", cfg.les[-1], "smag", None), ("no_model", cfg.les[0], "bgk", None)):
+    for name, m, kind, alpha in plan:
         if f"{name}_{m}" in runs:
             continue
         if kind == "mlp":
@@ -440,15 +456,18 @@ def run(cfg: HITConfig, out_dir: pathlib.Path, device="cuda:0", log=print) -> di
     model.nu_scale = base_scale * alpha_best
     model.invalidate()
     res["les"] = runs
-    mlp_key, big_key = f"mlp_{cfg.les[0]}", f"smagorinsky_{cfg.les[-1]}"
+    m0 = closure_grids[0]
+    mlp_key, big_key = f"mlp_{m0}", f"smagorinsky_{cfg.les[-1]}"
     res["summary"] = {
         "mlp_les_error": runs[mlp_key]["spectrum_error_k_le_21"],
-        "mlp_uncalibrated_les_error": runs[f"mlp_uncalibrated_{cfg.les[0]}"]["spectrum_error_k_le_21"],
-        "smagorinsky_coarse_error": runs[f"smagorinsky_{cfg.les[0]}"]["spectrum_error_k_le_21"],
+        "mlp_uncalibrated_les_error": runs[f"mlp_uncalibrated_{m0}"]["spectrum_error_k_le_21"],
+        "smagorinsky_coarse_error": runs[f"smagorinsky_{m0}"]["spectrum_error_k_le_21"],
         "smagorinsky_fine_error": runs[big_key]["spectrum_error_k_le_21"],
-        "no_model_coarse_error": runs[f"no_model_{cfg.les[0]}"]["spectrum_error_k_le_21"],
+        "no_model_coarse_error": runs[f"no_model_{m0}"]["spectrum_error_k_le_21"],
         "calibration_alpha": alpha_best,
         "wall_time_ratio_smagorinsky_fine_over_mlp": runs[big_key]["seconds"] / max(runs[mlp_key]["seconds"], 1e-12),
+        "per_grid": {str(m): {k: runs[f"{k}_{m}"]["spectrum_error_k_le_21"]
+                              for k in ("mlp", "mlp_uncalibrated", "smagorinsky", "no_model")} for m in closure_grids},
     }
     (out_dir / "hit_les.json").write_text(json.dumps(res))
     return res

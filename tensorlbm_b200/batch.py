@@ -31,8 +31,11 @@ def _fn(name):
 
 @dataclass
 class DomainSpec:
-    """One channel domain: (ny, nx) grid, BGK/MRT relaxation time, Zou/He inlet
-    velocity and outlet density (None disables the plane), wall and obstacle masks."""
+    """One domain: (ny, nx) grid (D2Q9) or (nz, ny, nx) with nz > 1 (D3Q19),
+    BGK/MRT relaxation time, Zou/He inlet velocity and outlet density (None
+    disables the plane), moving-lid velocity at y = ny - 1 (None: no lid),
+    wall and obstacle masks, and how the walls bounce back ("fullway" after
+    streaming, or "halfway": pre-streaming, from the pre-collision state)."""
 
     nx: int
     ny: int
@@ -41,6 +44,53 @@ class DomainSpec:
     rho_out: float | None = 1.0
     wall_mask: torch.Tensor | None = None
     obstacle_mask: torch.Tensor | None = None
+    nz: int = 1
+    u_lid: float | None = None
+    wall_mode: str = "fullway"
+
+    @property
+    def shape(self) -> tuple[int, ...]:
+        return (self.ny, self.nx) if self.nz == 1 else (self.nz, self.ny, self.nx)
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def bc(self) -> int:
+        return ((_lib.BC_ZH_INLET if self.u_in is not None else 0) |
+                (_lib.BC_ZH_OUTLET if self.rho_out is not None else 0) |
+                (_lib.BC_LID if self.u_lid is not None else 0))
+
+
+def cavity_point(resolution, re: float = 400.0, *, u_lid: float = 0.06, span: int | None = None,
+                 device=None) -> DomainSpec:
+    """TensorLBM's lid-driven cavity case (cases/cavity.py:25-110) as one
+    D3Q19 domain: resolution n gives (nz, ny, nx) = (span or max(4, n // 4), n, n)
+    (or an explicit (nz, ny, nx)); stationary walls x = 0, x = nx - 1, y = 0
+    bounce back half-way before streaming from the pre-collision state; the
+    Zou/He lid moves at y = ny - 1; z is periodic; tau = 1/2 + nu / (1/3) with
+    nu = u_lid nx / Re (cases/base.py:67-75 CaseUnits.from_reference); the
+    state starts at rest (rho = 1)."""
+    if isinstance(resolution, int):
+        if resolution < 8:
+            raise ValueError(f"resolution must be >= 8, got {resolution}")
+        shape = (span if span is not None else max(4, resolution // 4), resolution, resolution)
+    else:
+        if len(resolution) != 3:
+            raise ValueError("resolution sequence must be (nz, ny, nx)")
+        shape = tuple(int(v) for v in resolution)
+    nz, ny, nx = shape
+    if re <= 0 or u_lid <= 0:
+        raise ValueError("re and u_lid must be positive")
+    nu = u_lid * float(nx) / re
+    tau = 0.5 + nu / (1.0 / 3.0)
+    dev = _ops.cuda_device(device)
+    wall = torch.zeros(shape, dtype=torch.bool, device=dev)
+    wall[:, :, 0] = True
+    wall[:, :, -1] = True
+    wall[:, 0, :] = True
+    return DomainSpec(nx, ny, tau, None, None, wall, None, nz=nz, u_lid=float(u_lid), wall_mode="halfway")
 
 
 def cylinder_channel(nx: int, re: float, u_in: float = 0.05, device=None) -> DomainSpec:
@@ -57,7 +107,7 @@ def cylinder_channel(nx: int, re: float, u_in: float = 0.05, device=None) -> Dom
 
 
 class BatchedSolver:
-    """Packed multi-domain D2Q9 solver (float32).
+    """Packed multi-domain D2Q9 or D3Q19 solver (float32).
 
     State phase and API follow :class:`tensorlbm_b200.LBMSolver`: ``load``
     takes TensorLBM-phase fields, ``f(i)`` returns domain i in that phase, and
@@ -67,13 +117,22 @@ class BatchedSolver:
     ALIGN = 32  # elements: every domain block starts on a 128-byte boundary
 
     def __init__(self, domains: list[DomainSpec], collision: str = "bgk", *, device=None,
-                 tile: tuple[int, int] = (64, 4), mode: str = "graph", ctas_per_sm: int = 0):
+                 tile: tuple[int, int] = (64, 4), mode: str = "graph", ctas_per_sm: int = 0,
+                 lattice: str = "D2Q9", order: str = "domain", retire: bool = False):
         if collision not in ("bgk", "mrt"):
             raise ValueError("the batched runner supports 'bgk' and 'mrt'")
         if mode not in ("graph", "launch", "persistent"):
             raise ValueError("mode must be 'graph', 'launch' or 'persistent'")
+        if lattice not in ("D2Q9", "D3Q19"):
+            raise ValueError("the batched runner supports D2Q9 and D3Q19 domains")
+        self.q = 9 if lattice == "D2Q9" else 19
+        self.lattice = lattice
         self.device = _ops.cuda_device(device)
         self.domains = list(domains)
+        for i, d in enumerate(self.domains):
+            if (self.q == 9) != (d.nz == 1):
+                raise ValueError(f"domain {i} has nz = {d.nz}: {lattice} domains need "
+                                 f"{'nz == 1' if self.q == 9 else 'nz > 1'}")
         self.collision = collision
         self.mode = mode
         n = len(self.domains)
@@ -81,17 +140,18 @@ class BatchedSolver:
         f_off, c_off = 0, 0
         self.f_offsets, self.cell_offsets = [], []
         for i, d in enumerate(self.domains):
-            cells = d.nx * d.ny
+            cells = d.cells
             doms[i].f_offset, doms[i].cell_offset = f_off, c_off
-            doms[i].nx, doms[i].ny, doms[i].tau = d.nx, d.ny, float(d.tau)
+            doms[i].nx, doms[i].ny, doms[i].nz, doms[i].tau = d.nx, d.ny, d.nz, float(d.tau)
             doms[i].u_in = float(d.u_in or 0.0)
             doms[i].rho_out = float(1.0 if d.rho_out is None else d.rho_out)
-            doms[i].bc = (_lib.BC_ZH_INLET if d.u_in is not None else 0) | (_lib.BC_ZH_OUTLET if d.rho_out is not None else 0)
+            doms[i].u_lid = float(d.u_lid or 0.0)
+            doms[i].bc = d.bc
             self.f_offsets.append(f_off)
             self.cell_offsets.append(c_off)
-            f_off += -(-9 * cells // self.ALIGN) * self.ALIGN
+            f_off += -(-self.q * cells // self.ALIGN) * self.ALIGN
             c_off += -(-cells // self.ALIGN) * self.ALIGN
-        self.n_cells = sum(d.nx * d.ny for d in self.domains)
+        self.n_cells = sum(d.cells for d in self.domains)
         self._host_domains = doms
         self.domains_dev = torch.frombuffer(bytearray(doms), dtype=torch.uint8).to(self.device)
         self.fa = torch.zeros(f_off, dtype=torch.float32, device=self.device)
@@ -99,11 +159,17 @@ class BatchedSolver:
         self.flags = torch.zeros(c_off, dtype=torch.uint8, device=self.device)
         for i, d in enumerate(self.domains):
             if d.wall_mask is not None or d.obstacle_mask is not None:
-                fl = _ops.build_flags((d.ny, d.nx), self.device, d.wall_mask, d.obstacle_mask)
-                self.flags[self.cell_offsets[i]: self.cell_offsets[i] + d.nx * d.ny] = fl.reshape(-1)
+                fl = _ops.build_flags(d.shape, self.device, d.wall_mask, d.obstacle_mask, d.wall_mode)
+                self.flags[self.cell_offsets[i]: self.cell_offsets[i] + d.cells] = fl.reshape(-1)
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # retire: a domain that turns non-finite is skipped from then on (a
+        # scan marks such a point failed; its cells cost nothing more)
+        self.domain_status = torch.zeros(n, dtype=torch.int32, device=self.device) if retire else None
         self.sync = torch.zeros(3, dtype=torch.int32, device=self.device)
+        self._pgraphs: dict = {}
+        self._pgraph_capture = True   # persistent launches go through CUDA graphs
         self.ctas_per_sm = ctas_per_sm
+        self.order = order
         self.set_tile(*tile)
         self.steps_done = 0
         self.step_offsets = [0] * n   # steps each domain had completed before the last load()/resume()
@@ -113,46 +179,64 @@ class BatchedSolver:
 
     # -- layout -----------------------------------------------------------------
 
-    def set_tile(self, tx: int, ty: int) -> None:
+    ORDERS = ("domain", "interleave", "largest_first")
+
+    def set_tile(self, tx: int, ty: int, order: str | None = None) -> None:
+        """Tile shape (tx x ty cells over the rows of each domain) and the
+        order of the tile list, which is the CTA-to-domain mapping: the launch
+        gives CTA b tile b, the persistent kernel gives CTA b tiles b, b + G,
+        b + 2G ...  "domain": each domain's tiles together, row by row;
+        "interleave": round robin over the domains (one tile of each in turn);
+        "largest_first": the domains by decreasing size, each contiguous."""
         if tx % 32 or tx * ty > 256 or ty < 1:
             raise ValueError("tile_x must be a multiple of 32 and tile_x * tile_y <= 256")
+        order = order or getattr(self, "order", "domain")
+        if order not in self.ORDERS:
+            raise ValueError(f"order must be one of {self.ORDERS}")
         self.tile = (tx, ty)
-        tiles = []
+        self.order = order
+        per = []
         for i, d in enumerate(self.domains):
-            for y0 in range(0, d.ny, ty):
-                for x0 in range(0, d.nx, tx):
-                    tiles.append((i, x0, y0))
+            per.append([(i, x0, r0) for r0 in range(0, d.ny * d.nz, ty) for x0 in range(0, d.nx, tx)])
+        if order == "interleave":
+            tiles = [t for k in range(max(len(p) for p in per)) for p in per if k < len(p)]
+        elif order == "largest_first":
+            tiles = [t for i in sorted(range(len(per)), key=lambda i: -self.domains[i].cells) for t in per[i]]
+        else:
+            tiles = [t for p in per for t in p]
         self.ntiles = len(tiles)
         self.tiles_dev = torch.tensor(tiles, dtype=torch.int32, device=self.device).reshape(-1)
         self._graph = None
+        self._pgraphs = {}
 
     def _desc(self) -> BatchDesc:
         b = BatchDesc()
-        b.lattice, b.dtype = 9, _lib.F32
+        b.lattice, b.dtype = self.q, _lib.F32
         b.collision = _lib.COLL_BGK if self.collision == "bgk" else _lib.COLL_MRT
         b.ndomains = len(self.domains)
         b.tile_x, b.tile_y = self.tile
         b.ctas_per_sm = self.ctas_per_sm
+        b.domain_status = _lib.ptr(self.domain_status)
         return b
 
     def _view(self, buf: torch.Tensor, i: int) -> torch.Tensor:
         d = self.domains[i]
         o = self.f_offsets[i]
-        return buf[o: o + 9 * d.nx * d.ny].view(9, d.ny, d.nx)
+        return buf[o: o + self.q * d.cells].view((self.q,) + d.shape)
 
     def _flags_view(self, i: int) -> torch.Tensor:
         d = self.domains[i]
         o = self.cell_offsets[i]
-        return self.flags[o: o + d.nx * d.ny].view(d.ny, d.nx)
+        return self.flags[o: o + d.cells].view(d.shape)
 
     def _single_desc(self, i: int, collision: str):
         from .solvers import COLLISIONS
 
         d = self.domains[i]
-        bc = (_lib.BC_ZH_INLET if d.u_in is not None else 0) | (_lib.BC_ZH_OUTLET if d.rho_out is not None else 0)
-        return _ops.make_desc(9, (d.nx, d.ny, 1), _lib.F32, COLLISIONS[collision], d.tau, s_e=1.64, s_eps=1.54,
-                              s_q=1.7, bc=bc, u_in=(float(d.u_in or 0.0), 0.0, 0.0),
-                              rho_out=float(1.0 if d.rho_out is None else d.rho_out))
+        rates = dict(s_e=1.64, s_eps=1.54, s_q=1.7) if self.q == 9 else dict(s_e=1.19, s_eps=1.4, s_q=1.2)
+        return _ops.make_desc(self.q, (d.nx, d.ny, d.nz), _lib.F32, COLLISIONS[collision], d.tau, bc=d.bc,
+                              u_in=(float(d.u_in or 0.0), 0.0, 0.0), u_lid=float(d.u_lid or 0.0),
+                              rho_out=float(1.0 if d.rho_out is None else d.rho_out), **rates)
 
     # -- state ----------------------------------------------------------------
 
@@ -164,8 +248,8 @@ class BatchedSolver:
         s = _lib.stream_of(self.device)
         for i, f in enumerate(fields):
             d = self.domains[i]
-            if tuple(f.shape) != (9, d.ny, d.nx):
-                raise ValueError(f"domain {i}: expected {(9, d.ny, d.nx)}, got {tuple(f.shape)}")
+            if tuple(f.shape) != (self.q,) + d.shape:
+                raise ValueError(f"domain {i}: expected {(self.q,) + d.shape}, got {tuple(f.shape)}")
             src = f.to(device=self.device, dtype=torch.float32).contiguous()
             desc = self._single_desc(i, self.collision)
             _lib.check(lib.tlbm_collide(ctypes.byref(desc), _lib.F32, src.data_ptr(), self._view(self.fa, i).data_ptr(),
@@ -175,8 +259,17 @@ class BatchedSolver:
         self.step_offsets = [0] * len(self.domains)
         self.forces = []
         self._graph = None
+        self._pgraphs = {}
+        if self.domain_status is not None:
+            self.domain_status.zero_()
         self._f0 = [f.to(self.device, torch.float32).clone() for f in fields]
         return self
+
+    def retired_domains(self) -> torch.Tensor:
+        """Bool per domain: retired after a non-finite density (retire=True only)."""
+        if self.domain_status is None:
+            return torch.zeros(len(self.domains), dtype=torch.bool, device=self.device)
+        return self.domain_status != 0
 
     def resume(self, fields: list[torch.Tensor], steps: list[int]) -> "BatchedSolver":
         """Continue from checkpointed TensorLBM-phase fields; ``steps[i]`` is the
@@ -253,16 +346,52 @@ class BatchedSolver:
         if record_every > 0:
             hist = torch.zeros((-(-n // record_every), len(self.domains), 3), dtype=torch.float64, device=self.device)
         if self.mode == "persistent":
-            a, b = self._bufs()
-            st = _fn("tlbm_batch_run")(ctypes.byref(self._desc()), self.domains_dev.data_ptr(),
-                                      self.tiles_dev.data_ptr(), self.ntiles, a.data_ptr(), b.data_ptr(),
-                                      self.flags.data_ptr(), n, _lib.ptr(hist), record_every,
-                                      self.sync.data_ptr(), self.status.data_ptr(), max_spins,
-                                      _lib.stream_of(self.device))
-            _lib.check(st, "tlbm_batch_run")
+            # one persistent cooperative launch of n steps, captured in a CUDA
+            # graph the first time (per n, recording interval and parity) and
+            # replayed after that; the forces go to the graph's own history
+            key = (n, record_every, self._cur, max_spins)
+            entry = self._pgraphs.get(key)
+            if entry is None and not self._pgraph_capture:
+                a, b = self._bufs()
+                st = _fn("tlbm_batch_run")(ctypes.byref(self._desc()), self.domains_dev.data_ptr(),
+                                          self.tiles_dev.data_ptr(), self.ntiles, a.data_ptr(), b.data_ptr(),
+                                          self.flags.data_ptr(), n, _lib.ptr(hist), record_every,
+                                          self.sync.data_ptr(), self.status.data_ptr(), max_spins,
+                                          _lib.stream_of(self.device))
+                _lib.check(st, "tlbm_batch_run")
+                self._cur ^= n & 1
+                self.steps_done += n
+                return hist
+            if entry is None:
+                ghist = None if hist is None else torch.zeros_like(hist)
+                a, b = self._bufs()
+                desc = self._desc()
+                s = torch.cuda.Stream(self.device)
+                s.wait_stream(torch.cuda.current_stream(self.device))
+                g = torch.cuda.CUDAGraph()
+                try:
+                    with torch.cuda.stream(s), torch.cuda.graph(g, stream=s):
+                        if ghist is not None:
+                            ghist.zero_()
+                        st = _fn("tlbm_batch_run")(ctypes.byref(desc), self.domains_dev.data_ptr(),
+                                                  self.tiles_dev.data_ptr(), self.ntiles, a.data_ptr(),
+                                                  b.data_ptr(), self.flags.data_ptr(), n, _lib.ptr(ghist),
+                                                  record_every, self.sync.data_ptr(), self.status.data_ptr(),
+                                                  max_spins, _lib.stream_of(self.device))
+                        _lib.check(st, "tlbm_batch_run (capture)")
+                except RuntimeError:
+                    # a runtime without graph capture of cooperative launches:
+                    # launch directly from now on
+                    torch.cuda.current_stream(self.device).wait_stream(s)
+                    self._pgraph_capture = False
+                    return self.run(n, record_every=record_every, chunk=chunk, max_spins=max_spins)
+                torch.cuda.current_stream(self.device).wait_stream(s)
+                entry = (g, ghist)
+                self._pgraphs[key] = entry
+            entry[0].replay()
             self._cur ^= n & 1
             self.steps_done += n
-            return hist
+            return None if hist is None else entry[1].clone()
         if record_every > 0 and self.mode == "graph":
             done = self._run_recorded_graph(n, record_every, hist)
             for k in range(done, n):
@@ -308,7 +437,7 @@ class BatchedSolver:
             return self._f0[i].clone()
         prev = self.fb if self._cur == 0 else self.fa
         d = self.domains[i]
-        out = torch.empty((9, d.ny, d.nx), dtype=torch.float32, device=self.device)
+        out = torch.empty((self.q,) + d.shape, dtype=torch.float32, device=self.device)
         desc = self._single_desc(i, "none")
         st = _lib.load().tlbm_step(ctypes.byref(desc), self._view(prev, i).data_ptr(), out.data_ptr(),
                                    self._flags_view(i).data_ptr(), None, None, None, _lib.stream_of(self.device))
@@ -336,71 +465,39 @@ class BatchedSolver:
 
 def autotune(solver: BatchedSolver, steps: int = 20,
              tiles=((32, 8), (64, 4), (128, 2), (256, 1), (32, 4), (64, 2), (128, 1)),
-             modes=("graph", "persistent")) -> dict:
-    """Time every (tile, mode) candidate on the solver's own domains and keep the
-    fastest.  The state is advanced by the trials; reload it afterwards."""
+             modes=("graph", "persistent"), orders=BatchedSolver.ORDERS, ctas_per_sm=(0, 2, 4)) -> dict:
+    """Time every candidate on the solver's own domains and keep the fastest:
+    tile shape x execution mode x CTA-to-domain mapping (the tile order of
+    BatchedSolver.set_tile) and, for the persistent kernel, the CTAs per SM
+    (0 = as many as fit).  Every trial updates every domain (retired ones
+    too).  The state is advanced by the trials; reload it afterwards."""
     results = []
     for mode in modes:
         for tx, ty in tiles:
-            solver.mode = mode
-            solver.set_tile(tx, ty)
-            try:
-                t = solver.timed_steps(steps)
-            except (RuntimeError, NotImplementedError):
-                continue
-            results.append({"mode": mode, "tile": (tx, ty), "seconds": t,
-                            "mlups": solver.n_cells * steps / t / 1e6})
+            for order in orders:
+                for cps in (ctas_per_sm if mode == "persistent" else (0,)):
+                    solver.mode = mode
+                    solver.ctas_per_sm = cps
+                    solver.set_tile(tx, ty, order)
+                    if solver.domain_status is not None:
+                        solver.domain_status.zero_()     # every trial updates every domain
+                    try:
+                        t = solver.timed_steps(steps)
+                    except (RuntimeError, NotImplementedError):
+                        continue
+                    results.append({"mode": mode, "tile": (tx, ty), "order": order, "ctas_per_sm": cps,
+                                    "seconds": t, "mlups": solver.n_cells * steps / t / 1e6})
     best = max(results, key=lambda r: r["mlups"])
     solver.mode = best["mode"]
-    solver.set_tile(*best["tile"])
+    solver.ctas_per_sm = best["ctas_per_sm"]
+    solver.set_tile(*best["tile"], best["order"])
     return {"best": best, "trials": results}
 
 
-def uniform_scan(n_domains: int, seed: int, device=None, nx_range=(128, 1024), re_range=(40.0, 300.0),
-                 u_in: float = 0.05) -> list[DomainSpec]:
-    """Seeded design of the batched-form case: nx ~ U{nx_range} (multiple of 8 so
-    that ny = nx/4 and D = ny/8 stay whole), Re ~ U(re_range)."""
-    g = torch.Generator().manual_seed(seed)
-    nxs = torch.randint(nx_range[0] // 8, nx_range[1] // 8 + 1, (n_domains,), generator=g) * 8
-    res = re_range[0] + (re_range[1] - re_range[0]) * torch.rand(n_domains, generator=g, dtype=torch.float64)
-    return [cylinder_channel(int(nx), float(re), u_in, device) for nx, re in zip(nxs.tolist(), res.tolist())]
 
 
-def equilibrium_start(domains: list[DomainSpec], device=None) -> list[torch.Tensor]:
-    """Uniform inlet flow with zero velocity in the obstacle (cylinder_flow.py start state)."""
-    from .d2q9 import equilibrium
-
-    out = []
-    for d in domains:
-        ux = torch.full((d.ny, d.nx), float(d.u_in or 0.0), device=device)
-        if d.obstacle_mask is not None:
-            ux[d.obstacle_mask.to(ux.device)] = 0.0
-        out.append(equilibrium(torch.ones_like(ux), ux, torch.zeros_like(ux)))
-    return out
-
-
-def strouhal(lift: torch.Tensor, length_ref: float, u_ref: float, sample_every: int = 1,
-             st_band=(0.05, 0.35)) -> float | None:
-    """Dominant shedding frequency of a lift history as St = f D / U: Hann
-    window, band-limited FFT peak (the FFT branch of postprocess.py:646)."""
-    x = lift.detach().double().cpu()
-    x = x - x.mean()
-    n = x.numel()
-    if n < 32:
-        return None
-    w = torch.hann_window(n, periodic=False, dtype=torch.float64)
-    spec = torch.fft.rfft(x * w).abs()
-    freq = torch.fft.rfftfreq(n, d=float(sample_every), dtype=torch.float64)
-    st = freq * length_ref / u_ref
-    band = (st >= st_band[0]) & (st <= st_band[1])
-    if not bool(band.any()):
-        return None
-    k = int(torch.argmax(torch.where(band, spec, torch.zeros_like(spec))))
-    return float(st[k])
-
-
-__all__ = ["DomainSpec", "BatchedSolver", "autotune", "cylinder_channel", "uniform_scan", "equilibrium_start",
-           "strouhal"]
+__all__ = ["DomainSpec", "BatchedSolver", "autotune", "cavity_point", "cylinder_channel", "uniform_scan",
+           "equilibrium_start", "strouhal"]
 
 
 def scan(n_domains: int = 512, steps: int = 50_000, record_every: int = 10, seed: int = 20261203,

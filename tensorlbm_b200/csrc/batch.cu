@@ -10,7 +10,8 @@
 //  * tlbm_batch_step: one launch per step, grid = tiles (the caller replays a
 //    CUDA graph of these launches);
 //  * tlbm_batch_run: one persistent cooperative launch that runs nsteps steps,
-//    each CTA striding over the tile list, with a grid barrier between steps.
+//    each CTA striding over the tile list, with a grid barrier between steps
+//    (launched with cudaLaunchKernelEx, so it can be captured in a CUDA graph).
 //    The barrier spins a bounded number of times; on expiry the kernel records
 //    TLBM_ERR_TIMEOUT in *status and every CTA returns.
 #include <cooperative_groups.h>
@@ -20,54 +21,63 @@
 namespace tlbm {
 namespace {
 
-template <typename T>
-__device__ __forceinline__ void domain_params(const tlbm_batch_domain& dm, int collision, CollideParams<T>& cp,
-                                              BcParams<T>& bp) {
-  // per-domain relaxation time; the other rates are TensorLBM's D2Q9 defaults
-  cp = make_collide_params<T>(dm.tau, 1.64, 1.54, 1.7, -1.0, 1.0, 1.0, 1.0, 0.0);
-  bp = make_bc_params<T>(dm.u_in, 0.0, 0.0, dm.rho_out, 0.0);
-  (void)collision;
+template <class L, typename T>
+__device__ __forceinline__ void domain_params(const tlbm_batch_domain& dm, CollideParams<T>& cp, BcParams<T>& bp) {
+  // per-domain relaxation time; the other MRT rates are TensorLBM's defaults
+  // of the lattice (solver.py:249 collide_mrt, solver3d.py:107 collide_mrt3d)
+  if constexpr (L::Q == 9) cp = make_collide_params<T>(dm.tau, 1.64, 1.54, 1.7, -1.0, 1.0, 1.0, 1.0, 0.0);
+  else cp = make_collide_params<T>(dm.tau, 1.19, 1.4, 1.2, -1.0, 1.0, 1.0, 1.0, 0.0);
+  bp = make_bc_params<T>(dm.u_in, 0.0, 0.0, dm.rho_out, dm.u_lid);
 }
 
+// dom_status (may be null): one status word per domain.  A domain whose word
+// is non-zero (a non-finite density seen in an earlier tile or step) is
+// retired: its tiles are skipped, and its state stays as it was when that
+// happened.  Without it every domain is updated and the non-finite bit goes to
+// the one status word.
 template <class L, typename S, int COLL>
 __device__ __forceinline__ void process_tile(const tlbm_batch_domain* __restrict__ doms, const int* __restrict__ tiles,
                                              long long t, const S* fin, S* fout, const uint8_t* flags,
-                                             double* forces, unsigned int* status) {
+                                             double* forces, unsigned int* status, unsigned int* dom_status) {
   using T = typename Storage<S>::T;
   const int di = tiles[3 * t + 0];
+  if (dom_status && *(volatile unsigned int*)(dom_status + di)) return;   // uniform over the tile
   const int x = tiles[3 * t + 1] + threadIdx.x;
-  const int y = tiles[3 * t + 2] + threadIdx.y;
+  const int row = tiles[3 * t + 2] + threadIdx.y;   // over the nz * ny rows of the domain
   const tlbm_batch_domain dm = doms[di];
+  const int nz = dm.nz > 1 ? dm.nz : 1;
+  const int y = row % dm.ny, z = row / dm.ny;
   CollideParams<T> cp;
   BcParams<T> bp;
-  domain_params<T>(dm, COLL, cp, bp);
+  domain_params<L, T>(dm, cp, bp);
   Domain<S, S> d;
   d.fin = fin + dm.f_offset;
   d.fout = fout + dm.f_offset;
   d.flags = flags ? flags + dm.cell_offset : nullptr;
   d.tau_field = nullptr;
   d.force = forces ? forces + 3 * (long long)di : nullptr;
-  d.status = status;
+  d.status = dom_status ? dom_status + di : status;
   d.wall_u = nullptr;
   d.link_row = nullptr;
   d.link_q = nullptr;
   d.nx = dm.nx;
   d.ny = dm.ny;
-  d.nz = 1;
+  d.nz = nz;
   d.plane = (long long)dm.nx * dm.ny;
-  d.n = d.plane;
+  d.n = d.plane * nz;
   d.bc = dm.bc;
-  cell_update<L, S, S, COLL, true>(d, x, y, 0, x < dm.nx && y < dm.ny, cp, bp);
+  cell_update<L, S, S, COLL, true>(d, x, y, z, x < dm.nx && row < dm.ny * nz, cp, bp);
 }
 
 template <class L, typename S, int COLL>
 __global__ void __launch_bounds__(256) k_batch_step(const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
                                                     const S* fin, S* fout, const uint8_t* flags, double* forces,
-                                                    const int* force_slot, int ndomains, unsigned int* status) {
+                                                    const int* force_slot, int ndomains, unsigned int* status,
+                                                    unsigned int* dom_status) {
   // with a slot counter, the forces of this step go to record *force_slot
   if (forces && force_slot) forces += 3LL * ndomains * (*force_slot);
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x)
-    process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status);
+    process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status, dom_status);
 }
 
 // Grid barrier over a cooperative launch, bounded: sync[0] counts arrivals,
@@ -107,7 +117,8 @@ template <class L, typename S, int COLL>
 __global__ void __launch_bounds__(256) k_batch_run(const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
                                                    S* fa, S* fb, const uint8_t* flags, int nsteps, double* force_hist,
                                                    int ndomains, int record_every, unsigned int* sync,
-                                                   unsigned int* status, unsigned long long max_spins) {
+                                                   unsigned int* status, unsigned long long max_spins,
+                                                   unsigned int* dom_status) {
   for (int s = 0; s < nsteps; ++s) {
     const S* fin = (s & 1) ? fb : fa;
     S* fout = (s & 1) ? fa : fb;
@@ -115,7 +126,7 @@ __global__ void __launch_bounds__(256) k_batch_run(const tlbm_batch_domain* doms
     if (force_hist && record_every > 0 && (s % record_every) == 0)
       forces = force_hist + 3 * (long long)ndomains * (s / record_every);
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x)
-      process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status);
+      process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status, dom_status);
     if (!grid_barrier(sync, max_spins)) {
       if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x == 0) atomicOr(status, 2u);
       return;
@@ -130,7 +141,8 @@ int launch_batch(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, const 
   const dim3 block(b.tile_x, b.tile_y);
   const long long grid = ntiles < 0x7fffffffLL ? ntiles : 0x7fffffffLL;
   k_batch_step<L, S, COLL><<<(unsigned)grid, block, 0, s>>>(doms, tiles, ntiles, (const S*)fin, (S*)fout, flags,
-                                                           forces, force_slot, b.ndomains, status);
+                                                           forces, force_slot, b.ndomains, status,
+                                                           b.domain_status);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }
 
@@ -152,21 +164,21 @@ int launch_batch_run(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, co
   long long grid = (long long)sms * per_sm;
   if (grid > ntiles) grid = ntiles;
   if (grid < 1) return TLBM_OK;
-  const tlbm_batch_domain* a0 = doms;
-  const int* a1 = tiles;
-  long long a2 = ntiles;
-  S* a3 = (S*)fa;
-  S* a4 = (S*)fb;
-  const uint8_t* a5 = flags;
-  int a6 = nsteps;
-  double* a7 = force_hist;
-  int a8 = b.ndomains;
-  int a9 = record_every;
-  unsigned int* a10 = sync;
-  unsigned int* a11 = status;
-  unsigned long long a12 = (unsigned long long)max_spins;
-  void* args[] = {&a0, &a1, &a2, &a3, &a4, &a5, &a6, &a7, &a8, &a9, &a10, &a11, &a12};
-  if (cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)grid), block, args, 0, s) != cudaSuccess)
+  // cudaLaunchKernelEx with the cooperative attribute: the same guarantees as
+  // cudaLaunchCooperativeKernel (every CTA resident at once), and the launch
+  // can be captured into a CUDA graph
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, kern, doms, tiles, ntiles, (S*)fa, (S*)fb, flags, nsteps, force_hist, b.ndomains,
+                         record_every, sync, status, (unsigned long long)max_spins, b.domain_status) != cudaSuccess)
     return TLBM_ERR_LAUNCH;
   return TLBM_OK;
 }
@@ -175,7 +187,7 @@ __global__ void k_advance_slot(int* slot) { slot[0] += 1; }
 
 int check_batch(const tlbm_batch_desc* b, const tlbm_batch_domain* doms, const int* tiles, long long ntiles) {
   if (!b || !doms || !tiles) return TLBM_ERR_ARG;
-  if (b->lattice != TLBM_D2Q9) return TLBM_ERR_UNSUPPORTED;
+  if (b->lattice != TLBM_D2Q9 && b->lattice != TLBM_D3Q19) return TLBM_ERR_UNSUPPORTED;
   if (b->dtype != TLBM_F32) return TLBM_ERR_DTYPE;
   if (b->collision != TLBM_COLL_BGK && b->collision != TLBM_COLL_MRT) return TLBM_ERR_UNSUPPORTED;
   if (b->tile_x < 32 || (b->tile_x % 32) != 0 || b->tile_y < 1 || b->tile_x * b->tile_y > 256) return TLBM_ERR_ARG;
@@ -199,6 +211,13 @@ TLBM_API int tlbm_batch_step(const tlbm_batch_desc* b, const tlbm_batch_domain* 
   if (f_in == f_out) return TLBM_ERR_ALIAS;
   if (ntiles == 0) return TLBM_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (b->lattice == TLBM_D3Q19) {
+    if (b->collision == TLBM_COLL_BGK)
+      return launch_batch<D3Q19, float, TLBM_COLL_BGK>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces,
+                                                       force_slot, status, s);
+    return launch_batch<D3Q19, float, TLBM_COLL_MRT>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces,
+                                                     force_slot, status, s);
+  }
   if (b->collision == TLBM_COLL_BGK)
     return launch_batch<D2Q9, float, TLBM_COLL_BGK>(*b, domains, tiles, ntiles, f_in, f_out, flags, forces,
                                                     force_slot, status, s);
@@ -223,6 +242,13 @@ TLBM_API int tlbm_batch_run(const tlbm_batch_desc* b, const tlbm_batch_domain* d
   if (nsteps < 0 || max_spins < 1) return TLBM_ERR_ARG;
   if (ntiles == 0 || nsteps == 0) return TLBM_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (b->lattice == TLBM_D3Q19) {
+    if (b->collision == TLBM_COLL_BGK)
+      return launch_batch_run<D3Q19, float, TLBM_COLL_BGK>(*b, domains, tiles, ntiles, f_a, f_b, flags, nsteps,
+                                                           force_history, record_every, sync, status, max_spins, s);
+    return launch_batch_run<D3Q19, float, TLBM_COLL_MRT>(*b, domains, tiles, ntiles, f_a, f_b, flags, nsteps,
+                                                         force_history, record_every, sync, status, max_spins, s);
+  }
   if (b->collision == TLBM_COLL_BGK)
     return launch_batch_run<D2Q9, float, TLBM_COLL_BGK>(*b, domains, tiles, ntiles, f_a, f_b, flags, nsteps,
                                                         force_history, record_every, sync, status, max_spins, s);

@@ -376,6 +376,15 @@ TLBM_API const char* tlbm_status_string(int status) {
 
 TLBM_API int tlbm_abi_version(void) { return TLBM_ABI_VERSION; }
 
+TLBM_API int64_t tlbm_struct_size(int32_t which) {
+  switch (which) {
+    case 0: return (int64_t)sizeof(tlbm_desc);
+    case 1: return (int64_t)sizeof(tlbm_batch_domain);
+    case 2: return (int64_t)sizeof(tlbm_batch_desc);
+    default: return -1;
+  }
+}
+
 TLBM_API int tlbm_aa_load(const tlbm_desc* d, const void* f0, void* f, const uint8_t* flags, const float* tau_field,
                           void* stream) {
   const int st = check_aa(d);

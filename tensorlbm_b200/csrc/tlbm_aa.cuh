@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(256) k_step_aa(StepParams p, CollideParams<typ
 // otherwise.  Same per-cell path and the same packed stochastic rounding as
 // k_step_x2.  Requires what pair_layout_ok checks.
 template <class L, typename S, int COLL, int READ, int WRITE, bool FORCED = false>
-__global__ void __launch_bounds__(256) k_step_aa_x2(StepParams p, CollideParams<typename Storage<S>::T> cp,
-                                                    BcParams<typename Storage<S>::T> bp) {
+__device__ __forceinline__ void step_aa_x2(const StepParams& p, const CollideParams<typename Storage<S>::T>& cp,
+                                           const BcParams<typename Storage<S>::T>& bp) {
   using T = typename Storage<S>::T;
   using IO = PairIO<S>;
   using V = typename IO::V;
@@ -205,29 +205,16 @@ __global__ void __launch_bounds__(256) k_step_aa_x2(StepParams p, CollideParams<
     accumulate_force(d.force, __any_sync(0xffffffffu, oa || ob), mx, my, mz);
   }
   if (!active) return;
-  if constexpr (!uniform_edge_branch<L, COLL>()) {
+  // packed collisions exactly where the two-buffer pair kernel packs them
+  constexpr bool kPack = TLBM_PACK && std::is_same<T, float>::value && !FORCED &&
+                         packed_collision<L, COLL, Storage<S>::kFast>();
+  if (!uniform_edge_branch<L, COLL>() || edge) {
     double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
     apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
     apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
-    relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
-    relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
+    relax_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fla, flb, fa, fb, cp);
   } else {
-    bool keep_a = false, keep_b = false;   // half-way wall cells: reversed, not collided
-    if (edge) {
-      double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-      apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-      apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
-      if (fla & TLBM_FLAG_HALFWAY) {
-        bounce_back<L>(fa);
-        keep_a = true;
-      }
-      if (flb & TLBM_FLAG_HALFWAY) {
-        bounce_back<L>(fb);
-        keep_b = true;
-      }
-    }
-    if (!keep_a) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c, fa, cp);
-    if (!keep_b) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c + 1, fb, cp);
+    relax_interior_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fa, fb, cp);
   }
   uint32_t h = 0;
   if constexpr (Storage<S>::kShifted)
@@ -257,6 +244,26 @@ __global__ void __launch_bounds__(256) k_step_aa_x2(StepParams p, CollideParams<
   }
 }
 
+// Resident blocks per SM the AA pair kernel is compiled for: the caps of the
+// two-buffer kernel, except the D3Q19 MRT (the AA addressing adds registers,
+// and the capped form spilled and ran slower)
+template <class L, typename S, int COLL>
+__host__ __device__ constexpr int aa_x2_min_blocks() {
+  return (L::Q == 19 && COLL == TLBM_COLL_MRT) ? TLBM_MINB_AA_MRT : x2_min_blocks<L, S, COLL>();
+}
+
+template <class L, typename S, int COLL, int READ, int WRITE, bool FORCED = false>
+__global__ void __launch_bounds__(256) k_step_aa_x2(StepParams p, CollideParams<typename Storage<S>::T> cp,
+                                                    BcParams<typename Storage<S>::T> bp) {
+  step_aa_x2<L, S, COLL, READ, WRITE, FORCED>(p, cp, bp);
+}
+// the same kernel compiled for MINB resident blocks per SM (x2_min_blocks)
+template <class L, typename S, int COLL, int READ, int WRITE, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_aa_x2_capped(StepParams p, CollideParams<typename Storage<S>::T> cp,
+                                                                  BcParams<typename Storage<S>::T> bp) {
+  step_aa_x2<L, S, COLL, READ, WRITE, false>(p, cp, bp);
+}
+
 template <class L, typename SI, typename SO, int COLL, int READ, int WRITE, int BC, bool FORCED = false>
 int launch_aa(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   using T = typename Storage<SI>::T;
@@ -278,7 +285,9 @@ int launch_aa(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   if constexpr (kStep) {
     if (pair_layout_ok<L, SI>(p)) {
       step_launch_shape(p.nx / 2, p.ny, p.nz, grid, block);
-      k_step_aa_x2<L, SI, COLL, READ, WRITE, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
+      constexpr int minb = aa_x2_min_blocks<L, SI, COLL>();
+      if constexpr (minb > 0) k_step_aa_x2_capped<L, SI, COLL, READ, WRITE, minb><<<grid, block, 0, s>>>(p, cp, bp);
+      else k_step_aa_x2<L, SI, COLL, READ, WRITE, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
       return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
     }
   }

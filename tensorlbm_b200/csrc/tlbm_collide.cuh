@@ -47,6 +47,12 @@ __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
 
+// 1 / x for the fused-arithmetic collisions (no reference rounding order to
+// keep): the hardware reciprocal approximation (pk::rcp_approx) instead of the
+// instruction sequence of an IEEE division.  float64 keeps the division.
+__device__ __forceinline__ float rcp_fast(float x) { return pk::rcp_approx(x); }
+__device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
+
 // a > lo ? a : lo and a < hi ? a : hi (F2 has per-component forms in tlbm_pair.cuh)
 __device__ __forceinline__ float clamp_lo(float a, float lo) { return a > lo ? a : lo; }
 __device__ __forceinline__ double clamp_lo(double a, double lo) { return a > lo ? a : lo; }
@@ -152,7 +158,7 @@ __device__ __forceinline__ void macroscopic_fused(const T (&f)[L::Q], T& rho, T&
     if (L::cy(q) != 0) jy = (L::cy(q) > 0) ? jy + f[q] : jy - f[q];
     if (L::cz(q) != 0) jz = (L::cz(q) > 0) ? jz + f[q] : jz - f[q];
   }
-  const T ir = T(1) / clamp_lo(rho, T(1e-12));
+  const T ir = rcp_fast(clamp_lo(rho, T(1e-12)));
   ux = jx * ir;
   uy = jy * ir;
   uz = (L::DIM == 3) ? jz * ir : T(0);
@@ -533,9 +539,10 @@ template <typename T>
 __device__ __forceinline__ void cascaded_relax_second(T& kxx, T& kyy, T& kzz, T& kxy, T& kxz, T& kyz, T om, T sb) {
   const T tr = kxx + kyy + kzz;
   const T trs = (T(1) - sb) * tr, ks = T(1) - om;
-  kxx = ks * (kxx - tr / T(3)) + trs / T(3);
-  kyy = ks * (kyy - tr / T(3)) + trs / T(3);
-  kzz = ks * (kzz - tr / T(3)) + trs / T(3);
+  const T tr3 = tr * T(1.0 / 3.0), trs3 = trs * T(1.0 / 3.0);
+  kxx = ks * (kxx - tr3) + trs3;
+  kyy = ks * (kyy - tr3) + trs3;
+  kzz = ks * (kzz - tr3) + trs3;
   kxy = ks * kxy;
   kxz = ks * kxz;
   kyz = ks * kyz;
@@ -716,8 +723,8 @@ __device__ __forceinline__ void collide_cumulant_legacy_unit(T (&f)[27], T om) {
   // relaxation: deviatoric second order by 1 - omega, bulk and orders >= 3 to zero
   const T ks = T(1) - om;
   const T tr = m[2][0][0] + m[0][2][0] + m[0][0][2];
-  const T c200 = ks * (m[2][0][0] - tr / T(3)), c020 = ks * (m[0][2][0] - tr / T(3)),
-          c002 = ks * (m[0][0][2] - tr / T(3));
+  const T tr3 = tr * T(1.0 / 3.0);
+  const T c200 = ks * (m[2][0][0] - tr3), c020 = ks * (m[0][2][0] - tr3), c002 = ks * (m[0][0][2] - tr3);
   const T c110 = ks * m[1][1][0], c101 = ks * m[1][0][1], c011 = ks * m[0][1][1];
   // central moments of the relaxed cumulants (cumulant.py:580-651 with zeros)
 #pragma unroll
@@ -775,12 +782,14 @@ __device__ __forceinline__ void collide_cumulant_legacy(T (&f)[27], const Collid
   // relaxation (cumulant.py:654-740): trace / deviatoric split at 2nd order
   const T om = cp.inv_tau;
   const T tr = c[4] + c[5] + c[6];
-  const T dxx = c[4] - tr / T(3), dyy = c[5] - tr / T(3), dzz = c[6] - tr / T(3);
+  const T tr3 = tr * T(1.0 / 3.0);
+  const T dxx = c[4] - tr3, dyy = c[5] - tr3, dzz = c[6] - tr3;
   const T trs = (T(1) - cp.omega_b) * tr;
   const T ks = T(1) - om;
-  c[4] = ks * dxx + trs / T(3);
-  c[5] = ks * dyy + trs / T(3);
-  c[6] = ks * dzz + trs / T(3);
+  const T trs3 = trs * T(1.0 / 3.0);
+  c[4] = ks * dxx + trs3;
+  c[5] = ks * dyy + trs3;
+  c[6] = ks * dzz + trs3;
   c[7] = ks * c[7];
   c[8] = ks * c[8];
   c[9] = ks * c[9];
@@ -802,7 +811,7 @@ __device__ __forceinline__ void collide_cumulant_legacy(T (&f)[27], const Collid
 template <typename T>
 __device__ __forceinline__ void geier_forward(T (&k)[27]) {
   const T rho = k[0];
-  const T ir = T(1) / rho;
+  const T ir = rcp_fast(rho);
   T t[27];
 #pragma unroll
   for (int i = 0; i < 27; ++i) t[i] = k[i] * ir;
@@ -830,7 +839,7 @@ __device__ __forceinline__ void geier_forward(T (&k)[27]) {
 template <typename T>
 __device__ __forceinline__ void geier_inverse(T (&c)[27]) {
   const T rho = c[0];
-  const T ir = T(1) / rho;
+  const T ir = rcp_fast(rho);
   T t[27];
 #pragma unroll
   for (int i = 0; i < 27; ++i) t[i] = c[i] * ir;
@@ -876,7 +885,7 @@ __device__ __forceinline__ void collide_cumulant_geier(T (&f)[27], const Collide
   const T om = cp.inv_tau;
   const T dxx = c[4] - ce[4], dyy = c[5] - ce[5], dzz = c[6] - ce[6];
   const T tr = dxx + dyy + dzz;
-  const T tr3 = tr / T(3);
+  const T tr3 = tr * T(1.0 / 3.0);
   c[4] = c[4] - (om * (dxx - tr3) + cp.omega_b * tr3);
   c[5] = c[5] - (om * (dyy - tr3) + cp.omega_b * tr3);
   c[6] = c[6] - (om * (dzz - tr3) + cp.omega_b * tr3);
@@ -918,11 +927,11 @@ __device__ __forceinline__ void collide_bgk_fast(T (&f)[L::Q], T inv_tau) {
     if (L::cx(q) != 0) cu = (L::cx(q) > 0) ? cu + ux : cu - ux;
     if (L::cy(q) != 0) cu = (L::cy(q) > 0) ? cu + uy : cu - uy;
     if (L::cz(q) != 0) cu = (L::cz(q) > 0) ? cu + uz : cu - uz;
-    const T w = weight<L, T>(q);
-    const T sq = fma((T(4.5) * w * orho) * cu, cu, w * obase);
-    const T k3 = T(3) * w * orho;
+    const double w = L::w(q);
+    const T sq = fma(T(T(4.5 * w) * orho) * cu, cu, T(T(w) * obase));
+    const T k3 = T(T(3.0 * w) * orho), k3n = T(T(-3.0 * w) * orho);
     f[q] = fma(f[q], keep, fma(k3, cu, sq));
-    f[qb] = fma(f[qb], keep, fma(-k3, cu, sq));
+    f[qb] = fma(f[qb], keep, fma(k3n, cu, sq));
   }
 }
 
@@ -945,7 +954,7 @@ __device__ __forceinline__ void collide_bgk_deviation(T (&g)[L::Q], T om, T s) {
   }
   const T rho = fma(R, T(1) / s, T(1));
   const T srho = s * clamp_lo(rho, T(1e-12));
-  const T irs = T(1) / srho;
+  const T irs = rcp_fast(srho);
   const T ux = jx * irs, uy = jy * irs, uz = (L::DIM == 3) ? jz * irs : T(0);
   const T usq = usq_fused<L>(ux, uy, uz);
   const T keep = T(1) - om;
@@ -989,11 +998,11 @@ __device__ __forceinline__ void collide_smagorinsky_fast(T (&f)[L::Q], const Col
   if constexpr (L::DIM == 3) rad += pzz * pzz + T(2) * (pxz * pxz + pyz * pyz);
   rad = clamp_lo(rad, T(1e-30));
   const T rs = clamp_lo(rho, T(1e-12));
-  T disc = cp.tau_sq + cp.smag_coef * sqrt(rad) / rs;
+  T disc = cp.tau_sq + cp.smag_coef * sqrt(rad) * rcp_fast(rs);
   disc = clamp_lo(disc, T(0));
   T te = T(0.5) * (cp.tau + sqrt(disc));
   te = clamp_hi(clamp_lo(te, T(0.5001)), cp.tau_eff_max);
-  const T ninv = T(-1) / te;
+  const T ninv = -rcp_fast(te);
 #pragma unroll
   for (int q = 0; q < L::Q; ++q) f[q] = fma(fn[q], ninv, f[q]);
 }
@@ -1004,7 +1013,7 @@ __device__ __forceinline__ void collide_smagorinsky_fast(T (&f)[L::Q], const Col
 template <class L, int COLL, typename T, bool FAST = false>
 __device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp, T tau_cell, bool has_tau_cell) {
   if constexpr (COLL == TLBM_COLL_BGK && FAST) {
-    collide_bgk_fast<L>(f, has_tau_cell ? T(1) / tau_cell : cp.inv_tau);
+    collide_bgk_fast<L>(f, has_tau_cell ? rcp_fast(tau_cell) : cp.inv_tau);
   } else if constexpr (COLL == TLBM_COLL_SMAGORINSKY && FAST) {
     collide_smagorinsky_fast<L>(f, cp);
   } else if constexpr (COLL == TLBM_COLL_BGK) {
@@ -1012,7 +1021,7 @@ __device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp
     else collide_bgk<L>(f, cp.tau, cp.inv_tau64);
   } else if constexpr (COLL == TLBM_COLL_MRT) {
     MrtRates<T> r = cp.mrt;
-    if (has_tau_cell) r.s_nu = T(1) / tau_cell;
+    if (has_tau_cell) r.s_nu = rcp_fast(tau_cell);
     collide_mrt<L>(f, r);
   } else if constexpr (COLL == TLBM_COLL_SMAGORINSKY) {
     collide_smagorinsky<L>(f, cp);
@@ -1031,6 +1040,43 @@ __device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp
     static_assert(L::Q == 27, "D3Q27 only");
     collide_cumulant_geier(f, cp);
   }
+}
+
+// The parameters of the explicit-rounding types (F1 one cell, F2 a pair):
+// every scalar broadcast to every lane.
+template <class F>
+__host__ __device__ __forceinline__ CollideParams<F> pack_params(const CollideParams<float>& c) {
+  CollideParams<F> p;
+  p.tau = F(c.tau);
+  p.inv_tau = F(c.inv_tau);
+  p.inv_tau64 = c.inv_tau64;
+  p.mrt = {F(c.mrt.s_e), F(c.mrt.s_eps), F(c.mrt.s_q), F(c.mrt.s_nu), F(c.mrt.s_pi)};
+  p.omega_b = F(c.omega_b);
+  p.omega_odd = F(c.omega_odd);
+  p.omega_even = F(c.omega_even);
+  p.c_smag = F(c.c_smag);
+  p.smag_coef = F(c.smag_coef);
+  p.smag_coef_cum = F(c.smag_coef_cum);
+  p.omega_b_minus_omega = F(c.omega_b_minus_omega);
+  p.keep_even = F(c.keep_even);
+  p.tau_sq = F(c.tau_sq);
+  p.tau_eff_max = F(c.tau_eff_max);
+  p.force_a = F(c.force_a);
+  p.cum_unit_rates = c.cum_unit_rates;
+  p.cm_s5 = F(c.cm_s5);
+  p.cm_s6 = F(c.cm_s6);
+  p.tau_minus = F(c.tau_minus);
+  p.inv_tau_minus64 = c.inv_tau_minus64;
+  return p;
+}
+
+// Collisions that run on the explicit-rounding types (F2 in the pair kernels,
+// F1 in the single-cell kernels): the fused-arithmetic forms (no reference
+// rounding order to keep), in float32.
+template <class L, int COLL, bool FAST>
+__host__ __device__ constexpr bool packed_collision() {
+  return COLL == TLBM_COLL_MRT || (COLL == TLBM_COLL_BGK && FAST) || (COLL == TLBM_COLL_SMAGORINSKY && FAST) ||
+         (L::Q == 27 && COLL == TLBM_COLL_CUMULANT);
 }
 
 template <typename T>

@@ -1,4 +1,5 @@
-// Packed arithmetic on the two cells of a pair (sm_100a).
+// Explicit-rounding arithmetic for the fused collisions, on one cell (F1) or
+// on the two cells of a pair (F2, sm_100a packed float32).
 //
 // The pair kernels hold cells x and x + 1 of a row in one thread and apply
 // the same operation sequence to both.  F2 holds the two cells' values of one
@@ -6,82 +7,194 @@
 // instructions of sm_100a (fma.rn.f32x2, add.rn.f32x2, mul.rn.f32x2 through
 // __ffma2_rn / __fadd2_rn / __fmul2_rn): one instruction does the operation
 // for both cells, rounded per component exactly as the scalar instruction
-// would.  Division and square root have no packed form and run per component.
+// would.  Division, square root and the reciprocal have no packed form and run
+// per component.
 //
-// A product a * b is kept unevaluated (P2) until it meets an addition or a
-// subtraction, where it becomes one fused multiply-add: the packed intrinsics
-// are never contracted by the compiler, so the contraction of a scalar
-// expression like a * b + c is reproduced here by the types.  Chains such as
-// c0 * e0 + c1 * e1 + c2 * e2 become one multiply and two fused multiply-adds.
+// A product a * b is kept unevaluated (a P value) until it meets an addition
+// or a subtraction, where it becomes one fused multiply-add: the intrinsics are
+// never contracted by the compiler, so the contraction of a scalar expression
+// like a * b + c is made by the types.  Chains such as c0 * e0 + c1 * e1 +
+// c2 * e2 become one multiply and two fused multiply-adds.
+//
+// F1 is the same type on one cell, with the scalar round-to-nearest
+// intrinsics.  The single-cell kernels run the fused collisions on F1, so a
+// cell gets bit for bit the same result whether a pair kernel or a
+// single-cell kernel (the collide-only pass, the batched runner, the odd-nx
+// fallback, the first AA step) updates it.
 #pragma once
+
+#include <type_traits>
 
 #include <cuda_runtime.h>
 
+#ifndef TLBM_FAST_RCP
+#define TLBM_FAST_RCP 1
+#endif
+
 namespace tlbm {
+// The types and their functions live in a namespace of their own: calls from
+// the generic collision code find them by argument-dependent lookup, and they
+// do not hide the scalar sqrt / fma of the global namespace.
+namespace pk {
 
-struct P2;
+// 1 / x with the hardware approximation (rcp.approx.ftz.f32: relative error
+// below 2^-23) instead of the instruction sequence of an IEEE division
+__device__ __forceinline__ float rcp_approx(float x) {
+#if TLBM_FAST_RCP
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+#else
+  return 1.0f / x;
+#endif
+}
 
-struct F2 {
-  float2 v;
-  F2() = default;
-  __host__ __device__ __forceinline__ constexpr F2(float2 a) : v(a) {}
-  __host__ __device__ __forceinline__ constexpr F2(float a, float b) : v{a, b} {}
-  // a scalar value broadcast to both cells (constants, uniform parameters)
-  __host__ __device__ __forceinline__ constexpr F2(double c) : v{float(c), float(c)} {}
-  __host__ __device__ __forceinline__ constexpr F2(float c) : v{c, c} {}
-  __host__ __device__ __forceinline__ constexpr F2(int c) : v{float(c), float(c)} {}
-  __device__ __forceinline__ F2(const P2& p);
+// the operations on one lane type: float (one cell) or float2 (two cells)
+template <class V> struct Lane;
+template <> struct Lane<float> {
+  __host__ __device__ static constexpr float bcast(float c) { return c; }
+  __device__ __forceinline__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+  __device__ __forceinline__ static float add(float a, float b) { return __fadd_rn(a, b); }
+  __device__ __forceinline__ static float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+  __device__ __forceinline__ static float neg(float a) { return -a; }
+  __device__ __forceinline__ static float div(float a, float b) { return a / b; }
+  __device__ __forceinline__ static float xdiv(float a, float b) { return __fdiv_rn(a, b); }
+  __device__ __forceinline__ static float sqrt(float a) { return sqrtf(a); }
+  __device__ __forceinline__ static float rcp(float a) { return rcp_approx(a); }
+  __device__ __forceinline__ static float max(float a, float b) { return fmaxf(a, b); }
+  __device__ __forceinline__ static float min(float a, float b) { return fminf(a, b); }
+};
+template <> struct Lane<float2> {
+  __host__ __device__ static constexpr float2 bcast(float c) { return float2{c, c}; }
+  __device__ __forceinline__ static float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+  __device__ __forceinline__ static float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+  __device__ __forceinline__ static float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+  __device__ __forceinline__ static float2 neg(float2 a) { return make_float2(-a.x, -a.y); }
+  __device__ __forceinline__ static float2 div(float2 a, float2 b) { return make_float2(a.x / b.x, a.y / b.y); }
+  __device__ __forceinline__ static float2 xdiv(float2 a, float2 b) {
+    return make_float2(__fdiv_rn(a.x, b.x), __fdiv_rn(a.y, b.y));
+  }
+  __device__ __forceinline__ static float2 sqrt(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
+  __device__ __forceinline__ static float2 rcp(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
+  __device__ __forceinline__ static float2 max(float2 a, float2 b) {
+    return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y));
+  }
+  __device__ __forceinline__ static float2 min(float2 a, float2 b) {
+    return make_float2(fminf(a.x, b.x), fminf(a.y, b.y));
+  }
+};
+
+template <class V> struct PV;
+
+template <class V> struct FV {
+  using Ln = Lane<V>;
+  V v;
+  FV() = default;
+  __host__ __device__ __forceinline__ constexpr FV(V a) : v(a) {}
+  // a scalar value broadcast to every lane (constants, uniform parameters)
+  __host__ __device__ __forceinline__ explicit constexpr FV(double c) : v(Ln::bcast(float(c))) {}
+  template <class W = V, typename std::enable_if<std::is_same<W, float2>::value, int>::type = 0>
+  __host__ __device__ __forceinline__ explicit constexpr FV(float c) : v(Ln::bcast(c)) {}
+  __host__ __device__ __forceinline__ explicit constexpr FV(int c) : v(Ln::bcast(float(c))) {}
+  // the two cells of a pair
+  template <class W = V, typename std::enable_if<std::is_same<W, float2>::value, int>::type = 0>
+  __host__ __device__ __forceinline__ constexpr FV(float a, float b) : v{a, b} {}
+  __device__ __forceinline__ FV(const PV<V>& p) : v(Ln::mul(p.x, p.y)) {}
+  template <class W = V, typename std::enable_if<std::is_same<W, float2>::value, int>::type = 0>
   __host__ __device__ __forceinline__ float a() const { return v.x; }
+  template <class W = V, typename std::enable_if<std::is_same<W, float2>::value, int>::type = 0>
   __host__ __device__ __forceinline__ float b() const { return v.y; }
 };
 
 // an unevaluated product x * y
-struct P2 {
-  float2 x, y;
+template <class V> struct PV {
+  V x, y;
 };
 
-__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
-__device__ __forceinline__ F2::F2(const P2& p) : v(__fmul2_rn(p.x, p.y)) {}
+using F1 = FV<float>;
+using F2 = FV<float2>;
+using P1 = PV<float>;
+using P2 = PV<float2>;
 
-__device__ __forceinline__ P2 operator*(F2 a, F2 b) { return {a.v, b.v}; }
-__device__ __forceinline__ P2 operator*(const P2& a, F2 b) { return {F2(a).v, b.v}; }
-__device__ __forceinline__ P2 operator*(F2 a, const P2& b) { return {a.v, F2(b).v}; }
-__device__ __forceinline__ P2 operator*(const P2& a, const P2& b) { return {F2(a).v, F2(b).v}; }
+template <class V> __device__ __forceinline__ PV<V> operator*(FV<V> a, FV<V> b) { return {a.v, b.v}; }
+template <class V> __device__ __forceinline__ PV<V> operator*(const PV<V>& a, FV<V> b) { return {FV<V>(a).v, b.v}; }
+template <class V> __device__ __forceinline__ PV<V> operator*(FV<V> a, const PV<V>& b) { return {a.v, FV<V>(b).v}; }
+template <class V> __device__ __forceinline__ PV<V> operator*(const PV<V>& a, const PV<V>& b) {
+  return {FV<V>(a).v, FV<V>(b).v};
+}
 
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return __fadd2_rn(a.v, b.v); }
-__device__ __forceinline__ F2 operator+(const P2& p, F2 c) { return __ffma2_rn(p.x, p.y, c.v); }
-__device__ __forceinline__ F2 operator+(F2 c, const P2& p) { return __ffma2_rn(p.x, p.y, c.v); }
-__device__ __forceinline__ F2 operator+(const P2& p, const P2& q) { return __ffma2_rn(p.x, p.y, F2(q).v); }
+template <class V> __device__ __forceinline__ FV<V> operator+(FV<V> a, FV<V> b) { return Lane<V>::add(a.v, b.v); }
+template <class V> __device__ __forceinline__ FV<V> operator+(const PV<V>& p, FV<V> c) {
+  return Lane<V>::fma(p.x, p.y, c.v);
+}
+template <class V> __device__ __forceinline__ FV<V> operator+(FV<V> c, const PV<V>& p) {
+  return Lane<V>::fma(p.x, p.y, c.v);
+}
+template <class V> __device__ __forceinline__ FV<V> operator+(const PV<V>& p, const PV<V>& q) {
+  return Lane<V>::fma(p.x, p.y, FV<V>(q).v);
+}
 
-// a - b as a + b * (-1): one instruction, exact like the scalar subtraction
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return __ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v); }
-__device__ __forceinline__ F2 operator-(F2 c, const P2& p) { return __ffma2_rn(neg2(p.x), p.y, c.v); }
-__device__ __forceinline__ F2 operator-(const P2& p, F2 c) { return __ffma2_rn(p.x, p.y, neg2(c.v)); }
-__device__ __forceinline__ F2 operator-(const P2& p, const P2& q) { return __ffma2_rn(neg2(q.x), q.y, F2(p).v); }
+// a - b as a + b * (-1): one instruction, exact like the subtraction
+template <class V> __device__ __forceinline__ FV<V> operator-(FV<V> a, FV<V> b) {
+  return Lane<V>::fma(b.v, Lane<V>::bcast(-1.0f), a.v);
+}
+template <class V> __device__ __forceinline__ FV<V> operator-(FV<V> c, const PV<V>& p) {
+  return Lane<V>::fma(Lane<V>::neg(p.x), p.y, c.v);
+}
+template <class V> __device__ __forceinline__ FV<V> operator-(const PV<V>& p, FV<V> c) {
+  return Lane<V>::fma(p.x, p.y, Lane<V>::neg(c.v));
+}
+template <class V> __device__ __forceinline__ FV<V> operator-(const PV<V>& p, const PV<V>& q) {
+  return Lane<V>::fma(Lane<V>::neg(q.x), q.y, FV<V>(p).v);
+}
 
-__device__ __forceinline__ F2 operator-(F2 a) { return __fmul2_rn(a.v, make_float2(-1.0f, -1.0f)); }
-__device__ __forceinline__ P2 operator-(const P2& p) { return {neg2(p.x), p.y}; }
+template <class V> __device__ __forceinline__ FV<V> operator-(FV<V> a) {
+  return Lane<V>::mul(a.v, Lane<V>::bcast(-1.0f));
+}
+template <class V> __device__ __forceinline__ PV<V> operator-(const PV<V>& p) { return {Lane<V>::neg(p.x), p.y}; }
 
-__device__ __forceinline__ F2 operator/(F2 a, F2 b) { return F2(a.v.x / b.v.x, a.v.y / b.v.y); }
-__device__ __forceinline__ F2 operator/(const P2& a, F2 b) { return F2(a) / b; }
+template <class V> __device__ __forceinline__ FV<V> operator/(FV<V> a, FV<V> b) { return Lane<V>::div(a.v, b.v); }
+template <class V> __device__ __forceinline__ FV<V> operator/(const PV<V>& a, FV<V> b) { return FV<V>(a) / b; }
 
-__device__ __forceinline__ F2& operator+=(F2& a, F2 b) { return a = a + b; }
-__device__ __forceinline__ F2& operator+=(F2& a, const P2& p) { return a = a + p; }
-__device__ __forceinline__ F2& operator-=(F2& a, F2 b) { return a = a - b; }
-__device__ __forceinline__ F2& operator-=(F2& a, const P2& p) { return a = a - p; }
-__device__ __forceinline__ F2& operator*=(F2& a, F2 b) { return a = F2(a * b); }
+template <class V> __device__ __forceinline__ FV<V>& operator+=(FV<V>& a, FV<V> b) { return a = a + b; }
+template <class V> __device__ __forceinline__ FV<V>& operator+=(FV<V>& a, const PV<V>& p) { return a = a + p; }
+template <class V> __device__ __forceinline__ FV<V>& operator-=(FV<V>& a, FV<V> b) { return a = a - b; }
+template <class V> __device__ __forceinline__ FV<V>& operator-=(FV<V>& a, const PV<V>& p) { return a = a - p; }
+template <class V> __device__ __forceinline__ FV<V>& operator*=(FV<V>& a, FV<V> b) { return a = FV<V>(a * b); }
 
-__device__ __forceinline__ F2 fma(F2 a, F2 b, F2 c) { return __ffma2_rn(a.v, b.v, c.v); }
-__device__ __forceinline__ F2 sqrt(F2 a) { return F2(sqrtf(a.v.x), sqrtf(a.v.y)); }
+// the lane type of an operand (FV or PV); no member for other types, so the
+// fma below takes part only where an operand is one of these types
+template <class T> struct LaneOf {};
+template <class V> struct LaneOf<FV<V>> { using type = V; };
+template <class V> struct LaneOf<PV<V>> { using type = V; };
 
-// per-component max / min against a bound (the clamps of the collisions)
-__device__ __forceinline__ F2 clamp_lo(F2 a, F2 lo) { return F2(fmaxf(a.v.x, lo.v.x), fmaxf(a.v.y, lo.v.y)); }
-__device__ __forceinline__ F2 clamp_hi(F2 a, F2 hi) { return F2(fminf(a.v.x, hi.v.x), fminf(a.v.y, hi.v.y)); }
+// fma with any operand an unevaluated product: the product is rounded first,
+// as the scalar code rounds a * b before the fused multiply-add that takes it
+template <class A, class B, class C, class V = typename LaneOf<A>::type>
+__device__ __forceinline__ FV<V> fma(const A& a, const B& b, const C& c) {
+  return Lane<V>::fma(FV<V>(a).v, FV<V>(b).v, FV<V>(c).v);
+}
+template <class V> __device__ __forceinline__ FV<V> sqrt(FV<V> a) { return Lane<V>::sqrt(a.v); }
+// the fast reciprocal of tlbm_collide.cuh, per lane
+template <class V> __device__ __forceinline__ FV<V> rcp_fast(FV<V> a) { return Lane<V>::rcp(a.v); }
 
-// reference-rounded operations (no contraction), per component as __f*_rn
-__device__ __forceinline__ F2 xadd(F2 a, F2 b) { return __fadd2_rn(a.v, b.v); }
-__device__ __forceinline__ F2 xsub(F2 a, F2 b) { return __ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v); }
-__device__ __forceinline__ F2 xmul(F2 a, F2 b) { return __fmul2_rn(a.v, b.v); }
-__device__ __forceinline__ F2 xdiv(F2 a, F2 b) { return F2(__fdiv_rn(a.v.x, b.v.x), __fdiv_rn(a.v.y, b.v.y)); }
+// per-lane max / min against a bound (the clamps of the collisions)
+template <class V> __device__ __forceinline__ FV<V> clamp_lo(FV<V> a, FV<V> lo) { return Lane<V>::max(a.v, lo.v); }
+template <class V> __device__ __forceinline__ FV<V> clamp_hi(FV<V> a, FV<V> hi) { return Lane<V>::min(a.v, hi.v); }
+
+// reference-rounded operations (no contraction), per lane as __f*_rn
+template <class V> __device__ __forceinline__ FV<V> xadd(FV<V> a, FV<V> b) { return Lane<V>::add(a.v, b.v); }
+template <class V> __device__ __forceinline__ FV<V> xsub(FV<V> a, FV<V> b) {
+  return Lane<V>::fma(b.v, Lane<V>::bcast(-1.0f), a.v);
+}
+template <class V> __device__ __forceinline__ FV<V> xmul(FV<V> a, FV<V> b) { return Lane<V>::mul(a.v, b.v); }
+template <class V> __device__ __forceinline__ FV<V> xdiv(FV<V> a, FV<V> b) { return Lane<V>::xdiv(a.v, b.v); }
+
+}  // namespace pk
+
+using pk::F1;
+using pk::F2;
+using pk::P1;
+using pk::P2;
 
 }  // namespace tlbm

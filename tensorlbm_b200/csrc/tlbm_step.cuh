@@ -13,6 +13,26 @@
 #include <type_traits>
 
 #include "tlbm_bc.cuh"
+#include "tlbm_pair.cuh"
+
+#ifndef TLBM_PACK
+#define TLBM_PACK 1
+#endif
+#ifndef TLBM_MINB_MRT
+#define TLBM_MINB_MRT 3
+#endif
+#ifndef TLBM_MINB_MRT_HALF
+#define TLBM_MINB_MRT_HALF 3
+#endif
+#ifndef TLBM_MINB_BGK_HALF
+#define TLBM_MINB_BGK_HALF 4
+#endif
+#ifndef TLBM_MINB_CUM
+#define TLBM_MINB_CUM 2
+#endif
+#ifndef TLBM_MINB_AA_MRT
+#define TLBM_MINB_AA_MRT 0
+#endif
 
 namespace tlbm {
 
@@ -185,6 +205,15 @@ __device__ __forceinline__ void relax_fluid(const Domain<SI, SO>& d, long long c
 #pragma unroll
         for (int q = 0; q < Q; ++q)
           f[q] += feq_fused<L>(q, rho, ux * k, uy * k, uz * k, usq_k) - feq_fused<L>(q, rho, ux, uy, uz, usq);
+      } else if constexpr (std::is_same<T, float>::value && packed_collision<L, COLL, Storage<SI>::kFast>()) {
+        // the explicit-rounding form of the pair kernels, on one cell: the
+        // same result bit for bit as a pair kernel gives this cell
+        F1 g[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) g[q] = F1(f[q]);
+        collide<L, COLL, F1, Storage<SI>::kFast>(g, pack_params<F1>(cp), F1(tau_cell), has_tau);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) f[q] = g[q].v;
       } else {
         collide<L, COLL, T, Storage<SI>::kFast>(f, cp, tau_cell, has_tau);
       }
@@ -319,11 +348,89 @@ __device__ __forceinline__ void pull_pair(typename PairIO<S>::V v, T w, T& a, T&
 template <class L, typename SI, typename SO, typename T>
 __device__ __forceinline__ void relax_deviation(const Domain<SI, SO>& d, long long cell, T (&g)[L::Q],
                                                 const CollideParams<T>& cp) {
-  const T om = d.tau_field ? T(1) / T(d.tau_field[cell]) : cp.inv_tau;
+  const T om = d.tau_field ? rcp_fast(T(d.tau_field[cell])) : cp.inv_tau;
   collide_bgk_deviation<L>(g, om, T(Storage<SI>::kRaw));
   if (d.status) {
     const T r = g[0];
     if (!(r == r) || r - r != T(0)) atomicOr(d.status, 1u);
+  }
+}
+
+// Interior cells of a shifted half format with BGK, both cells of the pair in
+// packed arithmetic.
+template <class L, typename S>
+__device__ __forceinline__ void relax_deviation_pair(const Domain<S, S>& d, long long cell, float (&ga)[L::Q],
+                                                     float (&gb)[L::Q], const CollideParams<float>& cp) {
+  F2 g[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) g[q] = F2(ga[q], gb[q]);
+  const F2 om = d.tau_field ? rcp_fast(F2(d.tau_field[cell], d.tau_field[cell + 1])) : F2(cp.inv_tau);
+  collide_bgk_deviation<L>(g, om, F2(Storage<S>::kRaw));
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    ga[q] = g[q].a();
+    gb[q] = g[q].b();
+  }
+  if (d.status) {
+    const float ra = ga[0], rb = gb[0];
+    if (!(ra == ra) || ra - ra != 0.0f || !(rb == rb) || rb - rb != 0.0f) atomicOr(d.status, 1u);
+  }
+}
+
+// The collision of two fluid cells of a pair in packed arithmetic (the
+// collisions packed_collision() admits), with the per-cell tau and the
+// status bit.
+template <class L, typename S, int COLL>
+__device__ __forceinline__ void relax_fluid_pair(const Domain<S, S>& d, long long cell, float (&fa)[L::Q],
+                                                 float (&fb)[L::Q], const CollideParams<float>& cp) {
+  F2 g[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) g[q] = F2(fa[q], fb[q]);
+  const bool has_tau = d.tau_field != nullptr;
+  const F2 tau_cell = has_tau ? F2(d.tau_field[cell], d.tau_field[cell + 1]) : F2(0.0f);
+  collide<L, COLL, F2, Storage<S>::kFast>(g, pack_params<F2>(cp), tau_cell, has_tau);
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    fa[q] = g[q].a();
+    fb[q] = g[q].b();
+  }
+  if (d.status) {
+    const float ra = fa[0], rb = fb[0];
+    if (!(ra == ra) || ra - ra != 0.0f || !(rb == rb) || rb - rb != 0.0f) atomicOr(d.status, 1u);
+  }
+}
+
+// The collisions of the two cells of a pair after their boundaries (the
+// half-way reversal of a wall cell included): one packed collision when PACK
+// and both are fluid cells, else one per cell.  The two-buffer and the AA pair
+// kernels share it, so their results stay identical.
+template <class L, typename S, int COLL, bool FORCED, bool PACK>
+__device__ __forceinline__ void relax_two(const Domain<S, S>& d, long long c, uint8_t fla, uint8_t flb,
+                                          typename Storage<S>::T (&fa)[L::Q], typename Storage<S>::T (&fb)[L::Q],
+                                          const CollideParams<typename Storage<S>::T>& cp) {
+  if constexpr (PACK && COLL != TLBM_COLL_NONE) {
+    if (!((fla | flb) & TLBM_FLAG_HALFWAY)) {
+      relax_fluid_pair<L, S, COLL>(d, c, fa, fb, cp);
+      return;
+    }
+  }
+  relax<L, S, S, COLL, FORCED>(d, c, fla, fa, cp);
+  relax<L, S, S, COLL, FORCED>(d, c + 1, flb, fb, cp);
+}
+
+// relax_two for two fluid cells without flags (a warp that took no boundary code)
+template <class L, typename S, int COLL, bool FORCED, bool PACK>
+__device__ __forceinline__ void relax_interior_two(const Domain<S, S>& d, long long c,
+                                                   typename Storage<S>::T (&fa)[L::Q],
+                                                   typename Storage<S>::T (&fb)[L::Q],
+                                                   const CollideParams<typename Storage<S>::T>& cp) {
+  if constexpr (COLL == TLBM_COLL_NONE) {
+    return;
+  } else if constexpr (PACK) {
+    relax_fluid_pair<L, S, COLL>(d, c, fa, fb, cp);
+  } else {
+    relax_fluid<L, S, S, COLL, FORCED>(d, c, fa, cp);
+    relax_fluid<L, S, S, COLL, FORCED>(d, c + 1, fb, cp);
   }
 }
 
@@ -348,8 +455,8 @@ __host__ __device__ constexpr bool uniform_edge_branch() {
 // Requires nx even, (Q/2 + 2) n < 2^31 (32-bit offsets), and f_in / f_out
 // aligned to two values.
 template <class L, typename S, int COLL, bool FORCED = false>
-__global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typename Storage<S>::T> cp,
-                                                 BcParams<typename Storage<S>::T> bp) {
+__device__ __forceinline__ void step_x2(const StepParams& p, const CollideParams<typename Storage<S>::T>& cp,
+                                        const BcParams<typename Storage<S>::T>& bp) {
   using T = typename Storage<S>::T;
   using IO = PairIO<S>;
   using V = typename IO::V;
@@ -361,6 +468,9 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
   // (3 instead of 4 blocks per SM, 7 % slower).
   constexpr bool kDev = std::is_same<S, __half>::value && COLL == TLBM_COLL_BGK && !FORCED &&
                         uniform_edge_branch<L, COLL>();
+  // both cells' collisions as one stream of packed float32 instructions
+  constexpr bool kPack = TLBM_PACK && std::is_same<T, float>::value && !FORCED &&
+                         (kDev || packed_collision<L, COLL, Storage<S>::kFast>());
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -458,40 +568,41 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
     double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
     apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
     apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
-    relax<L, S, S, COLL, FORCED>(d, (long long)c, fla, fa, cp);
-    relax<L, S, S, COLL, FORCED>(d, (long long)c + 1, flb, fb, cp);
-  } else {
+    relax_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fla, flb, fa, fb, cp);
+  } else if constexpr (kDev) {
     bool keep_a = false, keep_b = false;   // half-way wall cells: reversed, not collided
     if (edge) {
       double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
       apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
       apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
-      if (COLL != TLBM_COLL_NONE && (fla & TLBM_FLAG_HALFWAY)) {
+      if (fla & TLBM_FLAG_HALFWAY) {
         bounce_back<L>(fa);
         keep_a = true;
       }
-      if (COLL != TLBM_COLL_NONE && (flb & TLBM_FLAG_HALFWAY)) {
+      if (flb & TLBM_FLAG_HALFWAY) {
         bounce_back<L>(fb);
         keep_b = true;
       }
-    }
-    if constexpr (kDev) {
-      if (edge) {
-        if (!keep_a) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c, fa, cp);
-        if (!keep_b) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c + 1, fb, cp);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {   // back to the stored deviations
-          fa[q] = (fa[q] - weight<L, T>(q)) * T(Storage<S>::kRaw);
-          fb[q] = (fb[q] - weight<L, T>(q)) * T(Storage<S>::kRaw);
-        }
-      } else {
-        relax_deviation<L>(d, (long long)c, fa, cp);
-        relax_deviation<L>(d, (long long)c + 1, fb, cp);
-      }
-    } else {
       if (!keep_a) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c, fa, cp);
       if (!keep_b) relax_fluid<L, S, S, COLL, FORCED>(d, (long long)c + 1, fb, cp);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {   // back to the stored deviations
+        fa[q] = (fa[q] - weight<L, T>(q)) * T(Storage<S>::kRaw);
+        fb[q] = (fb[q] - weight<L, T>(q)) * T(Storage<S>::kRaw);
+      }
+    } else if constexpr (kPack) {
+      relax_deviation_pair<L>(d, (long long)c, fa, fb, cp);
+    } else {
+      relax_deviation<L>(d, (long long)c, fa, cp);
+      relax_deviation<L>(d, (long long)c + 1, fb, cp);
     }
+  } else if (edge) {
+    double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
+    apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+    relax_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fla, flb, fa, fb, cp);
+  } else {
+    relax_interior_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fa, fb, cp);   // no flag in the warp
   }
 
   // one hash per pair of its index and of this step's f_0 values (so the bits
@@ -508,6 +619,30 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
     else
       __stwb(reinterpret_cast<V*>(at_offset(pout, (q - MID) * N)), IO::join(fa[q], fb[q], weight<L, T>(q), h, q));
   }
+}
+
+// Resident blocks of 256 threads per SM that the pair kernel is compiled for
+// (the register cap __launch_bounds__ derives from it); 0 = no cap.
+template <class L, typename S, int COLL>
+__host__ __device__ constexpr int x2_min_blocks() {
+  constexpr bool f64 = std::is_same<S, double>::value;
+  constexpr bool shifted = std::is_same<S, __half>::value || std::is_same<S, __nv_bfloat16>::value;
+  if (L::Q == 19 && COLL == TLBM_COLL_MRT && !f64) return shifted ? TLBM_MINB_MRT_HALF : TLBM_MINB_MRT;
+  if (L::Q == 19 && COLL == TLBM_COLL_BGK && shifted) return TLBM_MINB_BGK_HALF;
+  if (L::Q == 27 && COLL == TLBM_COLL_CUMULANT && !f64) return TLBM_MINB_CUM;
+  return 0;
+}
+
+template <class L, typename S, int COLL, bool FORCED = false>
+__global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typename Storage<S>::T> cp,
+                                                 BcParams<typename Storage<S>::T> bp) {
+  step_x2<L, S, COLL, FORCED>(p, cp, bp);
+}
+// the same kernel compiled for MINB resident blocks per SM
+template <class L, typename S, int COLL, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_x2_capped(StepParams p, CollideParams<typename Storage<S>::T> cp,
+                                                               BcParams<typename Storage<S>::T> bp) {
+  step_x2<L, S, COLL, false>(p, cp, bp);
 }
 
 // Whether the pair kernel can run this step: no Bouzidi link tables, nx even
@@ -547,7 +682,9 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   if constexpr (PULL && !FORCED && std::is_same<SI, SO>::value) {
     if (pair_layout_ok<L, SI>(p)) {
       step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block);
-      k_step_x2<L, SI, COLL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
+      constexpr int minb = x2_min_blocks<L, SI, COLL>();
+      if constexpr (minb > 0) k_step_x2_capped<L, SI, COLL, minb><<<grid, block, 0, s>>>(p, cp, bp);
+      else k_step_x2<L, SI, COLL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
       return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
     }
   }

@@ -322,6 +322,99 @@ def mass(torch) -> None:
     print("wrote mass.npz")
 
 
+def c4_divergence(torch, max_steps: int = 5_000, nx_max: int = 160) -> None:
+    """The smallest design points of the batched-form scan (nx <= 160, ny = nx/4,
+    cylinder D = ny/8; the seeded design of tensorlbm_b200.batch.uniform_scan
+    with seed 20261203), run through TensorLBM's own D2Q9 cylinder chain
+    (cylinder_flow.py:854-899, zou_he outlet mode): collide_bgk -> stream ->
+    compute_obstacle_forces -> zou_he_inlet_velocity -> zou_he_outlet_pressure ->
+    bounce_back_cells(wall) -> bounce_back_cells(cylinder), for up to
+    max_steps steps.  Records the first step whose populations are not all
+    finite (-1 if none), and for two nx = 128 points the last finite state at
+    or before step 200."""
+    from tensorlbm import boundaries as b2
+    from tensorlbm.d2q9 import equilibrium
+    from tensorlbm.solver import collide_bgk, stream
+
+    g = torch.Generator().manual_seed(20261203)
+    n = 512
+    nxs = torch.randint(128 // 8, 1024 // 8 + 1, (n,), generator=g) * 8
+    res = 40.0 + 260.0 * torch.rand(n, generator=g, dtype=torch.float64)
+    pick = [i for i in range(n) if int(nxs[i]) <= nx_max]
+    cpu = torch.device("cpu")
+    out = {"domains": np.array(pick), "max_steps": max_steps}
+    for i in pick:
+        nx = int(nxs[i])
+        ny = nx // 4
+        d = ny / 8.0
+        re = float(res[i])
+        tau = 3.0 * 0.05 * d / re + 0.5
+        obst = b2.cylinder_mask(nx, ny, ny / 2.0, ny / 2.0, d / 2.0, cpu)
+        wall = b2.make_channel_wall_mask(ny, nx, obst, cpu)
+        ux = torch.full((ny, nx), 0.05)
+        ux[obst] = 0.0
+        f = equilibrium(torch.ones((ny, nx)), ux, torch.zeros((ny, nx)))
+        nan_step, check, check_step = -1, f.clone(), 0
+        t0 = time.time()
+        for step in range(1, max_steps + 1):
+            f = collide_bgk(f, tau)
+            f = stream(f)
+            b2.compute_obstacle_forces(f, obst)
+            f = b2.zou_he_inlet_velocity(f, 0.05)
+            f = b2.zou_he_outlet_pressure(f, rho_out=1.0)
+            f = b2.bounce_back_cells(f, wall)
+            f = b2.bounce_back_cells(f, obst)
+            if not bool(torch.isfinite(f).all()):
+                nan_step = step
+                break
+            if step <= 200:
+                check, check_step = f.clone(), step
+        out[f"re_{i}"] = re
+        out[f"tau_{i}"] = tau
+        out[f"nan_step_{i}"] = nan_step
+        if i in (118, 364):   # the last finite state at or before step 200
+            out[f"check_{i}"] = check.numpy()
+            out[f"check_step_{i}"] = check_step
+        print(f"  domain {i}: nx {nx} Re {re:.1f} tau {tau:.5f} -> non-finite at step {nan_step} "
+              f"({time.time() - t0:.0f} s)")
+    np.savez_compressed(HERE / "c4_divergence.npz", **out)
+    print("wrote c4_divergence.npz")
+
+
+def cavity_case(torch) -> None:
+    """TensorLBM's registered lid-driven cavity case (cases/cavity.py:25-110),
+    stepped with the case's own chain (CaseBase.make_step, cases/base.py:270-289:
+    collide -> pre-streaming half-way walls from the pre-collision state ->
+    stream -> Zou/He lid) from case.initial_f(), for three scan points: BGK at
+    resolution 32 (Re 100), MRT at 24 (Re 150) and MRT on (6, 20, 40) (Re 200).
+    Stores the mid-plane z = nz // 2 of the final populations, the float64 sum
+    of every direction, the case's tau and the point's parameters."""
+    from tensorlbm.cases import get_case
+
+    points = {"bgk32": dict(resolution=32, re=100.0, collision="bgk", steps=300),
+              "mrt24": dict(resolution=24, re=150.0, collision="mrt", steps=300),
+              "mrt6x20x40": dict(resolution=(6, 20, 40), re=200.0, collision="mrt", steps=300)}
+    out = {}
+    for tag, pt in points.items():
+        case = get_case("cavity", resolution=pt["resolution"], re=pt["re"], collision=pt["collision"],
+                        device="cpu")
+        step = case.make_step()
+        f = case.initial_f()
+        for _ in range(pt["steps"]):
+            f = step(f)
+        nz = f.shape[1]
+        out[f"{tag}_shape"] = np.array(f.shape[1:])
+        out[f"{tag}_tau"] = case.units.tau
+        out[f"{tag}_re"] = pt["re"]
+        out[f"{tag}_u_lid"] = case.u_lid
+        out[f"{tag}_steps"] = pt["steps"]
+        out[f"{tag}_mid"] = f[:, nz // 2].numpy()
+        out[f"{tag}_qsum"] = f.double().sum(dim=(1, 2, 3)).numpy()
+        print(f"  cavity {tag}: grid {tuple(f.shape[1:])}, tau {case.units.tau:.5f}, finite {bool(torch.isfinite(f).all())}")
+    np.savez_compressed(HERE / "cavity_case.npz", **out)
+    print(f"wrote cavity_case.npz ({(HERE / 'cavity_case.npz').stat().st_size / 1024:.0f} KB)")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -355,6 +448,12 @@ def main() -> None:
         return
     if args.only == "mass":
         mass(torch)
+        return
+    if args.only == "c4_divergence":
+        c4_divergence(torch)
+        return
+    if args.only == "cavity_case":
+        cavity_case(torch)
         return
     from tensorlbm import boundaries as b2
     from tensorlbm import boundaries3d as b3

@@ -35,13 +35,26 @@ def test_library_exports_every_declared_symbol():
     lib = _lib.load()
     for name in _declared_symbols():
         assert hasattr(lib, name), name
-    assert lib.tlbm_abi_version() == 1
+    assert lib.tlbm_abi_version() == 2
     assert lib.tlbm_status_string(3) == b"input and output buffers alias"
     # the Python binding types exactly the declared set
     assert sorted(_lib.exported_symbols()) == sorted(_declared_symbols())
     out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)], capture_output=True, text=True).stdout
     exported = set(re.findall(r"\b(tlbm_\w+)\b", out))
     assert set(_declared_symbols()) == exported
+
+
+def test_struct_layouts_match_the_library():
+    """The ctypes mirrors of tlbm_desc, tlbm_batch_domain and tlbm_batch_desc
+    have the sizes the compiled library has."""
+    import ctypes
+
+    from tensorlbm_b200 import _lib
+
+    lib = _lib.load()
+    for which, cls in enumerate((_lib.Desc, _lib.BatchDomain, _lib.BatchDesc)):
+        assert lib.tlbm_struct_size(which) == ctypes.sizeof(cls), cls.__name__
+    assert lib.tlbm_struct_size(3) == -1
 
 
 def test_argument_checks_without_gpu():

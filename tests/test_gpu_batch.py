@@ -84,3 +84,94 @@ def test_autotune_and_strouhal_smoke(cuda):
     hist = b.run(400, record_every=1)
     assert hist.shape == (400, 6, 3)
     assert torch.isfinite(hist).all()
+
+
+def test_scan_divergence_matches_reference(cuda):
+    """The 21 smallest design points of the seeded 512-domain scan (nx <= 160,
+    BGK tau - 1/2 between 0.0027 and 0.0068 on cylinders of D = 4-5 cells)
+    turn non-finite in TensorLBM's own D2Q9 cylinder chain at steps 54-64
+    (golden c4_divergence, generated from the unmodified reference).  The
+    batched runner must reach the same onset step on every one of them, and
+    the same populations bit for bit on the last finite state the fixture
+    holds."""
+    from tensorlbm_b200 import batch
+
+    from tests.conftest import golden
+
+    g = golden("c4_divergence")
+    pick = [int(i) for i in g["domains"]]
+    design = batch.uniform_scan(512, seed=20261203, device=cuda)
+    doms = [design[i] for i in pick]
+    for k, i in enumerate(pick):
+        assert doms[k].tau == pytest.approx(float(g[f"tau_{i}"]), rel=0, abs=1e-15)
+    b = batch.BatchedSolver(doms, "bgk", device=cuda).load(batch.equilibrium_start(doms, cuda))
+    onset = {i: -1 for i in pick}
+    last = max(int(g[f"nan_step_{i}"]) for i in pick)
+    assert 0 < last < 100
+    for step in range(1, last + 1):
+        b.step()
+        for k, i in enumerate(pick):
+            if onset[i] >= 0:
+                continue
+            f = b.f(k)
+            if not bool(torch.isfinite(f).all()):
+                onset[i] = step
+            elif f"check_step_{i}" in g and step == int(g[f"check_step_{i}"]):
+                assert same(f.cpu().numpy(), g[f"check_{i}"]), i
+    assert onset == {i: int(g[f"nan_step_{i}"]) for i in pick}
+
+
+@pytest.mark.parametrize("mode", ["graph", "persistent"])
+def test_cavity_scan_points_match_reference_case(cuda, mode):
+    """Scan points of TensorLBM's registered cavity case (cases/cavity.py),
+    advanced as one batch, against the case's own chain run by the reference
+    (golden cavity_case): BGK bit for bit, MRT to float32 rounding of the
+    reference's BLAS products (1e-5 relative)."""
+    from tensorlbm_b200 import batch, scan
+
+    from tests.conftest import golden
+
+    g = golden("cavity_case")
+    res = {"bgk32": 32, "mrt24": 24, "mrt6x20x40": (6, 20, 40)}
+    for collision, tags in (("bgk", ["bgk32"]), ("mrt", ["mrt24", "mrt6x20x40"])):
+        pts = [dict(resolution=res[t], re=float(g[f"{t}_re"]), u_lid=float(g[f"{t}_u_lid"])) for t in tags]
+        for t, p in zip(tags, pts):
+            d = batch.cavity_point(p["resolution"], p["re"], u_lid=p["u_lid"], device=cuda)
+            assert d.tau == float(g[f"{t}_tau"]) and d.shape == tuple(int(v) for v in g[f"{t}_shape"])
+        steps = int(g[f"{tags[0]}_steps"])
+        fs = scan.run_cavity_points(pts, steps, collision=collision, device=cuda, mode=mode)
+        for t, f in zip(tags, fs):
+            mid = f[:, f.shape[1] // 2].cpu().numpy()
+            qsum = f.double().sum(dim=(1, 2, 3)).cpu().numpy()
+            if collision == "bgk":
+                assert same(mid, g[f"{t}_mid"]), t
+                np.testing.assert_allclose(qsum, g[f"{t}_qsum"], rtol=1e-12)
+            else:
+                assert float(np.max(np.abs(mid - g[f"{t}_mid"]))) <= 1e-5 * float(np.max(np.abs(g[f"{t}_mid"]))), t
+                np.testing.assert_allclose(qsum, g[f"{t}_qsum"], rtol=1e-6)
+
+
+@pytest.mark.parametrize("mode", ["launch", "graph", "persistent"])
+def test_retire_skips_diverged_domains(cuda, mode):
+    """With retire=True a domain that turns non-finite is skipped from then on
+    (its own status word); the other domains still evolve bit for bit as
+    without it."""
+    from tensorlbm_b200 import batch
+
+    from tests.conftest import golden
+
+    g = golden("c4_divergence")
+    design = batch.uniform_scan(512, seed=20261203, device=cuda)
+    bad = [int(i) for i in g["domains"]][:4]
+    good = [batch.cylinder_channel(nx, re, 0.05, cuda) for nx, re in ((128, 10.0), (160, 12.0))]
+    doms = [design[i] for i in bad] + good
+    f0 = batch.equilibrium_start(doms, cuda)
+    b = batch.BatchedSolver(doms, "bgk", device=cuda, mode=mode, retire=True).load(f0)
+    b.run(128)
+    assert b.retired_domains().tolist() == [True] * 4 + [False] * 2
+    ref = batch.BatchedSolver(good, "bgk", device=cuda, mode=mode).load(f0[4:])
+    ref.run(128)
+    for k in range(2):
+        assert torch.equal(b.f(4 + k), ref.f(k))
+    torch.cuda.synchronize(cuda)
+    assert int(b.status.item()) == 0          # the non-finite bits went to the domains' own words

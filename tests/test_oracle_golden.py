@@ -284,3 +284,32 @@ def test_correct_mass(q, tag):
     tol = 1e-6 if tag == "f32" else 1e-14
     assert got.dtype == ref.dtype and np.max(np.abs(got - ref)) <= tol * np.max(np.abs(ref))
     assert same(O.correct_mass(np.zeros((19, 2, 3, 4), np.float32), 5.0), g["zero_out"])
+
+
+def test_c4_divergence_onset():
+    """The oracle's D2Q9 cylinder chain on the smallest design points of the
+    batched scan: bit-exact to TensorLBM up to the last finite state the
+    fixture holds, and non-finite at the same step as TensorLBM."""
+    g = golden("c4_divergence")
+    for i in (118, 364):
+        nx = 128
+        ny = nx // 4
+        d = ny / 8.0
+        tau = float(g[f"tau_{i}"])
+        obst = O.cylinder_mask(nx, ny, ny / 2.0, ny / 2.0, d / 2.0)
+        wall = np.zeros((ny, nx), bool)
+        wall[0, :] = wall[-1, :] = True
+        wall[obst] = False
+        ux = np.full((ny, nx), 0.05, np.float32)
+        ux[obst] = 0.0
+        f = O.equilibrium(9, np.ones((ny, nx), np.float32), ux, np.zeros_like(ux))
+        onset = -1
+        with np.errstate(all="ignore"):
+            for step in range(1, 100):
+                f, _ = O.channel_step(f, tau, 0.05, 1.0, wall, obst)
+                if step == int(g[f"check_step_{i}"]):
+                    assert same(f, g[f"check_{i}"])
+                if not np.isfinite(f).all():
+                    onset = step
+                    break
+        assert onset == int(g[f"nan_step_{i}"])
