@@ -1,4 +1,4 @@
-"""Batched runner: many independent small D2Q9 domains advanced together.
+"""Batched runner: many independent small D2Q9 or D3Q19 domains advanced together.
 
 TensorLBM's scan runner advances design points one after the other in worker
 processes (``scan_runner.py:697`` ``run_scan_point``, ``:979``
@@ -199,7 +199,7 @@ class BatchedSolver:
         for i, d in enumerate(self.domains):
             per.append([(i, x0, r0) for r0 in range(0, d.ny * d.nz, ty) for x0 in range(0, d.nx, tx)])
         if order == "interleave":
-            tiles = [t for k in range(max(len(p) for p in per)) for p in per if k < len(p)]
+            tiles = [p[k] for k in range(max(len(p) for p in per)) for p in per if k < len(p)]
         elif order == "largest_first":
             tiles = [t for i in sorted(range(len(per)), key=lambda i: -self.domains[i].cells) for t in per[i]]
         else:
@@ -494,9 +494,55 @@ def autotune(solver: BatchedSolver, steps: int = 20,
     return {"best": best, "trials": results}
 
 
+def uniform_scan(n_domains: int, seed: int, device=None, nx_range=(128, 1024), re_range=(40.0, 300.0),
+                 u_in: float = 0.05) -> list[DomainSpec]:
+    """Seeded design of the batched-form case: nx ~ U{nx_range} (multiple of 8 so
+    that ny = nx/4 and D = ny/8 stay whole), Re ~ U(re_range)."""
+    g = torch.Generator().manual_seed(seed)
+    nxs = torch.randint(nx_range[0] // 8, nx_range[1] // 8 + 1, (n_domains,), generator=g) * 8
+    res = re_range[0] + (re_range[1] - re_range[0]) * torch.rand(n_domains, generator=g, dtype=torch.float64)
+    return [cylinder_channel(int(nx), float(re), u_in, device) for nx, re in zip(nxs.tolist(), res.tolist())]
 
 
-__all__ = ["DomainSpec", "BatchedSolver", "autotune", "cavity_point", "cylinder_channel", "uniform_scan",
+def equilibrium_start(domains: list[DomainSpec], device=None) -> list[torch.Tensor]:
+    """Start state of each domain: the equilibrium at rho = 1 with the inlet
+    velocity in x and zero velocity in the obstacle (cylinder_flow.py start
+    state); domains without an inlet start at rest (the cavity case)."""
+    from .d2q9 import equilibrium
+    from .d3q19 import equilibrium3d
+
+    out = []
+    for d in domains:
+        ux = torch.full(d.shape, float(d.u_in or 0.0), device=device)
+        if d.obstacle_mask is not None:
+            ux[d.obstacle_mask.to(ux.device)] = 0.0
+        z = torch.zeros_like(ux)
+        out.append(equilibrium(torch.ones_like(ux), ux, z) if d.nz == 1 else
+                   equilibrium3d(torch.ones_like(ux), ux, z, z))
+    return out
+
+
+def strouhal(lift: torch.Tensor, length_ref: float, u_ref: float, sample_every: int = 1,
+             st_band=(0.05, 0.35)) -> float | None:
+    """Dominant shedding frequency of a lift history as St = f D / U: Hann
+    window, band-limited FFT peak (the FFT branch of postprocess.py:646)."""
+    x = lift.detach().double().cpu()
+    x = x - x.mean()
+    n = x.numel()
+    if n < 32:
+        return None
+    w = torch.hann_window(n, periodic=False, dtype=torch.float64)
+    spec = torch.fft.rfft(x * w).abs()
+    freq = torch.fft.rfftfreq(n, d=float(sample_every), dtype=torch.float64)
+    st = freq * length_ref / u_ref
+    band = (st >= st_band[0]) & (st <= st_band[1])
+    if not bool(band.any()):
+        return None
+    k = int(torch.argmax(torch.where(band, spec, torch.zeros_like(spec))))
+    return float(st[k])
+
+
+__all__ =["DomainSpec", "BatchedSolver", "autotune", "cavity_point", "cylinder_channel", "uniform_scan",
            "equilibrium_start", "strouhal"]
 
 
