@@ -481,8 +481,10 @@ def _c2_long_variant(torch, dev, steps, every):
             "steps": steps, "tau": TAU, "history": hist,
             "drag_fx_mean_last10pct_f32": float(d32[tail, 0].mean()),
             "drag_fx_mean_last10pct_f64": float(d64[tail, 0].mean()),
-            "drag_fx_max_rel_after_1000": float(((d32[1000:, 0] - d64[1000:, 0]).abs()
-                                                 / d64[1000:, 0].abs()).max()) if steps > 1000 else None,
+            # the instantaneous drag passes near zero in the start-up transient: the
+            # difference is scaled by the window's mean |Fx|, not by each step's value
+            "drag_fx_max_abs_diff_over_mean_after_1000": float((d32[1000:, 0] - d64[1000:, 0]).abs().max()
+                                                                / d64[1000:, 0].abs().mean()) if steps > 1000 else None,
             "mlups_f32": round(cells * steps / t["f32"] / 1e6, 1),
             "mlups_f64": round(cells * steps / t["f64"] / 1e6, 1)}
         del runs, d32, d64
