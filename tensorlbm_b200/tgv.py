@@ -13,6 +13,9 @@ rho = 1 + 3 (u0^2 / 16) (cos 2x + cos 2y)(cos 2z + 2) on x = 2 pi i / n;
 nu = u0 L / Re with L = n / (2 pi); one convective time = L / u0 steps.
 
     python -m tensorlbm_b200.tgv --n 384 --re 1600 --out <dir>
+
+:func:`laminar_decay` is TensorLBM's verified laminar decay benchmark (D3Q19
+BGK, Re 24) on the fused kernel: ``python -m tensorlbm_b200.tgv --laminar 64,96,128``.
 """
 
 from __future__ import annotations
@@ -77,7 +80,7 @@ def run(n: int = 384, re: float = 1600.0, u0: float = 0.05, t_end: float = 20.0,
         del f0
         torch.cuda.empty_cache()
         m0 = float(s.moment_sums()[0])
-        hist = {"t": [], "kinetic_energy": [], "mass_drift": []}
+        hist = {"t": [], "kinetic_energy": [], "energy": [], "mass_drift": []}
         errs = {}
         secs = 0.0
         done = 0
@@ -94,6 +97,7 @@ def run(n: int = 384, re: float = 1600.0, u0: float = 0.05, t_end: float = 20.0,
                 k = 0.5 * float((rho * (u * u).sum(0)).mean())
                 hist["t"].append(done / tc)
                 hist["kinetic_energy"].append(k)
+                hist["energy"].append(0.5 * float((u * u).sum(0).mean()))
                 hist["mass_drift"].append((float(s.moment_sums()[0]) - m0) / m0)
                 if done in marks:
                     c = marks[done]
@@ -104,12 +108,18 @@ def run(n: int = 384, re: float = 1600.0, u0: float = 0.05, t_end: float = 20.0,
                         errs[str(c)] = float(torch.linalg.vector_norm(u - ref) / torch.linalg.vector_norm(ref))
                 del rho, u
         t = hist["t"]
-        e = hist["kinetic_energy"]
-        hist["dissipation"] = [-(e[i + 1] - e[i - 1]) / ((t[i + 1] - t[i - 1]) * tc) if 0 < i < len(t) - 1 else None
-                               for i in range(len(t))]
+        # -dK/dt per lattice step by central differences (K rho-weighted); the
+        # same for E = <|u|^2>/2, TensorLBM's convention
+        for key, src in (("dissipation", "kinetic_energy"), ("dissipation_energy", "energy")):
+            e = hist[src]
+            hist[key] = [-(e[i + 1] - e[i - 1]) / ((t[i + 1] - t[i - 1]) * tc) if 0 < i < len(t) - 1 else None
+                         for i in range(len(t))]
+        eps = [(v, t[i]) for i, v in enumerate(hist["dissipation_energy"]) if v is not None]
+        peak = max(eps) if eps else (None, None)
         entry = {"mlups": n ** 3 * total / max(secs, 1e-12) / 1e6, "seconds": secs,
                  "finite": not s.nonfinite_seen(), "velocity_l2_vs_f64": errs, "history": hist,
-                 "mass_drift_end": hist["mass_drift"][-1]}
+                 "mass_drift_end": hist["mass_drift"][-1],
+                 "peak_dissipation": peak[0], "peak_dissipation_t": peak[1]}
         res["runs"][storage] = entry
         log(f"{storage}: {entry['mlups']:.0f} MLUPS, L2 vs f64 {errs}, mass drift {entry['mass_drift_end']:.2e}")
         del s
@@ -120,6 +130,60 @@ def run(n: int = 384, re: float = 1600.0, u0: float = 0.05, t_end: float = 20.0,
     return res
 
 
+def laminar_decay(n: int, re: float = 24.0, u0: float = 0.05, steps: int = 2000, record_every: int = 50,
+                  device="cuda:0") -> dict:
+    """TensorLBM's verified laminar Taylor-Green decay
+    (benchmarks/verified/taylor_green_3d/run.py:87-230) on the fused kernel.
+
+    D3Q19 BGK in float32, f <- collide(stream(f)) every step on a periodic n^3
+    box; nu = u0 n / Re, tau = 1/2 + 3 nu, k = 2 pi / n,
+    u = (u0 sin kx cos ky cos kz, -u0 cos kx sin ky cos kz, 0), rho = 1, f = feq.
+    Every record_every steps E = <|u|^2> / 2 (no density weight, the
+    benchmark's convention); gamma_E is minus the slope of a least-squares line
+    through ln E over the recorded steps t >= record_every, against the linear
+    viscous rate 6 nu k^2 (modes (+-k, +-k, +-k))."""
+    from . import FusedSolver3D
+    from .d3q19 import equilibrium3d, macroscopic3d
+
+    dev = torch.device(device)
+    nu = u0 * n / re
+    tau = 0.5 + 3.0 * nu
+    k = 2.0 * math.pi / float(n)
+    ax = torch.arange(n, device=dev, dtype=torch.float32)
+    z, y, x = torch.meshgrid(ax, ax, ax, indexing="ij")
+    ux0 = u0 * torch.sin(k * x) * torch.cos(k * y) * torch.cos(k * z)
+    uy0 = -u0 * torch.cos(k * x) * torch.sin(k * y) * torch.cos(k * z)
+    uz0 = torch.zeros_like(ux0)
+    f = equilibrium3d(torch.ones_like(ux0), ux0, uy0, uz0)
+    e0 = float((0.5 * (ux0 * ux0)).mean()) + float((0.5 * (uy0 * uy0)).mean())
+    del z, y, x
+    s = FusedSolver3D(n, n, n, tau=tau, device=dev)
+    times, energies = [0], [e0]
+    secs = 0.0
+    for step in range(record_every, steps + 1, record_every):
+        def advance():
+            nonlocal f
+            for _ in range(record_every):
+                f = s.step(f)
+        secs += _timed(advance, dev)
+        _, ux, uy, uz = macroscopic3d(f)
+        energies.append(float((0.5 * (ux * ux)).mean()) + float((0.5 * (uy * uy)).mean()) +
+                        float((0.5 * (uz * uz)).mean()))
+        times.append(step)
+    import numpy as np
+
+    t = np.asarray(times[1:], dtype=np.float64)
+    ln_e = np.log(np.asarray(energies[1:], dtype=np.float64))
+    slope, icept = np.polyfit(t, ln_e, 1)
+    resid = ln_e - (icept + slope * t)
+    gamma_theory = 6.0 * nu * k * k
+    return {"n": n, "re": re, "u0": u0, "nu": nu, "tau": tau, "steps": steps, "record_every": record_every,
+            "times": times, "energies": energies, "gamma_e_sim": float(-slope), "gamma_e_theory": gamma_theory,
+            "err_e_pct": float((-slope - gamma_theory) / gamma_theory * 100.0),
+            "r2": 1.0 - float(np.sum(resid ** 2) / np.sum((ln_e - ln_e.mean()) ** 2)),
+            "mlups": n ** 3 * steps / max(secs, 1e-12) / 1e6}
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description="Taylor-Green precision study (D3Q27 cumulant)")
     ap.add_argument("--n", type=int, default=384)
@@ -128,7 +192,16 @@ def main(argv=None) -> None:
     ap.add_argument("--collision", default="cumulant")
     ap.add_argument("--storages", default="f64,f32,f16,bf16")
     ap.add_argument("--out", default="tgv_out")
+    ap.add_argument("--laminar", default=None,
+                    help="comma list of grid sizes: run TensorLBM's verified laminar decay (Re 24) instead")
     args = ap.parse_args(argv)
+    if args.laminar:
+        res = {str(n): laminar_decay(int(n), steps=2600 if int(n) >= 128 else 2000) for n in args.laminar.split(",")}
+        out = pathlib.Path(args.out)
+        out.mkdir(parents=True, exist_ok=True)
+        (out / "tgv_laminar.json").write_text(json.dumps(res))
+        print(json.dumps({n: {k: v for k, v in r.items() if k not in ("times", "energies")} for n, r in res.items()}))
+        return
     res = run(args.n, args.re, t_end=args.t_end, storages=tuple(args.storages.split(",")), collision=args.collision,
               log=lambda s: print(s, flush=True))
     out = pathlib.Path(args.out)

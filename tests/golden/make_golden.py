@@ -415,12 +415,37 @@ def cavity_case(torch) -> None:
     print(f"wrote cavity_case.npz ({(HERE / 'cavity_case.npz').stat().st_size / 1024:.0f} KB)")
 
 
+def tgv_laminar(src: str) -> None:
+    """TensorLBM's verified laminar Taylor-Green decay
+    (benchmarks/verified/taylor_green_3d: run.py, result.json and the
+    energy_history_N*.csv files it wrote, D3Q19 BGK float32 at Re 24 on
+    N = 64, 96, 128): the recorded steps, energies E = <|u|^2>/2 and the
+    fitted gamma_E of each grid, copied from the reference's own outputs."""
+    import json
+
+    bench = pathlib.Path(src).parent / "benchmarks" / "verified" / "taylor_green_3d"
+    res = json.loads((bench / "result.json").read_text())
+    out = {}
+    for case in res["cases"]:
+        n = int(case["n"])
+        rows = np.loadtxt(bench / f"energy_history_N{n}.csv", delimiter=",", skiprows=1)
+        out[f"n{n}_record_steps"] = rows[:, 0].astype(np.int64)
+        out[f"n{n}_energy"] = rows[:, 1]
+        for key in ("re", "u0", "tau", "steps", "record_every", "gamma_e_sim", "gamma_e_theory", "r2"):
+            out[f"n{n}_{key}"] = np.asarray(case[key])
+    np.savez_compressed(HERE / "tgv_laminar.npz", **out)
+    print(f"wrote tgv_laminar.npz ({len(res['cases'])} grids)")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
     ap.add_argument("--skip-long", action="store_true", help="skip the 64^3 x 1000-step cavity run")
     ap.add_argument("--only", default=None, help="write only this group of fixtures (e.g. moving_wall)")
     args = ap.parse_args()
+    if args.only == "tgv_laminar":
+        tgv_laminar(args.reference)
+        return
     import_reference(args.reference)
     import torch
 

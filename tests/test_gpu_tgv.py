@@ -27,3 +27,26 @@ def test_tgv_precision_small(cuda):
     # kinetic energy decays
     k = runs["f64"]["history"]["kinetic_energy"]
     assert k[-1] < k[0] and all(math.isfinite(v) for v in k)
+
+
+@pytest.mark.parametrize("n", [64, 96])
+def test_laminar_decay_matches_reference_benchmark(cuda, n):
+    """TensorLBM's verified laminar Taylor-Green decay (D3Q19 BGK, Re 24,
+    float32, 2000 steps) on the fused kernel against the energy history and the
+    fitted decay rate that the reference benchmark recorded (golden
+    tgv_laminar, from benchmarks/verified/taylor_green_3d).  The reference ran
+    torch's CUDA operators, so agreement is to float32 rounding, not bitwise."""
+    import numpy as np
+
+    from tensorlbm_b200 import tgv
+
+    from tests.conftest import golden
+
+    g = golden("tgv_laminar")
+    res = tgv.laminar_decay(n, re=float(g[f"n{n}_re"]), u0=float(g[f"n{n}_u0"]), steps=int(g[f"n{n}_steps"]),
+                            record_every=int(g[f"n{n}_record_every"]), device=cuda)
+    assert res["tau"] == pytest.approx(float(g[f"n{n}_tau"]), rel=1e-12)
+    assert np.array_equal(np.asarray(res["times"]), g[f"n{n}_record_steps"])
+    np.testing.assert_allclose(res["energies"], g[f"n{n}_energy"], rtol=1e-5)
+    assert res["gamma_e_sim"] == pytest.approx(float(g[f"n{n}_gamma_e_sim"]), rel=1e-5)
+    assert res["r2"] > 0.99999
