@@ -415,6 +415,7 @@ def _batched_variant(torch, dev, steps, peak):
             "mlups_live_recording_forces_every_10": round(live_rec / t_rec / 1e6, 1),
             "roofline_frac_live": round(72 * live_updates / t / 1e9 / peak, 4), "bytes_per_cell": 72,
             "mode": tune["best"]["mode"], "tile": list(tune["best"]["tile"]), "order": tune["best"]["order"],
+            "cells_per_thread": tune["best"]["cells_per_thread"],
             "ctas_per_sm": tune["best"]["ctas_per_sm"],
             "finite_domains": int(finite.sum()), "retired_domains": 512 - int(finite.sum()),
             "sequential_mlups_16_finite_domains": round(seq_mlups, 1),

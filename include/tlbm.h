@@ -136,7 +136,9 @@ typedef struct tlbm_desc {
  * f_in must not alias f_out.  force (3 doubles, may be NULL) accumulates
  * 2*sum_{obstacle} sum_q c_q f_q (post-stream, pre-bounce-back; obstacles.py:91,
  * :197, boundaries.py:162) - zero it before the first step you want summed.
- * status (may be NULL) gets bit 0 set if a non-finite density was seen.
+ * status (may be NULL) gets bit 0 set if a non-finite density was seen, and
+ * bit 3 if the row-staged kernel (tlbm_set_row_staging) gave up waiting for
+ * its shared-memory copies (the step is then incomplete).
  * tau_field (may be NULL) gives a per-cell tau for BGK / MRT shear rates.
  * Replaces: cases/base.py:270-289 make_step() closures, triton_fused.py:804
  * TritonFusedSolver3D.step, triton_fused_obstacle.py:1695. */
@@ -327,10 +329,12 @@ typedef struct tlbm_batch_desc {
   int32_t dtype;        /* TLBM_F32 */
   int32_t collision;    /* TLBM_COLL_BGK or TLBM_COLL_MRT */
   int32_t ndomains;
-  int32_t tile_x;       /* multiple of 32, tile_x * tile_y <= 256 */
-  int32_t tile_y;
+  int32_t tile_x;       /* cells: a multiple of 32 * cells_per_thread */
+  int32_t tile_y;       /* rows; (tile_x / cells_per_thread) * tile_y <= 256 threads */
   int32_t ctas_per_sm;  /* persistent mode: CTAs per SM (0 = occupancy limit) */
-  int32_t reserved;
+  int32_t cells_per_thread; /* 0 or 1: one cell per thread; 2: two cells of a
+                             * row per thread (the pair update in domains of
+                             * even nx), same results bit for bit */
   uint32_t* domain_status; /* device, ndomains words, or NULL.  When given, a
                             * domain's non-finite density sets its own word
                             * (bit 0) instead of the status word, and a domain
@@ -439,6 +443,15 @@ TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, doub
 
 TLBM_API const char* tlbm_status_string(int status);
 TLBM_API int tlbm_abi_version(void);
+/* Kernel choice of the fused pull step: with enable != 0 the unforced D3Q19
+ * BGK / MRT and D3Q27 cumulant steps on float32 or shifted half storage run
+ * the row-staged kernel (bulk asynchronous copies of whole x-rows into
+ * shared memory) where the layout allows it (nx a multiple of 64 up to 512,
+ * 16-byte aligned buffers); enable == 0 (the default) keeps them on the
+ * two-cells-per-thread kernel, which measured faster on B200.  Both give the
+ * same results bit for bit.  Returns the previous setting; process-wide.  No
+ * reference counterpart (a tuning switch of this library's kernels). */
+TLBM_API int tlbm_set_row_staging(int32_t enable);
 /* sizeof of the structs a binding mirrors: 0 tlbm_desc, 1 tlbm_batch_domain,
  * 2 tlbm_batch_desc (-1 otherwise), so that a binding can check its layout.
  * No reference counterpart. */

@@ -79,7 +79,8 @@ class BatchDesc(ctypes.Structure):
 
     _fields_ = [("lattice", ctypes.c_int32), ("dtype", ctypes.c_int32), ("collision", ctypes.c_int32),
                 ("ndomains", ctypes.c_int32), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32), ("domain_status", ctypes.c_void_p)]
+                ("ctas_per_sm", ctypes.c_int32), ("cells_per_thread", ctypes.c_int32),
+                ("domain_status", ctypes.c_void_p)]
 
 
 _P = ctypes.c_void_p
@@ -135,6 +136,7 @@ SIGNATURES: dict[str, list] = {
     "tlbm_status_string": [ctypes.c_int],
     "tlbm_abi_version": [],
     "tlbm_struct_size": [_I32],
+    "tlbm_set_row_staging": [_I32],
 }
 _RESTYPES = {"tlbm_link_blocks": _I64, "tlbm_link_list_static_capacity": _I64, "tlbm_status_string": ctypes.c_char_p,
              "tlbm_mlp_param_count": _I32, "tlbm_mlp_blob_bytes": _I32, "tlbm_mlp_grad_blocks": _I64,
@@ -212,3 +214,11 @@ def real_dtype(t: torch.Tensor) -> int:
 
 def exported_symbols() -> list[str]:
     return list(SIGNATURES)
+
+
+def set_row_staging(enable: bool) -> bool:
+    """Choose the kernel of the fused pull step: True runs the row-staged
+    kernel where it is built and the layout allows it, False (the default)
+    the two-cells-per-thread kernel (same results bit for bit).  Returns the
+    previous setting."""
+    return bool(load().tlbm_set_row_staging(1 if enable else 0))

@@ -118,7 +118,7 @@ class BatchedSolver:
 
     def __init__(self, domains: list[DomainSpec], collision: str = "bgk", *, device=None,
                  tile: tuple[int, int] = (64, 4), mode: str = "graph", ctas_per_sm: int = 0,
-                 lattice: str = "D2Q9", order: str = "domain", retire: bool = False):
+                 lattice: str = "D2Q9", order: str = "domain", retire: bool = False, cells_per_thread: int = 1):
         if collision not in ("bgk", "mrt"):
             raise ValueError("the batched runner supports 'bgk' and 'mrt'")
         if mode not in ("graph", "launch", "persistent"):
@@ -170,6 +170,9 @@ class BatchedSolver:
         self._pgraph_capture = True   # persistent launches go through CUDA graphs
         self.ctas_per_sm = ctas_per_sm
         self.order = order
+        if cells_per_thread not in (1, 2):
+            raise ValueError("cells_per_thread must be 1 or 2")
+        self.cells_per_thread = cells_per_thread
         self.set_tile(*tile)
         self.steps_done = 0
         self.step_offsets = [0] * n   # steps each domain had completed before the last load()/resume()
@@ -181,15 +184,21 @@ class BatchedSolver:
 
     ORDERS = ("domain", "interleave", "largest_first")
 
-    def set_tile(self, tx: int, ty: int, order: str | None = None) -> None:
+    def set_tile(self, tx: int, ty: int, order: str | None = None, cells_per_thread: int | None = None) -> None:
         """Tile shape (tx x ty cells over the rows of each domain) and the
         order of the tile list, which is the CTA-to-domain mapping: the launch
         gives CTA b tile b, the persistent kernel gives CTA b tiles b, b + G,
         b + 2G ...  "domain": each domain's tiles together, row by row;
         "interleave": round robin over the domains (one tile of each in turn);
-        "largest_first": the domains by decreasing size, each contiguous."""
-        if tx % 32 or tx * ty > 256 or ty < 1:
-            raise ValueError("tile_x must be a multiple of 32 and tile_x * tile_y <= 256")
+        "largest_first": the domains by decreasing size, each contiguous.
+        cells_per_thread 2 runs a tile on tx / 2 x ty threads, two cells of a
+        row each (the pair update where nx is even)."""
+        cpt = cells_per_thread or getattr(self, "cells_per_thread", 1)
+        if cpt not in (1, 2):
+            raise ValueError("cells_per_thread must be 1 or 2")
+        if tx % (32 * cpt) or (tx // cpt) * ty > 256 or ty < 1:
+            raise ValueError(f"tile_x must be a multiple of {32 * cpt} and (tile_x / {cpt}) * tile_y <= 256")
+        self.cells_per_thread = cpt
         order = order or getattr(self, "order", "domain")
         if order not in self.ORDERS:
             raise ValueError(f"order must be one of {self.ORDERS}")
@@ -204,8 +213,28 @@ class BatchedSolver:
             tiles = [t for i in sorted(range(len(per)), key=lambda i: -self.domains[i].cells) for t in per[i]]
         else:
             tiles = [t for p in per for t in p]
+        self._tiles_all = torch.tensor(tiles, dtype=torch.int32, device=self.device).reshape(-1, 3)
+        self._tiles_live = None       # retired-domain mask the tile list was last compacted for
         self.ntiles = len(tiles)
-        self.tiles_dev = torch.tensor(tiles, dtype=torch.int32, device=self.device).reshape(-1)
+        self.tiles_dev = self._tiles_all.reshape(-1)
+        self._graph = None
+        self._pgraphs = {}
+
+    def _compact_tiles(self) -> None:
+        """With retire=True: drop the tiles of retired domains from the tile
+        list (in the list's order), so that no launch visits them; the list is
+        rebuilt on the device from the full one whenever the set of retired
+        domains changes (one read of the per-domain status words)."""
+        if self.domain_status is None:
+            return
+        live = self.domain_status == 0
+        key = live.cpu()
+        if self._tiles_live is not None and torch.equal(key, self._tiles_live):
+            return
+        tiles = self._tiles_all[live[self._tiles_all[:, 0].long()]]
+        self._tiles_live = key
+        self.ntiles = int(tiles.shape[0])
+        self.tiles_dev = tiles.reshape(-1).contiguous()
         self._graph = None
         self._pgraphs = {}
 
@@ -216,6 +245,7 @@ class BatchedSolver:
         b.ndomains = len(self.domains)
         b.tile_x, b.tile_y = self.tile
         b.ctas_per_sm = self.ctas_per_sm
+        b.cells_per_thread = self.cells_per_thread
         b.domain_status = _lib.ptr(self.domain_status)
         return b
 
@@ -345,6 +375,11 @@ class BatchedSolver:
         hist = None
         if record_every > 0:
             hist = torch.zeros((-(-n // record_every), len(self.domains), 3), dtype=torch.float64, device=self.device)
+        self._compact_tiles()
+        if self.ntiles == 0:   # every domain retired
+            self._cur ^= n & 1
+            self.steps_done += n
+            return hist
         if self.mode == "persistent":
             # one persistent cooperative launch of n steps, captured in a CUDA
             # graph the first time (per n, recording interval and parity) and
@@ -464,33 +499,39 @@ class BatchedSolver:
 
 
 def autotune(solver: BatchedSolver, steps: int = 20,
-             tiles=((32, 8), (64, 4), (128, 2), (256, 1), (32, 4), (64, 2), (128, 1)),
-             modes=("graph", "persistent"), orders=BatchedSolver.ORDERS, ctas_per_sm=(0, 2, 4)) -> dict:
+             tiles=((32, 8), (64, 4), (128, 2), (256, 1), (32, 4), (64, 2), (128, 1), (128, 4), (256, 2), (512, 1)),
+             modes=("graph", "persistent"), orders=BatchedSolver.ORDERS, ctas_per_sm=(0, 2, 4),
+             cells_per_thread=(1, 2)) -> dict:
     """Time every candidate on the solver's own domains and keep the fastest:
-    tile shape x execution mode x CTA-to-domain mapping (the tile order of
-    BatchedSolver.set_tile) and, for the persistent kernel, the CTAs per SM
-    (0 = as many as fit).  Every trial updates every domain (retired ones
-    too).  The state is advanced by the trials; reload it afterwards."""
+    tile shape x cells per thread x execution mode x CTA-to-domain mapping
+    (the tile order of BatchedSolver.set_tile) and, for the persistent
+    kernel, the CTAs per SM (0 = as many as fit).  Shapes a cells-per-thread
+    choice does not admit are skipped.  Every trial updates every domain
+    (retired ones too).  The state is advanced by the trials; reload it
+    afterwards."""
     results = []
     for mode in modes:
-        for tx, ty in tiles:
-            for order in orders:
-                for cps in (ctas_per_sm if mode == "persistent" else (0,)):
-                    solver.mode = mode
-                    solver.ctas_per_sm = cps
-                    solver.set_tile(tx, ty, order)
-                    if solver.domain_status is not None:
-                        solver.domain_status.zero_()     # every trial updates every domain
-                    try:
-                        t = solver.timed_steps(steps)
-                    except (RuntimeError, NotImplementedError):
-                        continue
-                    results.append({"mode": mode, "tile": (tx, ty), "order": order, "ctas_per_sm": cps,
-                                    "seconds": t, "mlups": solver.n_cells * steps / t / 1e6})
+        for cpt in cells_per_thread:
+            for tx, ty in tiles:
+                if tx % (32 * cpt) or (tx // cpt) * ty > 256:
+                    continue
+                for order in orders:
+                    for cps in (ctas_per_sm if mode == "persistent" else (0,)):
+                        solver.mode = mode
+                        solver.ctas_per_sm = cps
+                        solver.set_tile(tx, ty, order, cpt)
+                        if solver.domain_status is not None:
+                            solver.domain_status.zero_()     # every trial updates every domain
+                        try:
+                            t = solver.timed_steps(steps)
+                        except (RuntimeError, NotImplementedError):
+                            continue
+                        results.append({"mode": mode, "tile": (tx, ty), "cells_per_thread": cpt, "order": order,
+                                        "ctas_per_sm": cps, "seconds": t, "mlups": solver.n_cells * steps / t / 1e6})
     best = max(results, key=lambda r: r["mlups"])
     solver.mode = best["mode"]
     solver.ctas_per_sm = best["ctas_per_sm"]
-    solver.set_tile(*best["tile"], best["order"])
+    solver.set_tile(*best["tile"], best["order"], best["cells_per_thread"])
     return {"best": best, "trials": results}
 
 

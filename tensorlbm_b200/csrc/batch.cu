@@ -35,14 +35,21 @@ __device__ __forceinline__ void domain_params(const tlbm_batch_domain& dm, Colli
 // retired: its tiles are skipped, and its state stays as it was when that
 // happened.  Without it every domain is updated and the non-finite bit goes to
 // the one status word.
+//
+// cells_per_thread 2: the tile's tile_x cells of a row run on tile_x / 2
+// threads.  In a domain of even nx a thread takes the pair (x, x + 1) through
+// the pair update of k_step_x2 (the same results bit for bit as one cell per
+// thread); in a domain of odd nx it updates x and x + tile_x / 2 one after
+// the other.  The choice is uniform over the tile.
 template <class L, typename S, int COLL>
 __device__ __forceinline__ void process_tile(const tlbm_batch_domain* __restrict__ doms, const int* __restrict__ tiles,
                                              long long t, const S* fin, S* fout, const uint8_t* flags,
-                                             double* forces, unsigned int* status, unsigned int* dom_status) {
+                                             double* forces, unsigned int* status, unsigned int* dom_status,
+                                             int cells_per_thread) {
   using T = typename Storage<S>::T;
   const int di = tiles[3 * t + 0];
   if (dom_status && *(volatile unsigned int*)(dom_status + di)) return;   // uniform over the tile
-  const int x = tiles[3 * t + 1] + threadIdx.x;
+  const int x0 = tiles[3 * t + 1];
   const int row = tiles[3 * t + 2] + threadIdx.y;   // over the nz * ny rows of the domain
   const tlbm_batch_domain dm = doms[di];
   const int nz = dm.nz > 1 ? dm.nz : 1;
@@ -66,18 +73,32 @@ __device__ __forceinline__ void process_tile(const tlbm_batch_domain* __restrict
   d.plane = (long long)dm.nx * dm.ny;
   d.n = d.plane * nz;
   d.bc = dm.bc;
-  cell_update<L, S, S, COLL, true>(d, x, y, z, x < dm.nx && row < dm.ny * nz, cp, bp);
+  const bool row_ok = row < dm.ny * nz;
+  if (cells_per_thread == 2) {
+    if ((dm.nx & 1) == 0) {
+      const int x = x0 + 2 * int(threadIdx.x);
+      pair_update<L, S, COLL>(d, cp, bp, x, y, z, x < dm.nx && row_ok);
+    } else {
+      const int x = x0 + int(threadIdx.x);
+      cell_update<L, S, S, COLL, true>(d, x, y, z, x < dm.nx && row_ok, cp, bp);
+      const int x2 = x + int(blockDim.x);
+      cell_update<L, S, S, COLL, true>(d, x2, y, z, x2 < dm.nx && row_ok, cp, bp);
+    }
+  } else {
+    const int x = x0 + int(threadIdx.x);
+    cell_update<L, S, S, COLL, true>(d, x, y, z, x < dm.nx && row_ok, cp, bp);
+  }
 }
 
 template <class L, typename S, int COLL>
 __global__ void __launch_bounds__(256) k_batch_step(const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
                                                     const S* fin, S* fout, const uint8_t* flags, double* forces,
                                                     const int* force_slot, int ndomains, unsigned int* status,
-                                                    unsigned int* dom_status) {
+                                                    unsigned int* dom_status, int cells_per_thread) {
   // with a slot counter, the forces of this step go to record *force_slot
   if (forces && force_slot) forces += 3LL * ndomains * (*force_slot);
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x)
-    process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status, dom_status);
+    process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status, dom_status, cells_per_thread);
 }
 
 // Grid barrier over a cooperative launch, bounded: sync[0] counts arrivals,
@@ -118,7 +139,7 @@ __global__ void __launch_bounds__(256) k_batch_run(const tlbm_batch_domain* doms
                                                    S* fa, S* fb, const uint8_t* flags, int nsteps, double* force_hist,
                                                    int ndomains, int record_every, unsigned int* sync,
                                                    unsigned int* status, unsigned long long max_spins,
-                                                   unsigned int* dom_status) {
+                                                   unsigned int* dom_status, int cells_per_thread) {
   for (int s = 0; s < nsteps; ++s) {
     const S* fin = (s & 1) ? fb : fa;
     S* fout = (s & 1) ? fa : fb;
@@ -126,7 +147,7 @@ __global__ void __launch_bounds__(256) k_batch_run(const tlbm_batch_domain* doms
     if (force_hist && record_every > 0 && (s % record_every) == 0)
       forces = force_hist + 3 * (long long)ndomains * (s / record_every);
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x)
-      process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status, dom_status);
+      process_tile<L, S, COLL>(doms, tiles, t, fin, fout, flags, forces, status, dom_status, cells_per_thread);
     if (!grid_barrier(sync, max_spins)) {
       if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x == 0) atomicOr(status, 2u);
       return;
@@ -138,11 +159,12 @@ template <class L, typename S, int COLL>
 int launch_batch(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
                  const void* fin, void* fout, const uint8_t* flags, double* forces, const int* force_slot,
                  unsigned int* status, cudaStream_t s) {
-  const dim3 block(b.tile_x, b.tile_y);
+  const int cpt = b.cells_per_thread == 2 ? 2 : 1;
+  const dim3 block(b.tile_x / cpt, b.tile_y);
   const long long grid = ntiles < 0x7fffffffLL ? ntiles : 0x7fffffffLL;
   k_batch_step<L, S, COLL><<<(unsigned)grid, block, 0, s>>>(doms, tiles, ntiles, (const S*)fin, (S*)fout, flags,
                                                            forces, force_slot, b.ndomains, status,
-                                                           b.domain_status);
+                                                           b.domain_status, cpt);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }
 
@@ -150,7 +172,8 @@ template <class L, typename S, int COLL>
 int launch_batch_run(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, const int* tiles, long long ntiles,
                      void* fa, void* fb, const uint8_t* flags, int nsteps, double* force_hist, int record_every,
                      unsigned int* sync, unsigned int* status, long long max_spins, cudaStream_t s) {
-  const dim3 block(b.tile_x, b.tile_y);
+  const int cpt = b.cells_per_thread == 2 ? 2 : 1;
+  const dim3 block(b.tile_x / cpt, b.tile_y);
   int dev = 0, sms = 0, per_sm = 0, coop = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
@@ -178,7 +201,8 @@ int launch_batch_run(const tlbm_batch_desc& b, const tlbm_batch_domain* doms, co
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (cudaLaunchKernelEx(&cfg, kern, doms, tiles, ntiles, (S*)fa, (S*)fb, flags, nsteps, force_hist, b.ndomains,
-                         record_every, sync, status, (unsigned long long)max_spins, b.domain_status) != cudaSuccess)
+                         record_every, sync, status, (unsigned long long)max_spins, b.domain_status, cpt) !=
+      cudaSuccess)
     return TLBM_ERR_LAUNCH;
   return TLBM_OK;
 }
@@ -190,7 +214,11 @@ int check_batch(const tlbm_batch_desc* b, const tlbm_batch_domain* doms, const i
   if (b->lattice != TLBM_D2Q9 && b->lattice != TLBM_D3Q19) return TLBM_ERR_UNSUPPORTED;
   if (b->dtype != TLBM_F32) return TLBM_ERR_DTYPE;
   if (b->collision != TLBM_COLL_BGK && b->collision != TLBM_COLL_MRT) return TLBM_ERR_UNSUPPORTED;
-  if (b->tile_x < 32 || (b->tile_x % 32) != 0 || b->tile_y < 1 || b->tile_x * b->tile_y > 256) return TLBM_ERR_ARG;
+  if (b->cells_per_thread != 0 && b->cells_per_thread != 1 && b->cells_per_thread != 2) return TLBM_ERR_ARG;
+  // threads of a CTA: tile_x / cells_per_thread (whole warps) x tile_y, at most 256
+  const int cpt = b->cells_per_thread == 2 ? 2 : 1;
+  if (b->tile_x < 32 * cpt || (b->tile_x % (32 * cpt)) != 0 || b->tile_y < 1 || (b->tile_x / cpt) * b->tile_y > 256)
+    return TLBM_ERR_ARG;
   if (ntiles < 0 || b->ndomains < 1) return TLBM_ERR_SHAPE;
   return TLBM_OK;
 }

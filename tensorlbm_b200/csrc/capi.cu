@@ -1,5 +1,6 @@
 // extern "C" entry points (include/tlbm.h): argument checks, then dispatch to
 // the typed kernels.  No entry point allocates or synchronises.
+#include <atomic>
 #include "ops.cuh"
 #include "tlbm_aa.cuh"
 #include "tlbm_dispatch.cuh"
@@ -147,6 +148,14 @@ int check_aa(const tlbm_desc* d) {
 }
 
 }  // namespace
+
+namespace tlbm {
+namespace {
+std::atomic<int> g_row_staging{0};
+}
+int row_staging_enabled() { return g_row_staging.load(std::memory_order_relaxed); }
+int set_row_staging(bool enable) { return g_row_staging.exchange(enable ? 1 : 0); }
+}  // namespace tlbm
 
 extern "C" {
 
@@ -375,6 +384,10 @@ TLBM_API const char* tlbm_status_string(int status) {
 }
 
 TLBM_API int tlbm_abi_version(void) { return TLBM_ABI_VERSION; }
+
+TLBM_API int tlbm_set_row_staging(int32_t enable) {
+  return tlbm::set_row_staging(enable != 0);
+}
 
 TLBM_API int64_t tlbm_struct_size(int32_t which) {
   switch (which) {

@@ -454,31 +454,8 @@ __host__ __device__ constexpr bool uniform_edge_branch() {
 // float64 results are those of k_step bit for bit.
 // Requires nx even, (Q/2 + 2) n < 2^31 (32-bit offsets), and f_in / f_out
 // aligned to two values.
-template <class L, typename S, int COLL, bool FORCED = false>
-__device__ __forceinline__ void step_x2(const StepParams& p, const CollideParams<typename Storage<S>::T>& cp,
-                                        const BcParams<typename Storage<S>::T>& bp) {
-  using T = typename Storage<S>::T;
-  using IO = PairIO<S>;
-  using V = typename IO::V;
-  constexpr int Q = L::Q;
-  constexpr int MID = Q / 2;
-  // shifted float16 storage with BGK: interior warps collide on the stored
-  // deviations (no shift or scale around the loads and stores).  Not bf16: it
-  // saves only an add per value there and took the kernel past 64 registers
-  // (3 instead of 4 blocks per SM, 7 % slower).
-  constexpr bool kDev = std::is_same<S, __half>::value && COLL == TLBM_COLL_BGK && !FORCED &&
-                        uniform_edge_branch<L, COLL>();
-  // both cells' collisions as one stream of packed float32 instructions
-  constexpr bool kPack = TLBM_PACK && std::is_same<T, float>::value && !FORCED &&
-                         (kDev || packed_collision<L, COLL, Storage<S>::kFast>());
-  const int nx = p.nx, ny = p.ny, nz = p.nz;
-  const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = p.z0 + int(blockIdx.z);
-  const bool active = (x < nx) && (y < ny);
-  const int plane = nx * ny;
-  const int N = int(p.n);
-  const int c = z * plane + y * nx + x;
+template <typename S>
+__device__ __forceinline__ Domain<S, S> pair_domain(const StepParams& p) {
   Domain<S, S> d;
   d.fin = static_cast<const S*>(p.f_in);
   d.fout = static_cast<S*>(p.f_out);
@@ -489,12 +466,47 @@ __device__ __forceinline__ void step_x2(const StepParams& p, const CollideParams
   d.wall_u = p.wall_velocity;
   d.link_row = p.link_row;
   d.link_q = p.link_q;
-  d.nx = nx;
-  d.ny = ny;
-  d.nz = nz;
+  d.nx = p.nx;
+  d.ny = p.ny;
+  d.nz = p.nz;
   d.plane = p.plane;
   d.n = p.n;
   d.bc = p.bc;
+  return d;
+}
+
+// Shifted float16 storage with BGK: interior warps collide on the stored
+// deviations (no shift or scale around the loads and stores).  Not bf16: it
+// saves only an add per value there and took the kernel past 64 registers
+// (3 instead of 4 blocks per SM, 7 % slower).
+template <class L, typename S, int COLL, bool FORCED>
+__host__ __device__ constexpr bool pair_deviation_form() {
+  return std::is_same<S, __half>::value && COLL == TLBM_COLL_BGK && !FORCED && uniform_edge_branch<L, COLL>();
+}
+
+template <class L, typename S, int COLL, bool FORCED>
+__device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const CollideParams<typename Storage<S>::T>& cp,
+                                            const BcParams<typename Storage<S>::T>& bp, int x, int y, int c,
+                                            bool active, typename Storage<S>::T (&fa)[L::Q],
+                                            typename Storage<S>::T (&fb)[L::Q], uint32_t fl2);
+
+// The pair update of cells (x, y, z) and (x + 1, y, z) of domain d (x even):
+// the pull (periodic wrap on every axis) and pair_finish.  Every thread of a
+// warp must call it, inactive ones with active = false.
+template <class L, typename S, int COLL, bool FORCED = false>
+__device__ __forceinline__ void pair_update(const Domain<S, S>& d, const CollideParams<typename Storage<S>::T>& cp,
+                                            const BcParams<typename Storage<S>::T>& bp, int x, int y, int z,
+                                            bool active) {
+  using T = typename Storage<S>::T;
+  using IO = PairIO<S>;
+  using V = typename IO::V;
+  constexpr int Q = L::Q;
+  constexpr int MID = Q / 2;
+  constexpr bool kDev = pair_deviation_form<L, S, COLL, FORCED>();
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const int plane = nx * ny;
+  const int N = int(d.n);
+  const int c = z * plane + y * nx + x;
 
   T fa[Q], fb[Q];
   uint32_t fl2 = 0;
@@ -529,13 +541,46 @@ __device__ __forceinline__ void step_x2(const StepParams& p, const CollideParams
     }
     if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));
   }
+  pair_finish<L, S, COLL, FORCED>(d, cp, bp, x, y, c, active, fa, fb, fl2);
+}
+
+template <class L, typename S, int COLL, bool FORCED = false>
+__device__ __forceinline__ void step_x2(const StepParams& p, const CollideParams<typename Storage<S>::T>& cp,
+                                        const BcParams<typename Storage<S>::T>& bp) {
+  const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = p.z0 + int(blockIdx.z);
+  pair_update<L, S, COLL, FORCED>(pair_domain<S>(p), cp, bp, x, y, z, (x < p.nx) && (y < p.ny));
+}
+
+// The pair update after the pull: boundary conditions, drag sample,
+// collisions and the stores of cells c and c + 1 (x even).  fa / fb hold the
+// pulled values (the stored deviations for the deviation-form BGK), fl2 the
+// two flag bytes.  Every thread of a warp must call it (the force reduction
+// and the edge test are warp-wide).
+template <class L, typename S, int COLL, bool FORCED>
+__device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const CollideParams<typename Storage<S>::T>& cp,
+                                            const BcParams<typename Storage<S>::T>& bp, int x, int y, int c,
+                                            bool active, typename Storage<S>::T (&fa)[L::Q],
+                                            typename Storage<S>::T (&fb)[L::Q], uint32_t fl2) {
+  using T = typename Storage<S>::T;
+  using IO = PairIO<S>;
+  using V = typename IO::V;
+  constexpr int Q = L::Q;
+  constexpr int MID = Q / 2;
+  constexpr bool kDev = pair_deviation_form<L, S, COLL, FORCED>();
+  // both cells' collisions as one stream of packed float32 instructions
+  constexpr bool kPack = TLBM_PACK && std::is_same<T, float>::value && !FORCED &&
+                         (kDev || packed_collision<L, COLL, Storage<S>::kFast>());
+  const int nx = d.nx, ny = d.ny;
+  const int N = int(d.n);
   const uint8_t fla = uint8_t(fl2), flb = uint8_t(fl2 >> 8);
   // whether any lane of the warp has a flagged cell or sits on a plane with a
   // condition: warps of the interior then skip all boundary code on a
   // warp-uniform branch
-  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || ((p.bc & TLBM_BC_ZH_INLET) && x == 0) ||
-                                                       ((p.bc & TLBM_BC_ZH_OUTLET) && x + 2 == nx) ||
-                                                       ((p.bc & TLBM_BC_LID) && y == ny - 1)));
+  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || ((d.bc & TLBM_BC_ZH_INLET) && x == 0) ||
+                                                       ((d.bc & TLBM_BC_ZH_OUTLET) && x + 2 == nx) ||
+                                                       ((d.bc & TLBM_BC_LID) && y == ny - 1)));
   if constexpr (kDev) {
     if (edge) {
       // the boundary code and the drag work on the populations themselves
@@ -645,6 +690,12 @@ __global__ void __launch_bounds__(256, MINB) k_step_x2_capped(StepParams p, Coll
   step_x2<L, S, COLL, false>(p, cp, bp);
 }
 
+}  // namespace tlbm
+
+#include "tlbm_rows.cuh"
+
+namespace tlbm {
+
 // Whether the pair kernel can run this step: no Bouzidi link tables, nx even
 // (pairs never straddle a row), offsets of +-(Q/2 + 1) n within 32 bits, and
 // both population buffers (and the flags) aligned to two values.
@@ -680,6 +731,8 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   // per SM) and ran slower than k_step (26.8 against 28.0 GLUPS, forced
   // Smagorinsky at 256^3)
   if constexpr (PULL && !FORCED && std::is_same<SI, SO>::value) {
+    int st = TLBM_OK;
+    if (launch_rows<L, SI, COLL>(p, cp, bp, s, st)) return st;
     if (pair_layout_ok<L, SI>(p)) {
       step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block);
       constexpr int minb = x2_min_blocks<L, SI, COLL>();

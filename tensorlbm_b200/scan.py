@@ -30,7 +30,8 @@ def cavity_initial_f(domain, device=None) -> torch.Tensor:
 
 
 def run_cavity_points(points: list[dict], steps: int, *, collision: str = "mrt", device=None,
-                      mode: str = "graph", tile: tuple[int, int] = (32, 4)) -> list[torch.Tensor]:
+                      mode: str = "graph", tile: tuple[int, int] = (64, 4),
+                      cells_per_thread: int = 2) -> list[torch.Tensor]:
     """Final TensorLBM-phase populations ``(19, nz, ny, nx)`` of every point
     after ``steps`` steps of the cavity case's chain.
 
@@ -43,7 +44,8 @@ def run_cavity_points(points: list[dict], steps: int, *, collision: str = "mrt",
     dev = _ops.cuda_device(device)
     domains = [cavity_point(p["resolution"], float(p.get("re", 400.0)), u_lid=float(p.get("u_lid", 0.06)),
                             span=p.get("span"), device=dev) for p in points]
-    b = BatchedSolver(domains, collision, device=dev, lattice="D3Q19", mode=mode, tile=tile)
+    b = BatchedSolver(domains, collision, device=dev, lattice="D3Q19", mode=mode, tile=tile,
+                      cells_per_thread=cells_per_thread)
     b.load([cavity_initial_f(d, dev) for d in domains])
     if steps:
         b.run(steps)

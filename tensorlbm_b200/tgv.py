@@ -84,29 +84,26 @@ def run(n: int = 384, re: float = 1600.0, u0: float = 0.05, t_end: float = 20.0,
         errs = {}
         secs = 0.0
         done = 0
-        while done < total:
-            step = min(every, total - done)
-            # stop exactly at the next checkpoint
-            nxt = [m for m in marks if m > done]
-            if nxt:
-                step = min(step, min(nxt) - done)
+        # sample every `every` steps, at the checkpoints and at the end
+        stops = sorted(set(range(every, total, every)) | {m for m in marks if m <= total} | {total})
+        for stop in stops:
+            step = stop - done
             secs += _timed(lambda: s.run(step), dev)
-            done += step
-            if done % every == 0 or done in marks or done == total:
-                rho, u = _velocity(s)
-                k = 0.5 * float((rho * (u * u).sum(0)).mean())
-                hist["t"].append(done / tc)
-                hist["kinetic_energy"].append(k)
-                hist["energy"].append(0.5 * float((u * u).sum(0).mean()))
-                hist["mass_drift"].append((float(s.moment_sums()[0]) - m0) / m0)
-                if done in marks:
-                    c = marks[done]
-                    if storage == "f64":
-                        ref_u[c] = u.clone()
-                    elif c in ref_u:
-                        ref = ref_u[c]
-                        errs[str(c)] = float(torch.linalg.vector_norm(u - ref) / torch.linalg.vector_norm(ref))
-                del rho, u
+            done = stop
+            rho, u = _velocity(s)
+            k = 0.5 * float((rho * (u * u).sum(0)).mean())
+            hist["t"].append(done / tc)
+            hist["kinetic_energy"].append(k)
+            hist["energy"].append(0.5 * float((u * u).sum(0).mean()))
+            hist["mass_drift"].append((float(s.moment_sums()[0]) - m0) / m0)
+            if done in marks:
+                c = marks[done]
+                if storage == "f64":
+                    ref_u[c] = u.clone()
+                elif c in ref_u:
+                    ref = ref_u[c]
+                    errs[str(c)] = float(torch.linalg.vector_norm(u - ref) / torch.linalg.vector_norm(ref))
+            del rho, u
         t = hist["t"]
         # -dK/dt per lattice step by central differences (K rho-weighted); the
         # same for E = <|u|^2>/2, TensorLBM's convention

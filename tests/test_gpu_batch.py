@@ -30,14 +30,22 @@ def _alone(dom, f0, steps, dev):
     return s
 
 
-@pytest.mark.parametrize("mode,tile", [("launch", (64, 4)), ("graph", (32, 8)), ("persistent", (128, 2))])
-def test_batched_domains_equal_single_runs(cuda, mode, tile):
+@pytest.mark.parametrize("mode,tile,cpt", [("launch", (64, 4), 1), ("graph", (32, 8), 1), ("persistent", (128, 2), 1),
+                                          ("launch", (128, 2), 2), ("graph", (64, 4), 2), ("persistent", (256, 2), 2)])
+def test_batched_domains_equal_single_runs(cuda, mode, tile, cpt):
+    """cpt = 2: two cells per thread (the pair update; the odd-nx domain takes
+    two single-cell updates), still bit for bit the single runs."""
     from tensorlbm_b200 import batch
 
     doms = _domains(cuda)
+    if cpt == 2:   # one domain of odd nx for the per-cell fallback of the pair tiles
+        odd = batch.cylinder_channel(96, 12.0, 0.05, cuda)
+        odd = batch.DomainSpec(95, odd.ny, odd.tau, odd.u_in, odd.rho_out, odd.wall_mask[:, :95].contiguous(),
+                               odd.obstacle_mask[:, :95].contiguous())
+        doms.append(odd)
     f0 = batch.equilibrium_start(doms, cuda)
     steps = 120
-    b = batch.BatchedSolver(doms, "bgk", device=cuda, tile=tile, mode=mode).load(f0)
+    b = batch.BatchedSolver(doms, "bgk", device=cuda, tile=tile, mode=mode, cells_per_thread=cpt).load(f0)
     rec = 3 if mode == "graph" else 1  # graph mode: an odd record period exercises the slot counter
     hist = b.run(steps, record_every=rec)
     assert int(b.status.item()) == 0
