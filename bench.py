@@ -225,12 +225,12 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 
 
-def _make_solver(torch, dev, lattice, collision, storage, track_force, pattern="ab"):
+def _make_solver(torch, dev, lattice, collision, storage, track_force, pattern="ab", **rates):
     from tensorlbm_b200 import LBMSolver, boundaries3d
 
     obst = boundaries3d.sphere_mask(NX, NY, NZ, CX, CY, CZ, D / 2, dev)
     s = LBMSolver(lattice, (NZ, NY, NX), TAU, collision, device=dev, storage=storage, obstacle_mask=obst,
-                  u_in=U_IN, rho_out=1.0, track_force=track_force, pattern=pattern)
+                  u_in=U_IN, rho_out=1.0, track_force=track_force, pattern=pattern, **rates)
     return s, obst
 
 
@@ -282,8 +282,8 @@ def _time_steps(torch, s, steps, warmup, force_buf):
     return e0.elapsed_time(e1) / 1e3
 
 
-def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_cell, peak, pattern="ab"):
-    s, obst = _make_solver(torch, dev, lattice, collision, storage, False, pattern)
+def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_cell, peak, pattern="ab", **rates):
+    s, obst = _make_solver(torch, dev, lattice, collision, storage, False, pattern, **rates)
     s.load(_initial_state(torch, dev, lattice, obst))
     force = torch.zeros(3, dtype=torch.float64, device=dev)
     t = _time_steps(torch, s, steps, warmup, force)
@@ -297,6 +297,8 @@ def _variant(torch, dev, lattice, collision, storage, steps, warmup, bytes_per_c
            "roofline_frac": round(gbs / peak, 4), "bytes_per_cell": bytes_per_cell, "finite": finite}
     if pattern == "aa":
         out["pattern"] = "aa (one population buffer, in place)"
+    if rates:
+        out["rates"] = rates
     return out
 
 
@@ -743,11 +745,26 @@ def run_ours(args) -> None:
             ("d3q27_cumulant_f16_shifted", "D3Q27", "cumulant", "f16", 2 * 27 * 2, max(args.steps // 2, 3))):
         if want(name):
             variants[name] = _variant(torch, dev, lat, coll, st, steps_v, args.warmup, bpc_v, peak)
+    # the D3Q27 cumulants away from the unit-rate special case: the general
+    # moment transform (non-unit omega_b / omega_odd / omega_even) and Geier's
+    # cumulant (cumulant.py:935, :1050)
+    general = dict(omega_b=1.2, omega_odd=1.5, omega_even=1.5)
+    for name, coll, st, bpc_v, rates in (
+            ("d3q27_cumulant_general_f32", "cumulant", "f32", 2 * 27 * 4, general),
+            ("d3q27_cumulant_general_f16_shifted", "cumulant", "f16", 2 * 27 * 2, general),
+            ("d3q27_cumulant_geier_f32", "cumulant_geier", "f32", 2 * 27 * 4, {})):
+        if want(name):
+            variants[name] = _variant(torch, dev, "D3Q27", coll, st, max(args.steps // 2, 3), args.warmup, bpc_v,
+                                      peak, **rates)
     # half storage against float32 for the same collision (MLUPS ratio)
     for half, full in (("d3q19_bgk_f16_shifted", "d3q19_bgk_f32"), ("d3q19_bgk_bf16_shifted", "d3q19_bgk_f32"),
-                       ("d3q19_mrt_f16_shifted", None), ("d3q27_cumulant_f16_shifted", "d3q27_cumulant_f32")):
+                       ("d3q27_cumulant_f16_shifted", "d3q27_cumulant_f32"),
+                       ("d3q27_cumulant_general_f16_shifted", "d3q27_cumulant_general_f32")):
         if half in variants and full in variants:
             variants[half]["speedup_vs_f32"] = round(variants[half]["mlups"] / variants[full]["mlups"], 3)
+    if "d3q19_mrt_f16_shifted" in variants:   # against the headline (FP32 MRT, same grid, one GPU's share)
+        variants["d3q19_mrt_f16_shifted"]["speedup_vs_f32"] = round(
+            variants["d3q19_mrt_f16_shifted"]["mlups"] / (value / world), 3)
     for name, lat, coll, st, bpc_v in (("d3q19_mrt_f32_aa", "D3Q19", "mrt", "f32", bpc),
                                        ("d3q19_bgk_f16_shifted_aa", "D3Q19", "bgk", "f16", 2 * 19 * 2)):
         if want(name):

@@ -48,8 +48,8 @@ __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
 
 // 1 / x for the fused-arithmetic collisions (no reference rounding order to
-// keep): the hardware reciprocal approximation (pk::rcp_approx) instead of the
-// instruction sequence of an IEEE division.  float64 keeps the division.
+// keep): pk::rcp_approx (the IEEE division unless TLBM_FAST_RCP); float64
+// keeps the division.
 __device__ __forceinline__ float rcp_fast(float x) { return pk::rcp_approx(x); }
 __device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
 
