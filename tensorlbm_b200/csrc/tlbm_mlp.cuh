@@ -52,7 +52,8 @@ constexpr int SM_SLOT = SM_BAR + 16;             // TMEM base address
 constexpr int SM_FLAG = SM_SLOT + 4;             // one timeout flag per half
 constexpr int SM_BYTES = SM_FLAG + 8 + 1024;     // with alignment slack
 constexpr uint32_t TMEM_COLS = 128;              // 64 accumulator columns per half
-constexpr uint32_t MAX_WAIT = 1u << 20;          // mbarrier polls before giving up
+constexpr uint32_t MAX_WAIT = 1u << 16;          // mbarrier waits before giving up
+constexpr uint32_t WAIT_HINT_NS = 20000;         // each may suspend the polling warp up to 20 us
 
 // ---- features --------------------------------------------------------------
 // Nine rotation- and Galilean-invariant inputs from the non-equilibrium
@@ -185,7 +186,7 @@ struct Engine {
         umma::commit(mbar);
       }
       __syncwarp();
-      const bool done = umma::mbar_wait(mbar, phase, MAX_WAIT);
+      const bool done = umma::mbar_wait_sleep(mbar, phase, MAX_WAIT, WAIT_HINT_NS);
       if (lt == 0 && !done) *flag = 1;
     }
     phase ^= 1u;
@@ -212,10 +213,15 @@ struct Engine {
         const float4 b0 = *reinterpret_cast<const float4*>(hb + 32 * part + 8 * c);
         const float4 b1 = *reinterpret_cast<const float4*>(hb + 32 * part + 8 * c + 4);
         const float* u = v + 8 * c;
-        put_chunk(4 * part + c, silu_half_bf16x2(pack_bf16x2(fmaf(u[0], 0.5f, b0.x), fmaf(u[1], 0.5f, b0.y))),
-                  silu_half_bf16x2(pack_bf16x2(fmaf(u[2], 0.5f, b0.z), fmaf(u[3], 0.5f, b0.w))),
-                  silu_half_bf16x2(pack_bf16x2(fmaf(u[4], 0.5f, b1.x), fmaf(u[5], 0.5f, b1.y))),
-                  silu_half_bf16x2(pack_bf16x2(fmaf(u[6], 0.5f, b1.z), fmaf(u[7], 0.5f, b1.w))));
+        // 0.5 acc + b/2 for two columns per packed fma.rn.f32x2 (each lane
+        // rounded as fmaf would)
+        const float2 half = make_float2(0.5f, 0.5f);
+        const float2 h0 = __ffma2_rn(make_float2(u[0], u[1]), half, make_float2(b0.x, b0.y));
+        const float2 h1 = __ffma2_rn(make_float2(u[2], u[3]), half, make_float2(b0.z, b0.w));
+        const float2 h2 = __ffma2_rn(make_float2(u[4], u[5]), half, make_float2(b1.x, b1.y));
+        const float2 h3 = __ffma2_rn(make_float2(u[6], u[7]), half, make_float2(b1.z, b1.w));
+        put_chunk(4 * part + c, silu_half_bf16x2(pack_bf16x2(h0.x, h0.y)), silu_half_bf16x2(pack_bf16x2(h1.x, h1.y)),
+                  silu_half_bf16x2(pack_bf16x2(h2.x, h2.y)), silu_half_bf16x2(pack_bf16x2(h3.x, h3.y)));
       }
     }
   }

@@ -119,5 +119,27 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32
   return false;
 }
 
+// try_wait that may suspend the thread for up to hint_ns nanoseconds (it
+// resumes when the phase completes): a waiting warp then sleeps through a
+// tensor-core round trip instead of spinning on the barrier
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t mbar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait of at most about max_tries * hint_ns nanoseconds
+__device__ __forceinline__ bool mbar_wait_sleep(uint32_t mbar, uint32_t parity, uint32_t max_tries, uint32_t hint_ns) {
+  for (uint32_t i = 0; i < max_tries; ++i)
+    if (mbar_try_wait_sleep(mbar, parity, hint_ns)) return true;
+  return false;
+}
+
 }  // namespace umma
 }  // namespace tlbm
