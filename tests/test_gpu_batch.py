@@ -182,5 +182,12 @@ def test_retire_skips_diverged_domains(cuda, mode):
     ref.run(128)
     for k in range(2):
         assert torch.equal(b.f(4 + k), ref.f(k))
+    # the next run() drops the retired domains' tiles from the tile list
+    n_all = b.ntiles
+    b.run(64)
+    ref.run(64)
+    assert b.ntiles == ref.ntiles < n_all
+    for k in range(2):
+        assert torch.equal(b.f(4 + k), ref.f(k))
     torch.cuda.synchronize(cuda)
     assert int(b.status.item()) == 0          # the non-finite bits went to the domains' own words
