@@ -437,6 +437,27 @@ def tgv_laminar(src: str) -> None:
     print(f"wrote tgv_laminar.npz ({len(res['cases'])} grids)")
 
 
+def cavity3d_full(src: str) -> None:
+    """TensorLBM's verified 3-D lid-driven cavity at Re 1000
+    (benchmarks/verified/cavity_3d_full: run.py and the case_643.json /
+    case_963.json it wrote, D3Q19 TRT, five half-way walls, Zou/He lid,
+    100 000 steps): the centre-plane centre lines, u_min and the mass drift of
+    each grid, copied from the reference's own outputs."""
+    import json
+
+    bench = pathlib.Path(src).parent / "benchmarks" / "verified" / "cavity_3d_full"
+    out = {}
+    for tag in ("643", "963"):
+        case = json.loads((bench / f"case_{tag}.json").read_text())
+        n = int(case["nx"])
+        for key in ("u_centerline_mid", "v_centerline_mid"):
+            out[f"n{n}_{key}"] = np.asarray(case[key], dtype=np.float64)
+        for key in ("re", "u_lid", "tau", "n_steps_run", "u_min_3d_mid", "mass_drift", "last_resid"):
+            out[f"n{n}_{key}"] = np.asarray(case[key])
+    np.savez_compressed(HERE / "cavity3d_full.npz", **out)
+    print(f"wrote cavity3d_full.npz ({sorted(out)})")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -445,6 +466,9 @@ def main() -> None:
     args = ap.parse_args()
     if args.only == "tgv_laminar":
         tgv_laminar(args.reference)
+        return
+    if args.only == "cavity3d_full":
+        cavity3d_full(args.reference)
         return
     import_reference(args.reference)
     import torch
