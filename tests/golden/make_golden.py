@@ -458,6 +458,25 @@ def cavity3d_full(src: str) -> None:
     print(f"wrote cavity3d_full.npz ({sorted(out)})")
 
 
+def cavity2d_re100(src: str) -> None:
+    """TensorLBM's verified 2-D lid-driven cavity at Re 100
+    (benchmarks/verified/cavity/re100: run.py and the result.json it wrote,
+    D2Q9 MRT, three half-way walls, Zou/He lid, 128^2 and 192^2, 100 000
+    steps): the point values u(0.5, 0.5), u(0.5, 0.0625), v(0.5, 0.5) of each
+    grid, copied from the reference's own outputs."""
+    import json
+
+    res = json.loads((pathlib.Path(src).parent / "benchmarks" / "verified" / "cavity" / "re100" /
+                      "result.json").read_text())
+    out = {}
+    for key, case in res["grids"].items():
+        n = int(case["nx"])
+        for k in ("re", "u_lid", "tau", "steps", "u_mid", "u_bot", "v_mid", "last_resid"):
+            out[f"n{n}_{k}"] = np.asarray(case[k])
+    np.savez_compressed(HERE / "cavity2d_re100.npz", **out)
+    print(f"wrote cavity2d_re100.npz ({sorted(out)})")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -469,6 +488,9 @@ def main() -> None:
         return
     if args.only == "cavity3d_full":
         cavity3d_full(args.reference)
+        return
+    if args.only == "cavity2d_re100":
+        cavity2d_re100(args.reference)
         return
     import_reference(args.reference)
     import torch
