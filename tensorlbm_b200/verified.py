@@ -1,0 +1,93 @@
+"""TensorLBM's verified benchmarks (benchmarks/verified/*) run on the fused kernel.
+
+Each runner builds the benchmark's case as its run.py does, advances it with
+:class:`tensorlbm_b200.LBMSolver` (one fused kernel per step) and returns the
+quantities the benchmark records, so that they can be compared with the
+values in the reference's own result files:
+
+* :func:`pipe_3d` — Hagen-Poiseuille pipe (poiseuille_3d_pipe/run.py);
+* :func:`tensorlbm_b200.lid_driven_cavity.cavity_3d_full` — 3-D cavity, Re 1000;
+* :func:`tensorlbm_b200.lid_driven_cavity.cavity_2d` — 2-D cavity, Re 100;
+* :func:`tensorlbm_b200.tgv.laminar_decay` — laminar 3-D Taylor-Green decay.
+"""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import torch
+
+from . import _ops
+from .lid_driven_cavity import cavity_2d, cavity_3d_full
+from .tgv import laminar_decay
+
+
+def pipe_3d(R: int, tau: float = 0.8, u_in: float = 0.02, steps: int = 20_000, average: int = 400,
+            L_over_R: int = 6, device=None) -> dict:
+    """TensorLBM's verified Hagen-Poiseuille pipe in velocity mode
+    (benchmarks/verified/poiseuille_3d_pipe/run.py:76-101, :187-300).
+
+    Domain (nz, ny, nx) = (2R + 3, 2R + 3, L_over_R R), axis at y = z = R + 1;
+    cells farther than R from the axis (float32 distances) are solid and take
+    the full-way swap after streaming; D3Q19 BGK, Zou/He velocity inlet u_in
+    at x = 0 and pressure outlet rho = 1 at x = nx - 1 (the chain collide ->
+    stream -> inlet -> outlet -> bounce-back); start: the equilibrium of the
+    parabola 2 u_in (1 - d^2 / (R + 1/2)^2) in the fluid.  After `steps` steps,
+    `average` more steps average u_x on the mid plane x = nx // 2 and rho on the
+    inlet plane.  Returns the radial profile (means over the bins
+    k <= d < k + 1 of the fluid cells), the centre velocity (mean over d < 1/2),
+    the flow rate (sum over the fluid cells), the mean inlet density over the
+    fluid cells and the mass drift of sum(f) in percent."""
+    from .d3q19 import equilibrium3d, macroscopic3d
+    from .solvers import LBMSolver
+
+    dev = _ops.cuda_device(device)
+    ny = nz = 2 * R + 3
+    nx = L_over_R * R
+    yc = zc = R + 1
+    iz = torch.arange(nz, device=dev, dtype=torch.float32).view(-1, 1)
+    iy = torch.arange(ny, device=dev, dtype=torch.float32).view(1, -1)
+    d = torch.sqrt((iy - yc) ** 2 + (iz - zc) ** 2)
+    fluid2d = d <= R
+    wall = (~fluid2d).unsqueeze(-1).expand(nz, ny, nx).contiguous()
+    r_eff = R + 0.5
+    d3 = d.unsqueeze(-1)
+    ux0 = torch.where(fluid2d.unsqueeze(-1), 2.0 * u_in * (1.0 - d3 ** 2 / r_eff ** 2), torch.zeros_like(d3))
+    ux0 = ux0.expand(nz, ny, nx).contiguous()
+    rho0 = torch.ones((nz, ny, nx), dtype=torch.float32, device=dev)
+    zero = torch.zeros_like(rho0)
+    f0 = equilibrium3d(rho0, ux0, zero, zero)
+    mass0 = float(f0.sum())
+    s = LBMSolver("D3Q19", (nz, ny, nx), tau, "bgk", device=dev, wall_mask=wall, u_in=u_in, rho_out=1.0)
+    s.load(f0)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    s.run(steps)
+    torch.cuda.synchronize(dev)
+    secs = time.perf_counter() - t0
+    x_meas = nx // 2
+    acc_u = torch.zeros((nz, ny), dtype=torch.float32, device=dev)
+    acc_rho = torch.zeros((nz, ny), dtype=torch.float32, device=dev)
+    for _ in range(average):
+        s.step(1)
+        rho, ux, _, _ = macroscopic3d(s.f)
+        acc_u += ux[:, :, x_meas]
+        acc_rho += rho[:, :, 0]
+    acc_u /= float(average)
+    acc_rho /= float(average)
+    f = s.f
+    mass_drift_pct = (float(f.sum()) - mass0) / mass0 * 100.0
+    d_np = d.cpu().numpy()
+    u_np = acc_u.cpu().numpy().astype(np.float64)
+    fluid = d_np <= R
+    bins = np.floor(d_np).astype(int)
+    profile = [float(u_np[fluid & (bins == k)].mean()) for k in range(R + 1) if (fluid & (bins == k)).any()]
+    centre = fluid & (d_np < 0.5)
+    return {"R": R, "nx": nx, "ny": ny, "nz": nz, "tau": tau, "u_in": u_in, "steps": steps, "average": average,
+            "u_profile": profile, "u_center": float(u_np[centre].mean()), "Q": float(u_np[fluid].sum()),
+            "rho_in_measured": float(acc_rho[fluid2d].mean()), "mass_drift_pct": mass_drift_pct,
+            "finite": not s.nonfinite_seen(), "seconds": secs, "mlups": nx * ny * nz * steps / secs / 1e6}
+
+
+__all__ = ["pipe_3d", "cavity_3d_full", "cavity_2d", "laminar_decay"]

@@ -477,6 +477,26 @@ def cavity2d_re100(src: str) -> None:
     print(f"wrote cavity2d_re100.npz ({sorted(out)})")
 
 
+def pipe3d(src: str) -> None:
+    """TensorLBM's verified Hagen-Poiseuille pipe (benchmarks/verified/
+    poiseuille_3d_pipe: run.py and the case_R20.json / case_R40.json it wrote,
+    D3Q19 BGK, Zou/He velocity inlet and pressure outlet, full-way swap at the
+    staircase pipe wall): the radial profile, centre velocity, flow rate,
+    inlet density and mass drift of each radius, copied from the reference's
+    own outputs."""
+    import json
+
+    bench = pathlib.Path(src).parent / "benchmarks" / "verified" / "poiseuille_3d_pipe"
+    out = {}
+    for r in (20, 40):
+        case = json.loads((bench / f"case_R{r}.json").read_text())
+        out[f"r{r}_u_profile"] = np.asarray(case["u_profile"], dtype=np.float64)
+        for k in ("tau", "u_in", "n_steps", "u_center", "Q", "rho_in_measured", "mass_drift_pct", "L_over_R"):
+            out[f"r{r}_{k}"] = np.asarray(case[k])
+    np.savez_compressed(HERE / "pipe3d.npz", **out)
+    print(f"wrote pipe3d.npz ({sorted(out)})")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -491,6 +511,9 @@ def main() -> None:
         return
     if args.only == "cavity2d_re100":
         cavity2d_re100(args.reference)
+        return
+    if args.only == "pipe3d":
+        pipe3d(args.reference)
         return
     import_reference(args.reference)
     import torch

@@ -1,7 +1,8 @@
-"""TensorLBM's verified 3-D lid-driven cavity (Re 1000, D3Q19 TRT, five
-half-way walls, Zou/He lid, 100 000 steps) on the fused kernel, against the
-centre-line profiles, u_min and mass drift that the reference benchmark
-recorded (golden cavity3d_full, from benchmarks/verified/cavity_3d_full)."""
+"""TensorLBM's verified benchmarks (benchmarks/verified/*) run on the fused
+kernel, against the values each benchmark recorded in the reference's own
+result files: the 3-D lid-driven cavity at Re 1000 (golden cavity3d_full),
+the 2-D cavity at Re 100 (cavity2d_re100) and the Hagen-Poiseuille pipe
+(pipe3d)."""
 
 from __future__ import annotations
 
@@ -13,6 +14,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("n", [64, 96])
 def test_cavity_3d_full_matches_reference_benchmark(cuda, n):
+    """D3Q19 TRT, five half-way walls, Zou/He lid, 100 000 steps: the
+    centre-plane centre lines, u_min and the mass drift."""
     from tensorlbm_b200.lid_driven_cavity import cavity_3d_full
 
     from tests.conftest import golden
@@ -49,3 +52,28 @@ def test_cavity_2d_re100_matches_reference_benchmark(cuda, n):
     assert r["tau"] == pytest.approx(float(g[f"n{n}_tau"]), abs=1e-12)
     for key in ("u_mid", "u_bot", "v_mid"):
         assert r[key] == pytest.approx(float(g[f"n{n}_{key}"]), abs=2e-4), key
+
+
+@pytest.mark.parametrize("r", [20, 40])
+def test_pipe_3d_matches_reference_benchmark(cuda, r):
+    """TensorLBM's verified Hagen-Poiseuille pipe (D3Q19 BGK, Zou/He velocity
+    inlet and pressure outlet, full-way swap at the staircase wall, 20 000 /
+    23 600 steps plus a 400-step average) against the profile, centre velocity,
+    flow rate, inlet density and mass drift the reference benchmark recorded
+    (golden pipe3d).  Measured: profile within 1.8e-5 relative, inlet density
+    within 4e-7."""
+    from tensorlbm_b200.verified import pipe_3d
+
+    from tests.conftest import golden
+
+    g = golden("pipe3d")
+    res = pipe_3d(r, tau=float(g[f"r{r}_tau"]), u_in=float(g[f"r{r}_u_in"]), steps=int(g[f"r{r}_n_steps"]),
+                  L_over_R=int(g[f"r{r}_L_over_R"]), device=cuda)
+    assert res["finite"]
+    prof, ref = np.asarray(res["u_profile"]), g[f"r{r}_u_profile"]
+    assert prof.shape == ref.shape
+    assert np.max(np.abs(prof - ref) / np.abs(ref)) <= 1e-4
+    assert res["u_center"] == pytest.approx(float(g[f"r{r}_u_center"]), rel=1e-4)
+    assert res["Q"] == pytest.approx(float(g[f"r{r}_Q"]), rel=1e-4)
+    assert res["rho_in_measured"] == pytest.approx(float(g[f"r{r}_rho_in_measured"]), abs=1e-5)
+    assert res["mass_drift_pct"] == pytest.approx(float(g[f"r{r}_mass_drift_pct"]), rel=2e-2)
