@@ -6,6 +6,7 @@ quantities the benchmark records, so that they can be compared with the
 values in the reference's own result files:
 
 * :func:`pipe_3d` — Hagen-Poiseuille pipe (poiseuille_3d_pipe/run.py);
+* :func:`shear_wave` — decaying 2-D shear wave (shear_wave_decay/run.py);
 * :func:`tensorlbm_b200.lid_driven_cavity.cavity_3d_full` — 3-D cavity, Re 1000;
 * :func:`tensorlbm_b200.lid_driven_cavity.cavity_2d` — 2-D cavity, Re 100;
 * :func:`tensorlbm_b200.tgv.laminar_decay` — laminar 3-D Taylor-Green decay.
@@ -90,4 +91,46 @@ def pipe_3d(R: int, tau: float = 0.8, u_in: float = 0.02, steps: int = 20_000, a
             "finite": not s.nonfinite_seen(), "seconds": secs, "mlups": nx * ny * nz * steps / secs / 1e6}
 
 
-__all__ = ["pipe_3d", "cavity_3d_full", "cavity_2d", "laminar_decay"]
+def shear_wave(n: int, tau: float = 0.8, u0: float = 0.05, steps: int = 3200, record_every: int = 100,
+               device=None) -> dict:
+    """TensorLBM's verified decaying shear wave (benchmarks/verified/shear_wave_decay/run.py:46-140)
+    on the fused kernel.
+
+    Periodic n x n, D2Q9 BGK in float32, f <- collide(stream(f)); start: the
+    equilibrium of u_x = u0 sin(2 pi y / n), rho = 1.  Every record_every
+    steps E = <|u|^2> / 2 and the largest |u|; the decay rates are minus the
+    slopes of least-squares lines through ln E and ln max|u|, against
+    2 nu k^2 and nu k^2 with k = 2 pi / n."""
+    from .d2q9 import equilibrium, macroscopic
+    from .solvers import LBMSolver
+
+    dev = _ops.cuda_device(device)
+    k = 2.0 * np.pi / float(n)
+    # the initial field as the benchmark builds it (float32 on the CPU)
+    ax = torch.arange(n, dtype=torch.float32)
+    y, _ = torch.meshgrid(ax, ax, indexing="ij")
+    ux0 = (u0 * torch.sin(k * y)).to(dev)
+    zero = torch.zeros_like(ux0)
+    f0 = equilibrium(torch.ones_like(ux0), ux0, zero)
+    s = LBMSolver("D2Q9", (n, n), tau, "bgk", device=dev)
+    # stored state P_0 = f_0, then P_j = collide(stream(P_j-1)) is the
+    # benchmark's f_j (load() would store collide(f_0))
+    s.resume(f0, stored_state=f0)
+    times, energies, umaxs = [], [], []
+    for step in range(record_every, steps + 1, record_every):
+        s.run(record_every, chunk=record_every)
+        _, ux, uy = macroscopic(s.state)
+        energies.append(float((0.5 * (ux * ux + uy * uy)).mean()))
+        umaxs.append(float((ux * ux + uy * uy).sqrt().max()))
+        times.append(step)
+    t = np.asarray(times, dtype=np.float64)
+    nu = (tau - 0.5) / 3.0
+    return {"n": n, "tau": tau, "u0": u0, "steps": steps, "record_every": record_every, "times": times,
+            "energies": energies, "umaxs": umaxs,
+            "gamma_e_sim": float(-np.polyfit(t, np.log(np.asarray(energies)), 1)[0]),
+            "gamma_vel_sim": float(-np.polyfit(t, np.log(np.asarray(umaxs)), 1)[0]),
+            "gamma_e_theory": 2.0 * nu * k * k, "gamma_vel_theory": nu * k * k,
+            "finite": not s.nonfinite_seen()}
+
+
+__all__ = ["pipe_3d", "shear_wave", "cavity_3d_full", "cavity_2d", "laminar_decay"]

@@ -497,6 +497,50 @@ def pipe3d(src: str) -> None:
     print(f"wrote pipe3d.npz ({sorted(out)})")
 
 
+def shear_wave(src: str, torch) -> None:
+    """TensorLBM's verified decaying shear wave (benchmarks/verified/
+    shear_wave_decay, D2Q9 BGK float32, tau 0.8, H = 64 and 128).  Two sets per
+    grid: the case's parameters with the energies, largest |u| and decay rates
+    the benchmark recorded (case_H*.json, energy_history_H*.csv; its step ran
+    through torch.compile), and the same run of TensorLBM's eager operators
+    here (collide_bgk(stream(f)), the benchmark's initial field and sampling,
+    run.py:59-100), whose arithmetic the fused kernel reproduces."""
+    import json
+    import math
+
+    from tensorlbm.d2q9 import equilibrium, macroscopic
+    from tensorlbm.solver import collide_bgk, stream
+
+    bench = pathlib.Path(src).parent / "benchmarks" / "verified" / "shear_wave_decay"
+    out = {}
+    for h in (64, 128):
+        case = json.loads((bench / f"case_H{h}.json").read_text())
+        rows = np.loadtxt(bench / f"energy_history_H{h}.csv", delimiter=",", skiprows=1)
+        out[f"h{h}_record_steps"] = rows[:, 0].astype(np.int64)
+        out[f"h{h}_energy_compiled"] = rows[:, 1]
+        out[f"h{h}_umax_compiled"] = rows[:, 2]
+        for k in ("tau", "u0", "steps", "record_every", "gamma_e_sim", "gamma_vel_sim"):
+            out[f"h{h}_{k}"] = np.asarray(case[k])
+        tau, u0, steps, every = float(case["tau"]), float(case["u0"]), int(case["steps"]), int(case["record_every"])
+        k = 2.0 * math.pi / float(h)
+        y, _ = torch.meshgrid(torch.arange(h, dtype=torch.float32), torch.arange(h, dtype=torch.float32), indexing="ij")
+        ux0 = u0 * torch.sin(k * y)
+        f = equilibrium(torch.ones_like(ux0), ux0, torch.zeros_like(ux0))
+        energies, umaxs = [], []
+        for step in range(1, steps + 1):
+            f = collide_bgk(stream(f), tau)
+            if step % every == 0:
+                _, uxm, uym = macroscopic(f)
+                energies.append(float((0.5 * (uxm * uxm + uym * uym)).mean().item()))
+                umaxs.append(float((uxm * uxm + uym * uym).sqrt().max().item()))
+        out[f"h{h}_energy"] = np.asarray(energies)
+        out[f"h{h}_umax"] = np.asarray(umaxs)
+        print(f"  shear wave H{h}: eager vs compiled energy max rel "
+              f"{np.max(np.abs(out[f'h{h}_energy'] - rows[:, 1]) / rows[:, 1]):.2e}")
+    np.savez_compressed(HERE / "shear_wave.npz", **out)
+    print(f"wrote shear_wave.npz ({sorted(out)})")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
@@ -514,6 +558,13 @@ def main() -> None:
         return
     if args.only == "pipe3d":
         pipe3d(args.reference)
+        return
+    if args.only == "shear_wave":
+        import_reference(args.reference)
+        import torch
+
+        torch.set_num_threads(8)
+        shear_wave(args.reference, torch)
         return
     import_reference(args.reference)
     import torch

@@ -77,3 +77,26 @@ def test_pipe_3d_matches_reference_benchmark(cuda, r):
     assert res["Q"] == pytest.approx(float(g[f"r{r}_Q"]), rel=1e-4)
     assert res["rho_in_measured"] == pytest.approx(float(g[f"r{r}_rho_in_measured"]), abs=1e-5)
     assert res["mass_drift_pct"] == pytest.approx(float(g[f"r{r}_mass_drift_pct"]), rel=2e-2)
+
+
+@pytest.mark.parametrize("h", [64, 128])
+def test_shear_wave_matches_reference_benchmark(cuda, h):
+    """TensorLBM's verified decaying shear wave (D2Q9 BGK float32, periodic,
+    tau 0.8) against TensorLBM's own eager run of the benchmark (golden
+    shear_wave; it reproduces the histories the benchmark recorded exactly):
+    the energy and max|u| histories to the order of the GPU's mean/max
+    reductions, and the fitted decay rates."""
+    from tensorlbm_b200.verified import shear_wave
+
+    from tests.conftest import golden
+
+    g = golden("shear_wave")
+    r = shear_wave(h, tau=float(g[f"h{h}_tau"]), u0=float(g[f"h{h}_u0"]), steps=int(g[f"h{h}_steps"]),
+                   record_every=int(g[f"h{h}_record_every"]), device=cuda)
+    assert r["finite"]
+    assert np.array_equal(np.asarray(r["times"]), g[f"h{h}_record_steps"])
+    np.testing.assert_array_equal(g[f"h{h}_energy"], g[f"h{h}_energy_compiled"])
+    np.testing.assert_allclose(r["energies"], g[f"h{h}_energy"], rtol=1e-6)
+    np.testing.assert_allclose(r["umaxs"], g[f"h{h}_umax"], rtol=1e-6)
+    assert r["gamma_e_sim"] == pytest.approx(float(g[f"h{h}_gamma_e_sim"]), rel=1e-6)
+    assert r["gamma_vel_sim"] == pytest.approx(float(g[f"h{h}_gamma_vel_sim"]), rel=1e-6)
