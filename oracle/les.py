@@ -8,7 +8,7 @@ The closure is new (TensorLBM's closure is 2-D: ai/model.py:40-92 maps three
 strain components through a 2x16 tanh MLP to nu_t, ai/inference.py:68-92
 applies tau + 3 nu_t).  What it shares with the reference and is restated here:
 
-* Smagorinsky tau_eff (turbulence.py:183-208, the fallback and judge) through
+* Smagorinsky tau_eff (turbulence.py:183-208, the fallback and the comparison) through
   oracle.lbm.smagorinsky_tau, i.e. nu_t = C_s^2 |S|_F in lattice units;
 * block-mean coarsening (ai/pipeline.py:93 _coarsen_mean, here in 3-D);
 * the energy spectrum of benchmarks/pending/dit_turbulence/run.py:158-177

@@ -11,7 +11,7 @@ Blanquart 2013).  A grid filtered by a factor r uses dx_r = dt_r = r (acoustic
 scaling): nu_r = nu / r, epsilon_r = epsilon r, and one filtered step covers r
 DNS steps.  ``HITConfig.les`` lists the LES grids: every grid but the last
 runs the learned closure (its nu_t scale calibrated on that grid), Smagorinsky
-and no model; the last runs Smagorinsky, the fine-grid judge (a single grid
+and no model; the last runs Smagorinsky, the fine-grid reference (a single grid
 runs all three).
 
 The a-posteriori error of an LES is mean |ln(E_LES(k) / E_fDNS(k))| over the

@@ -1,7 +1,7 @@
 """End to end at small scale: forced DNS 128^3 -> block-filtered (factor 4)
 training data -> the library's training kernels -> LES 32^3 with the fused
 learned-closure step.  Shows what the trained network gains over the method
-without it (Smagorinsky, the fallback and judge) on the filtered DNS, a-priori
+without it (Smagorinsky, the fallback and the comparison) on the filtered DNS, a-priori
 and a-posteriori."""
 
 from __future__ import annotations
