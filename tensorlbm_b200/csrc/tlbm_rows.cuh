@@ -242,22 +242,30 @@ bool launch_rows(const StepParams& p, const CollideParams<typename Storage<S>::T
     if (smem > 227 * 1024) return false;
     constexpr int minb = rows::min_blocks<L, S, COLL>();
     auto kern = k_step_rows<L, S, COLL, minb>;
-    static int sms = -1;
-    static int per_sm_nx[rows::kMaxNx / 64 + 1] = {};
-    if (sms < 0) {
-      int dev = 0;
-      if (cudaGetDevice(&dev) != cudaSuccess ||
-          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+    // per device: SM count and resident CTAs for each row length (the
+    // function attributes are set on each device before its first launch)
+    constexpr int kDevices = 64;
+    static int sms_of[kDevices] = {};
+    static int per_sm_of[kDevices][rows::kMaxNx / 64 + 1] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) {
+      cudaGetLastError();
+      return false;
+    }
+    int& sms = sms_of[dev];
+    if (sms <= 0) {
+      int n = 0;
+      if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kMaxSmem < 227 * 1024 ? kMaxSmem : 227 * 1024)) != cudaSuccess ||
           cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                cudaSharedmemCarveoutMaxShared) != cudaSuccess) {
-        sms = -1;
         cudaGetLastError();
         return false;
       }
+      sms = n;
     }
-    int& per_sm = per_sm_nx[p.nx / 64];
+    int& per_sm = per_sm_of[dev][p.nx / 64];
     if (per_sm == 0) {
       int nb = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, p.nx / 2, size_t(smem)) != cudaSuccess || nb < 1) {
