@@ -64,8 +64,10 @@ typedef enum tlbm_collision {
   TLBM_COLL_CUMULANT_D3Q19 = 5,   /* cumulant.py:1159 (Smagorinsky via c_smag) */
   TLBM_COLL_SMAGORINSKY = 6,      /* turbulence.py:245 (D3Q19), :216 (D2Q9), :472 (D3Q27) */
   TLBM_COLL_TRT = 7,              /* solver.py:440, solver3d.py:303, d3q27.py:438 (tau = tau_plus > 1/2) */
-  TLBM_COLL_CASCADED = 8          /* cascaded_collision.py:445 (D3Q19), :512 (D3Q27); rates: omega_b = s_bulk,
+  TLBM_COLL_CASCADED = 8,         /* cascaded_collision.py:445 (D3Q19), :512 (D3Q27); rates: omega_b = s_bulk,
                                      omega_odd = s_3, omega_even = s_4, cm_s5 / cm_s6 (D3Q27) */
+  TLBM_COLL_RLBM = 9              /* regularised BGK: solver.py:338 (D2Q9), solver3d.py:342 (D3Q19),
+                                     d3q27.py:481 (D3Q27); a tau field is ignored */
 } tlbm_collision;
 
 /* Boundary conditions applied by tlbm_step after the pull, in this order:

@@ -336,6 +336,36 @@ def collide_smagorinsky(f: np.ndarray, tau: float, c_s: float = 0.1) -> np.ndarr
     return f - fneq / te[None]
 
 
+def collide_rlbm(f: np.ndarray, tau: float) -> np.ndarray:
+    """Regularised BGK (Latt & Chopard 2006): solver.py:338-392 (D2Q9),
+    solver3d.py:342-403 (D3Q19), d3q27.py:481-540 (D3Q27).  The second moment
+    of f - feq is projected on the Hermite basis H = c c - I/3 and relaxed:
+    feq + (1 - 1/tau) * ((9/2 w) * (H_xx Pi_xx + H_yy Pi_yy [+ H_zz Pi_zz]
+    + 2 H_xy Pi_xy [+ 2 H_xz Pi_xz + 2 H_yz Pi_yz])), each operation rounded in
+    the field's dtype with Python scalars taken at that dtype.  The projection
+    takes the float32-rounded weights for every dtype (the default dtype of
+    _w_on, d3q19.py:75-80, d3q27.py:345-350); the equilibrium keeps its own."""
+    q = f.shape[0]
+    nd = f.ndim - 1
+    t = f.dtype.type
+    rho, ux, uy, uz = macroscopic(f)
+    feq = equilibrium(q, rho, ux, uy, uz)
+    fneq = f - feq
+    pxx, pyy, pzz, pxy, pxz, pyz = neq_stress(fneq)
+    c = C[q].astype(f.dtype)
+    cx, cy = _view(c[:, 0], nd), _view(c[:, 1], nd)
+    cs2 = t(1.0 / 3.0)
+    s = (cx * cx - cs2) * pxx + (cy * cy - cs2) * pyy
+    if q == 9:
+        s = s + (t(2) * (cx * cy)) * pxy
+    else:
+        cz = _view(c[:, 2], nd)
+        s = s + (cz * cz - cs2) * pzz
+        s = s + (t(2) * (cx * cy)) * pxy + (t(2) * (cx * cz)) * pxz + (t(2) * (cy * cz)) * pyz
+    reg = (t(4.5) * _view(W64[q].astype(np.float32).astype(f.dtype), nd)) * s
+    return feq + t(1.0 - 1.0 / tau) * reg
+
+
 def collide_cumulant_d3q19(f: np.ndarray, tau: float, omega_b=1.0, omega_odd=1.0, omega_even=1.0, c_s=0.0):
     """Hermite-regularised stress relaxation, cumulant.py:1159-1420 (Smagorinsky branch only)."""
     rho, ux, uy, uz = macroscopic(f)
@@ -554,6 +584,7 @@ COLLIDERS = {
     "bgk": collide_bgk,
     "mrt": collide_mrt,
     "trt": collide_trt,
+    "rlbm": collide_rlbm,
     "cascaded": collide_cascaded,
     "smagorinsky": collide_smagorinsky,
     "cumulant_d3q19": collide_cumulant_d3q19,

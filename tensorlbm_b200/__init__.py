@@ -20,10 +20,10 @@ __version__ = "0.1.0"
 _PATCHES = {
     "d2q9": ["equilibrium", "macroscopic"],
     "d3q19": ["equilibrium3d", "macroscopic3d", "equilibrium3d_low_memory", "macroscopic3d_low_memory"],
-    "d3q27": ["equilibrium27", "macroscopic27", "collide_bgk27", "collide_mrt27", "collide_trt27", "stream27",
+    "d3q27": ["equilibrium27", "macroscopic27", "collide_bgk27", "collide_mrt27", "collide_trt27", "collide_rlbm27", "stream27",
               "stream27_roll", "correct_mass27"],
-    "solver": ["collide_bgk", "collide_bgk_fused", "collide_mrt", "collide_trt", "stream", "correct_mass"],
-    "solver3d": ["collide_bgk3d", "collide_mrt3d", "collide_trt3d", "collide_mrt3d_low_memory", "stream3d",
+    "solver": ["collide_bgk", "collide_bgk_fused", "collide_mrt", "collide_trt", "collide_rlbm", "stream", "correct_mass"],
+    "solver3d": ["collide_bgk3d", "collide_mrt3d", "collide_trt3d", "collide_rlbm3d", "collide_mrt3d_low_memory", "stream3d",
                  "stream3d_roll",
                  "correct_mass3d"],
     "cumulant": ["collide_cumulant_d3q27", "collide_cumulant_geier_d3q27", "collide_cumulant_d3q19"],

@@ -24,7 +24,7 @@ ERR_TOO_LARGE = 9
 F32, F64, F16_SHIFTED, BF16_SHIFTED, F16, BF16 = 0, 1, 2, 3, 4, 5
 # tlbm_collision
 (COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY, COLL_TRT,
- COLL_CASCADED) = range(9)
+ COLL_CASCADED, COLL_RLBM) = range(10)
 # tlbm_bc_bits / tlbm_flag_bits
 BC_LID, BC_ZH_INLET, BC_ZH_OUTLET = 1, 2, 4
 FLAG_SOLID, FLAG_OBSTACLE, FLAG_HALFWAY, FLAG_MOVING, FLAG_CURVED = 1, 2, 4, 8, 16

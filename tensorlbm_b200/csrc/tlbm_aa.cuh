@@ -343,6 +343,7 @@ int dispatch_aa_collision(int mode, const StepParams& p, const tlbm_desc& d, cud
     case TLBM_COLL_BGK: return dispatch_aa_mode<L, S, TLBM_COLL_BGK>(mode, p, d, s);
     case TLBM_COLL_MRT: return dispatch_aa_mode<L, S, TLBM_COLL_MRT>(mode, p, d, s);
     case TLBM_COLL_TRT: return dispatch_aa_mode<L, S, TLBM_COLL_TRT>(mode, p, d, s);
+    case TLBM_COLL_RLBM: return dispatch_aa_mode<L, S, TLBM_COLL_RLBM>(mode, p, d, s);
     case TLBM_COLL_SMAGORINSKY: return dispatch_aa_mode<L, S, TLBM_COLL_SMAGORINSKY>(mode, p, d, s);
     case TLBM_COLL_CUMULANT:
       if constexpr (L::Q == 27) return dispatch_aa_mode<L, S, TLBM_COLL_CUMULANT>(mode, p, d, s);

@@ -29,6 +29,7 @@ template <typename T> struct CollideParams {
   T cm_s5, cm_s6;           // cascaded D3Q27 5th / 6th-order rates (omega_odd, omega_even are s_3, s_4)
   T tau_minus;              // TRT antisymmetric relaxation time
   double inv_tau_minus64;   // RN64(1 / float(tau_minus)) for the exact TRT quotient
+  T rlbm_keep;              // 1 - 1/tau formed in float64 (regularised BGK)
 };
 
 // ---------------------------------------------------------------------------
@@ -323,6 +324,47 @@ __device__ __forceinline__ T hermite_contract(int a, int b, int c, T hxx, T hyy,
   if (a * c != 0) r = xadd(r, xmul(T(2 * a * c), s.xz));
   if (b * c != 0) r = xadd(r, xmul(T(2 * b * c), s.yz));
   return r;
+}
+
+// ---------------------------------------------------------------------------
+// Regularised BGK, Latt & Chopard 2006 (solver.py:338-392, solver3d.py:342-403,
+// d3q27.py:481-540), bit-exact: Pi = sum c c (f - feq) in the reference's
+// summation order, then per direction
+//   f = feq + keep * ((4.5 w) * (h_xx Pi_xx + h_yy Pi_yy [+ h_zz Pi_zz]
+//                                + (2 h_xy) Pi_xy [+ (2 h_xz) Pi_xz + (2 h_yz) Pi_yz]))
+// with h_aa = c_a^2 - 1/3, h_ab = c_a c_b and keep = 1 - 1/tau (formed in
+// float64, a Python scalar there), every operation rounded on its own.  The
+// weights of the projection are the float32 ones for every field dtype (the
+// reference's _w_on default, d3q19.py:75-80, d3q27.py:345-350), while the
+// equilibrium keeps weight<L, T>.  A zero h_ab term is skipped: adding the
+// zero product does not change the sum.
+// ---------------------------------------------------------------------------
+template <class L, typename T>
+__device__ __forceinline__ void collide_rlbm(T (&f)[L::Q], T keep) {
+  T rho, ux, uy, uz;
+  macroscopic<L>(f, rho, ux, uy, uz);
+  const T usq = usq_of<L>(ux, uy, uz);
+  T fe[L::Q], fn[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    fe[q] = feq_q<L>(q, rho, ux, uy, uz, usq);
+    fn[q] = xsub(f[q], fe[q]);
+  }
+  const Pi6<T> p = neq_stress<L>(fn);
+  const T cs2 = T(1.0 / 3.0);
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    const int a = L::cx(q), b = L::cy(q), c = L::cz(q);
+    const T hxx = xsub(T(a * a), cs2), hyy = xsub(T(b * b), cs2);
+    T r;
+    if constexpr (L::DIM == 3) {
+      r = hermite_contract(a, b, c, hxx, hyy, xsub(T(c * c), cs2), p);
+    } else {
+      r = xadd(xmul(hxx, p.xx), xmul(hyy, p.yy));
+      if (a * b != 0) r = xadd(r, xmul(T(2 * a * b), p.xy));
+    }
+    f[q] = xadd(fe[q], xmul(keep, xmul(xmul(T(4.5), T(float(L::w(q)))), r)));
+  }
 }
 
 template <typename T>
@@ -1030,6 +1072,8 @@ __device__ __forceinline__ void collide(T (&f)[L::Q], const CollideParams<T>& cp
     else if constexpr (L::Q == 27) collide_cascaded_d3q27(f, cp);
   } else if constexpr (COLL == TLBM_COLL_TRT) {
     collide_trt<L>(f, cp.tau, cp.inv_tau64, cp.tau_minus, cp.inv_tau_minus64);
+  } else if constexpr (COLL == TLBM_COLL_RLBM) {
+    collide_rlbm<L>(f, cp.rlbm_keep);
   } else if constexpr (COLL == TLBM_COLL_CUMULANT_D3Q19) {
     static_assert(L::Q == 19, "D3Q19 only");
     collide_cumulant_d3q19(f, cp);
@@ -1067,6 +1111,7 @@ __host__ __device__ __forceinline__ CollideParams<F> pack_params(const CollidePa
   p.cm_s6 = F(c.cm_s6);
   p.tau_minus = F(c.tau_minus);
   p.inv_tau_minus64 = c.inv_tau_minus64;
+  p.rlbm_keep = F(c.rlbm_keep);
   return p;
 }
 
@@ -1104,6 +1149,7 @@ __host__ __device__ CollideParams<T> make_collide_params(double tau, double s_e,
   cp.cm_s6 = cp.omega_even;
   cp.tau_minus = cp.tau;
   cp.inv_tau_minus64 = cp.inv_tau64;
+  cp.rlbm_keep = T(1.0 - 1.0 / tau);
   cp.tau_sq = T(tau * tau);
   cp.tau_eff_max = T(tau + 0.5 > 1.0 ? tau + 0.5 : 1.0);
   cp.force_a = T(0);

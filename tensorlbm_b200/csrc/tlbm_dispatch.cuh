@@ -33,6 +33,7 @@ int dispatch_collision(const tlbm_desc& d, const StepParams& p, cudaStream_t s) 
     case TLBM_COLL_MRT: return launch_step<L, S, S, TLBM_COLL_MRT, PULL>(p, d, s);
     case TLBM_COLL_SMAGORINSKY: return launch_step<L, S, S, TLBM_COLL_SMAGORINSKY, PULL>(p, d, s);
     case TLBM_COLL_TRT: return launch_step<L, S, S, TLBM_COLL_TRT, PULL>(p, d, s);
+    case TLBM_COLL_RLBM: return launch_step<L, S, S, TLBM_COLL_RLBM, PULL>(p, d, s);
     case TLBM_COLL_CASCADED:
       if constexpr (L::Q != 9) return launch_step<L, S, S, TLBM_COLL_CASCADED, PULL>(p, d, s);
       else return TLBM_ERR_UNSUPPORTED;

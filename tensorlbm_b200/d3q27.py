@@ -32,6 +32,11 @@ def collide_trt27(f: torch.Tensor, tau_plus: float, lambda_trt: float = 3.0 / 16
     return _ops.collide(27, f, _lib.COLL_TRT, tau_plus, lambda_trt=lambda_trt)
 
 
+def collide_rlbm27(f: torch.Tensor, tau: float) -> torch.Tensor:
+    """Regularised BGK (Latt & Chopard 2006), bit-exact.  tensorlbm/d3q27.py:481."""
+    return _ops.collide(27, f, _lib.COLL_RLBM, tau)
+
+
 def collide_mrt27(f: torch.Tensor, tau: float, s_e: float = 1.19, s_eps: float = 1.4, s_q: float = 1.2,
                   s_pi: float | None = None) -> torch.Tensor:
     """Gram-Schmidt 27x27 MRT, tensorlbm/d3q27.py:643."""
@@ -51,4 +56,4 @@ def stream27_roll(f: torch.Tensor) -> torch.Tensor:
 stream27 = stream27_roll
 
 __all__ = ["C", "W", "W_EXACT64", "OPPOSITE", "equilibrium27", "macroscopic27", "collide_bgk27",
-           "collide_mrt27", "correct_mass27", "stream27", "stream27_roll"]
+           "collide_mrt27", "collide_rlbm27", "collide_trt27", "correct_mass27", "stream27", "stream27_roll"]

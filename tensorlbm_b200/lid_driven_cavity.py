@@ -76,17 +76,20 @@ def cavity_3d_full(nx: int = 64, re: float = 1000.0, u_lid: float = 0.06, steps:
 
 
 def cavity_2d(nx: int = 128, re: float = 100.0, u_lid: float = 0.06, steps: int = 100_000, device=None,
-              chunk: int = 500) -> dict:
-    """TensorLBM's verified 2-D lid-driven cavity (benchmarks/verified/cavity/re100/run.py:45-150)
-    on the fused kernel.
+              chunk: int = 500, collision: str = "mrt") -> dict:
+    """TensorLBM's verified 2-D lid-driven cavity (benchmarks/verified/cavity/re100/run.py:45-150;
+    re1000/run.py:45-150 with collision="rlbm") on the fused kernel.
 
-    Square nx x nx, D2Q9 MRT with the library's default rates, tau = 3 u_lid nx / Re + 1/2;
+    Square nx x nx, D2Q9 MRT with the library's default rates (Re 100) or the
+    regularised BGK (Re 1000, where the MRT diverges), tau = 3 u_lid nx / Re + 1/2;
     the walls y = 0, x = 0, x = nx-1 bounce back half-way before streaming
     from the pre-collision state; the Zou/He lid moves the row y = ny-1 at
     u_lid; rho = 1, u = 0 start.  After `steps` steps: the centre lines
     u(x = nx//2, y) and v(x, y = ny//2) divided by u_lid with the wall cells
     zeroed, and the benchmark's point values u(0.5, 0.5), u(0.5, 0.0625) and
-    v(0.5, 0.5), linearly interpolated on the node positions linspace(0, 1, n)."""
+    v(0.5, 0.5), linearly interpolated on the node positions linspace(0, 1, n),
+    and the primary vortex centre (re1000/run.py:117-131): the slowest cell of
+    x in [0.2, 0.85], y in [0.2, 0.9] in node coordinates rounded to 4 places."""
     import time
 
     import numpy as np
@@ -103,7 +106,7 @@ def cavity_2d(nx: int = 128, re: float = 100.0, u_lid: float = 0.06, steps: int 
     wall[:, -1] = True
     rho0 = torch.ones((n, n), dtype=torch.float32, device=dev)
     zero = torch.zeros_like(rho0)
-    s = LBMSolver("D2Q9", (n, n), tau, "mrt", device=dev, wall_mask=wall, wall_mode="halfway", u_lid=u_lid)
+    s = LBMSolver("D2Q9", (n, n), tau, collision, device=dev, wall_mask=wall, wall_mode="halfway", u_lid=u_lid)
     s.load(equilibrium(rho0, zero, zero))
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -115,7 +118,11 @@ def cavity_2d(nx: int = 128, re: float = 100.0, u_lid: float = 0.06, steps: int 
     uy = (uy.masked_fill(wall, 0.0) / u_lid).double().cpu().numpy()
     pos = np.linspace(0.0, 1.0, n)
     u_cl, v_cl = ux[:, n // 2], uy[n // 2, :]
-    return {"nx": n, "re": re, "u_lid": u_lid, "tau": tau, "steps": steps,
+    speed2 = ux * ux + uy * uy
+    region = (pos[None, :] >= 0.2) & (pos[None, :] <= 0.85) & (pos[:, None] >= 0.2) & (pos[:, None] <= 0.9)
+    iy, ix = np.unravel_index(np.argmin(np.where(region, speed2, np.inf)), speed2.shape)
+    return {"nx": n, "re": re, "u_lid": u_lid, "tau": tau, "steps": steps, "collision": collision,
+            "primary_vortex": [round(ix / (n - 1), 4), round(iy / (n - 1), 4)],
             "u_centerline": u_cl.tolist(), "v_centerline": v_cl.tolist(),
             "u_mid": float(np.interp(0.5, pos, u_cl)), "u_bot": float(np.interp(0.0625, pos, u_cl)),
             "v_mid": float(np.interp(0.5, pos, v_cl)), "finite": not s.nonfinite_seen(), "seconds": secs,

@@ -29,6 +29,11 @@ def collide_trt(f: torch.Tensor, tau_plus: float, lambda_trt: float = 3.0 / 16.0
     return _ops.collide(9, f, _lib.COLL_TRT, tau_plus, lambda_trt=lambda_trt)
 
 
+def collide_rlbm(f: torch.Tensor, tau: float) -> torch.Tensor:
+    """Regularised BGK (Latt & Chopard 2006), bit-exact.  tensorlbm/solver.py:338."""
+    return _ops.collide(9, f, _lib.COLL_RLBM, tau)
+
+
 def stream(f: torch.Tensor) -> torch.Tensor:
     """Periodic pull streaming.  tensorlbm/solver.py:396."""
     return _ops.stream(9, f)
@@ -39,4 +44,4 @@ def correct_mass(f: torch.Tensor, target_mass: float) -> torch.Tensor:
     return _ops.correct_mass(f, target_mass)
 
 
-__all__ = ["collide_bgk", "collide_bgk_fused", "collide_mrt", "stream", "correct_mass"]
+__all__ = ["collide_bgk", "collide_bgk_fused", "collide_mrt", "collide_rlbm", "collide_trt", "stream", "correct_mass"]

@@ -26,6 +26,11 @@ def collide_trt3d(f: torch.Tensor, tau_plus: float, lambda_trt: float = 3.0 / 16
     return _ops.collide(19, f, _lib.COLL_TRT, tau_plus, lambda_trt=lambda_trt)
 
 
+def collide_rlbm3d(f: torch.Tensor, tau: float) -> torch.Tensor:
+    """Regularised BGK (Latt & Chopard 2006), bit-exact.  tensorlbm/solver3d.py:342."""
+    return _ops.collide(19, f, _lib.COLL_RLBM, tau)
+
+
 def stream3d(f: torch.Tensor) -> torch.Tensor:
     """Periodic pull streaming.  tensorlbm/solver3d.py:210."""
     return _ops.stream(19, f)
@@ -39,5 +44,5 @@ def correct_mass3d(f: torch.Tensor, target_mass: float) -> torch.Tensor:
     return _ops.correct_mass(f, target_mass)
 
 
-__all__ = ["collide_bgk3d", "collide_mrt3d", "collide_mrt3d_low_memory", "stream3d", "stream3d_roll",
-           "correct_mass3d"]
+__all__ = ["collide_bgk3d", "collide_mrt3d", "collide_mrt3d_low_memory", "collide_rlbm3d", "collide_trt3d",
+           "stream3d", "stream3d_roll", "correct_mass3d"]

@@ -36,6 +36,7 @@ COLLISIONS = {
     "smagorinsky": _lib.COLL_SMAGORINSKY,
     "trt": _lib.COLL_TRT,
     "cascaded": _lib.COLL_CASCADED,
+    "rlbm": _lib.COLL_RLBM,
 }
 _LATTICES = {"D2Q9": 9, "D3Q19": 19, "D3Q27": 27, 9: 9, 19: 19, 27: 27}
 # storage dtype -> (C code, torch dtype of the buffer)

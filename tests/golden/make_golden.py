@@ -127,6 +127,29 @@ def checkpoints(torch) -> None:
     print(f"wrote {out}")
 
 
+def rlbm(torch) -> None:
+    """Regularised BGK collisions (solver.py:338, solver3d.py:342, d3q27.py:481)
+    on seeded near-equilibrium fields, and on the same fields with a seeded
+    perturbation of 5 % that puts weight in the higher-order (ghost) moments."""
+    from tensorlbm.d3q27 import collide_rlbm27
+    from tensorlbm.solver import collide_rlbm
+    from tensorlbm.solver3d import collide_rlbm3d
+
+    out = {}
+    fns = {9: collide_rlbm, 19: collide_rlbm3d, 27: collide_rlbm27}
+    shapes = {9: (8, 8), 19: (4, 4, 8), 27: (4, 4, 8)}
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        for q, seed in ((9, 13), (19, 23), (27, 33)):
+            _, _, f = near_eq_field(torch, q, shapes[q], dt, seed)
+            g = torch.Generator().manual_seed(seed + 100)
+            fr = f * (1.0 + 0.05 * (2.0 * torch.rand(f.shape, generator=g, dtype=torch.float64) - 1.0)).to(dt)
+            out.update({f"f{q}_{tag}": f, f"rlbm{q}_{tag}": fns[q](f, 0.6), f"rlbm{q}_low_{tag}": fns[q](f, 0.5046),
+                        f"fr{q}_{tag}": fr, f"rlbmr{q}_{tag}": fns[q](fr, 0.53)})
+    arrays = {k: v.detach().cpu().numpy() for k, v in out.items()}
+    np.savez_compressed(HERE / "collide_rlbm.npz", **arrays)
+    print("wrote collide_rlbm.npz")
+
+
 def trt(torch) -> None:
     """TRT collisions (solver.py:440, solver3d.py:303, d3q27.py:438) on the
     seeded near-equilibrium fields of the other collision fixtures."""
@@ -458,23 +481,26 @@ def cavity3d_full(src: str) -> None:
     print(f"wrote cavity3d_full.npz ({sorted(out)})")
 
 
-def cavity2d_re100(src: str) -> None:
-    """TensorLBM's verified 2-D lid-driven cavity at Re 100
-    (benchmarks/verified/cavity/re100: run.py and the result.json it wrote,
-    D2Q9 MRT, three half-way walls, Zou/He lid, 128^2 and 192^2, 100 000
-    steps): the point values u(0.5, 0.5), u(0.5, 0.0625), v(0.5, 0.5) of each
-    grid, copied from the reference's own outputs."""
+def cavity2d(src: str, re: int) -> None:
+    """TensorLBM's verified 2-D lid-driven cavity (benchmarks/verified/cavity/
+    re100 and re1000: run.py and the result.json it wrote; three half-way
+    walls, Zou/He lid; Re 100: D2Q9 MRT, 128^2 and 192^2, 100 000 steps;
+    Re 1000: D2Q9 regularised BGK, 192^2 and 256^2, 200 000 steps): the point
+    values u(0.5, 0.5), u(0.5, 0.0625), v(0.5, 0.5) of each grid (and the
+    primary vortex centre where recorded), copied from the reference's own
+    outputs."""
     import json
 
-    res = json.loads((pathlib.Path(src).parent / "benchmarks" / "verified" / "cavity" / "re100" /
+    res = json.loads((pathlib.Path(src).parent / "benchmarks" / "verified" / "cavity" / f"re{re}" /
                       "result.json").read_text())
     out = {}
     for key, case in res["grids"].items():
         n = int(case["nx"])
-        for k in ("re", "u_lid", "tau", "steps", "u_mid", "u_bot", "v_mid", "last_resid"):
-            out[f"n{n}_{k}"] = np.asarray(case[k])
-    np.savez_compressed(HERE / "cavity2d_re100.npz", **out)
-    print(f"wrote cavity2d_re100.npz ({sorted(out)})")
+        for k in ("re", "u_lid", "tau", "steps", "u_mid", "u_bot", "v_mid", "last_resid", "primary_vortex"):
+            if k in case:
+                out[f"n{n}_{k}"] = np.asarray(case[k])
+    np.savez_compressed(HERE / f"cavity2d_re{re}.npz", **out)
+    print(f"wrote cavity2d_re{re}.npz ({sorted(out)})")
 
 
 def pipe3d(src: str) -> None:
@@ -553,8 +579,8 @@ def main() -> None:
     if args.only == "cavity3d_full":
         cavity3d_full(args.reference)
         return
-    if args.only == "cavity2d_re100":
-        cavity2d_re100(args.reference)
+    if args.only in ("cavity2d_re100", "cavity2d_re1000"):
+        cavity2d(args.reference, int(args.only[len("cavity2d_re"):]))
         return
     if args.only == "pipe3d":
         pipe3d(args.reference)
@@ -578,6 +604,9 @@ def main() -> None:
         return
     if args.only == "trt":
         trt(torch)
+        return
+    if args.only == "rlbm":
+        rlbm(torch)
         return
     if args.only == "bfl":
         bfl(torch)

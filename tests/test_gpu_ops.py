@@ -309,6 +309,19 @@ def test_collide_trt(cuda, tag):
         assert same(N(fn(f, 0.57, lambda_trt=0.25)), g[f"trt{q}_lam_{tag}"])
 
 
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_collide_rlbm(cuda, tag):
+    """The regularised-BGK kernels against the reference's outputs, bit for bit."""
+    from tensorlbm_b200 import d3q27, solver, solver3d
+
+    g = golden("collide_rlbm")
+    for q, fn in ((9, solver.collide_rlbm), (19, solver3d.collide_rlbm3d), (27, d3q27.collide_rlbm27)):
+        f, fr = T(g[f"f{q}_{tag}"], cuda), T(g[f"fr{q}_{tag}"], cuda)
+        assert same(N(fn(f, 0.6)), g[f"rlbm{q}_{tag}"])
+        assert same(N(fn(f, 0.5046)), g[f"rlbm{q}_low_{tag}"])
+        assert same(N(fn(fr, 0.53)), g[f"rlbmr{q}_{tag}"])
+
+
 def test_trt_sphere_channel_vs_oracle(cuda):
     """The fused step with TRT (pull, Zou/He, bounce-back, drag) against the
     oracle's collide -> stream -> boundaries chain: bit-exact."""
@@ -330,6 +343,49 @@ def test_trt_sphere_channel_vs_oracle(cuda):
         forces.append(fo)
     assert same(N(s.f), ref)
     assert np.max(np.abs(N(s.force_history()) - np.array(forces))) < 1e-6 * np.max(np.abs(np.array(forces)))
+
+
+def test_rlbm_cavity_2d_vs_oracle(cuda):
+    """The fused D2Q9 step with the regularised BGK in the verified Re 1000
+    cavity's scheme (three half-way walls from the pre-collision state, Zou/He
+    lid) against the oracle's collide -> where -> stream -> lid chain at a
+    low-viscosity tau: bit-exact."""
+    from tensorlbm_b200 import LBMSolver
+
+    n, tau, u_lid = 48, 0.5144, 0.06
+    wall = np.zeros((n, n), bool)
+    wall[0, :] = wall[:, 0] = wall[:, -1] = True
+    z = np.zeros((n, n), np.float32)
+    f0 = O.equilibrium(9, np.ones_like(z), z, z)
+    s = LBMSolver("D2Q9", (n, n), tau, "rlbm", device=cuda, wall_mask=T(wall, cuda), wall_mode="halfway",
+                  u_lid=u_lid)
+    s.load(T(f0, cuda)).step(40)
+    ref = f0
+    for _ in range(40):
+        ref = O.cavity_step(ref, tau, wall, u_lid, "rlbm", mode="halfway")
+    assert same(N(s.f), ref)
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_rlbm_sphere_channel_vs_oracle(cuda, q):
+    """The fused 3-D step with the regularised BGK (pull, Zou/He, bounce-back,
+    drag) against the oracle's chain: bit-exact populations."""
+    from tensorlbm_b200 import LBMSolver, boundaries3d
+
+    nz, ny, nx = 8, 10, 20
+    obst = boundaries3d.sphere_mask(nx, ny, nz, 7.0, 5.0, 4.0, 2.2, cuda)
+    o = obst.cpu().numpy()
+    ux = np.full((nz, ny, nx), 0.04, np.float32)
+    ux[o] = 0.0
+    z = np.zeros_like(ux)
+    f0 = O.equilibrium(q, np.ones_like(ux), ux, z, z)
+    s = LBMSolver(f"D3Q{q}", (nz, ny, nx), 0.53, "rlbm", device=cuda, obstacle_mask=obst, u_in=0.04, rho_out=1.0,
+                  track_force=True)
+    s.load(T(f0, cuda)).step(6)
+    ref = f0
+    for _ in range(6):
+        ref, _ = O.channel_step(ref, 0.53, 0.04, 1.0, None, o, "rlbm")
+    assert same(N(s.f), ref)
 
 
 @pytest.mark.parametrize("tag,tol", [("f32", 5 * F32_TOL), ("f64", 1e-12)])

@@ -182,6 +182,18 @@ def test_collide_trt():
             assert same(O.collide_trt(g[f"f{q}_{tag}"], 0.57, 0.25), g[f"trt{q}_lam_{tag}"])
 
 
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+@pytest.mark.parametrize("q", [9, 19, 27])
+def test_collide_rlbm(q, tag):
+    """Regularised BGK (solver.py:338, solver3d.py:342, d3q27.py:481): the
+    oracle against the reference's own outputs, bit for bit, near equilibrium
+    (tau 0.6 and 0.5046) and with 5 % seeded ghost-mode content (tau 0.53)."""
+    g = golden("collide_rlbm")
+    assert same(O.collide_rlbm(g[f"f{q}_{tag}"], 0.6), g[f"rlbm{q}_{tag}"])
+    assert same(O.collide_rlbm(g[f"f{q}_{tag}"], 0.5046), g[f"rlbm{q}_low_{tag}"])
+    assert same(O.collide_rlbm(g[f"fr{q}_{tag}"], 0.53), g[f"rlbmr{q}_{tag}"])
+
+
 def test_bfl_links_update_and_chain():
     """Bouzidi links of a sphere (bfl_common.py:384, interpolated_bc_common.py:136),
     the link update (bfl_common.py:106) and the 8-step chain in bfl_step's
