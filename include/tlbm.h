@@ -36,7 +36,7 @@ typedef enum tlbm_status {
   TLBM_ERR_NONFINITE = 6,   /* reported by callers that read the status word */
   TLBM_ERR_ARG = 7,         /* null pointer or invalid parameter */
   TLBM_ERR_UNSUPPORTED = 8, /* lattice / collision / boundary combination not built */
-  TLBM_ERR_TOO_LARGE = 9    /* input larger than a fixed-size static scratch array */
+  TLBM_ERR_TOO_LARGE = 9    /* input larger than a fixed-size static scratch array or an index width */
 } tlbm_status;
 
 typedef enum tlbm_lattice { TLBM_D2Q9 = 9, TLBM_D3Q19 = 19, TLBM_D3Q27 = 27 } tlbm_lattice;
@@ -437,7 +437,8 @@ TLBM_API int tlbm_mlp_infer(const void* blob, const float* x, int64_t count, flo
 /* One fused D3Q19 LES step on a periodic box (float32 populations, pull):
  * BGK with the learned tau_eff and exact-difference linear forcing
  * F = force_lin rho u.  tau_out (per cell), fallback_count (cells that used the
- * Smagorinsky tau of c_s) and status may be NULL.  Replaces
+ * Smagorinsky tau of c_s) and status may be NULL.  nx ny nz + 1024 must stay
+ * below 2^31 (32-bit cell offsets; else TLBM_ERR_TOO_LARGE).  Replaces
  * collide_ai_les_bgk (ai/inference.py:68-92) + stream for 3-D. */
 TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, double c_s, double force_lin,
                            const void* blob, const float* f_in, float* f_out, float* tau_out,

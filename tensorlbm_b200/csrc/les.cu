@@ -361,16 +361,18 @@ __global__ void k_mlp_pack(const float* __restrict__ theta, const float* __restr
 }
 
 // stand-alone tensor-core inference: y for count raw feature rows
-__global__ void __launch_bounds__(mlp::TILE) k_mlp_infer(const uint8_t* __restrict__ blob,
-                                                         const float* __restrict__ x, long long count,
-                                                         float* __restrict__ y_out, unsigned int* status) {
+using InferCta = mlp::Cta<2>;
+
+__global__ void __launch_bounds__(InferCta::THREADS)
+    k_mlp_infer(const uint8_t* __restrict__ blob, const float* __restrict__ x, long long count,
+                float* __restrict__ y_out, unsigned int* status) {
   extern __shared__ uint8_t raw[];
-  mlp::Engine e;
+  mlp::Engine<2> e;
   e.setup(raw, blob);
   const float* p = e.params();
-  const long long ntiles = (count + mlp::TILE - 1) / mlp::TILE;
+  const long long ntiles = (count + InferCta::THREADS - 1) / InferCta::THREADS;
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const long long i = t * mlp::TILE + threadIdx.x;
+    const long long i = t * InferCta::THREADS + threadIdx.x;
     float z[NF];
 #pragma unroll
     for (int k = 0; k < NF; ++k) z[k] = i < count ? (x[i * NF + k] - p[mlp::P_MEAN + k]) * p[mlp::P_ISTD + k] : 0.0f;
@@ -390,16 +392,16 @@ int infer_grid(long long count, int& grid) {
   if (per_sm < 0) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
-    if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::SM_BYTES) !=
+    if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, InferCta::SM_BYTES) !=
         cudaSuccess)
       return TLBM_ERR_LAUNCH;
     if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared) != cudaSuccess)
       return TLBM_ERR_LAUNCH;
-    per_sm = mlp::resident_ctas(k_mlp_infer, sms);
+    per_sm = mlp::resident_ctas<2>(k_mlp_infer, sms);
   }
   if (per_sm < 1) return TLBM_ERR_UNSUPPORTED;
-  const long long ntiles = (count + mlp::TILE - 1) / mlp::TILE;
+  const long long ntiles = (count + InferCta::THREADS - 1) / InferCta::THREADS;
   long long g = (long long)sms * per_sm;
   grid = int(g < ntiles ? g : ntiles);
   return TLBM_OK;
@@ -498,7 +500,7 @@ TLBM_API int tlbm_mlp_infer(const void* blob, const float* x, int64_t count, flo
   int grid = 0;
   int st = infer_grid(count, grid);
   if (st != TLBM_OK) return st;
-  k_mlp_infer<<<grid, mlp::TILE, mlp::SM_BYTES, static_cast<cudaStream_t>(stream)>>>(
+  k_mlp_infer<<<grid, InferCta::THREADS, InferCta::SM_BYTES, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const uint8_t*>(blob), x, count, y, status);
   return launch_ok();
 }

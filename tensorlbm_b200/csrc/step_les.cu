@@ -1,8 +1,8 @@
 // Fused D3Q19 LES step with the learned eddy-viscosity closure.
 //
 // Persistent kernel: each CTA loads the packed network once (shared memory),
-// allocates 128 TMEM columns, then walks tiles of 256 consecutive cells as two
-// independent halves of 128 (see tlbm_mlp.cuh):
+// allocates 64 TMEM columns per half, then walks tiles of TLBM_LES_HALVES x 128
+// consecutive cells as independent halves of 128 (see tlbm_mlp.cuh):
 //   pull (periodic) -> rho, u -> Pi_neq = sum_q c c (f - feq) -> 9 features
 //   -> tcgen05 MLP (three 64-wide layers and the output layer, bf16 x bf16 ->
 //      fp32 in TMEM)
@@ -14,14 +14,32 @@
 #include "tlbm_collide.cuh"
 #include "tlbm_mlp.cuh"
 
+// CTA shape: halves of 128 cells per CTA and CTAs per SM.  One CTA of eight
+// halves (1024 threads, 64 registers, all 512 TMEM columns, one 28 KB copy of
+// the weights) gives 32 warps per SM.  Measured on the forced-HIT step at
+// 128^3 / 256^3: 9.50 / 10.03 GLUPS, against 8.85 / 9.43 for two CTAs of four
+// halves and 8.51 / 8.81 for three CTAs of two halves (80 registers, 24 warps;
+// their shared memory, 61.7 KB each, stops a fourth).  Reading the
+// accumulators 16 columns at a time and 32-bit cell offsets then took the
+// spills from 124 to 8 bytes per thread: 10.39 / 10.93 GLUPS.  Results are
+// identical in every shape.
+#ifndef TLBM_LES_HALVES
+#define TLBM_LES_HALVES 8
+#endif
+#ifndef TLBM_LES_MINB
+#define TLBM_LES_MINB 1
+#endif
+
 namespace tlbm {
 namespace {
+
+using LesCta = mlp::Cta<TLBM_LES_HALVES>;
 
 struct LesStep {
   const float* fin;
   float* fout;
   int nx, ny, nz;
-  long long plane, n;
+  int plane, n;  // n < 2^31: 32-bit cell offsets within a direction's plane
   float tau0, c_s, a_lin;
   const uint8_t* blob;
   float* tau_out;                // per-cell tau_eff, may be null
@@ -29,17 +47,18 @@ struct LesStep {
   unsigned int* status;          // bit0 non-finite, bit2 tensor-core wait timeout; may be null
 };
 
-__global__ void __launch_bounds__(mlp::TILE, 3) k_step_les(LesStep p) {
+__global__ void __launch_bounds__(LesCta::THREADS, TLBM_LES_MINB) k_step_les(LesStep p) {
   using L = D3Q19;
   constexpr int Q = L::Q;
+  constexpr int TILE = LesCta::THREADS;
   extern __shared__ uint8_t raw[];
-  mlp::Engine e;
+  mlp::Engine<TLBM_LES_HALVES> e;
   e.setup(raw, p.blob);
   const float* P = e.params();
   const float tmax = p.tau0 + 0.5f > 1.0f ? p.tau0 + 0.5f : 1.0f;
-  const long long ntiles = (p.n + mlp::TILE - 1) / mlp::TILE;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const long long cell = t * mlp::TILE + threadIdx.x;
+  const int ntiles = int((p.n + (long long)TILE - 1) / TILE);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int cell = t * TILE + int(threadIdx.x);  // < n + TILE <= 2^31 - 1 + 1024: checked on the host
     const bool active = cell < p.n;
     float f[Q];
     float z[mlp::NF];
@@ -52,12 +71,16 @@ __global__ void __launch_bounds__(mlp::TILE, 3) k_step_les(LesStep p) {
       const int xm = x == 0 ? p.nx - 1 : x - 1, xp = x == p.nx - 1 ? 0 : x + 1;
       const int ym = y == 0 ? p.ny - 1 : y - 1, yp = y == p.ny - 1 ? 0 : y + 1;
       const int zm = zc == 0 ? p.nz - 1 : zc - 1, zp = zc == p.nz - 1 ? 0 : zc + 1;
+      // direction q's plane starts n values after direction q-1's; within it
+      // the source cell's offset fits 32 bits
+      const float* fq = p.fin;
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int sx = L::cx(q) > 0 ? xm : (L::cx(q) < 0 ? xp : x);
         const int sy = L::cy(q) > 0 ? ym : (L::cy(q) < 0 ? yp : y);
         const int sz = L::cz(q) > 0 ? zm : (L::cz(q) < 0 ? zp : zc);
-        f[q] = __ldg(p.fin + (long long)q * p.n + (long long)sz * p.plane + (long long)sy * p.nx + sx);
+        f[q] = __ldg(fq + (sz * p.plane + sy * p.nx + sx));
+        fq += p.n;
       }
       macroscopic_fused<L>(f, rho, ux, uy, uz);
       const float usq = ux * ux + uy * uy + uz * uz;
@@ -101,6 +124,7 @@ __global__ void __launch_bounds__(mlp::TILE, 3) k_step_les(LesStep p) {
       //   = w rho [3 A (c.u) + ((1+A)^2 - 1) (4.5 (c.u)^2 - 1.5 u^2)]
       const float a3 = 3.0f * p.a_lin;
       const float k2m1 = p.a_lin * (2.0f + p.a_lin);
+      float* oq = p.fout;
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         float cu = 0.0f;
@@ -111,7 +135,8 @@ __global__ void __launch_bounds__(mlp::TILE, 3) k_step_les(LesStep p) {
         const float quad = fmaf(4.5f * cu, cu, -1.5f * usq);
         const float feq = wr * (1.0f + fmaf(3.0f, cu, quad));
         const float force = wr * fmaf(a3, cu, k2m1 * quad);
-        p.fout[(long long)q * p.n + cell] = fmaf(feq - f[q], inv, f[q]) + force;
+        oq[cell] = fmaf(feq - f[q], inv, f[q]) + force;
+        oq += p.n;
       }
       if (p.tau_out) p.tau_out[cell] = tau;
       if (p.status && !(rho == rho && rho - rho == 0.0f)) atomicOr(p.status, 1u);
@@ -133,16 +158,17 @@ int les_grid(long long n, int& grid) {
   if (per_sm < 0) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return TLBM_ERR_LAUNCH;
-    if (cudaFuncSetAttribute(k_step_les, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::SM_BYTES) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_step_les, cudaFuncAttributeMaxDynamicSharedMemorySize, LesCta::SM_BYTES) !=
+        cudaSuccess)
       return TLBM_ERR_LAUNCH;
     // the largest shared-memory carveout, so that several CTAs fit per SM
     if (cudaFuncSetAttribute(k_step_les, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared) != cudaSuccess)
       return TLBM_ERR_LAUNCH;
-    per_sm = mlp::resident_ctas(k_step_les, sms);
+    per_sm = mlp::resident_ctas<TLBM_LES_HALVES>(k_step_les, sms);
   }
   if (per_sm < 1) return TLBM_ERR_UNSUPPORTED;
-  const long long ntiles = (n + mlp::TILE - 1) / mlp::TILE;
+  const long long ntiles = (n + LesCta::THREADS - 1) / LesCta::THREADS;
   const long long g = (long long)sms * per_sm;
   grid = int(g < ntiles ? g : ntiles);
   return TLBM_OK;
@@ -163,14 +189,16 @@ TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, doub
   if (reinterpret_cast<uintptr_t>(blob) % 16) return TLBM_ERR_ARG;
   if (nx < 1 || ny < 1 || nz < 1) return TLBM_ERR_SHAPE;
   if (!(tau0 > 0.5) || !(force_lin > -1.0 && force_lin < 1.0) || !(c_s >= 0.0)) return TLBM_ERR_ARG;
+  const long long n = (long long)nx * ny * nz;
+  if (n + LesCta::THREADS > 0x7fffffffLL) return TLBM_ERR_TOO_LARGE;  // 32-bit cell offsets
   LesStep p;
   p.fin = f_in;
   p.fout = f_out;
   p.nx = nx;
   p.ny = ny;
   p.nz = nz;
-  p.plane = (long long)nx * ny;
-  p.n = p.plane * nz;
+  p.plane = nx * ny;
+  p.n = int(n);
   p.tau0 = float(tau0);
   p.c_s = float(c_s);
   p.a_lin = float(force_lin);
@@ -181,7 +209,7 @@ TLBM_API int tlbm_les_step(int32_t nx, int32_t ny, int32_t nz, double tau0, doub
   int grid = 0;
   const int st = les_grid(p.n, grid);
   if (st != TLBM_OK) return st;
-  k_step_les<<<grid, mlp::TILE, mlp::SM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
+  k_step_les<<<grid, LesCta::THREADS, LesCta::SM_BYTES, static_cast<cudaStream_t>(stream)>>>(p);
   return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
 }
 

@@ -9,10 +9,10 @@
 // each thread turns its cell's accumulator row into the next A row:
 // h = bf16(0.5 (acc + b)), SiLU = h + h tanh(h) in packed bf16x2 arithmetic.
 //
-// A CTA of 256 threads is two independent halves of 128 rows.  Each half has
-// its own A tile, 64 TMEM columns, mbarrier and named barrier, so the halves
-// drift apart and one half's MMA round trip overlaps the other half's CUDA-core
-// work.
+// A CTA is HALVES independent halves of 128 rows (threads).  Each half has its
+// own A tile, 64 TMEM columns, mbarrier and named barrier, so the halves drift
+// apart and one half's MMA round trip overlaps the other halves' CUDA-core
+// work; the weights are one shared-memory copy per CTA.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -24,8 +24,7 @@ namespace mlp {
 
 constexpr int NF = 9;        // input features
 constexpr int H = 64;        // hidden width
-constexpr int TILE = 256;    // cells per CTA pass (two halves of M = 128)
-constexpr int HALF = 128;
+constexpr int HALF = 128;    // rows of one half (M of its MMAs)
 constexpr int N_PARAMS = H * NF + H + H * H + H + H * H + H + H + 1;  // 9025, flat training vector
 
 // ---- packed inference blob (global memory) --------------------------------
@@ -43,15 +42,20 @@ constexpr int P_BYTES = ((P_COUNT * 4 + 127) / 128) * 128;                      
 constexpr int BLOB_BYTES = OFF_P + P_BYTES;                                              // 27904
 
 // ---- shared memory of one CTA (offsets from a 1024-byte aligned base) -------
-constexpr int A_TILE_BYTES = HALF * 128;         // 16384: one half's activations
-constexpr int SM_A = 0;                          // 2 A tiles
-constexpr int SM_W = SM_A + 2 * A_TILE_BYTES;    // 32768: the blob
-constexpr int SM_P = SM_W + OFF_P;               // 59392: float block
-constexpr int SM_BAR = SM_P + P_BYTES;           // 60672: one mbarrier per half
-constexpr int SM_SLOT = SM_BAR + 16;             // TMEM base address
-constexpr int SM_FLAG = SM_SLOT + 4;             // one timeout flag per half
-constexpr int SM_BYTES = SM_FLAG + 8 + 1024;     // with alignment slack
-constexpr uint32_t TMEM_COLS = 128;              // 64 accumulator columns per half
+constexpr int A_TILE_BYTES = HALF * 128;  // 16384: one half's activations
+template <int HALVES>
+struct Cta {
+  static_assert(HALVES == 2 || HALVES == 4 || HALVES == 8, "the TMEM allocation must be a power of two");
+  static constexpr int THREADS = HALF * HALVES;             // = cells per CTA pass
+  static constexpr int SM_A = 0;                            // HALVES A tiles
+  static constexpr int SM_W = SM_A + HALVES * A_TILE_BYTES;  // the blob
+  static constexpr int SM_P = SM_W + OFF_P;                 // its float block
+  static constexpr int SM_BAR = SM_P + P_BYTES;             // one mbarrier per half
+  static constexpr int SM_SLOT = SM_BAR + 8 * HALVES;       // TMEM base address
+  static constexpr int SM_FLAG = SM_SLOT + 4;               // one timeout flag per half
+  static constexpr int SM_BYTES = SM_FLAG + 4 * HALVES + 1024;  // with alignment slack
+  static constexpr uint32_t TMEM_COLS = 64u * HALVES;       // 64 accumulator columns per half
+};
 constexpr uint32_t MAX_WAIT = 1u << 16;          // mbarrier waits before giving up
 constexpr uint32_t WAIT_HINT_NS = 20000;         // each may suspend the polling warp up to 20 us
 
@@ -115,7 +119,9 @@ __device__ __forceinline__ void named_sync(int id, int nthreads) {
 }
 
 // The tensor-core pass of one half-CTA (128 threads, one row each).
+template <int HALVES>
 struct Engine {
+  using C = Cta<HALVES>;
   uint8_t* sm;
   uint32_t tmem;   // this half's first accumulator column
   uint32_t mbar;   // this half's mbarrier
@@ -127,14 +133,14 @@ struct Engine {
   __device__ void setup(uint8_t* raw_smem, const uint8_t* __restrict__ blob) {
     sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(raw_smem) + 1023) & ~uintptr_t(1023));
     const int4* src = reinterpret_cast<const int4*>(blob);
-    int4* dst = reinterpret_cast<int4*>(sm + SM_W);
+    int4* dst = reinterpret_cast<int4*>(sm + C::SM_W);
     for (int i = threadIdx.x; i < (BLOB_BYTES / 16); i += blockDim.x) dst[i] = src[i];
-    if (threadIdx.x < 32) umma::tmem_alloc(umma::smem_addr(sm + SM_SLOT), TMEM_COLS);
+    if (threadIdx.x < 32) umma::tmem_alloc(umma::smem_addr(sm + C::SM_SLOT), C::TMEM_COLS);
     if (threadIdx.x == 0) {
-      umma::mbar_init(umma::smem_addr(sm + SM_BAR), 1);
-      umma::mbar_init(umma::smem_addr(sm + SM_BAR + 8), 1);
-      reinterpret_cast<volatile int*>(sm + SM_FLAG)[0] = 0;
-      reinterpret_cast<volatile int*>(sm + SM_FLAG)[1] = 0;
+      for (int h = 0; h < HALVES; ++h) {
+        umma::mbar_init(umma::smem_addr(sm + C::SM_BAR + 8 * h), 1);
+        reinterpret_cast<volatile int*>(sm + C::SM_FLAG)[h] = 0;
+      }
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     umma::fence_before_sync();
@@ -142,8 +148,8 @@ struct Engine {
     umma::fence_after_sync();
     half = threadIdx.x / HALF;
     lt = threadIdx.x % HALF;
-    tmem = *reinterpret_cast<volatile uint32_t*>(sm + SM_SLOT) + uint32_t(half * H);
-    mbar = umma::smem_addr(sm + SM_BAR + 8 * half);
+    tmem = *reinterpret_cast<volatile uint32_t*>(sm + C::SM_SLOT) + uint32_t(half * H);
+    mbar = umma::smem_addr(sm + C::SM_BAR + 8 * half);
     phase = 0;
   }
 
@@ -153,16 +159,16 @@ struct Engine {
     __syncthreads();
     if (threadIdx.x < 32) {
       umma::fence_after_sync();
-      umma::tmem_dealloc(*reinterpret_cast<volatile uint32_t*>(sm + SM_SLOT), TMEM_COLS);
+      umma::tmem_dealloc(*reinterpret_cast<volatile uint32_t*>(sm + C::SM_SLOT), C::TMEM_COLS);
     }
   }
 
-  __device__ const float* params() const { return reinterpret_cast<const float*>(sm + SM_P); }
+  __device__ const float* params() const { return reinterpret_cast<const float*>(sm + C::SM_P); }
   __device__ void sync_half() const { named_sync(1 + half, HALF); }
 
   // this thread's A row: 16-byte chunk c (8 bf16)
   __device__ void put_chunk(int c, uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3) {
-    uint8_t* a = sm + SM_A + half * A_TILE_BYTES + umma::sw128_offset(lt, c * 8);
+    uint8_t* a = sm + C::SM_A + half * A_TILE_BYTES + umma::sw128_offset(lt, c * 8);
     *reinterpret_cast<uint4*>(a) = make_uint4(w0, w1, w2, w3);
   }
 
@@ -171,15 +177,15 @@ struct Engine {
   // polls the mbarrier; the half meets at its named barrier.  False on timeout.
   template <int N>
   __device__ bool mma(int b_off, int k_slices) {
-    volatile int* flag = reinterpret_cast<volatile int*>(sm + SM_FLAG) + half;
+    volatile int* flag = reinterpret_cast<volatile int*>(sm + C::SM_FLAG) + half;
     umma::fence_proxy_async_smem();
     umma::fence_before_sync();
     sync_half();
     if (lt < 32) {
       if (lt == 0) {
         umma::fence_after_sync();
-        const uint32_t a0 = umma::smem_addr(sm + SM_A + half * A_TILE_BYTES);
-        const uint32_t b0 = umma::smem_addr(sm + SM_W + b_off);
+        const uint32_t a0 = umma::smem_addr(sm + C::SM_A + half * A_TILE_BYTES);
+        const uint32_t b0 = umma::smem_addr(sm + C::SM_W + b_off);
         for (int ks = 0; ks < k_slices; ++ks)
           umma::mma_bf16(tmem, umma::sw128_desc(a0 + 32u * ks), umma::sw128_desc(b0 + 32u * ks),
                          umma::IdescBf16<128, N>::value, ks > 0 ? 1u : 0u);
@@ -204,14 +210,16 @@ struct Engine {
   // accumulator row -> bf16(0.5 (acc + b)) -> SiLU (bf16x2) -> next A row
   __device__ void hidden_to_a(const float* hb) {
     const uint32_t ta = row_taddr();
+    // 16 accumulator columns at a time: fewer live registers beside the
+    // populations the caller holds across the pass
 #pragma unroll
-    for (int part = 0; part < 2; ++part) {
-      float v[32];
-      umma::tmem_ld32(ta + uint32_t(32 * part), v);
+    for (int part = 0; part < 4; ++part) {
+      float v[16];
+      umma::tmem_ld16(ta + uint32_t(16 * part), v);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const float4 b0 = *reinterpret_cast<const float4*>(hb + 32 * part + 8 * c);
-        const float4 b1 = *reinterpret_cast<const float4*>(hb + 32 * part + 8 * c + 4);
+      for (int c = 0; c < 2; ++c) {
+        const float4 b0 = *reinterpret_cast<const float4*>(hb + 16 * part + 8 * c);
+        const float4 b1 = *reinterpret_cast<const float4*>(hb + 16 * part + 8 * c + 4);
         const float* u = v + 8 * c;
         // 0.5 acc + b/2 for two columns per packed fma.rn.f32x2 (each lane
         // rounded as fmaf would)
@@ -220,7 +228,7 @@ struct Engine {
         const float2 h1 = __ffma2_rn(make_float2(u[2], u[3]), half, make_float2(b0.z, b0.w));
         const float2 h2 = __ffma2_rn(make_float2(u[4], u[5]), half, make_float2(b1.x, b1.y));
         const float2 h3 = __ffma2_rn(make_float2(u[6], u[7]), half, make_float2(b1.z, b1.w));
-        put_chunk(4 * part + c, silu_half_bf16x2(pack_bf16x2(h0.x, h0.y)), silu_half_bf16x2(pack_bf16x2(h1.x, h1.y)),
+        put_chunk(2 * part + c, silu_half_bf16x2(pack_bf16x2(h0.x, h0.y)), silu_half_bf16x2(pack_bf16x2(h1.x, h1.y)),
                   silu_half_bf16x2(pack_bf16x2(h2.x, h2.y)), silu_half_bf16x2(pack_bf16x2(h3.x, h3.y)));
       }
     }
@@ -246,13 +254,15 @@ struct Engine {
   }
 };
 
-// CTAs of a persistent tensor-core kernel (TILE threads, SM_BYTES dynamic
-// shared memory) that fit on one SM at once, from the device's limits and the
-// kernel's register count; the TMEM columns bound it too.  (The occupancy
-// query of the runtime plans for the default shared-memory split and answers 1.)
+// CTAs of a persistent tensor-core kernel (Cta<HALVES>::THREADS threads,
+// Cta<HALVES>::SM_BYTES dynamic shared memory) that fit on one SM at once,
+// from the device's limits and the kernel's register count; the TMEM columns
+// bound it too.  (The occupancy query of the runtime plans for the default
+// shared-memory split and answers 1.)
 // Also returns the SM count.  0 on a runtime error.
-template <typename Kernel>
+template <int HALVES, typename Kernel>
 inline int resident_ctas(Kernel kern, int& sms) {
+  using C = Cta<HALVES>;
   int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 0, threads_sm = 0;
   cudaFuncAttributes fa;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return 0;
@@ -263,10 +273,10 @@ inline int resident_ctas(Kernel kern, int& sms) {
       cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess)
     return 0;
   const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;  // allocation unit: 256 registers per warp
-  int n = smem_sm / (SM_BYTES + reserved);
-  const int by_regs = regs_sm / (regs_warp * (TILE / 32));
-  const int by_threads = threads_sm / TILE;
-  const int by_tmem = 512 / int(TMEM_COLS);
+  int n = smem_sm / (C::SM_BYTES + reserved);
+  const int by_regs = regs_sm / (regs_warp * (C::THREADS / 32));
+  const int by_threads = threads_sm / C::THREADS;
+  const int by_tmem = 512 / int(C::TMEM_COLS);
   n = n < by_regs ? n : by_regs;
   n = n < by_threads ? n : by_threads;
   n = n < by_tmem ? n : by_tmem;
