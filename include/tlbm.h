@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 #define TLBM_API __attribute__((visibility("default")))
-#define TLBM_ABI_VERSION 2
+#define TLBM_ABI_VERSION 3
 
 typedef enum tlbm_status {
   TLBM_OK = 0,
@@ -72,13 +72,20 @@ typedef enum tlbm_collision {
 
 /* Boundary conditions applied by tlbm_step after the pull, in this order:
  *   obstacle force sample -> Zou/He inlet (x=0) -> Zou/He outlet (x=nx-1)
- *   -> full-way bounce-back on TLBM_FLAG_SOLID cells -> moving lid (y=ny-1).
+ *   -> far field -> full-way bounce-back on TLBM_FLAG_SOLID cells -> moving lid (y=ny-1).
  * This is the order of tensorlbm/d3q27_sphere_flow.py:246-256 and
  * benchmarks/verified/cavity_3d_full (collide, stream, walls, lid). */
 typedef enum tlbm_bc_bits {
   TLBM_BC_LID = 1u,        /* boundaries3d.py:324 / lid_driven_cavity.py:431 */
   TLBM_BC_ZH_INLET = 2u,   /* boundaries.py:50, boundaries3d.py:205, boundaries_d3q27.py:107 */
-  TLBM_BC_ZH_OUTLET = 4u   /* boundaries.py:102, boundaries3d.py:269, boundaries_d3q27.py:179 */
+  TLBM_BC_ZH_OUTLET = 4u,  /* boundaries.py:102, boundaries3d.py:269, boundaries_d3q27.py:179 */
+  /* free-stream far field (boundaries.py:199 far_field_bc_2d, boundaries3d.py:446
+   * far_field_bc_3d, boundaries_d3q27.py:63 far_field_bc_27): the x = 0 plane and
+   * the y = 0, y = ny-1 planes take feq(1, u_in); the x = nx-1 plane takes the
+   * post-stream populations of x = nx-2 (zero gradient; the lateral planes win on
+   * their edges).  Not with the Zou/He bits. */
+  TLBM_BC_FAR_FIELD = 8u,
+  TLBM_BC_FAR_FIELD_Z = 16u /* with TLBM_BC_FAR_FIELD, 3-D: the z = 0, z = nz-1 planes too */
 } tlbm_bc_bits;
 
 /* Per-cell flag byte. */
@@ -126,6 +133,9 @@ typedef struct tlbm_desc {
   const float* link_q;     /* (rows, Q) wall fraction of each link of the row, in (0, 1]; 0 = no link */
   double cm_s5, cm_s6;     /* cascaded D3Q27 5th / 6th-order rates; negative = omega_even (TensorLBM's
                               defaults) */
+  double ff_inlet_du[3];   /* TLBM_BC_FAR_FIELD: the x = 0 plane takes feq(1, u_in + ff_inlet_du) (a
+                              perturbation seeded at the inlet, benchmarks/verified/cylinder); 0 = none.
+                              New in ABI version 3. */
 } tlbm_desc;
 
 /* ---- fused time step ------------------------------------------------------
@@ -217,6 +227,15 @@ TLBM_API int tlbm_zou_he_inlet(int32_t lattice, int32_t dtype, int32_t nx, int32
  * (boundaries3d.py:269), zou_he_outlet_pressure_27 (boundaries_d3q27.py:179). */
 TLBM_API int tlbm_zou_he_outlet(int32_t lattice, int32_t dtype, int32_t nx, int32_t ny, int32_t nz,
                                 void* f, double rho_out, void* stream);
+
+/* Free-stream far field, in place: the x = 0 plane and the y = 0 / y = ny-1
+ * planes (and with z_faces != 0 in 3-D the z = 0 / z = nz-1 planes) take
+ * feq(1, (ux, uy, uz)), after the x = nx-1 plane took the values of x = nx-2.
+ * The obstacle bounce-back of the reference functions is tlbm_bounce_back.
+ * Replaces far_field_bc_2d (boundaries.py:199), far_field_bc_3d
+ * (boundaries3d.py:446) and far_field_bc_27 (boundaries_d3q27.py:63). */
+TLBM_API int tlbm_far_field(int32_t lattice, int32_t dtype, int32_t nx, int32_t ny, int32_t nz, void* f,
+                            double ux, double uy, double uz, int32_t z_faces, void* stream);
 
 /* Zou/He moving lid on the y = ny-1 plane (all cells, corners included), in place.
  * Replaces zou_he_moving_lid (lid_driven_cavity.py:431) and zou_he_moving_lid_3d

@@ -970,6 +970,52 @@ def cavity_step(f: np.ndarray, tau: float, wall: np.ndarray, u_lid: float, colli
     return moving_lid(f, u_lid)
 
 
+def far_field(f: np.ndarray, ux: float, uy: float = 0.0, uz: float = 0.0, z_faces: bool = True,
+              inlet_du=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Free-stream far field: boundaries.py:199-220 (D2Q9), boundaries3d.py:446-538
+    (D3Q19), boundaries_d3q27.py:63-104 (D3Q27).  feq(1, u) of the lattice's
+    equilibrium on the inlet plane, the outlet plane copied from x = nx-2, then
+    feq on the y planes (and the z planes with z_faces, 3-D).  inlet_du, the
+    seeding of benchmarks/verified/cylinder (run.py:104-113), overwrites the
+    inlet plane afterwards with feq(1, u + inlet_du)."""
+    q = f.shape[0]
+    dt = f.dtype
+    one = np.ones((1,) * (f.ndim - 1), dtype=dt)
+
+    def feq_of(vx, vy, vz):
+        return equilibrium(q, one, one * dt.type(vx), one * dt.type(vy), None if q == 9 else one * dt.type(vz))
+
+    e = feq_of(ux, uy, uz)
+    out = f.copy()
+    out[..., 0] = e[..., 0]
+    out[..., -1] = out[..., -2]
+    if q == 9:
+        out[:, 0, :] = e[:, 0, :]
+        out[:, -1, :] = e[:, 0, :]
+    else:
+        out[:, :, 0, :] = e[:, :, 0, :]
+        out[:, :, -1, :] = e[:, :, 0, :]
+        if z_faces:
+            out[:, 0, :, :] = e[:, 0, :, :]
+            out[:, -1, :, :] = e[:, 0, :, :]
+    if any(v != 0.0 for v in inlet_du):
+        out[..., 0] = feq_of(ux + inlet_du[0], uy + inlet_du[1], uz + inlet_du[2])[..., 0]
+    return out
+
+
+def far_field_step(f, tau, u_in, obstacle, collision="bgk", z_faces=True, inlet_du=(0.0, 0.0, 0.0), **kw):
+    """collide -> stream -> force -> far field -> bounce-back(obstacle), the chain
+    of benchmarks/verified/cylinder/re100/run.py:97-113 and of the 3-D far-field
+    runners (sphere_gridconv_re100_worker.py:150-160)."""
+    f = COLLIDERS[collision](f, tau, **kw)
+    f = stream(f)
+    force = obstacle_force(f, obstacle) if obstacle is not None else None
+    f = far_field(f, u_in, z_faces=z_faces, inlet_du=inlet_du)
+    if obstacle is not None:
+        f = bounce_back(f, obstacle)
+    return f, force
+
+
 def channel_step(f, tau, u_in, rho_out, wall, obstacle, collision="bgk", wall_u=None, **kw):
     """collide -> stream -> force -> Zou/He inlet -> outlet -> bounce-back(wall)
     -> bounce-back(obstacle): d3q27_sphere_flow.py:246-256, cylinder_flow.py:854-899.

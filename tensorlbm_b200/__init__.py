@@ -29,10 +29,11 @@ _PATCHES = {
     "cumulant": ["collide_cumulant_d3q27", "collide_cumulant_geier_d3q27", "collide_cumulant_d3q19"],
     "turbulence": ["collide_smagorinsky_bgk", "collide_smagorinsky_bgk3d", "collide_smagorinsky_bgk27"],
     "boundaries": ["cylinder_mask", "bounce_back_cells", "zou_he_inlet_velocity", "zou_he_outlet_pressure",
-                   "compute_obstacle_forces"],
+                   "compute_obstacle_forces", "far_field_bc_2d", "make_sponge_strength"],
     "boundaries3d": ["sphere_mask", "bounce_back_cells_3d", "zou_he_inlet_velocity_3d",
-                     "zou_he_outlet_pressure_3d", "zou_he_moving_lid_3d"],
-    "boundaries_d3q27": ["bounce_back_cells_27", "zou_he_inlet_velocity_27", "zou_he_outlet_pressure_27"],
+                     "zou_he_outlet_pressure_3d", "zou_he_moving_lid_3d", "far_field_bc_3d"],
+    "boundaries_d3q27": ["bounce_back_cells_27", "zou_he_inlet_velocity_27", "zou_he_outlet_pressure_27",
+                         "far_field_bc_27"],
     "lid_driven_cavity": ["zou_he_moving_lid"],
     "obstacles": ["compute_obstacle_forces_3d", "compute_obstacle_forces_27"],
     "boundary_registry": ["derive_missing_mask"],

@@ -26,7 +26,7 @@ F32, F64, F16_SHIFTED, BF16_SHIFTED, F16, BF16 = 0, 1, 2, 3, 4, 5
 (COLL_NONE, COLL_BGK, COLL_MRT, COLL_CUMULANT, COLL_CUMULANT_GEIER, COLL_CUMULANT_D3Q19, COLL_SMAGORINSKY, COLL_TRT,
  COLL_CASCADED, COLL_RLBM) = range(10)
 # tlbm_bc_bits / tlbm_flag_bits
-BC_LID, BC_ZH_INLET, BC_ZH_OUTLET = 1, 2, 4
+BC_LID, BC_ZH_INLET, BC_ZH_OUTLET, BC_FAR_FIELD, BC_FAR_FIELD_Z = 1, 2, 4, 8, 16
 FLAG_SOLID, FLAG_OBSTACLE, FLAG_HALFWAY, FLAG_MOVING, FLAG_CURVED = 1, 2, 4, 8, 16
 
 TORCH_TO_DTYPE = {torch.float32: F32, torch.float64: F64}
@@ -62,6 +62,7 @@ class Desc(ctypes.Structure):
         ("link_q", ctypes.c_void_p),
         ("cm_s5", ctypes.c_double),
         ("cm_s6", ctypes.c_double),
+        ("ff_inlet_du", ctypes.c_double * 3),
     ]
 
 
@@ -101,6 +102,7 @@ SIGNATURES: dict[str, list] = {
     "tlbm_zou_he_inlet": [_I32, _I32, _I32, _I32, _I32, _P, _D, _D, _D, _P, _P, _P],
     "tlbm_zou_he_outlet": [_I32, _I32, _I32, _I32, _I32, _P, _D, _P],
     "tlbm_moving_lid": [_I32, _I32, _I32, _I32, _I32, _P, _D, _P],
+    "tlbm_far_field": [_I32, _I32, _I32, _I32, _I32, _P, _D, _D, _D, _I32, _P],
     "tlbm_obstacle_force": [_I32, _I32, _I64, _P, _P, _P, _P],
     "tlbm_correct_mass": [_I32, _I64, _P, _P, _D, _P, _P],
     "tlbm_moment_sums": [_I32, _I32, _I64, _P, _P, _P],

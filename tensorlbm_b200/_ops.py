@@ -263,6 +263,21 @@ def moving_lid_(q: int, f: torch.Tensor, u_lid: float) -> torch.Tensor:
     return f
 
 
+def far_field_(q: int, f: torch.Tensor, ux: float, uy: float = 0.0, uz: float = 0.0,
+               z_faces: bool = True) -> torch.Tensor:
+    """Free-stream far field in place: inlet and lateral planes feq(1, u),
+    zero-gradient outlet (boundaries.py:199, boundaries3d.py:446, boundaries_d3q27.py:63)."""
+    dev = _lib.require_cuda(f)
+    nx, ny, nz = grid_of(f, q)
+    code = _lib.real_dtype(f)
+    if not f.is_contiguous():
+        raise ValueError("the far field works in place and needs a contiguous f")
+    st = _lib.load().tlbm_far_field(q, code, nx, ny, nz, f.data_ptr(), float(ux), float(uy), float(uz),
+                                    int(bool(z_faces)), _lib.stream_of(dev))
+    _lib.check(st, "far_field_bc")
+    return f
+
+
 def obstacle_force(q: int, f: torch.Tensor, mask: torch.Tensor) -> torch.Tensor:
     """(3,) float64 tensor 2 * sum_mask sum_q c_q f_q."""
     dev = _lib.require_cuda(f, mask)

@@ -53,5 +53,23 @@ def apply_zou_he_channel_boundaries(f, u_in, wall_mask, obstacle_mask):
     return bounce_back_cells(f, obstacle_mask)
 
 
+def far_field_bc_2d(f: torch.Tensor, u_in: float, obstacle_mask: torch.Tensor | None = None) -> torch.Tensor:
+    """Free-stream far field: feq(1, u_in, 0) on the inlet and both lateral
+    rows, zero-gradient outlet, then bounce-back in the obstacle; returns a new
+    tensor.  tensorlbm/boundaries.py:199."""
+    out = _ops.far_field_(9, f.clone(memory_format=torch.contiguous_format), u_in, 0.0, 0.0, False)
+    return out if obstacle_mask is None else _ops.bounce_back(9, out, obstacle_mask)
+
+
+def make_sponge_strength(ny: int, nx: int, x0: int, width: int, power: float = 2.0, device=None) -> torch.Tensor:
+    """Absorbing-layer strength sigma(x) = clamp((x - x0) / width, 0, 1) ** power
+    (float32, shape (ny, nx)); with collide_mrt's tau_field as
+    tau (1 + alpha sigma).  tensorlbm/boundaries.py:388."""
+    x = torch.arange(nx, device=device, dtype=torch.float32)
+    ramp = ((x - x0) / width).clamp(min=0.0, max=1.0) ** power
+    return ramp.view(1, nx).expand(ny, nx)
+
+
 __all__ = ["cylinder_mask", "make_channel_wall_mask", "bounce_back_cells", "zou_he_inlet_velocity",
-           "zou_he_outlet_pressure", "compute_obstacle_forces", "apply_zou_he_channel_boundaries"]
+           "zou_he_outlet_pressure", "compute_obstacle_forces", "apply_zou_he_channel_boundaries", "far_field_bc_2d",
+           "make_sponge_strength"]

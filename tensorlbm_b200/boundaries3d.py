@@ -65,5 +65,27 @@ def apply_zou_he_channel_boundaries_3d(f, u_in, wall_mask, obstacle_mask):
     return bounce_back_cells_3d(f, obstacle_mask)
 
 
+def far_field_bc_3d(f: torch.Tensor, u_in: float, obstacle_mask: torch.Tensor | None = None, uy: float = 0.0,
+                    uz: float = 0.0, bc_config: dict | None = None) -> torch.Tensor:
+    """Free-stream far field: feq(1, (u_in, uy, uz)) on the inlet and the lateral
+    planes, zero-gradient outlet, then bounce-back in the obstacle; returns a
+    new tensor.  bc_config selects the lateral planes like the reference:
+    far-field y planes and z planes each as a pair ("y-" with "y+", "z-" with
+    "z+"); a periodic inlet or outlet is not built.  tensorlbm/boundaries3d.py:446."""
+    z_faces = True
+    if bc_config is not None:
+        ff = set(bc_config.get("far_field_faces", []))
+        periodic = set(bc_config.get("periodic_faces", []))
+        y_planes = {"y-", "y+"} <= ff and not ({"y-", "y+"} & periodic)
+        z_pair = ff & {"z-", "z+"}
+        if {"x-", "x+"} & periodic or not y_planes or z_pair not in (set(), {"z-", "z+"}) or (z_pair & periodic):
+            raise NotImplementedError("far_field_bc_3d: the far field is built for both y planes, optionally both "
+                                      "z planes, with the inlet and the outlet")
+        z_faces = bool(z_pair)
+    out = _ops.far_field_(19, f.clone(memory_format=torch.contiguous_format), u_in, uy, uz, z_faces)
+    return out if obstacle_mask is None else _ops.bounce_back(19, out, obstacle_mask)
+
+
 __all__ = ["sphere_mask", "make_channel_wall_mask_3d", "bounce_back_cells_3d", "zou_he_inlet_velocity_3d",
-           "zou_he_outlet_pressure_3d", "zou_he_moving_lid_3d", "apply_zou_he_channel_boundaries_3d"]
+           "zou_he_outlet_pressure_3d", "zou_he_moving_lid_3d", "apply_zou_he_channel_boundaries_3d",
+           "far_field_bc_3d"]

@@ -111,7 +111,16 @@ int check_desc(const tlbm_desc* d) {
   if (d->collision == TLBM_COLL_TRT && !(d->tau > 0.5 && d->lambda_trt == d->lambda_trt)) return TLBM_ERR_ARG;
   if (d->collision == TLBM_COLL_CASCADED && !(d->tau > 0.5)) return TLBM_ERR_ARG;
   if ((d->bc & TLBM_BC_LID) && d->lattice == TLBM_D3Q27) return TLBM_ERR_UNSUPPORTED;
-  if (d->bc & ~(uint32_t)(TLBM_BC_LID | TLBM_BC_ZH_INLET | TLBM_BC_ZH_OUTLET)) return TLBM_ERR_ARG;
+  if (d->bc & ~(uint32_t)(TLBM_BC_LID | TLBM_BC_ZH_INLET | TLBM_BC_ZH_OUTLET | TLBM_BC_FAR_FIELD | TLBM_BC_FAR_FIELD_Z))
+    return TLBM_ERR_ARG;
+  if (d->bc & (TLBM_BC_FAR_FIELD | TLBM_BC_FAR_FIELD_Z)) {
+    // the far field owns the x planes; its z planes exist in 3-D only
+    if (!(d->bc & TLBM_BC_FAR_FIELD) || (d->bc & (TLBM_BC_ZH_INLET | TLBM_BC_ZH_OUTLET)) || d->nx < 3 ||
+        ((d->bc & TLBM_BC_FAR_FIELD_Z) && d->lattice == TLBM_D2Q9))
+      return TLBM_ERR_ARG;
+    for (int i = 0; i < 3; ++i)
+      if (!(d->ff_inlet_du[i] == d->ff_inlet_du[i]) || !(d->u_in[i] == d->u_in[i])) return TLBM_ERR_ARG;
+  }
   if (d->force_lin != 0.0) {
     if (!(d->force_lin == d->force_lin) || d->force_lin <= -1.0 || d->force_lin >= 1.0) return TLBM_ERR_ARG;
     if (d->collision != TLBM_COLL_BGK && d->collision != TLBM_COLL_MRT && d->collision != TLBM_COLL_SMAGORINSKY &&
@@ -143,6 +152,9 @@ int check_aa(const tlbm_desc* d) {
   const int st = check_desc(d);
   if (st != TLBM_OK) return st;
   if (d->link_q || d->link_row || d->wall_velocity) return TLBM_ERR_UNSUPPORTED;
+  // the far field's zero-gradient outlet reads the neighbour's post-stream
+  // values, which the in-place AA steps do not keep
+  if (d->bc & TLBM_BC_FAR_FIELD) return TLBM_ERR_UNSUPPORTED;
   if (d->dtype != TLBM_F32 && d->dtype != TLBM_F16_SHIFTED && d->dtype != TLBM_BF16_SHIFTED) return TLBM_ERR_DTYPE;
   return TLBM_OK;
 }
@@ -177,6 +189,8 @@ TLBM_API int tlbm_step_planes(const tlbm_desc* d, const void* f_in, void* f_out,
   if (!f_in || !f_out) return TLBM_ERR_ARG;
   if (f_in == f_out) return TLBM_ERR_ALIAS;
   if (z_begin < 0 || z_count < 1 || (long long)z_begin + z_count > d->nz) return TLBM_ERR_SHAPE;
+  // z planes of a slab are not the domain's z faces
+  if (d->bc & TLBM_BC_FAR_FIELD_Z) return TLBM_ERR_UNSUPPORTED;
   StepParams p = make_params(*d, f_in, f_out, flags, tau_field, force, status);
   p.z0 = z_begin;
   p.z_count = z_count;
@@ -275,6 +289,27 @@ TLBM_API int tlbm_moving_lid(int32_t lattice, int32_t dtype, int32_t nx, int32_t
   if (lattice == TLBM_D2Q9)
     return f64 ? op_moving_lid<D2Q9, double>(nx, ny, nz, f, u_lid, s) : op_moving_lid<D2Q9, float>(nx, ny, nz, f, u_lid, s);
   return f64 ? op_moving_lid<D3Q19, double>(nx, ny, nz, f, u_lid, s) : op_moving_lid<D3Q19, float>(nx, ny, nz, f, u_lid, s);
+}
+
+TLBM_API int tlbm_far_field(int32_t lattice, int32_t dtype, int32_t nx, int32_t ny, int32_t nz, void* f,
+                            double ux, double uy, double uz, int32_t z_faces, void* stream) {
+  if (!valid_lattice(lattice)) return TLBM_ERR_UNSUPPORTED;
+  if (!shape_ok(lattice, nx, ny, nz) || nx < 2) return TLBM_ERR_SHAPE;
+  if (!f) return TLBM_ERR_ARG;
+  if (dtype != TLBM_F32 && dtype != TLBM_F64) return TLBM_ERR_DTYPE;
+  const bool f64 = dtype == TLBM_F64, zf = z_faces != 0 && lattice != TLBM_D2Q9;
+  cudaStream_t s = as_stream(stream);
+  switch (lattice) {
+    case TLBM_D2Q9:
+      return f64 ? op_far_field<D2Q9, double>(nx, ny, nz, f, ux, uy, uz, zf, s)
+                 : op_far_field<D2Q9, float>(nx, ny, nz, f, ux, uy, uz, zf, s);
+    case TLBM_D3Q19:
+      return f64 ? op_far_field<D3Q19, double>(nx, ny, nz, f, ux, uy, uz, zf, s)
+                 : op_far_field<D3Q19, float>(nx, ny, nz, f, ux, uy, uz, zf, s);
+    default:
+      return f64 ? op_far_field<D3Q27, double>(nx, ny, nz, f, ux, uy, uz, zf, s)
+                 : op_far_field<D3Q27, float>(nx, ny, nz, f, ux, uy, uz, zf, s);
+  }
 }
 
 TLBM_API int tlbm_obstacle_force(int32_t lattice, int32_t dtype, int64_t ncells, const void* f, const uint8_t* mask,

@@ -113,6 +113,35 @@ __global__ void k_zou_he_outlet(int nx, int ny, int nz, T* f, BcParams<T> bp) {
     if (L::cx(q) < 0) f[(long long)q * n + cell] = v[q];
 }
 
+// Free-stream far field, one thread per (y, z) row: a lateral row (y = 0,
+// ny-1; with zf also z = 0, nz-1) takes feq(1, u) everywhere; any other row
+// takes it at x = 0 and copies x = nx-2 to x = nx-1 (zero gradient).  Lateral
+// rows win on the outlet edges, as in boundaries3d.py:515-538.
+template <class L, typename T>
+__global__ void k_far_field(int nx, int ny, int nz, T* f, T ux, T uy, T uz, bool zf) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // (z, y) index
+  if (j >= (long long)ny * nz) return;
+  const long long n = (long long)nx * ny * nz;
+  const int y = (int)(j % ny);
+  const int z = (int)(j / ny);
+  const long long row = j * nx;
+  T v[L::Q];
+  far_field_feq<L>(v, ux, uy, uz);
+  const bool lateral = y == 0 || y == ny - 1 || (zf && (z == 0 || z == nz - 1));
+  if (lateral) {
+    for (int x = 0; x < nx; ++x) {
+#pragma unroll
+      for (int q = 0; q < L::Q; ++q) f[(long long)q * n + row + x] = v[q];
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+      f[(long long)q * n + row] = v[q];
+      f[(long long)q * n + row + nx - 1] = f[(long long)q * n + row + nx - 2];
+    }
+  }
+}
+
 template <class L, typename T>
 __global__ void k_moving_lid(int nx, int ny, int nz, T* f, T u_lid) {
   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // (z, x) index
@@ -392,6 +421,12 @@ int op_zou_he_outlet(int nx, int ny, int nz, void* f, double rho_out, cudaStream
   return launch_status();
 }
 template <class L, typename T>
+int op_far_field(int nx, int ny, int nz, void* f, double ux, double uy, double uz, bool z_faces, cudaStream_t s) {
+  k_far_field<L, T><<<blocks_for((long long)ny * nz), kThreads, 0, s>>>(nx, ny, nz, (T*)f, T(ux), T(uy), T(uz),
+                                                                        z_faces);
+  return launch_status();
+}
+template <class L, typename T>
 int op_moving_lid(int nx, int ny, int nz, void* f, double u_lid, cudaStream_t s) {
   k_moving_lid<L, T><<<blocks_for((long long)nx * nz), kThreads, 0, s>>>(nx, ny, nz, (T*)f, T(u_lid));
   return launch_status();
@@ -478,6 +513,12 @@ template int op_moving_wall<D2Q9, float>(long long, const void*, const uint8_t*,
 template int op_moving_wall<D2Q9, double>(long long, const void*, const uint8_t*, const void*, void*, cudaStream_t);
 template int op_moving_wall<D3Q19, float>(long long, const void*, const uint8_t*, const void*, void*, cudaStream_t);
 template int op_moving_wall<D3Q19, double>(long long, const void*, const uint8_t*, const void*, void*, cudaStream_t);
+template int op_far_field<D2Q9, float>(int, int, int, void*, double, double, double, bool, cudaStream_t);
+template int op_far_field<D2Q9, double>(int, int, int, void*, double, double, double, bool, cudaStream_t);
+template int op_far_field<D3Q19, float>(int, int, int, void*, double, double, double, bool, cudaStream_t);
+template int op_far_field<D3Q19, double>(int, int, int, void*, double, double, double, bool, cudaStream_t);
+template int op_far_field<D3Q27, float>(int, int, int, void*, double, double, double, bool, cudaStream_t);
+template int op_far_field<D3Q27, double>(int, int, int, void*, double, double, double, bool, cudaStream_t);
 template int op_moving_lid<D2Q9, float>(int, int, int, void*, double, cudaStream_t);
 template int op_moving_lid<D2Q9, double>(int, int, int, void*, double, cudaStream_t);
 template int op_moving_lid<D3Q19, float>(int, int, int, void*, double, cudaStream_t);

@@ -21,6 +21,8 @@ int op_zou_he_outlet(int nx, int ny, int nz, void* f, double rho_out, cudaStream
 template <class L, typename T>
 int op_moving_lid(int nx, int ny, int nz, void* f, double u_lid, cudaStream_t s);
 template <class L, typename T>
+int op_far_field(int nx, int ny, int nz, void* f, double ux, double uy, double uz, bool z_faces, cudaStream_t s);
+template <class L, typename T>
 int op_obstacle_force(long long n, const void* f, const uint8_t* mask, double* out, cudaStream_t s);
 template <class L, typename S>
 int op_moment_sums(long long n, const void* f, double* out, cudaStream_t s);

@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(256) k_step_aa(StepParams p, CollideParams<typ
       accumulate_force(d.force, __any_sync(0xffffffffu, ob), mx, my, mz);
     }
     double ux = 0.0, uy = 0.0, uz = 0.0;  // no Bouzidi links in the AA pattern
-    if (active) apply_boundaries<L, T, SI, SO, false>(d, x, y, cell, fl, f, bp, ux, uy, uz);
+    if (active) apply_boundaries<L, T, SI, SO, false>(d, x, y, z, cell, fl, f, bp, ux, uy, uz);
   }
   if (!active) return;
   relax<L, SI, SO, COLL, FORCED>(d, cell, fl, f, cp);
@@ -210,8 +210,8 @@ __device__ __forceinline__ void step_aa_x2(const StepParams& p, const CollidePar
                          packed_collision<L, COLL, Storage<S>::kFast>();
   if (!uniform_edge_branch<L, COLL>() || edge) {
     double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-    apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-    apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
     relax_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fla, flb, fa, fb, cp);
   } else {
     relax_interior_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fa, fb, cp);

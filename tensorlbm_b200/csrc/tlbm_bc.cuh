@@ -59,10 +59,13 @@ template <typename T> struct BcParams {
   T u_lid;
   // D2Q9 closed forms use python-side products with rho_out
   T two_thirds_rho_out, sixth_rho_out;
+  T ff_u[3];                // far field: free-stream velocity of the lateral planes (= u_in)
+  T ff_in[3];               // far field: velocity of the x = 0 plane (u_in + the inlet perturbation)
 };
 
 template <typename T>
-__host__ __device__ BcParams<T> make_bc_params(double u_in0, double u_in1, double u_in2, double rho_out, double u_lid) {
+__host__ __device__ BcParams<T> make_bc_params(double u_in0, double u_in1, double u_in2, double rho_out, double u_lid,
+                                               const double* ff_inlet_du = nullptr) {
   BcParams<T> b;
   b.u_in = T(u_in0);
   b.uy_in = T(u_in1);
@@ -72,7 +75,22 @@ __host__ __device__ BcParams<T> make_bc_params(double u_in0, double u_in1, doubl
   b.u_lid = T(u_lid);
   b.two_thirds_rho_out = T((2.0 / 3.0) * rho_out);
   b.sixth_rho_out = T((1.0 / 6.0) * rho_out);
+  const double u[3] = {u_in0, u_in1, u_in2};
+  for (int i = 0; i < 3; ++i) {
+    b.ff_u[i] = T(u[i]);
+    b.ff_in[i] = T(ff_inlet_du ? u[i] + ff_inlet_du[i] : u[i]);
+  }
   return b;
+}
+
+// Free-stream far field (boundaries.py:199-220, boundaries3d.py:446-538,
+// boundaries_d3q27.py:63-104): f = feq(1, u) of the lattice's equilibrium
+// function, bit for bit (rho = 1 exactly).
+template <class L, typename T>
+__device__ __forceinline__ void far_field_feq(T (&f)[L::Q], T ux, T uy, T uz) {
+  const T usq = usq_of<L>(ux, uy, uz);
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) f[q] = feq_q<L>(q, T(1), ux, uy, uz, usq);
 }
 
 // Known population paired with unknown q by the x-face Zou/He conditions.

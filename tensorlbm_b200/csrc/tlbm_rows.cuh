@@ -197,7 +197,7 @@ __device__ __forceinline__ void step_rows(const StepParams& p, const CollidePara
       }
       if (issued_ok) issue(issued++);
     }
-    pair_finish<L, S, COLL, false>(d, cp, bp, x, y, c, true, fa, fb, fl2);
+    pair_finish<L, S, COLL, false>(d, cp, bp, x, y, z, c, true, fa, fb, fl2);
     if (!__all_sync(0xffffffffu, issued_ok)) {
       ok = false;
       ++j;

@@ -33,6 +33,14 @@
 #ifndef TLBM_MINB_AA_MRT
 #define TLBM_MINB_AA_MRT 0
 #endif
+// threads per block of the D3Q19 MRT pair kernel on half storage, and its
+// resident blocks per SM at that size
+#ifndef TLBM_MRT_HALF_THREADS
+#define TLBM_MRT_HALF_THREADS 128
+#endif
+#ifndef TLBM_MINB_MRT_HALF_SMALL
+#define TLBM_MINB_MRT_HALF_SMALL 5
+#endif
 
 namespace tlbm {
 
@@ -125,14 +133,16 @@ __device__ __forceinline__ void curved_links(const Domain<SI, SO>& d, long long 
 }
 
 // Boundary conditions of one cell after the pull, in TensorLBM's order:
-// Zou/He inlet / outlet planes, full-way (or moving-wall) bounce-back or the
-// Bouzidi links of a curved wall, lid.  (mx, my, mz) collect the BFL force.
-// kCurved = false compiles the Bouzidi links out (the two-cells-per-thread
-// kernel, which never runs with link tables).
+// Zou/He inlet / outlet planes, the far field, full-way (or moving-wall)
+// bounce-back or the Bouzidi links of a curved wall, lid.  (mx, my, mz)
+// collect the BFL force.  kCurved = false compiles the Bouzidi links out (the
+// two-cells-per-thread kernel, which never runs with link tables).  The far
+// field's zero-gradient outlet is the caller's: the x = nx-1 cell holds the
+// post-stream populations of x = nx-2 when it gets here.
 template <class L, typename T, typename SI, typename SO, bool kCurved = true>
-__device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x, int y, long long cell, uint8_t fl,
-                                                 T (&f)[L::Q], const BcParams<T>& bp, double& mx, double& my,
-                                                 double& mz) {
+__device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x, int y, int z, long long cell,
+                                                 uint8_t fl, T (&f)[L::Q], const BcParams<T>& bp, double& mx,
+                                                 double& my, double& mz) {
   constexpr int Q = L::Q;
   const long long N = d.n;
   // Zou/He inlet / outlet planes
@@ -143,6 +153,15 @@ __device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x,
   if ((d.bc & TLBM_BC_ZH_OUTLET) && x == d.nx - 1) {
     if constexpr (Q == 9) zou_he_outlet_d2q9(f, bp.rho_out, bp.two_thirds_rho_out, bp.sixth_rho_out);
     else zou_he_outlet_3d<L>(f, bp.rho_out);
+  }
+  // far field: inlet plane, then the lateral planes (which win on the edges
+  // of the outlet plane)
+  if (d.bc & TLBM_BC_FAR_FIELD) {
+    if (x == 0) {
+      far_field_feq<L>(f, bp.ff_in[0], bp.ff_in[1], bp.ff_in[2]);
+    } else if (y == 0 || y == d.ny - 1 || ((d.bc & TLBM_BC_FAR_FIELD_Z) && (z == 0 || z == d.nz - 1))) {
+      far_field_feq<L>(f, bp.ff_u[0], bp.ff_u[1], bp.ff_u[2]);
+    }
   }
   // full-way bounce-back; Ladd moving wall where flagged.  A moving obstacle
   // cell that is also a wall cell has SOLID cleared (wall XOR obstacle): it
@@ -232,6 +251,26 @@ __device__ __forceinline__ void relax_fluid(const Domain<SI, SO>& d, long long c
 // PULL = false: local collide / format conversion only (no boundaries)
 // FORCED: add the exact-difference linear force after the collision (a
 // separate instantiation, so that the unforced kernels carry none of it)
+// Periodic pull of cell (x, y, z): f[q] = f_in[q, (x, y, z) - c_q]
+template <class L, typename SI, typename SO, typename T>
+__device__ __forceinline__ void pull_cell(const Domain<SI, SO>& d, int x, int y, int z, T (&f)[L::Q]) {
+  const long long N = d.n;
+  const int xm = (x == 0) ? d.nx - 1 : x - 1;
+  const int xp = (x == d.nx - 1) ? 0 : x + 1;
+  const int ym = (y == 0) ? d.ny - 1 : y - 1;
+  const int yp = (y == d.ny - 1) ? 0 : y + 1;
+  const int zm = (z == 0) ? d.nz - 1 : z - 1;
+  const int zp = (z == d.nz - 1) ? 0 : z + 1;
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    const int sx = L::cx(q) > 0 ? xm : (L::cx(q) < 0 ? xp : x);
+    const int sy = L::cy(q) > 0 ? ym : (L::cy(q) < 0 ? yp : y);
+    const int sz = L::cz(q) > 0 ? zm : (L::cz(q) < 0 ? zp : z);
+    const long long src = (long long)sz * d.plane + (long long)sy * d.nx + sx;
+    f[q] = Storage<SI>::load(ldg(d.fin + (long long)q * N + src), weight<L, T>(q));
+  }
+}
+
 template <class L, typename SI, typename SO, int COLL, bool PULL, bool FORCED = false>
 __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int y, int z, bool active,
                                             const CollideParams<typename Storage<SI>::T>& cp,
@@ -247,21 +286,7 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
   uint8_t fl = 0;
   if (active) {
     if constexpr (PULL) {
-      const int xm = (x == 0) ? d.nx - 1 : x - 1;
-      const int xp = (x == d.nx - 1) ? 0 : x + 1;
-      const int ym = (y == 0) ? d.ny - 1 : y - 1;
-      const int yp = (y == d.ny - 1) ? 0 : y + 1;
-      const int zm = (z == 0) ? d.nz - 1 : z - 1;
-      const int zp = (z == d.nz - 1) ? 0 : z + 1;
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        // source = cell - c_q
-        const int sx = L::cx(q) > 0 ? xm : (L::cx(q) < 0 ? xp : x);
-        const int sy = L::cy(q) > 0 ? ym : (L::cy(q) < 0 ? yp : y);
-        const int sz = L::cz(q) > 0 ? zm : (L::cz(q) < 0 ? zp : z);
-        const long long src = (long long)sz * d.plane + (long long)sy * d.nx + sx;
-        f[q] = Storage<SI>::load(ldg(fin + (long long)q * N + src), weight<L, T>(q));
-      }
+      pull_cell<L>(d, x, y, z, f);
     } else {
 #pragma unroll
       for (int q = 0; q < Q; ++q) f[q] = Storage<SI>::load(fin[(long long)q * N + cell], weight<L, T>(q));
@@ -277,9 +302,12 @@ __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int 
       if (ob) cell_momentum<L>(f, mx, my, mz);
       accumulate_force(d.force, __any_sync(0xffffffffu, ob), mx, my, mz);
     }
+    // far field: the outlet plane takes the post-stream populations of x = nx-2
+    // (after the force sample, as far_field_bc_* follows compute_obstacle_forces)
+    if ((d.bc & TLBM_BC_FAR_FIELD) && active && x == d.nx - 1) pull_cell<L>(d, d.nx - 2, y, z, f);
     // boundaries; the ledger of Bouzidi links is reduced on its own
     double bx = 0.0, by = 0.0, bz = 0.0;
-    if (active) apply_boundaries<L>(d, x, y, cell, fl, f, bp, bx, by, bz);
+    if (active) apply_boundaries<L>(d, x, y, z, cell, fl, f, bp, bx, by, bz);
     if (d.force && d.link_q)
       accumulate_force(d.force, __any_sync(0xffffffffu, active && (fl & TLBM_FLAG_CURVED)), bx, by, bz, 1.0);
   }
@@ -486,7 +514,7 @@ __host__ __device__ constexpr bool pair_deviation_form() {
 
 template <class L, typename S, int COLL, bool FORCED>
 __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const CollideParams<typename Storage<S>::T>& cp,
-                                            const BcParams<typename Storage<S>::T>& bp, int x, int y, int c,
+                                            const BcParams<typename Storage<S>::T>& bp, int x, int y, int z, int c,
                                             bool active, typename Storage<S>::T (&fa)[L::Q],
                                             typename Storage<S>::T (&fb)[L::Q], uint32_t fl2);
 
@@ -541,7 +569,7 @@ __device__ __forceinline__ void pair_update(const Domain<S, S>& d, const Collide
     }
     if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));
   }
-  pair_finish<L, S, COLL, FORCED>(d, cp, bp, x, y, c, active, fa, fb, fl2);
+  pair_finish<L, S, COLL, FORCED>(d, cp, bp, x, y, z, c, active, fa, fb, fl2);
 }
 
 template <class L, typename S, int COLL, bool FORCED = false>
@@ -560,7 +588,7 @@ __device__ __forceinline__ void step_x2(const StepParams& p, const CollideParams
 // and the edge test are warp-wide).
 template <class L, typename S, int COLL, bool FORCED>
 __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const CollideParams<typename Storage<S>::T>& cp,
-                                            const BcParams<typename Storage<S>::T>& bp, int x, int y, int c,
+                                            const BcParams<typename Storage<S>::T>& bp, int x, int y, int z, int c,
                                             bool active, typename Storage<S>::T (&fa)[L::Q],
                                             typename Storage<S>::T (&fb)[L::Q], uint32_t fl2) {
   using T = typename Storage<S>::T;
@@ -578,7 +606,10 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
   // whether any lane of the warp has a flagged cell or sits on a plane with a
   // condition: warps of the interior then skip all boundary code on a
   // warp-uniform branch
-  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || ((d.bc & TLBM_BC_ZH_INLET) && x == 0) ||
+  const bool far = (d.bc & TLBM_BC_FAR_FIELD) &&
+                   (x == 0 || x + 2 == nx || y == 0 || y == ny - 1 ||
+                    ((d.bc & TLBM_BC_FAR_FIELD_Z) && (z == 0 || z == d.nz - 1)));
+  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || far || ((d.bc & TLBM_BC_ZH_INLET) && x == 0) ||
                                                        ((d.bc & TLBM_BC_ZH_OUTLET) && x + 2 == nx) ||
                                                        ((d.bc & TLBM_BC_LID) && y == ny - 1)));
   if constexpr (kDev) {
@@ -609,17 +640,23 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
     accumulate_force(d.force, __any_sync(0xffffffffu, oa || ob), mx, my, mz);
   }
   if (!active) return;
+  // far field: the outlet cell x + 1 = nx - 1 takes the post-stream
+  // populations of its pair partner x = nx - 2 (after the force sample)
+  if ((d.bc & TLBM_BC_FAR_FIELD) && x + 2 == nx) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) fb[q] = fa[q];
+  }
   if constexpr (!uniform_edge_branch<L, COLL>()) {
     double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-    apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-    apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
     relax_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fla, flb, fa, fb, cp);
   } else if constexpr (kDev) {
     bool keep_a = false, keep_b = false;   // half-way wall cells: reversed, not collided
     if (edge) {
       double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-      apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-      apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+      apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+      apply_boundaries<L, T, S, S, false>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
       if (fla & TLBM_FLAG_HALFWAY) {
         bounce_back<L>(fa);
         keep_a = true;
@@ -643,8 +680,8 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
     }
   } else if (edge) {
     double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-    apply_boundaries<L, T, S, S, false>(d, x, y, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-    apply_boundaries<L, T, S, S, false>(d, x + 1, y, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
     relax_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fla, flb, fa, fb, cp);
   } else {
     relax_interior_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fa, fb, cp);   // no flag in the warp
@@ -683,11 +720,25 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
                                                  BcParams<typename Storage<S>::T> bp) {
   step_x2<L, S, COLL, FORCED>(p, cp, bp);
 }
-// the same kernel compiled for MINB resident blocks per SM
-template <class L, typename S, int COLL, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_step_x2_capped(StepParams p, CollideParams<typename Storage<S>::T> cp,
-                                                               BcParams<typename Storage<S>::T> bp) {
+// the same kernel compiled for blocks of NT threads, MINB resident per SM
+template <class L, typename S, int COLL, int MINB, int NT = 256>
+__global__ void __launch_bounds__(NT, MINB) k_step_x2_capped(StepParams p, CollideParams<typename Storage<S>::T> cp,
+                                                              BcParams<typename Storage<S>::T> bp) {
   step_x2<L, S, COLL, false>(p, cp, bp);
+}
+
+// Block size of the pair kernel, and its resident blocks per SM (0: no cap).
+// The D3Q19 MRT on half storage runs blocks of 128: five of them per SM give
+// 96 registers and no spills, where three blocks of 256 (80 registers) spill
+// 128 bytes per thread.
+template <class L, typename S, int COLL>
+__host__ __device__ constexpr int x2_threads() {
+  constexpr bool shifted = std::is_same<S, __half>::value || std::is_same<S, __nv_bfloat16>::value;
+  return (L::Q == 19 && COLL == TLBM_COLL_MRT && shifted) ? TLBM_MRT_HALF_THREADS : 256;
+}
+template <class L, typename S, int COLL>
+__host__ __device__ constexpr int x2_launch_blocks() {
+  return x2_threads<L, S, COLL>() == 256 ? x2_min_blocks<L, S, COLL>() : TLBM_MINB_MRT_HALF_SMALL;
 }
 
 }  // namespace tlbm
@@ -706,10 +757,10 @@ inline bool pair_layout_ok(const StepParams& p) {
          (p.flags == nullptr || al(p.flags, 2));
 }
 
-inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block) {
+inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block, int threads = 256) {
   int bx = 32;
-  while (bx < nx && bx < 256) bx <<= 1;
-  int by = 256 / bx;
+  while (bx < nx && bx < threads) bx <<= 1;
+  int by = threads / bx;
   block = dim3(bx, by, 1);
   grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
 }
@@ -725,7 +776,7 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   if (d.collision == TLBM_COLL_TRT) set_trt_rates(cp, d.tau, d.lambda_trt);
   if (d.cm_s5 >= 0.0) cp.cm_s5 = T(d.cm_s5);
   if (d.cm_s6 >= 0.0) cp.cm_s6 = T(d.cm_s6);
-  const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid);
+  const BcParams<T> bp = make_bc_params<T>(d.u_in[0], d.u_in[1], d.u_in[2], d.rho_out, d.u_lid, d.ff_inlet_du);
   // the forced instantiations stay on one cell per thread: two cells with
   // the pre-collision moments held for the force need 121 registers (2 blocks
   // per SM) and ran slower than k_step (26.8 against 28.0 GLUPS, forced
@@ -734,9 +785,10 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
     int st = TLBM_OK;
     if (launch_rows<L, SI, COLL>(p, cp, bp, s, st)) return st;
     if (pair_layout_ok<L, SI>(p)) {
-      step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block);
-      constexpr int minb = x2_min_blocks<L, SI, COLL>();
-      if constexpr (minb > 0) k_step_x2_capped<L, SI, COLL, minb><<<grid, block, 0, s>>>(p, cp, bp);
+      constexpr int nt = x2_threads<L, SI, COLL>();
+      step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block, nt);
+      constexpr int minb = x2_launch_blocks<L, SI, COLL>();
+      if constexpr (minb > 0) k_step_x2_capped<L, SI, COLL, minb, nt><<<grid, block, 0, s>>>(p, cp, bp);
       else k_step_x2<L, SI, COLL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
       return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
     }

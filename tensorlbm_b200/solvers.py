@@ -75,6 +75,11 @@ class StepConfig:
     lambda_trt: float = 3.0 / 16.0   # TRT magic parameter (solver.py:440)
     cm_s5: float | None = None       # cascaded D3Q27 5th / 6th-order rates (None: omega_even)
     cm_s6: float | None = None
+    # free-stream far field at velocity u_in (boundaries.py:199, boundaries3d.py:446,
+    # boundaries_d3q27.py:63): None, "y" (inlet, outlet and the y planes) or "yz"
+    # (3-D: the z planes too, the reference's default)
+    far_field: str | None = None
+    inlet_du: tuple[float, float, float] = (0.0, 0.0, 0.0)  # far field: extra velocity of the x = 0 plane
     extra: dict = field(default_factory=dict)
 
     @property
@@ -93,8 +98,16 @@ class StepConfig:
         if self.u_lid is not None:
             bc |= _lib.BC_LID
         if self.u_in is not None:
-            bc |= _lib.BC_ZH_INLET
             u_in = (float(self.u_in), 0.0, 0.0) if isinstance(self.u_in, (int, float)) else tuple(self.u_in)
+            if self.far_field is None:
+                bc |= _lib.BC_ZH_INLET
+        if self.far_field is not None:
+            if self.far_field not in ("y", "yz") or (self.far_field == "yz" and q == 9):
+                allowed = "'y'" if q == 9 else "'y' or 'yz'"
+                raise ValueError(f"far_field must be {allowed}, got {self.far_field!r}")
+            if self.u_in is None or self.rho_out is not None:
+                raise ValueError("the far field takes u_in (its free-stream velocity) and no Zou/He rho_out")
+            bc |= _lib.BC_FAR_FIELD | (_lib.BC_FAR_FIELD_Z if self.far_field == "yz" else 0)
         if self.rho_out is not None:
             bc |= _lib.BC_ZH_OUTLET
         coll = COLLISIONS[collision or self.collision]
@@ -108,6 +121,7 @@ class StepConfig:
             rho_out=1.0 if self.rho_out is None else self.rho_out, lambda_trt=self.lambda_trt,
             cm_s5=self.cm_s5, cm_s6=self.cm_s6,
         )
+        d.ff_inlet_du[0], d.ff_inlet_du[1], d.ff_inlet_du[2] = (float(v) for v in self.inlet_du)
         if coll in (_lib.COLL_BGK, _lib.COLL_MRT, _lib.COLL_SMAGORINSKY):
             d.force_lin = float(self.force_lin)
         elif self.force_lin and coll != _lib.COLL_NONE:
@@ -132,6 +146,9 @@ class LBMSolver:
         wall_mask, obstacle_mask: bool fields; both bounce back, only the
             obstacle enters the momentum-exchange force.
         u_lid, u_in, rho_out: enable the lid / Zou-He inlet / outlet planes.
+        far_field: "y" or "yz" (3-D) with u_in: the free-stream far field of
+            far_field_bc_2d / far_field_bc_3d / far_field_bc_27 instead of Zou/He;
+            ``set_inlet_perturbation`` seeds the inlet plane.
         tau_field: optional per-cell tau (BGK and MRT shear rate).
         track_force: record the float64 force of every step.
         curved_wall: a :class:`tensorlbm_b200.bfl.CurvedWall` (Bouzidi links of a
@@ -196,9 +213,10 @@ class LBMSolver:
         full = (q,) + shape
         if pattern not in ("ab", "aa"):
             raise ValueError(f"pattern must be 'ab' (two buffers) or 'aa' (one buffer, in place), got {pattern!r}")
-        if pattern == "aa" and (self.curved is not None or storage == "f64" or self.wall_u is not None):
+        if pattern == "aa" and (self.curved is not None or storage == "f64" or self.wall_u is not None or
+                                self.cfg.far_field is not None):
             raise NotImplementedError("the AA pattern supports f32 / f16 / bf16 storage without curved or "
-                                      "moving walls")
+                                      "moving walls or the far field")
         self.pattern = pattern
         # two buffers (index of the current one in _cur), or one AA buffer
         # (its layout in _cur: 0 swapped, 1 natural)
@@ -327,6 +345,17 @@ class LBMSolver:
         if self.pattern == "aa":
             return 1 if c == 0 else 0   # loaded / natural -> swapped, swapped -> natural
         return c ^ 1
+
+    def set_inlet_perturbation(self, dux: float = 0.0, duy: float = 0.0, duz: float = 0.0) -> "LBMSolver":
+        """Far field: the x = 0 plane takes feq(1, u_in + (dux, duy, duz)) from the
+        next step on, as benchmarks/verified/cylinder seeds its wake (drops the
+        captured graph)."""
+        if self.cfg.far_field is None:
+            raise ValueError("the inlet perturbation belongs to the far field (far_field='y' or 'yz')")
+        self.cfg.inlet_du = (float(dux), float(duy), float(duz))
+        self._desc = self._attach(self.cfg.desc(self.code))
+        self._graph = None
+        return self
 
     def set_force_lin(self, a: float) -> "LBMSolver":
         """Change the linear body force A of F = A rho u (drops the captured graph)."""

@@ -150,6 +150,36 @@ def rlbm(torch) -> None:
     print("wrote collide_rlbm.npz")
 
 
+def far_field(torch) -> None:
+    """Free-stream far field (boundaries.py:199, boundaries3d.py:446 with and
+    without a y-only bc_config, boundaries_d3q27.py:63) on seeded fields with a
+    small obstacle, float32 and float64, and the sponge strength of
+    boundaries.py:388."""
+    from tensorlbm.boundaries import far_field_bc_2d, make_sponge_strength
+    from tensorlbm.boundaries3d import far_field_bc_3d
+    from tensorlbm.boundaries_d3q27 import far_field_bc_27
+
+    out = {}
+    for dt, tag in ((torch.float32, "f32"), (torch.float64, "f64")):
+        _, _, f9 = near_eq_field(torch, 9, (8, 16), dt, 41)
+        _, _, f19 = near_eq_field(torch, 19, (4, 6, 8), dt, 43)
+        _, _, f27 = near_eq_field(torch, 27, (4, 6, 8), dt, 47)
+        ob9 = torch.zeros((8, 16), dtype=torch.bool)
+        ob9[3:5, 6:8] = True
+        ob3 = torch.zeros((4, 6, 8), dtype=torch.bool)
+        ob3[1:3, 2:4, 3:5] = True
+        cfg_y = {"far_field_faces": ["y-", "y+"], "periodic_faces": ["z-", "z+"]}
+        out.update({f"f9_{tag}": f9, f"ff9_{tag}": far_field_bc_2d(f9, 0.07, ob9),
+                    f"f19_{tag}": f19, f"ff19_{tag}": far_field_bc_3d(f19, 0.06, ob3),
+                    f"ff19y_{tag}": far_field_bc_3d(f19, 0.06, None, bc_config=cfg_y),
+                    f"ff19uv_{tag}": far_field_bc_3d(f19, 0.06, None, uy=0.01, uz=-0.02),
+                    f"f27_{tag}": f27, f"ff27_{tag}": far_field_bc_27(f27, 0.05, ob3)})
+    out.update(ob9=ob9, ob3=ob3, sponge=make_sponge_strength(8, 40, 25, 10, power=2.0))
+    arrays = {k: v.detach().cpu().numpy() for k, v in out.items()}
+    np.savez_compressed(HERE / "far_field.npz", **arrays)
+    print("wrote far_field.npz")
+
+
 def trt(torch) -> None:
     """TRT collisions (solver.py:440, solver3d.py:303, d3q27.py:438) on the
     seeded near-equilibrium fields of the other collision fixtures."""
@@ -503,6 +533,51 @@ def cavity2d(src: str, re: int) -> None:
     print(f"wrote cavity2d_re{re}.npz ({sorted(out)})")
 
 
+def cylinder2d(src: str) -> None:
+    """TensorLBM's verified free-stream cylinder at Re 100
+    (benchmarks/verified/cylinder/re100: run.py and the result.json it wrote;
+    D2Q9 MRT with a sponge tau field, far field, seeded wake, D = 48 and 64,
+    60 000 / 90 000 steps): the drag coefficient and Strouhal number of each
+    grid, copied from the reference's own outputs."""
+    import json
+
+    res = json.loads((pathlib.Path(src).parent / "benchmarks" / "verified" / "cylinder" / "re100" /
+                      "result.json").read_text())
+    out = {}
+    for case in res["grids"].values():
+        d = int(case["D"])
+        for k in ("steps", "cd", "st"):
+            out[f"d{d}_{k}"] = np.asarray(case[k])
+    np.savez_compressed(HERE / "cylinder2d_re100.npz", **out)
+    print(f"wrote cylinder2d_re100.npz ({sorted(out)})")
+
+
+def cylinder2d_small(src: str) -> None:
+    """The verified cylinder's own run.py (benchmarks/verified/cylinder/re100,
+    run_case, eager torch on the CPU) at D = 8 (320 x 320) for 3000 steps:
+    its per-step drag and lift coefficient series, Cd and St."""
+    import importlib.util
+    import tempfile
+
+    import torch
+
+    torch.set_num_threads(8)
+    path = pathlib.Path(src).parent / "benchmarks" / "verified" / "cylinder" / "re100" / "run.py"
+    spec = importlib.util.spec_from_file_location("cylinder_re100_run", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    with tempfile.TemporaryDirectory() as tmp:
+        series = pathlib.Path(tmp) / "series.npz"
+        res = mod.run_case(8, 100.0, 0.05, 3000, torch.device("cpu"), compile_mode=None, warmup_frac=0.5,
+                           series_path=str(series))
+        s = np.load(series)
+        out = {"cd_series": s["cd"], "cl_series": s["cl"], "cd": np.asarray(res["cd"]),
+               "st": np.asarray(res["st"] if res["st"] is not None else np.nan), "steps": np.asarray(3000),
+               "seed_steps": np.asarray(res["seed"]["steps"])}
+    np.savez_compressed(HERE / "cylinder2d_small.npz", **out)
+    print(f"wrote cylinder2d_small.npz (Cd {float(res['cd'])}, St {res['st']})")
+
+
 def pipe3d(src: str) -> None:
     """TensorLBM's verified Hagen-Poiseuille pipe (benchmarks/verified/
     poiseuille_3d_pipe: run.py and the case_R20.json / case_R40.json it wrote,
@@ -579,6 +654,13 @@ def main() -> None:
     if args.only == "cavity3d_full":
         cavity3d_full(args.reference)
         return
+    if args.only == "cylinder2d_re100":
+        cylinder2d(args.reference)
+        return
+    if args.only == "cylinder2d_small":
+        import_reference(args.reference)
+        cylinder2d_small(args.reference)
+        return
     if args.only in ("cavity2d_re100", "cavity2d_re1000"):
         cavity2d(args.reference, int(args.only[len("cavity2d_re"):]))
         return
@@ -607,6 +689,9 @@ def main() -> None:
         return
     if args.only == "rlbm":
         rlbm(torch)
+        return
+    if args.only == "far_field":
+        far_field(torch)
         return
     if args.only == "bfl":
         bfl(torch)

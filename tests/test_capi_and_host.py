@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol():
     lib = _lib.load()
     for name in _declared_symbols():
         assert hasattr(lib, name), name
-    assert lib.tlbm_abi_version() == 2
+    assert lib.tlbm_abi_version() == 3
     assert lib.tlbm_status_string(3) == b"input and output buffers alias"
     # the Python binding types exactly the declared set
     assert sorted(_lib.exported_symbols()) == sorted(_declared_symbols())
@@ -163,3 +163,16 @@ def test_step_config_bits():
     c2 = StepConfig(9, (5, 6), 0.6, "bgk", u_lid=0.1)
     d2 = c2.desc(_lib.F64)
     assert d2.bc == _lib.BC_LID and (d2.nx, d2.ny, d2.nz) == (6, 5, 1) and abs(d2.s_e - 1.64) < 1e-15
+
+
+def test_sponge_strength_matches_reference():
+    """make_sponge_strength (boundaries.py:388) on the CPU, bit for bit."""
+    import numpy as np
+
+    from tensorlbm_b200 import boundaries
+    from tests.conftest import golden
+
+    g = golden("far_field")
+    s = boundaries.make_sponge_strength(8, 40, 25, 10, power=2.0)
+    assert s.shape == (8, 40) and s.dtype == torch.float32
+    assert np.array_equal(s.numpy(), g["sponge"])

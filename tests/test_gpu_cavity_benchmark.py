@@ -2,7 +2,8 @@
 kernel, against the values each benchmark recorded in the reference's own
 result files: the 3-D lid-driven cavity at Re 1000 (golden cavity3d_full),
 the 2-D cavity at Re 100 (cavity2d_re100) and Re 1000 (cavity2d_re1000, the
-regularised BGK) and the Hagen-Poiseuille pipe (pipe3d)."""
+regularised BGK), the free-stream cylinder at Re 100 (cylinder2d_small,
+cylinder2d_re100) and the Hagen-Poiseuille pipe (pipe3d)."""
 
 from __future__ import annotations
 
@@ -75,6 +76,46 @@ def test_cavity_2d_re1000_rlbm_matches_reference_benchmark(cuda, n):
     for key in ("u_mid", "u_bot", "v_mid"):
         assert r[key] == pytest.approx(float(g[f"n{n}_{key}"]), abs=5e-5), key
     assert r["primary_vortex"] == pytest.approx(g[f"n{n}_primary_vortex"].tolist(), abs=2.0 / (n - 1))
+
+
+def test_cylinder_2d_small_matches_reference_run(cuda):
+    """The verified cylinder's chain (D2Q9 MRT with the sponge tau field, far
+    field, seeded wake, drag every step) against the benchmark's own run.py
+    run eagerly on the CPU at D = 8 for 3000 steps (golden cylinder2d_small):
+    the per-step drag and lift coefficients agree to the MRT's float32
+    rounding (measured 1.3e-6 of their scale), Cd to the 4 decimals the
+    reference reports."""
+    from tensorlbm_b200.verified import cylinder_2d
+
+    from tests.conftest import golden
+
+    g = golden("cylinder2d_small")
+    r = cylinder_2d(8, steps=int(g["steps"]), device=cuda, return_series=True)
+    assert r["finite"] and r["seed_steps"] == int(g["seed_steps"])
+    scale = np.max(np.abs(g["cd_series"]))
+    assert np.max(np.abs(r["cd_series"] - g["cd_series"])) <= 1e-5 * scale
+    assert np.max(np.abs(r["cl_series"] - g["cl_series"])) <= 1e-5 * scale
+    assert r["cd"] == pytest.approx(float(g["cd"]), abs=6e-5)
+    assert r["st"] == pytest.approx(float(g["st"]), abs=6e-5)
+
+
+@pytest.mark.parametrize("d", [48, 64])
+def test_cylinder_2d_re100_benchmark_criteria(cuda, d):
+    """The verified cylinder at D = 48 / 64 (60 000 / 90 000 steps) meets the
+    benchmark's own acceptance test: Cd within 3 % of Braza's 1.35 and St
+    within 3 % of 0.1645 (run.py:58-59; README).  The values recorded in its
+    result.json (golden cylinder2d_re100) came from an earlier script
+    (README: /tmp/b5_sponge.py), not from the committed run.py whose chain
+    this runner follows; they are reported beside ours, not asserted."""
+    from tensorlbm_b200.verified import cylinder_2d
+
+    from tests.conftest import golden
+
+    g = golden("cylinder2d_re100")
+    r = cylinder_2d(d, steps=int(g[f"d{d}_steps"]), device=cuda)
+    assert r["finite"]
+    assert abs(r["cd"] / 1.35 - 1.0) <= 0.03
+    assert abs(r["st"] / 0.1645 - 1.0) <= 0.03
 
 
 @pytest.mark.parametrize("r", [20, 40])

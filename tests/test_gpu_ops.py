@@ -388,6 +388,92 @@ def test_rlbm_sphere_channel_vs_oracle(cuda, q):
     assert same(N(s.f), ref)
 
 
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_far_field_dropins(cuda, tag):
+    """far_field_bc_2d / _3d / _27 against the reference's outputs, bit for bit."""
+    from tensorlbm_b200 import boundaries, boundaries3d, boundaries_d3q27
+
+    g = golden("far_field")
+    ob9, ob3 = T(g["ob9"], cuda), T(g["ob3"], cuda)
+    assert same(N(boundaries.far_field_bc_2d(T(g[f"f9_{tag}"], cuda), 0.07, ob9)), g[f"ff9_{tag}"])
+    f19 = T(g[f"f19_{tag}"], cuda)
+    assert same(N(boundaries3d.far_field_bc_3d(f19, 0.06, ob3)), g[f"ff19_{tag}"])
+    cfg_y = {"far_field_faces": ["y-", "y+"], "periodic_faces": ["z-", "z+"]}
+    assert same(N(boundaries3d.far_field_bc_3d(f19, 0.06, None, bc_config=cfg_y)), g[f"ff19y_{tag}"])
+    assert same(N(boundaries3d.far_field_bc_3d(f19, 0.06, None, uy=0.01, uz=-0.02)), g[f"ff19uv_{tag}"])
+    assert same(N(boundaries_d3q27.far_field_bc_27(T(g[f"f27_{tag}"], cuda), 0.05, ob3)), g[f"ff27_{tag}"])
+
+
+@pytest.mark.parametrize("q,shape,faces", [(9, (12, 32), "y"), (9, (12, 33), "y"), (19, (6, 8, 16), "yz"),
+                                           (19, (6, 8, 15), "yz"), (19, (6, 8, 16), "y"), (27, (6, 8, 16), "yz")])
+def test_far_field_step_vs_oracle(cuda, q, shape, faces):
+    """The fused step with the far field (BGK, obstacle with drag, a seeded
+    inlet perturbation for part of the run) against the oracle's collide ->
+    stream -> force -> far field -> bounce-back chain: bit-exact populations
+    on the pair kernel (even nx) and the one-cell kernel (odd nx)."""
+    from tensorlbm_b200 import LBMSolver
+
+    obst = np.zeros(shape, bool)
+    if q == 9:
+        obst[4:7, 10:13] = True
+    else:
+        obst[2:4, 3:5, 6:9] = True
+    rng = np.random.default_rng(q + shape[-1])
+    u = 0.05
+    z = np.zeros(shape, np.float32)
+    ux = (u + 0.01 * rng.standard_normal(shape)).astype(np.float32)
+    ux[obst] = 0.0
+    uy = (0.01 * rng.standard_normal(shape)).astype(np.float32)
+    f0 = O.equilibrium(q, np.ones_like(z), ux, uy, None if q == 9 else z)
+    lat = {9: "D2Q9", 19: "D3Q19", 27: "D3Q27"}[q]
+    s = LBMSolver(lat, shape, 0.58, "bgk", device=cuda, obstacle_mask=T(obst, cuda), u_in=u, far_field=faces,
+                  track_force=True)
+    s.load(T(f0, cuda))
+    ref, forces = f0, []
+    for k in range(8):
+        du = (0.0, 0.004 * np.sin(0.7 * k), 0.0) if k < 5 else (0.0, 0.0, 0.0)
+        s.set_inlet_perturbation(*du).step(1)
+        ref, fo = O.far_field_step(ref, 0.58, u, obst, "bgk", z_faces=faces == "yz", inlet_du=du)
+        forces.append(fo)
+    assert same(N(s.f), ref)
+    fh, fr = N(s.force_history()), np.array(forces)
+    k = min(fh.shape[1], fr.shape[1])
+    assert np.max(np.abs(fh[:, :k] - fr[:, :k])) <= 1e-6 * np.max(np.abs(fr))
+
+
+def test_far_field_mrt_sponge_vs_oracle(cuda):
+    """D2Q9 MRT with a sponge tau field and the far field (the verified
+    cylinder's step) against the oracle chain, to the MRT's float32 rounding."""
+    from tensorlbm_b200 import LBMSolver, boundaries
+
+    ny, nx, u = 24, 64, 0.05
+    obst = np.zeros((ny, nx), bool)
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    obst[(xx - 16) ** 2 + (yy - 12) ** 2 <= 9] = True
+    sigma = N(boundaries.make_sponge_strength(ny, nx, 44, 20, device=cuda))
+    tau_field = (0.56 * (1.0 + 10.0 * sigma)).astype(np.float32)
+    z = np.zeros((ny, nx), np.float32)
+    f0 = O.equilibrium(9, np.ones_like(z), np.where(obst, 0.0, u).astype(np.float32), z)
+    s = LBMSolver("D2Q9", (ny, nx), 0.56, "mrt", device=cuda, obstacle_mask=T(obst, cuda), u_in=u, far_field="y",
+                  tau_field=T(tau_field, cuda))
+    s.load(T(f0, cuda)).step(20)
+    ref = f0
+    for _ in range(20):
+        ref, _ = O.far_field_step(ref, 0.56, u, obst, "mrt", z_faces=False, tau_field=tau_field)
+    assert np.max(np.abs(N(s.f) - ref)) <= 2e-6
+
+
+def test_far_field_rejections(cuda):
+    from tensorlbm_b200 import LBMSolver
+
+    with pytest.raises(ValueError):
+        LBMSolver("D2Q9", (8, 16), 0.6, "bgk", device=cuda, u_in=0.05, far_field="yz")
+    with pytest.raises(ValueError):
+        LBMSolver("D3Q19", (4, 8, 16), 0.6, "bgk", device=cuda, u_in=0.05, rho_out=1.0, far_field="y")
+    with pytest.raises(NotImplementedError):
+        LBMSolver("D3Q19", (4, 8, 16), 0.6, "bgk", device=cuda, u_in=0.05, far_field="y", pattern="aa")
+
+
 @pytest.mark.parametrize("tag,tol", [("f32", 5 * F32_TOL), ("f64", 1e-12)])
 def test_collide_cascaded(cuda, tag, tol):
     """The cascaded kernels against the reference's outputs (fused moment

@@ -194,6 +194,20 @@ def test_collide_rlbm(q, tag):
     assert same(O.collide_rlbm(g[f"fr{q}_{tag}"], 0.53), g[f"rlbmr{q}_{tag}"])
 
 
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+def test_far_field(tag):
+    """Free-stream far field (boundaries.py:199, boundaries3d.py:446,
+    boundaries_d3q27.py:63): the oracle against the reference's outputs, bit
+    for bit, with the obstacle bounce-back after it."""
+    g = golden("far_field")
+    ob9, ob3 = g["ob9"], g["ob3"]
+    assert same(O.bounce_back(O.far_field(g[f"f9_{tag}"], 0.07), ob9), g[f"ff9_{tag}"])
+    assert same(O.bounce_back(O.far_field(g[f"f19_{tag}"], 0.06), ob3), g[f"ff19_{tag}"])
+    assert same(O.far_field(g[f"f19_{tag}"], 0.06, z_faces=False), g[f"ff19y_{tag}"])
+    assert same(O.far_field(g[f"f19_{tag}"], 0.06, 0.01, -0.02), g[f"ff19uv_{tag}"])
+    assert same(O.bounce_back(O.far_field(g[f"f27_{tag}"], 0.05), ob3), g[f"ff27_{tag}"])
+
+
 def test_bfl_links_update_and_chain():
     """Bouzidi links of a sphere (bfl_common.py:384, interpolated_bc_common.py:136),
     the link update (bfl_common.py:106) and the 8-step chain in bfl_step's
