@@ -33,14 +33,6 @@
 #ifndef TLBM_MINB_AA_MRT
 #define TLBM_MINB_AA_MRT 0
 #endif
-// threads per block of the D3Q19 MRT pair kernel on half storage, and its
-// resident blocks per SM at that size
-#ifndef TLBM_MRT_HALF_THREADS
-#define TLBM_MRT_HALF_THREADS 128
-#endif
-#ifndef TLBM_MINB_MRT_HALF_SMALL
-#define TLBM_MINB_MRT_HALF_SMALL 5
-#endif
 
 namespace tlbm {
 
@@ -720,25 +712,11 @@ __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typ
                                                  BcParams<typename Storage<S>::T> bp) {
   step_x2<L, S, COLL, FORCED>(p, cp, bp);
 }
-// the same kernel compiled for blocks of NT threads, MINB resident per SM
-template <class L, typename S, int COLL, int MINB, int NT = 256>
-__global__ void __launch_bounds__(NT, MINB) k_step_x2_capped(StepParams p, CollideParams<typename Storage<S>::T> cp,
-                                                              BcParams<typename Storage<S>::T> bp) {
+// the same kernel compiled for MINB resident blocks per SM
+template <class L, typename S, int COLL, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_step_x2_capped(StepParams p, CollideParams<typename Storage<S>::T> cp,
+                                                               BcParams<typename Storage<S>::T> bp) {
   step_x2<L, S, COLL, false>(p, cp, bp);
-}
-
-// Block size of the pair kernel, and its resident blocks per SM (0: no cap).
-// The D3Q19 MRT on half storage runs blocks of 128: five of them per SM give
-// 96 registers and no spills, where three blocks of 256 (80 registers) spill
-// 128 bytes per thread.
-template <class L, typename S, int COLL>
-__host__ __device__ constexpr int x2_threads() {
-  constexpr bool shifted = std::is_same<S, __half>::value || std::is_same<S, __nv_bfloat16>::value;
-  return (L::Q == 19 && COLL == TLBM_COLL_MRT && shifted) ? TLBM_MRT_HALF_THREADS : 256;
-}
-template <class L, typename S, int COLL>
-__host__ __device__ constexpr int x2_launch_blocks() {
-  return x2_threads<L, S, COLL>() == 256 ? x2_min_blocks<L, S, COLL>() : TLBM_MINB_MRT_HALF_SMALL;
 }
 
 }  // namespace tlbm
@@ -757,10 +735,10 @@ inline bool pair_layout_ok(const StepParams& p) {
          (p.flags == nullptr || al(p.flags, 2));
 }
 
-inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block, int threads = 256) {
+inline void step_launch_shape(int nx, int ny, int nz, dim3& grid, dim3& block) {
   int bx = 32;
-  while (bx < nx && bx < threads) bx <<= 1;
-  int by = threads / bx;
+  while (bx < nx && bx < 256) bx <<= 1;
+  int by = 256 / bx;
   block = dim3(bx, by, 1);
   grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
 }
@@ -785,10 +763,9 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
     int st = TLBM_OK;
     if (launch_rows<L, SI, COLL>(p, cp, bp, s, st)) return st;
     if (pair_layout_ok<L, SI>(p)) {
-      constexpr int nt = x2_threads<L, SI, COLL>();
-      step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block, nt);
-      constexpr int minb = x2_launch_blocks<L, SI, COLL>();
-      if constexpr (minb > 0) k_step_x2_capped<L, SI, COLL, minb, nt><<<grid, block, 0, s>>>(p, cp, bp);
+      step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block);
+      constexpr int minb = x2_min_blocks<L, SI, COLL>();
+      if constexpr (minb > 0) k_step_x2_capped<L, SI, COLL, minb><<<grid, block, 0, s>>>(p, cp, bp);
       else k_step_x2<L, SI, COLL, FORCED><<<grid, block, 0, s>>>(p, cp, bp);
       return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
     }
