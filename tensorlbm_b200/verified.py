@@ -135,6 +135,25 @@ def shear_wave(n: int, tau: float = 0.8, u0: float = 0.05, steps: int = 3200, re
             "finite": not s.nonfinite_seen()}
 
 
+def lift_strouhal(cl: np.ndarray, D: float, u_in: float) -> float:
+    """Strouhal number of a lift-coefficient window as benchmarks/verified/cylinder
+    computes it (run.py:150-165): peak of the spectrum of the Hann-windowed,
+    mean-removed signal, refined by a parabola through the peak bin and its
+    neighbours; NaN for fewer than 256 samples."""
+    cl_w = np.asarray(cl, dtype=np.float64)
+    cl_w = cl_w - cl_w.mean()
+    if cl_w.size < 256:
+        return float("nan")
+    spec = np.abs(np.fft.rfft(cl_w * np.hanning(cl_w.size)))
+    k = int(np.argmax(spec[1:])) + 1
+    delta = 0.0
+    if 0 < k < spec.size - 1:
+        den = spec[k - 1] - 2.0 * spec[k] + spec[k + 1]
+        if abs(den) > 1e-30:
+            delta = float(0.5 * (spec[k - 1] - spec[k + 1]) / den)
+    return float((k + delta) / cl_w.size * D / u_in)
+
+
 def cylinder_2d(D: int, re: float = 100.0, u_in: float = 0.05, steps: int = 60_000, warmup_frac: float = 0.5,
                 domain_d: float = 40.0, cyl_x_d: float = 10.0, sponge_d: float = 10.0, sponge_alpha: float = 10.0,
                 st_seed: float = 0.165, seed_ampl: float = 0.10, seed_periods: float = 2.0, device=None,
@@ -187,16 +206,7 @@ def cylinder_2d(D: int, re: float = 100.0, u_in: float = 0.05, steps: int = 60_0
     cd, cl = fh[:, 0] / q_dyn, fh[:, 1] / q_dyn
     w0 = int(warmup_frac * steps)
     cl_w = cl[w0:] - cl[w0:].mean()
-    st = float("nan")
-    if cl_w.size >= 256:
-        spec = np.abs(np.fft.rfft(cl_w * np.hanning(cl_w.size)))
-        k = int(np.argmax(spec[1:])) + 1
-        delta = 0.0
-        if 0 < k < spec.size - 1:
-            den = spec[k - 1] - 2.0 * spec[k] + spec[k + 1]
-            if abs(den) > 1e-30:
-                delta = float(0.5 * (spec[k - 1] - spec[k + 1]) / den)
-        st = float((k + delta) / cl_w.size * D / u_in)
+    st = lift_strouhal(cl[w0:], D, u_in)
     out = {"D": D, "nx": nx, "ny": ny, "re": re, "u_in": u_in, "tau": tau, "steps": steps, "seed_steps": seed_steps,
            "cd": float(cd[w0:].mean()), "st": st, "cl_amp": float(np.abs(cl_w).max()),
            "finite": not s.nonfinite_seen(), "seconds": secs, "mlups": nx * ny * steps / secs / 1e6}
@@ -205,4 +215,4 @@ def cylinder_2d(D: int, re: float = 100.0, u_in: float = 0.05, steps: int = 60_0
     return out
 
 
-__all__ = ["pipe_3d", "shear_wave", "cylinder_2d", "cavity_3d_full", "cavity_2d", "laminar_decay"]
+__all__ = ["pipe_3d", "shear_wave", "cylinder_2d", "lift_strouhal", "cavity_3d_full", "cavity_2d", "laminar_decay"]
