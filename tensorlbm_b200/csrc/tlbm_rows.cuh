@@ -234,7 +234,9 @@ bool launch_rows(const StepParams& p, const CollideParams<typename Storage<S>::T
   } else {
     if (!row_staging_enabled()) return false;
     const auto al = [](const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; };
-    if (p.nx % 64 != 0 || p.nx > rows::kMaxNx || p.link_q != nullptr || p.z_count < 1 || p.ny < 1) return false;
+    if (p.nx % 64 != 0 || p.nx > rows::kMaxNx || p.link_q != nullptr || (p.bc & TLBM_BC_FAR_FIELD) ||
+        p.z_count < 1 || p.ny < 1)
+      return false;
     if (!al(p.f_in, 16) || !al(p.f_out, 2 * sizeof(S)) || (p.flags && !al(p.flags, 2))) return false;
     if ((long long)(L::Q / 2 + 2) * p.n >= (1LL << 31)) return false;
     const long long smem = rows::smem_bytes<L, S, COLL>(p.nx);

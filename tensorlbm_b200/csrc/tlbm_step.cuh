@@ -127,10 +127,11 @@ __device__ __forceinline__ void curved_links(const Domain<SI, SO>& d, long long 
 // Boundary conditions of one cell after the pull, in TensorLBM's order:
 // Zou/He inlet / outlet planes, the far field, full-way (or moving-wall)
 // bounce-back or the Bouzidi links of a curved wall, lid.  (mx, my, mz)
-// collect the BFL force.  kCurved = false compiles the Bouzidi links out (the
-// two-cells-per-thread kernel, which never runs with link tables).  The far
-// field's zero-gradient outlet is the caller's: the x = nx-1 cell holds the
-// post-stream populations of x = nx-2 when it gets here.
+// collect the BFL force.  kCurved = false compiles the Bouzidi links and the
+// far field out (the two-cells-per-thread kernels, which never run with link
+// tables or the far field).  The far field's zero-gradient outlet is the
+// caller's: the x = nx-1 cell holds the post-stream populations of x = nx-2
+// when it gets here.
 template <class L, typename T, typename SI, typename SO, bool kCurved = true>
 __device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x, int y, int z, long long cell,
                                                  uint8_t fl, T (&f)[L::Q], const BcParams<T>& bp, double& mx,
@@ -148,7 +149,7 @@ __device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x,
   }
   // far field: inlet plane, then the lateral planes (which win on the edges
   // of the outlet plane)
-  if (d.bc & TLBM_BC_FAR_FIELD) {
+  if (kCurved && (d.bc & TLBM_BC_FAR_FIELD)) {
     if (x == 0) {
       far_field_feq<L>(f, bp.ff_in[0], bp.ff_in[1], bp.ff_in[2]);
     } else if (y == 0 || y == d.ny - 1 || ((d.bc & TLBM_BC_FAR_FIELD_Z) && (z == 0 || z == d.nz - 1))) {
@@ -598,10 +599,7 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
   // whether any lane of the warp has a flagged cell or sits on a plane with a
   // condition: warps of the interior then skip all boundary code on a
   // warp-uniform branch
-  const bool far = (d.bc & TLBM_BC_FAR_FIELD) &&
-                   (x == 0 || x + 2 == nx || y == 0 || y == ny - 1 ||
-                    ((d.bc & TLBM_BC_FAR_FIELD_Z) && (z == 0 || z == d.nz - 1)));
-  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || far || ((d.bc & TLBM_BC_ZH_INLET) && x == 0) ||
+  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || ((d.bc & TLBM_BC_ZH_INLET) && x == 0) ||
                                                        ((d.bc & TLBM_BC_ZH_OUTLET) && x + 2 == nx) ||
                                                        ((d.bc & TLBM_BC_LID) && y == ny - 1)));
   if constexpr (kDev) {
@@ -632,12 +630,6 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
     accumulate_force(d.force, __any_sync(0xffffffffu, oa || ob), mx, my, mz);
   }
   if (!active) return;
-  // far field: the outlet cell x + 1 = nx - 1 takes the post-stream
-  // populations of its pair partner x = nx - 2 (after the force sample)
-  if ((d.bc & TLBM_BC_FAR_FIELD) && x + 2 == nx) {
-#pragma unroll
-    for (int q = 0; q < Q; ++q) fb[q] = fa[q];
-  }
   if constexpr (!uniform_edge_branch<L, COLL>()) {
     double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
     apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
@@ -647,7 +639,7 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
     bool keep_a = false, keep_b = false;   // half-way wall cells: reversed, not collided
     if (edge) {
       double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-      apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+        apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
       apply_boundaries<L, T, S, S, false>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
       if (fla & TLBM_FLAG_HALFWAY) {
         bounce_back<L>(fa);
@@ -725,13 +717,15 @@ __global__ void __launch_bounds__(256, MINB) k_step_x2_capped(StepParams p, Coll
 
 namespace tlbm {
 
-// Whether the pair kernel can run this step: no Bouzidi link tables, nx even
+// Whether the pair kernel can run this step: no Bouzidi link tables or far
+// field (the one-cell kernel runs those), nx even
 // (pairs never straddle a row), offsets of +-(Q/2 + 1) n within 32 bits, and
 // both population buffers (and the flags) aligned to two values.
 template <class L, typename S>
 inline bool pair_layout_ok(const StepParams& p) {
   const auto al = [](const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; };
-  return (p.nx % 2 == 0) && p.link_q == nullptr && (long long)(L::Q / 2 + 2) * p.n < (1LL << 31) && al(p.f_in, 2 * sizeof(S)) && al(p.f_out, 2 * sizeof(S)) &&
+  return (p.nx % 2 == 0) && p.link_q == nullptr && !(p.bc & TLBM_BC_FAR_FIELD) &&
+         (long long)(L::Q / 2 + 2) * p.n < (1LL << 31) && al(p.f_in, 2 * sizeof(S)) && al(p.f_out, 2 * sizeof(S)) &&
          (p.flags == nullptr || al(p.flags, 2));
 }
 
