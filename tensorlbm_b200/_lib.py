@@ -17,6 +17,8 @@ import torch
 _HERE = pathlib.Path(__file__).resolve().parent
 LIB_PATH = pathlib.Path(os.environ.get("TLBM_LIB", _HERE / "libtlbm.so"))
 
+# include/tlbm.h TLBM_ABI_VERSION this mirror (Desc, SIGNATURES) is written for
+ABI_VERSION = 3
 # tlbm_status
 OK, ERR_SHAPE, ERR_DTYPE, ERR_ALIAS, ERR_LAUNCH, ERR_TIMEOUT, ERR_NONFINITE, ERR_ARG, ERR_UNSUPPORTED = range(9)
 ERR_TOO_LARGE = 9
@@ -158,6 +160,10 @@ def load() -> ctypes.CDLL:
             "`python -c 'import __graft_entry__ as g; g.build()'` or `make -C tensorlbm_b200/csrc`"
         )
     lib = ctypes.CDLL(str(LIB_PATH))
+    lib.tlbm_abi_version.restype = ctypes.c_int
+    if lib.tlbm_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"tensorlbm_b200: {LIB_PATH} has ABI version {lib.tlbm_abi_version()}, this package "
+                           f"binds version {ABI_VERSION}; rebuild it")
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
