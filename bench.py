@@ -739,6 +739,9 @@ def run_ours(args) -> None:
                                                      2 * 19 * 2, peak)
     if want("d3q19_bgk_f32"):
         variants["d3q19_bgk_f32"] = _variant(torch, dev, "D3Q19", "bgk", "f32", args.steps, args.warmup, bpc, peak)
+    if want("d3q19_rlbm_f32"):
+        # regularised BGK (solver3d.py:342), bit-exact arithmetic, same channel
+        variants["d3q19_rlbm_f32"] = _variant(torch, dev, "D3Q19", "rlbm", "f32", args.steps, args.warmup, bpc, peak)
     for name, lat, coll, st, bpc_v, steps_v in (
             ("d3q19_bgk_f16_shifted", "D3Q19", "bgk", "f16", 2 * 19 * 2, args.steps),
             ("d3q19_bgk_bf16_shifted", "D3Q19", "bgk", "bf16", 2 * 19 * 2, args.steps),
@@ -969,7 +972,8 @@ def main() -> None:
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--variants", default="all",
                     help="comma list of variants to run (d3q27_cumulant_f32, d3q27_cumulant_f16_shifted, "
-                         "d3q19_mrt_f16_shifted, d3q19_bgk_f32, d3q19_bgk_f16_shifted, d3q19_bgk_bf16_shifted, "
+                         "d3q19_mrt_f16_shifted, d3q19_bgk_f32, d3q19_rlbm_f32, d3q19_bgk_f16_shifted, "
+                         "d3q19_bgk_bf16_shifted, "
                          "les_mlp_128_vs_smagorinsky_256, d2q9_batched_512_cylinders) or 'all'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-slab", type=int, default=16, help="z-planes of the CPU sample slab")
