@@ -127,12 +127,12 @@ __device__ __forceinline__ void curved_links(const Domain<SI, SO>& d, long long 
 // Boundary conditions of one cell after the pull, in TensorLBM's order:
 // Zou/He inlet / outlet planes, the far field, full-way (or moving-wall)
 // bounce-back or the Bouzidi links of a curved wall, lid.  (mx, my, mz)
-// collect the BFL force.  kCurved = false compiles the Bouzidi links and the
-// far field out (the two-cells-per-thread kernels, which never run with link
-// tables or the far field).  The far field's zero-gradient outlet is the
-// caller's: the x = nx-1 cell holds the post-stream populations of x = nx-2
-// when it gets here.
-template <class L, typename T, typename SI, typename SO, bool kCurved = true>
+// collect the BFL force.  kCurved = false compiles the Bouzidi links out (the
+// two-cells-per-thread kernels, which never run with link tables), kFar =
+// false the far field (all but the far-field instantiations of those
+// kernels).  The far field's zero-gradient outlet is the caller's: the
+// x = nx-1 cell holds the post-stream populations of x = nx-2 when it gets here.
+template <class L, typename T, typename SI, typename SO, bool kCurved = true, bool kFar = kCurved>
 __device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x, int y, int z, long long cell,
                                                  uint8_t fl, T (&f)[L::Q], const BcParams<T>& bp, double& mx,
                                                  double& my, double& mz) {
@@ -149,7 +149,7 @@ __device__ __forceinline__ void apply_boundaries(const Domain<SI, SO>& d, int x,
   }
   // far field: inlet plane, then the lateral planes (which win on the edges
   // of the outlet plane)
-  if (kCurved && (d.bc & TLBM_BC_FAR_FIELD)) {
+  if (kFar && (d.bc & TLBM_BC_FAR_FIELD)) {
     if (x == 0) {
       far_field_feq<L>(f, bp.ff_in[0], bp.ff_in[1], bp.ff_in[2]);
     } else if (y == 0 || y == d.ny - 1 || ((d.bc & TLBM_BC_FAR_FIELD_Z) && (z == 0 || z == d.nz - 1))) {
@@ -455,6 +455,20 @@ __device__ __forceinline__ void relax_interior_two(const Domain<S, S>& d, long l
   }
 }
 
+// Far field in the far-field instantiation of the pair kernels: the outlet
+// cell x + 1 = nx - 1 takes the post-stream populations of its pair partner
+// x = nx - 2 (after the force sample, as far_field_bc_* follows
+// compute_obstacle_forces).  Called in the boundary branch only.
+template <class L, bool FAR, typename S, typename T>
+__device__ __forceinline__ void far_field_outlet_pair(const Domain<S, S>& d, int x, T (&fa)[L::Q], T (&fb)[L::Q]) {
+  if constexpr (FAR) {
+    if (x + 2 == d.nx) {
+#pragma unroll
+      for (int q = 0; q < L::Q; ++q) fb[q] = fa[q];
+    }
+  }
+}
+
 // Pair kernels: interior warps skip the boundary code on a warp-uniform branch
 // (2-9 % faster for the D3Q19 collisions and the half formats on the sphere
 // channel).  The D3Q27 legacy cumulant ran 4 % slower that way; it and the
@@ -505,7 +519,7 @@ __host__ __device__ constexpr bool pair_deviation_form() {
   return std::is_same<S, __half>::value && COLL == TLBM_COLL_BGK && !FORCED && uniform_edge_branch<L, COLL>();
 }
 
-template <class L, typename S, int COLL, bool FORCED>
+template <class L, typename S, int COLL, bool FORCED, bool FAR = false>
 __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const CollideParams<typename Storage<S>::T>& cp,
                                             const BcParams<typename Storage<S>::T>& bp, int x, int y, int z, int c,
                                             bool active, typename Storage<S>::T (&fa)[L::Q],
@@ -514,7 +528,7 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
 // The pair update of cells (x, y, z) and (x + 1, y, z) of domain d (x even):
 // the pull (periodic wrap on every axis) and pair_finish.  Every thread of a
 // warp must call it, inactive ones with active = false.
-template <class L, typename S, int COLL, bool FORCED = false>
+template <class L, typename S, int COLL, bool FORCED = false, bool FAR = false>
 __device__ __forceinline__ void pair_update(const Domain<S, S>& d, const CollideParams<typename Storage<S>::T>& cp,
                                             const BcParams<typename Storage<S>::T>& bp, int x, int y, int z,
                                             bool active) {
@@ -562,16 +576,16 @@ __device__ __forceinline__ void pair_update(const Domain<S, S>& d, const Collide
     }
     if (d.flags) fl2 = __ldg(reinterpret_cast<const uint16_t*>(at_offset(d.flags, c)));
   }
-  pair_finish<L, S, COLL, FORCED>(d, cp, bp, x, y, z, c, active, fa, fb, fl2);
+  pair_finish<L, S, COLL, FORCED, FAR>(d, cp, bp, x, y, z, c, active, fa, fb, fl2);
 }
 
-template <class L, typename S, int COLL, bool FORCED = false>
+template <class L, typename S, int COLL, bool FORCED = false, bool FAR = false>
 __device__ __forceinline__ void step_x2(const StepParams& p, const CollideParams<typename Storage<S>::T>& cp,
                                         const BcParams<typename Storage<S>::T>& bp) {
   const int x = 2 * int(blockIdx.x * blockDim.x + threadIdx.x);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = p.z0 + int(blockIdx.z);
-  pair_update<L, S, COLL, FORCED>(pair_domain<S>(p), cp, bp, x, y, z, (x < p.nx) && (y < p.ny));
+  pair_update<L, S, COLL, FORCED, FAR>(pair_domain<S>(p), cp, bp, x, y, z, (x < p.nx) && (y < p.ny));
 }
 
 // The pair update after the pull: boundary conditions, drag sample,
@@ -579,7 +593,7 @@ __device__ __forceinline__ void step_x2(const StepParams& p, const CollideParams
 // pulled values (the stored deviations for the deviation-form BGK), fl2 the
 // two flag bytes.  Every thread of a warp must call it (the force reduction
 // and the edge test are warp-wide).
-template <class L, typename S, int COLL, bool FORCED>
+template <class L, typename S, int COLL, bool FORCED, bool FAR>
 __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const CollideParams<typename Storage<S>::T>& cp,
                                             const BcParams<typename Storage<S>::T>& bp, int x, int y, int z, int c,
                                             bool active, typename Storage<S>::T (&fa)[L::Q],
@@ -599,7 +613,13 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
   // whether any lane of the warp has a flagged cell or sits on a plane with a
   // condition: warps of the interior then skip all boundary code on a
   // warp-uniform branch
-  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || ((d.bc & TLBM_BC_ZH_INLET) && x == 0) ||
+  // (the far-field instantiation adds its planes: x = 0, the outlet pair, the
+  // y planes and with TLBM_BC_FAR_FIELD_Z the z planes)
+  bool far = false;
+  if constexpr (FAR)
+    far = x == 0 || x + 2 == nx || y == 0 || y == ny - 1 ||
+          ((d.bc & TLBM_BC_FAR_FIELD_Z) && (z == 0 || z == d.nz - 1));
+  const bool edge = __any_sync(0xffffffffu, active && (fl2 != 0 || far || ((d.bc & TLBM_BC_ZH_INLET) && x == 0) ||
                                                        ((d.bc & TLBM_BC_ZH_OUTLET) && x + 2 == nx) ||
                                                        ((d.bc & TLBM_BC_LID) && y == ny - 1)));
   if constexpr (kDev) {
@@ -632,15 +652,19 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
   if (!active) return;
   if constexpr (!uniform_edge_branch<L, COLL>()) {
     double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-    apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-    apply_boundaries<L, T, S, S, false>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+    far_field_outlet_pair<L, FAR>(d, x, fa, fb);
+    apply_boundaries<L, T, S, S, false, FAR>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false, FAR>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y,
+                                             unused_z);
     relax_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fla, flb, fa, fb, cp);
   } else if constexpr (kDev) {
     bool keep_a = false, keep_b = false;   // half-way wall cells: reversed, not collided
     if (edge) {
       double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-        apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-      apply_boundaries<L, T, S, S, false>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+      far_field_outlet_pair<L, FAR>(d, x, fa, fb);
+      apply_boundaries<L, T, S, S, false, FAR>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+      apply_boundaries<L, T, S, S, false, FAR>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y,
+                                               unused_z);
       if (fla & TLBM_FLAG_HALFWAY) {
         bounce_back<L>(fa);
         keep_a = true;
@@ -664,8 +688,10 @@ __device__ __forceinline__ void pair_finish(const Domain<S, S>& d, const Collide
     }
   } else if (edge) {
     double unused_x = 0.0, unused_y = 0.0, unused_z = 0.0;
-    apply_boundaries<L, T, S, S, false>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
-    apply_boundaries<L, T, S, S, false>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y, unused_z);
+    far_field_outlet_pair<L, FAR>(d, x, fa, fb);
+    apply_boundaries<L, T, S, S, false, FAR>(d, x, y, z, (long long)c, fla, fa, bp, unused_x, unused_y, unused_z);
+    apply_boundaries<L, T, S, S, false, FAR>(d, x + 1, y, z, (long long)c + 1, flb, fb, bp, unused_x, unused_y,
+                                             unused_z);
     relax_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fla, flb, fa, fb, cp);
   } else {
     relax_interior_two<L, S, COLL, FORCED, kPack>(d, (long long)c, fa, fb, cp);   // no flag in the warp
@@ -699,16 +725,24 @@ __host__ __device__ constexpr int x2_min_blocks() {
   return 0;
 }
 
-template <class L, typename S, int COLL, bool FORCED = false>
+template <class L, typename S, int COLL, bool FORCED = false, bool FAR = false>
 __global__ void __launch_bounds__(256) k_step_x2(StepParams p, CollideParams<typename Storage<S>::T> cp,
                                                  BcParams<typename Storage<S>::T> bp) {
-  step_x2<L, S, COLL, FORCED>(p, cp, bp);
+  step_x2<L, S, COLL, FORCED, FAR>(p, cp, bp);
+}
+
+// The collisions with a far-field instantiation of the pair kernel (float32
+// populations); other far-field steps run the one-cell kernel.
+template <class L, typename S, int COLL>
+__host__ __device__ constexpr bool far_pair() {
+  return std::is_same<S, float>::value && (COLL == TLBM_COLL_BGK || COLL == TLBM_COLL_MRT || COLL == TLBM_COLL_TRT ||
+                                          COLL == TLBM_COLL_RLBM || COLL == TLBM_COLL_SMAGORINSKY);
 }
 // the same kernel compiled for MINB resident blocks per SM
-template <class L, typename S, int COLL, int MINB>
+template <class L, typename S, int COLL, int MINB, bool FAR = false>
 __global__ void __launch_bounds__(256, MINB) k_step_x2_capped(StepParams p, CollideParams<typename Storage<S>::T> cp,
                                                                BcParams<typename Storage<S>::T> bp) {
-  step_x2<L, S, COLL, false>(p, cp, bp);
+  step_x2<L, S, COLL, false, FAR>(p, cp, bp);
 }
 
 }  // namespace tlbm
@@ -717,14 +751,14 @@ __global__ void __launch_bounds__(256, MINB) k_step_x2_capped(StepParams p, Coll
 
 namespace tlbm {
 
-// Whether the pair kernel can run this step: no Bouzidi link tables or far
-// field (the one-cell kernel runs those), nx even
-// (pairs never straddle a row), offsets of +-(Q/2 + 1) n within 32 bits, and
-// both population buffers (and the flags) aligned to two values.
+// Whether the pair kernel can run this step: no Bouzidi link tables, no far
+// field unless far_ok (its own instantiation), nx even (pairs never straddle
+// a row), offsets of +-(Q/2 + 1) n within 32 bits, and both population
+// buffers (and the flags) aligned to two values.
 template <class L, typename S>
-inline bool pair_layout_ok(const StepParams& p) {
+inline bool pair_layout_ok(const StepParams& p, bool far_ok = false) {
   const auto al = [](const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; };
-  return (p.nx % 2 == 0) && p.link_q == nullptr && !(p.bc & TLBM_BC_FAR_FIELD) &&
+  return (p.nx % 2 == 0) && p.link_q == nullptr && (far_ok || !(p.bc & TLBM_BC_FAR_FIELD)) &&
          (long long)(L::Q / 2 + 2) * p.n < (1LL << 31) && al(p.f_in, 2 * sizeof(S)) && al(p.f_out, 2 * sizeof(S)) &&
          (p.flags == nullptr || al(p.flags, 2));
 }
@@ -756,6 +790,15 @@ int launch_step(const StepParams& p, const tlbm_desc& d, cudaStream_t s) {
   if constexpr (PULL && !FORCED && std::is_same<SI, SO>::value) {
     int st = TLBM_OK;
     if (launch_rows<L, SI, COLL>(p, cp, bp, s, st)) return st;
+    if constexpr (far_pair<L, SI, COLL>()) {
+      if ((p.bc & TLBM_BC_FAR_FIELD) && pair_layout_ok<L, SI>(p, true)) {
+        step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block);
+        constexpr int minb = x2_min_blocks<L, SI, COLL>();
+        if constexpr (minb > 0) k_step_x2_capped<L, SI, COLL, minb, true><<<grid, block, 0, s>>>(p, cp, bp);
+        else k_step_x2<L, SI, COLL, false, true><<<grid, block, 0, s>>>(p, cp, bp);
+        return cudaGetLastError() == cudaSuccess ? TLBM_OK : TLBM_ERR_LAUNCH;
+      }
+    }
     if (pair_layout_ok<L, SI>(p)) {
       step_launch_shape(p.nx / 2, p.ny, p.z_count, grid, block);
       constexpr int minb = x2_min_blocks<L, SI, COLL>();

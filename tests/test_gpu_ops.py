@@ -410,7 +410,7 @@ def test_far_field_step_vs_oracle(cuda, q, shape, faces):
     """The fused step with the far field (BGK, obstacle with drag, a seeded
     inlet perturbation for part of the run) against the oracle's collide ->
     stream -> force -> far field -> bounce-back chain: bit-exact populations
-    (far-field steps run the one-cell kernel, even and odd nx alike)."""
+    on the far-field pair kernel (even nx) and the one-cell kernel (odd nx)."""
     from tensorlbm_b200 import LBMSolver
 
     obst = np.zeros(shape, bool)
