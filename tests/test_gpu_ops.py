@@ -463,6 +463,27 @@ def test_far_field_mrt_sponge_vs_oracle(cuda):
     assert np.max(np.abs(N(s.f) - ref)) <= 2e-6
 
 
+def test_far_field_d3q27_cumulant_vs_oracle(cuda):
+    """The D3Q27 legacy cumulant with the far field on all four lateral planes
+    and a drag body (the SUBOFF runners' far_field_bc_27 chain) against the
+    oracle, to the cumulant's float32 rounding."""
+    from tensorlbm_b200 import LBMSolver
+
+    shape = (8, 10, 24)
+    obst = np.zeros(shape, bool)
+    obst[3:5, 4:6, 8:11] = True
+    z = np.zeros(shape, np.float32)
+    ux = np.where(obst, 0.0, 0.05).astype(np.float32)
+    f0 = O.equilibrium(27, np.ones_like(z), ux, z, z)
+    s = LBMSolver("D3Q27", shape, 0.56, "cumulant", device=cuda, obstacle_mask=T(obst, cuda), u_in=0.05,
+                  far_field="yz", track_force=True)
+    s.load(T(f0, cuda)).step(10)
+    ref = f0
+    for _ in range(10):
+        ref, _ = O.far_field_step(ref, 0.56, 0.05, obst, "cumulant", z_faces=True)
+    assert np.max(np.abs(N(s.f) - ref)) <= 1e-5 * np.max(np.abs(ref))
+
+
 def test_far_field_rejections(cuda):
     from tensorlbm_b200 import LBMSolver
 
