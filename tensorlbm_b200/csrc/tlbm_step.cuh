@@ -237,13 +237,6 @@ __device__ __forceinline__ void relax_fluid(const Domain<SI, SO>& d, long long c
   }
 }
 
-// The update of cell (x, y, z) of one domain.  Every thread of a warp must
-// call it (inactive ones with active = false) because the force reduction is
-// warp-wide.
-// PULL = true : gather from neighbours, boundaries, collide (COLL may be NONE)
-// PULL = false: local collide / format conversion only (no boundaries)
-// FORCED: add the exact-difference linear force after the collision (a
-// separate instantiation, so that the unforced kernels carry none of it)
 // Periodic pull of cell (x, y, z): f[q] = f_in[q, (x, y, z) - c_q]
 template <class L, typename SI, typename SO, typename T>
 __device__ __forceinline__ void pull_cell(const Domain<SI, SO>& d, int x, int y, int z, T (&f)[L::Q]) {
@@ -264,6 +257,13 @@ __device__ __forceinline__ void pull_cell(const Domain<SI, SO>& d, int x, int y,
   }
 }
 
+// The update of cell (x, y, z) of one domain.  Every thread of a warp must
+// call it (inactive ones with active = false) because the force reduction is
+// warp-wide.
+// PULL = true : gather from neighbours, boundaries, collide (COLL may be NONE)
+// PULL = false: local collide / format conversion only (no boundaries)
+// FORCED: add the exact-difference linear force after the collision (a
+// separate instantiation, so that the unforced kernels carry none of it)
 template <class L, typename SI, typename SO, int COLL, bool PULL, bool FORCED = false>
 __device__ __forceinline__ void cell_update(const Domain<SI, SO>& d, int x, int y, int z, bool active,
                                             const CollideParams<typename Storage<SI>::T>& cp,
