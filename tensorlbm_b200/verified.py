@@ -7,6 +7,7 @@ values in the reference's own result files:
 
 * :func:`pipe_3d` — Hagen-Poiseuille pipe (poiseuille_3d_pipe/run.py);
 * :func:`shear_wave` — decaying 2-D shear wave (shear_wave_decay/run.py);
+* :func:`taylor_green_2d` — decaying 2-D Taylor-Green vortex (taylor_green_2d/run.py);
 * :func:`cylinder_2d` — free-stream cylinder at Re 100 with a sponge and a
   seeded wake (cylinder/re100/run.py);
 * :func:`tensorlbm_b200.lid_driven_cavity.cavity_3d_full` — 3-D cavity, Re 1000;
@@ -135,6 +136,47 @@ def shear_wave(n: int, tau: float = 0.8, u0: float = 0.05, steps: int = 3200, re
             "finite": not s.nonfinite_seen()}
 
 
+def taylor_green_2d(n: int = 128, re: float = 100.0, u0: float = 0.05, steps: int = 4900, record_every: int = 100,
+                    device=None) -> dict:
+    """TensorLBM's verified decaying 2-D Taylor-Green vortex
+    (benchmarks/verified/taylor_green_2d/run.py:52-160) on the fused kernel.
+
+    Periodic n x n, D2Q9 BGK in float32, nu = u0 n / Re, f <- collide(stream(f));
+    start: the equilibrium of u = u0 (-cos kx sin ky, sin kx cos ky), rho = 1,
+    built on the CPU as the benchmark builds it.  Every record_every steps
+    E = <|u|^2> / 2 and max|u|; the decay rates are minus the slopes of
+    least-squares lines through ln E and ln max|u| (theory 4 nu k^2 and
+    2 nu k^2); the relative mass drift of sum(f) over the run."""
+    from .d2q9 import equilibrium, macroscopic
+    from .solvers import LBMSolver
+
+    dev = _ops.cuda_device(device)
+    k = 2.0 * np.pi / float(n)
+    nu = u0 * float(n) / re
+    tau = 0.5 + 3.0 * nu
+    ax = torch.arange(n, dtype=torch.float32)
+    y, x = torch.meshgrid(ax, ax, indexing="ij")
+    ux0 = (-u0 * torch.cos(k * x) * torch.sin(k * y)).to(dev)
+    uy0 = (u0 * torch.sin(k * x) * torch.cos(k * y)).to(dev)
+    f0 = equilibrium(torch.ones_like(ux0), ux0, uy0)
+    mass0 = float(f0.sum())
+    s = LBMSolver("D2Q9", (n, n), tau, "bgk", device=dev)
+    s.resume(f0, stored_state=f0)  # the benchmark's phase: P_j = collide(stream(P_j-1)), P_0 = f_0
+    times, energies, umaxs = [], [], []
+    for step in range(record_every, steps + 1, record_every):
+        s.run(record_every, chunk=record_every)
+        _, ux, uy = macroscopic(s.state)
+        energies.append(float((0.5 * (ux * ux + uy * uy)).mean()))
+        umaxs.append(float((ux * ux + uy * uy).sqrt().max()))
+        times.append(step)
+    t = np.asarray(times, dtype=np.float64)
+    return {"n": n, "re": re, "u0": u0, "tau": tau, "steps": steps, "times": times, "energies": energies,
+            "umaxs": umaxs, "gamma_e_sim": float(-np.polyfit(t, np.log(np.asarray(energies)), 1)[0]),
+            "gamma_vel_sim": float(-np.polyfit(t, np.log(np.asarray(umaxs)), 1)[0]),
+            "gamma_e_theory": 4.0 * nu * k * k, "gamma_vel_theory": 2.0 * nu * k * k,
+            "mass_drift_rel": (float(s.state.sum()) - mass0) / mass0, "finite": not s.nonfinite_seen()}
+
+
 def lift_strouhal(cl: np.ndarray, D: float, u_in: float) -> float:
     """Strouhal number of a lift-coefficient window as benchmarks/verified/cylinder
     computes it (run.py:150-165): peak of the spectrum of the Hann-windowed,
@@ -215,4 +257,4 @@ def cylinder_2d(D: int, re: float = 100.0, u_in: float = 0.05, steps: int = 60_0
     return out
 
 
-__all__ = ["pipe_3d", "shear_wave", "cylinder_2d", "lift_strouhal", "cavity_3d_full", "cavity_2d", "laminar_decay"]
+__all__ = ["pipe_3d", "shear_wave", "taylor_green_2d", "cylinder_2d", "lift_strouhal", "cavity_3d_full", "cavity_2d", "laminar_decay"]

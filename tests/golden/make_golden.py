@@ -578,6 +578,23 @@ def cylinder2d_small(src: str) -> None:
     print(f"wrote cylinder2d_small.npz (Cd {float(res['cd'])}, St {res['st']})")
 
 
+def tgv2d(src: str) -> None:
+    """TensorLBM's verified decaying 2-D Taylor-Green vortex
+    (benchmarks/verified/taylor_green_2d: run.py and the energy_history.csv /
+    result.json it wrote; N = 128, Re 100, D2Q9 BGK float32 on the CPU, 4900
+    steps): the recorded energy and max|u| histories, decay rates and mass drift."""
+    import json
+
+    bench = pathlib.Path(src).parent / "benchmarks" / "verified" / "taylor_green_2d"
+    hist = np.loadtxt(bench / "energy_history.csv", delimiter=",", skiprows=1)
+    res = json.loads((bench / "result.json").read_text())
+    out = {"steps_recorded": hist[:, 0].astype(np.int64), "energy": hist[:, 1], "umax": hist[:, 2]}
+    for k in ("n", "re", "u0", "steps", "record_every", "gamma_e_sim", "gamma_vel_sim", "mass_drift_rel"):
+        out[k] = np.asarray(res[k])
+    np.savez_compressed(HERE / "tgv2d.npz", **out)
+    print(f"wrote tgv2d.npz ({sorted(out)})")
+
+
 def pipe3d(src: str) -> None:
     """TensorLBM's verified Hagen-Poiseuille pipe (benchmarks/verified/
     poiseuille_3d_pipe: run.py and the case_R20.json / case_R40.json it wrote,
@@ -653,6 +670,9 @@ def main() -> None:
         return
     if args.only == "cavity3d_full":
         cavity3d_full(args.reference)
+        return
+    if args.only == "tgv2d":
+        tgv2d(args.reference)
         return
     if args.only == "cylinder2d_re100":
         cylinder2d(args.reference)

@@ -3,7 +3,8 @@ kernel, against the values each benchmark recorded in the reference's own
 result files: the 3-D lid-driven cavity at Re 1000 (golden cavity3d_full),
 the 2-D cavity at Re 100 (cavity2d_re100) and Re 1000 (cavity2d_re1000, the
 regularised BGK), the free-stream cylinder at Re 100 (cylinder2d_small,
-cylinder2d_re100) and the Hagen-Poiseuille pipe (pipe3d)."""
+cylinder2d_re100), the Hagen-Poiseuille pipe (pipe3d), the shear wave and the
+2-D Taylor-Green vortex (tgv2d)."""
 
 from __future__ import annotations
 
@@ -147,6 +148,28 @@ def test_pipe_3d_matches_reference_benchmark(cuda, r):
     assert res["Q"] == pytest.approx(float(g[f"r{r}_Q"]), rel=1e-4)
     assert res["rho_in_measured"] == pytest.approx(float(g[f"r{r}_rho_in_measured"]), abs=1e-5)
     assert res["mass_drift_pct"] == pytest.approx(float(g[f"r{r}_mass_drift_pct"]), rel=2e-2)
+
+
+def test_taylor_green_2d_matches_reference_benchmark(cuda):
+    """TensorLBM's verified decaying 2-D Taylor-Green vortex (N = 128, Re 100,
+    D2Q9 BGK float32, 4900 steps) against the histories and fits the
+    benchmark recorded (golden tgv2d, its CPU run): the step is bit-exact, so
+    the energies agree to the order of the GPU's mean (measured 1.4e-7), max|u|
+    exactly, the decay rates to 1e-8 and the mass drift to 1e-10."""
+    from tensorlbm_b200.verified import taylor_green_2d
+
+    from tests.conftest import golden
+
+    g = golden("tgv2d")
+    r = taylor_green_2d(int(g["n"]), float(g["re"]), float(g["u0"]), int(g["steps"]), int(g["record_every"]),
+                        device=cuda)
+    assert r["finite"]
+    assert np.array_equal(np.asarray(r["times"]), g["steps_recorded"])
+    np.testing.assert_allclose(r["energies"], g["energy"], rtol=1e-6)
+    np.testing.assert_allclose(r["umaxs"], g["umax"], rtol=1e-7)
+    assert r["gamma_e_sim"] == pytest.approx(float(g["gamma_e_sim"]), rel=1e-6)
+    assert r["gamma_vel_sim"] == pytest.approx(float(g["gamma_vel_sim"]), rel=1e-6)
+    assert r["mass_drift_rel"] == pytest.approx(float(g["mass_drift_rel"]), abs=1e-9)
 
 
 @pytest.mark.parametrize("h", [64, 128])
